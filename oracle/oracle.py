@@ -1,0 +1,191 @@
+"""Python access to the oracle (TEST INFRASTRUCTURE ONLY).
+
+Two checkers live here, both used only by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg:
+
+* OracleTissue -- ctypes binding of the C restatement (oracle/epi_oracle.c),
+  built into oracle/liboracle.so by build_oracle().
+* run_reference -- runs the compiled reference harness (oracle/_ref, built by
+  oracle/build_ref.py from the reference sources) on a tissue and returns its
+  frames.
+
+Nothing in the product package imports this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import tempfile
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+REF_OUT = HERE / "_ref"
+
+_lib = None
+
+
+def build_oracle(force: bool = False) -> Path:
+    src = [HERE / "epi_oracle.c"]
+    hdr = HERE / "epi_oracle.h"
+    if (not force and LIB_PATH.exists()
+            and LIB_PATH.stat().st_mtime > max(p.stat().st_mtime for p in src + [hdr])):
+        return LIB_PATH
+    cmd = ["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-std=c11",
+           "-o", str(LIB_PATH), *map(str, src), "-lm"]
+    subprocess.run(cmd, check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build_oracle()
+        L = ctypes.CDLL(str(LIB_PATH))
+        P = ctypes.c_void_p
+        d = ctypes.POINTER(ctypes.c_double)
+        i32 = ctypes.POINTER(ctypes.c_int32)
+        u8 = ctypes.POINTER(ctypes.c_uint8)
+        L.ora_new.restype = P
+        L.ora_new.argtypes = [ctypes.c_int32] * 5 + [ctypes.c_double] * 3 + [d] * 7 + [u8, i32, i32]
+        L.ora_free.argtypes = [P]
+        for f in ("ora_connect", "ora_interact"):
+            getattr(L, f).argtypes = [P]
+            getattr(L, f).restype = ctypes.c_int
+        L.ora_step.argtypes = [P, ctypes.c_int32]
+        L.ora_step.restype = ctypes.c_int
+        L.ora_pos_copy.argtypes = [P]
+        L.ora_periodic_fix.argtypes = [P]
+        L.ora_get_positions.argtypes = [P, d, d, d]
+        L.ora_set_positions.argtypes = [P, d, d, d]
+        for f in ("ora_get_connections", "ora_get_connections_raw"):
+            getattr(L, f).argtypes = [P, i32, i32, ctypes.c_int64]
+            getattr(L, f).restype = ctypes.c_int64
+        L.ora_get_dermis.argtypes = [P, i32]
+        L.ora_error_info.argtypes = [P, i32, i32, d]
+        L.ora_error_info.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a, ct):
+    return a.ctypes.data_as(ctypes.POINTER(ct))
+
+
+class OracleTissue:
+    """FP64 serial restatement of the epi5_MT step for one tissue."""
+
+    def __init__(self, t, params=None):
+        L = lib()
+        p = np.array((params or t.params).as_tuple(), dtype=np.float64)
+        self._keep = [np.ascontiguousarray(a) for a in (
+            t.x, t.y, t.z, t.radius, t.agek, t.spr_nat_len)]
+        st = np.ascontiguousarray(t.state, dtype=np.uint8)
+        pr = np.ascontiguousarray(t.pair, dtype=np.int32)
+        rd = np.ascontiguousarray(t.rest_div_times, dtype=np.int32)
+        self.n = t.n
+        self._h = L.ora_new(t.n, t.nmemb, t.nder, t.nmx, t.nmy, t.lx, t.ly, t.lz,
+                            _p(p, ctypes.c_double),
+                            *[_p(a, ctypes.c_double) for a in self._keep],
+                            _p(st, ctypes.c_uint8), _p(pr, ctypes.c_int32),
+                            _p(rd, ctypes.c_int32))
+        if not self._h:
+            raise ValueError("oracle rejected the tissue")
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().ora_free(self._h)
+            self._h = None
+
+    def step(self, n: int = 1) -> int:
+        return lib().ora_step(self._h, n)
+
+    def connect(self) -> int:
+        return lib().ora_connect(self._h)
+
+    def positions(self):
+        x, y, z = (np.empty(self.n) for _ in range(3))
+        lib().ora_get_positions(self._h, _p(x, ctypes.c_double), _p(y, ctypes.c_double),
+                                _p(z, ctypes.c_double))
+        return x, y, z
+
+    def set_positions(self, x, y, z):
+        x, y, z = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z))
+        lib().ora_set_positions(self._h, _p(x, ctypes.c_double), _p(y, ctypes.c_double),
+                                _p(z, ctypes.c_double))
+
+    def connections(self, raw: bool = False):
+        off = np.zeros(self.n + 1, np.int32)
+        f = lib().ora_get_connections_raw if raw else lib().ora_get_connections
+        tot = f(self._h, _p(off, ctypes.c_int32), None, 0)
+        idx = np.zeros(max(int(tot), 1), np.int32)
+        f(self._h, _p(off, ctypes.c_int32), _p(idx, ctypes.c_int32), tot)
+        return off, idx[: int(tot)]
+
+    def dermis(self):
+        d = np.empty(self.n, np.int32)
+        lib().ora_get_dermis(self._h, _p(d, ctypes.c_int32))
+        return d
+
+    def error(self):
+        a = ctypes.c_int32()
+        b = ctypes.c_int32()
+        v = ctypes.c_double()
+        code = lib().ora_error_info(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(v))
+        return code, a.value, b.value, v.value
+
+
+def reference_binary(t, variant: str = "serial") -> Optional[Path]:
+    """Path of the compiled reference harness for this tissue's geometry, if built."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("epi_build_ref", HERE / "build_ref.py")
+    br = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(br)
+    try:
+        name = br.geometry_for(t.nmx, t.nmy, t.lx, t.ly, t.lz)
+    except KeyError:
+        return None
+    p = br.binary_path(name, variant)
+    return p if p.exists() else None
+
+
+def run_reference(t, nsteps: int, every: int, variant: str = "serial"):
+    """Run the compiled reference on `t` (default parameters only: the reference
+    fixes its constants at compile time). Returns the parsed frames."""
+    from epi_b200.tissue import read_reference_frames
+    exe = reference_binary(t, variant)
+    if exe is None:
+        raise FileNotFoundError("compiled reference harness not built for this geometry")
+    with tempfile.TemporaryDirectory() as d:
+        cells = os.path.join(d, "cells.dat")
+        out = os.path.join(d, "frames.bin")
+        t.write_reference_file(cells)
+        r = subprocess.run([str(exe), "run", cells, str(nsteps), out, str(every)],
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"reference harness failed ({r.returncode}): {r.stderr[-2000:]}")
+        return read_reference_frames(out)
+
+
+def time_reference(t, warmup: int, steps: int, threads: Optional[int] = None):
+    """Time the OpenMP build of the reference on `t`; returns its JSON summary."""
+    import json
+    exe = reference_binary(t, "omp")
+    if exe is None:
+        raise FileNotFoundError("compiled reference harness (omp) not built for this geometry")
+    env = dict(os.environ)
+    if threads:
+        env["OMP_NUM_THREADS"] = str(threads)
+    with tempfile.TemporaryDirectory() as d:
+        cells = os.path.join(d, "cells.dat")
+        t.write_reference_file(cells)
+        r = subprocess.run([str(exe), "time", cells, str(warmup), str(steps)],
+                           capture_output=True, text=True, env=env)
+        if r.returncode != 0:
+            raise RuntimeError(f"reference harness failed ({r.returncode}): {r.stderr[-2000:]}")
+        return json.loads(r.stdout.strip().splitlines()[-1])

@@ -1,0 +1,177 @@
+// Harness around the UNMODIFIED epi5_MT mechanics sources (test infrastructure).
+//
+// This file is the oracle's driver, not product code. It is compiled together
+// with the reference's own cellmanager.cpp / cell.cpp / cell_connection.cpp /
+// cell_interaction.cpp / cell_init.cpp (see oracle/build_ref.py) and replaces
+// only the reference's proc() loop, which stops on an interactive stdin prompt
+// (epi5_MT/proc.cpp:100-118). The step it runs is the reference's
+// cell_dynamics (epi5_MT/proc.cpp:22-32) without cell_state_renew:
+//     cell_interaction -> pos_copy -> cell_pos_periodic_fix -> connect_cell
+// Initialisation is the reference's cman_init (epi5_MT/cell_init.cpp:132-142),
+// which loads the text cell file, wires the membrane lattice and runs the
+// first connect_cell.
+//
+// Modes:
+//   ref_harness run  <cells.dat> <nsteps> <out.bin> <dump_every>
+//       writes frames (positions, per-cell sorted connection lists, dermis)
+//       at step 0, every dump_every steps and at the last step.
+//   ref_harness time <cells.dat> <warmup> <steps>
+//       times each step with steady_clock and prints one JSON line.
+#include "cellmanager.h"
+#include "cell.h"
+#include "cell_connection.h"
+#include "cell_interaction.h"
+#include "cell_init.h"
+
+#include <tbb/tbb_shim_config.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fcntl.h>
+#include <memory>
+#include <string>
+#include <unistd.h>
+#include <vector>
+
+namespace {
+
+// cman_init prints one line per loaded cell; keep the harness output clean.
+struct SilenceStdout {
+  int saved = -1;
+  SilenceStdout() {
+    std::fflush(stdout);
+    saved = dup(1);
+    int devnull = open("/dev/null", O_WRONLY);
+    dup2(devnull, 1);
+    close(devnull);
+  }
+  ~SilenceStdout() {
+    std::fflush(stdout);
+    dup2(saved, 1);
+    close(saved);
+  }
+};
+
+// Built with NDEBUG (the loader's DER-first assert rejects DER-free inputs),
+// so re-check the per-cell connection capacity the reference asserts on
+// (cell_connection.cpp:122, N2 = 400).
+void check_capacity(CellManager& cman) {
+  bool bad = false;
+  cman.all_foreach([&](Cell* c) {
+    if (c->connected_cell.size() >= 400) bad = true;
+  });
+  if (bad) {
+    std::fprintf(stderr, "connection list overflow (>= 400)\n");
+    std::exit(4);
+  }
+}
+
+void one_step(CellManager& cman) {
+  cell_interaction(cman);
+  pos_copy(cman);
+  cell_pos_periodic_fix(cman);
+  connect_cell(cman);
+}
+
+// CellManager keeps its cell array private; the public loop accessor
+// (epi5_MT/cellmanager.h:15-21, all_foreach_with_index) gives index order.
+std::vector<Cell*> cells_of(CellManager& cman) {
+  std::vector<Cell*> v(cman.size(), nullptr);
+  cman.all_foreach_with_index([&](Cell* c, size_t i) { v[i] = c; });
+  return v;
+}
+
+void write_frame(std::FILE* f, CellManager& cman, int step) {
+  const std::vector<Cell*> cells = cells_of(cman);
+  const int32_t n = static_cast<int32_t>(cells.size());
+  const int32_t tag = 0x454d5246;  // "FRME"
+  std::fwrite(&tag, 4, 1, f);
+  std::fwrite(&step, 4, 1, f);
+  std::fwrite(&n, 4, 1, f);
+  std::vector<double> buf(n);
+  for (int32_t i = 0; i < n; ++i) buf[i] = cells[i]->x();
+  std::fwrite(buf.data(), 8, n, f);
+  for (int32_t i = 0; i < n; ++i) buf[i] = cells[i]->y();
+  std::fwrite(buf.data(), 8, n, f);
+  for (int32_t i = 0; i < n; ++i) buf[i] = cells[i]->z();
+  std::fwrite(buf.data(), 8, n, f);
+  std::vector<int32_t> off(n + 1, 0), idx, dermis(n, -1);
+  for (int32_t i = 0; i < n; ++i) {
+    Cell* c = cells[i];
+    std::vector<int32_t> row;
+    for (size_t k = 0; k < c->connected_cell.size(); ++k)
+      row.push_back(static_cast<int32_t>(c->connected_cell[k]->get_index()));
+    std::sort(row.begin(), row.end());
+    idx.insert(idx.end(), row.begin(), row.end());
+    off[i + 1] = static_cast<int32_t>(idx.size());
+    if (c->dermis() != nullptr) dermis[i] = static_cast<int32_t>(c->dermis()->get_index());
+  }
+  std::fwrite(off.data(), 4, n + 1, f);
+  if (!idx.empty()) std::fwrite(idx.data(), 4, idx.size(), f);
+  std::fwrite(dermis.data(), 4, n, f);
+}
+
+int usage() {
+  std::fprintf(stderr,
+               "usage: ref_harness run <cells.dat> <nsteps> <out.bin> <dump_every>\n"
+               "       ref_harness time <cells.dat> <warmup> <steps>\n");
+  return 2;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  if (argc < 2) return usage();
+  const std::string mode = argv[1];
+  auto cman = std::unique_ptr<CellManager>(new CellManager());
+  if (mode == "run" && argc == 6) {
+    const int nsteps = std::atoi(argv[3]);
+    const int every = std::max(1, std::atoi(argv[5]));
+    {
+      SilenceStdout quiet;
+      cman_init(*cman, argv[2]);
+    }
+    std::FILE* f = std::fopen(argv[4], "wb");
+    if (!f) return 3;
+    check_capacity(*cman);
+    write_frame(f, *cman, 0);
+    for (int s = 1; s <= nsteps; ++s) {
+      one_step(*cman);
+      check_capacity(*cman);
+      if (s % every == 0 || s == nsteps) write_frame(f, *cman, s);
+    }
+    std::fclose(f);
+    return 0;
+  }
+  if (mode == "time" && argc == 5) {
+    const int warmup = std::atoi(argv[3]);
+    const int steps = std::atoi(argv[4]);
+    {
+      SilenceStdout quiet;
+      cman_init(*cman, argv[2]);
+    }
+    for (int s = 0; s < warmup; ++s) one_step(*cman);
+    std::vector<double> t(steps);
+    for (int s = 0; s < steps; ++s) {
+      auto a = std::chrono::steady_clock::now();
+      one_step(*cman);
+      auto b = std::chrono::steady_clock::now();
+      t[s] = std::chrono::duration<double>(b - a).count();
+    }
+    std::vector<double> sorted = t;
+    std::sort(sorted.begin(), sorted.end());
+    double total = 0;
+    for (double v : t) total += v;
+    const double median = steps > 0 ? sorted[steps / 2] : 0.0;
+    std::printf(
+        "{\"cells\": %zu, \"steps\": %d, \"warmup\": %d, \"threads\": %d, "
+        "\"median_s\": %.9g, \"mean_s\": %.9g, \"total_s\": %.9g}\n",
+        cman->size(), steps, warmup, tbb::shim_threads(), median,
+        steps > 0 ? total / steps : 0.0, total);
+    return 0;
+  }
+  return usage();
+}
