@@ -1,0 +1,393 @@
+"""Benchmark of the cell-mechanics step on B200.
+
+Default workload (N=1): the batched ensemble of 512 independent synthetic
+tissues (membrane side in {16,24,32,48,64}, 2-8 jittered cell layers, per-tissue
+spring / LJ / bending constants scaled log-uniform in [0.5, 2]), FP32 forces
+with FP64 sums and positions, one CUDA graph replaying the whole batch per
+step. A step is one full mechanics step of every tissue: interaction + commit +
+periodic wrap + re-binning + neighbour lists (the reference's cell_dynamics
+without cell_state_renew). value = particles (membrane + mobile, all tissues,
+all ranks) x steps / device time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload ensemble|c2|c3|c1] [--precision mixed|fp64]
+
+Under torchrun (N > 1) the tissues are sharded across ranks (no collective on
+the data path); the timed region is bracketed by barriers and the max over
+ranks is reported.
+
+--impl reference times the reference's own CPU implementation (epi5_MT built
+by oracle/build_ref.py, OpenMP TBB stand-in, all host threads) on a bounded
+sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+from epi_b200 import tissue as T  # noqa: E402
+from epi_b200.ensemble import shard_tissues  # noqa: E402
+
+METRIC = "cell-updates/s: FP32/batched vs plain FP64 GPU @≤1e-5 rel pos err; grad err"
+UNIT = "cell-updates/s"
+KERNEL_LAUNCHES_PER_STEP = 8  # force_commit, bin, 3 x scan, scatter, binsort, search
+
+
+def workload(name: str):
+    if name == "ensemble":
+        return T.config4(), "batched ensemble: 512 tissues, side {16..64}, 2-8 layers (config 4)"
+    if name == "c2":
+        return [T.config2()], "single tissue 64x64 membrane + 32,768 cells (config 2)"
+    if name == "c3":
+        return [T.config3()], "single tissue 256x256 membrane + 1,048,576 cells (config 3)"
+    if name == "c1":
+        return [T.config1()], "single tissue 16x16 membrane + 512 cells (config 1)"
+    raise SystemExit(f"unknown workload {name}")
+
+
+# --------------------------------------------------------------------------
+# clocks during the timed region (NVML)
+# --------------------------------------------------------------------------
+class ClockSampler:
+    REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap",
+               0x8: "hw_slowdown", 0x10: "sync_boost", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
+
+    def __init__(self, device: int, period: float = 0.02):
+        self.samples = []
+        self.reasons = 0
+        self.period = period
+        self._stop = threading.Event()
+        self.ok = False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.max_mhz = None
+
+    def _sample(self):
+        nv = self._nv
+        self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+        try:
+            r = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+        except Exception:
+            r = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self._h)
+        self.reasons |= int(r) & ~0x1
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self._sample()
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.ok:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.ok:
+            self._stop.set()
+            self._t.join()
+            try:
+                self._sample()
+            except Exception:
+                pass
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unavailable"]}
+        return {"sm_mhz": float(statistics.median(self.samples)), "sm_max_mhz": self.max_mhz,
+                "samples": len(self.samples),
+                "reasons": [n for b, n in self.REASONS.items() if self.reasons & b]}
+
+
+# --------------------------------------------------------------------------
+# CPU baseline / reference arm: compiled epi5_MT (OpenMP) on a sample
+# --------------------------------------------------------------------------
+def reference_sample(tissues, target_particles: int):
+    """Deterministic bounded sample: every k-th tissue, k = total / target."""
+    total = sum(t.n for t in tissues)
+    step = max(1, total // max(target_particles, 1))
+    return list(tissues[::step])
+
+
+def time_reference_cpu(tissues, warmup: int, steps: int, threads=None):
+    """Runs the compiled reference on each sampled tissue; returns
+    (cell-updates/s over the sample, details). The sample is advanced
+    `steps` timed steps; time per step = sum over tissues of the median."""
+    from oracle import oracle as O
+    per = []
+    for t in tissues:
+        r = O.time_reference(t, warmup, steps, threads)
+        per.append((t.n, r["median_s"], r["threads"]))
+    cells = sum(n for n, _, _ in per)
+    sec = sum(s for _, s, _ in per)
+    return cells / sec, dict(tissues=len(per), particles=cells, step_s=sec,
+                             threads=per[0][2] if per else 0)
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    tissues, desc = workload(args.workload)
+    sample = reference_sample(tissues, args.ref_particles)
+    try:
+        v, d = time_reference_cpu(sample, max(1, args.warmup), max(1, args.steps))
+    except FileNotFoundError as e:
+        print(json.dumps({"impl": "reference", "unavailable": str(e)}))
+        return 0
+    sample_desc = (f"{d['tissues']} of {len(tissues)} tissues ({d['particles']} particles), "
+                   f"median of {max(1, args.steps)} steps each after {max(1, args.warmup)} warm-up")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * d["step_s"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": desc, "sample": sample_desc},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": d["threads"], "kind": "reference",
+                         "sample": sample_desc},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# --------------------------------------------------------------------------
+# our arm
+# --------------------------------------------------------------------------
+def load_traffic(kernel: str, workload_name: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        return d.get(workload_name, {}).get(kernel)
+    except Exception:
+        return None
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "c1", "c2", "c3"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--plain-steps", type=int, default=3)
+    ap.add_argument("--ref-particles", type=int, default=120000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="timed region only (profiling)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 0)
+
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    from epi_b200 import capi
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    tissues, desc = workload(args.workload)
+    shards = shard_tissues([t.n for t in tissues], world)
+    mine = [tissues[i] for i in shards[rank]]
+    n_mine = sum(t.n for t in mine)
+    n_all = sum(t.n for t in tissues)
+    prec = capi.EPI_PREC_MIXED if args.precision == "mixed" else capi.EPI_PREC_FP64
+
+    ctx = capi.Context(precision=prec, max_conn=64, device=local)
+    ctx.upload(mine)
+    off, _ = ctx.connections()
+    kbar = float(off[-1]) / max(n_mine, 1)  # mean connected_cell length incl. lattice links
+    nmemb_mine = sum(t.nmemb for t in mine)
+    kbar_searched = (float(off[-1]) - 4 * nmemb_mine) / max(n_mine, 1)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # warm-up (also captures the graph)
+    if args.warmup:
+        ctx.step(args.warmup, "graph")
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        ctx.step(args.steps, "graph")
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = n_all * args.steps / (ms * 1e-3)
+
+    extras = {}
+    if not args.no_extras:
+        # per-kernel device time (events around each kernel class, not captured)
+        tk = ctx.time_kernels(5)
+        dom = max(tk, key=lambda k: tk[k][0])
+        dom_ms = tk[dom][0] / max(tk[dom][1], 1)
+        hbm, peak_kind = measured_peaks()
+        # algorithmic bytes per particle of each kernel class
+        kb = kbar_searched
+        per_particle = {
+            "force_commit": 32 + 4 + 4 + 4 * kb + 32,   # own pos+radius, attr, count, list, new pos
+            "search": 32 + 4 + 4 * kb + 4 + 4,          # sorted pos, key, list, count, dermis
+            "bin": 32 + 4 + 8,                          # pos, attr, bin + rank
+            "binsort": 4 + 32 + 4 + 32,                 # key in/out, pos gather, sorted copy
+            "scatter": 8 + 4,
+            "scan": 0,
+        }
+        alg = per_particle[dom] * n_mine
+        achieved = alg / (dom_ms * 1e-3) / 1e9
+        traffic = load_traffic(dom, args.workload)
+        extras["roofline"] = {
+            "bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+            if peak_kind == "measured" else "fallback",
+            "traffic": traffic, "alg_bytes_per_launch": alg,
+            "launch_ms": dom_ms,
+            "step_alg_bytes_per_particle": 52 + 8 * kbar,
+            "step_frac": (52 + 8 * kbar) * value / max(world, 1) / 1e9 / hbm,
+        }
+        extras["kernel_ms_per_step"] = {k: v[0] / max(v[1], 1) * (3 if k == "scan" else 1)
+                                        for k, v in tk.items()}
+
+        # e2e through the C ABI with host buffers: the drop-in's data flow per
+        # step (interaction+commit on device, positions to the host for the
+        # host-side state update, positions back, connect).
+        pin = [torch.empty(n_mine, dtype=torch.float64, pin_memory=True) for _ in range(3)]
+        host = tuple(p.numpy() for p in pin)
+        ctx.positions(host)
+        ctx.set_positions(*host)
+        torch.cuda.synchronize()
+        barrier()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.e2e_steps):
+            ctx.interact_commit()
+            ctx.positions(host)
+            ctx.set_positions(*host)
+        f1.record(stream)
+        f1.synchronize()
+        barrier()
+        e2e_ms = f0.elapsed_time(f1)
+        if dist is not None:
+            t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        extras["e2e"] = {"value": n_all * args.e2e_steps / (e2e_ms * 1e-3), "unit": UNIT,
+                         "h2d_bytes_per_step": 24 * n_mine, "d2h_bytes_per_step": 24 * n_mine,
+                         "steps": args.e2e_steps,
+                         "path": "epi_interact_commit + epi_download_positions + "
+                                 "epi_upload_positions(connect) per step, pinned host buffers"}
+
+        # plain FP64 GPU step: same kernels in FP64, one launch sequence per
+        # tissue, no graph (the denominator of the >= 3x target)
+        if args.plain_steps > 0:
+            with capi.Context(precision=capi.EPI_PREC_FP64, max_conn=64, device=local) as pc:
+                pc.upload(mine)
+                pc.step(1, "per_tissue")
+                ps = torch.cuda.ExternalStream(pc.stream_handle())
+                torch.cuda.synchronize()
+                barrier()
+                g0 = torch.cuda.Event(enable_timing=True)
+                g1 = torch.cuda.Event(enable_timing=True)
+                g0.record(ps)
+                pc.step(args.plain_steps, "per_tissue")
+                g1.record(ps)
+                g1.synchronize()
+                barrier()
+                pms = g0.elapsed_time(g1)
+            if dist is not None:
+                t = torch.tensor([pms], device="cuda", dtype=torch.float64)
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                pms = float(t.item())
+            plain = n_all * args.plain_steps / (pms * 1e-3)
+            extras["fp64_plain"] = {"value": plain, "unit": UNIT, "steps": args.plain_steps,
+                                    "speedup": value / plain}
+
+    if rank == 0:
+        cfg = {"workload": desc, "tissues": len(tissues), "particles": n_all,
+               "mean_connections": kbar, "precision": args.precision,
+               "launch": "one CUDA graph per 2 steps over the whole batch",
+               "l2": "inputs larger than L2 (working set >> 126 MB)"
+               if n_all * 200 > 126e6 else "working set fits in L2 (no flush)",
+               "parallelism": f"tissue sharding x{world}" if world > 1 else "1 GPU"}
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32-force/f64-sum" if args.precision == "mixed" else "f64",
+                "data": "synthetic (seeded splitmix64 jittered lattices)", "config": cfg,
+                "gpu_launches": KERNEL_LAUNCHES_PER_STEP * args.steps,
+                "clocks": clk.summary()}
+        line.update(extras)
+        if world == 1 and not args.no_cpu_baseline and not args.no_extras:
+            sample = reference_sample(tissues, args.ref_particles // 4)
+            try:
+                v, d = time_reference_cpu(sample, 2, 5)
+                line["cpu_baseline"] = {
+                    "value": v, "unit": UNIT, "cores": d["threads"], "kind": "reference",
+                    "sample": f"{d['tissues']} tissues, {d['particles']} particles, "
+                              f"median of 5 steps after 2 warm-up (epi5_MT, OpenMP TBB stand-in)"}
+            except Exception as e:  # reference build missing on this host
+                line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0,
+                                        "kind": "reference", "sample": f"unavailable: {e}"}
+        print(json.dumps(line))
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

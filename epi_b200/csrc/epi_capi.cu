@@ -1,0 +1,661 @@
+// C ABI of the mechanics library: context, upload, step drivers, export.
+//
+// Host-side mirror of the reference's call surface (include/epi_mech.h lists
+// the reference function each entry point stands for). All device memory is
+// owned by the context; every entry point returns an epi_status and catches
+// everything so no exception crosses the ABI.
+#include "epi_mech.h"
+#include "epi_kernels.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+using namespace epi;
+
+namespace epi {
+
+struct Timer {
+  struct Pair {
+    cudaEvent_t a, b;
+  };
+  std::vector<Pair> ev[KC_COUNT];
+  cudaEvent_t open[KC_COUNT] = {};
+  ~Timer() {
+    for (auto& v : ev)
+      for (auto& p : v) {
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+      }
+  }
+};
+
+void timer_begin(Timer* tm, int cls, cudaStream_t s) {
+  if (!tm) return;
+  cudaEventCreate(&tm->open[cls]);
+  cudaEventRecord(tm->open[cls], s);
+}
+
+void timer_end(Timer* tm, int cls, cudaStream_t s) {
+  if (!tm) return;
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  cudaEventRecord(e, s);
+  tm->ev[cls].push_back({tm->open[cls], e});
+}
+
+}  // namespace epi
+
+struct epi_ctx {
+  epi_config cfg{};
+  cudaStream_t stream = nullptr;
+  bool loaded = false;
+  int32_t ntissues = 0;
+  int64_t n = 0;
+  int32_t nbins = 0;
+  std::vector<TissueDev> tissues_h;
+  // device buffers
+  TissueDev* tissues = nullptr;
+  double4* pos[2] = {nullptr, nullptr};
+  int cur = 0;
+  uint32_t* attr = nullptr;
+  int32_t* pair = nullptr;
+  double* spr = nullptr;
+  int32_t* dermis = nullptr;
+  int32_t* nbr = nullptr;
+  int32_t* nn = nullptr;
+  double4* sn = nullptr;
+  double4* sm = nullptr;
+  int32_t* bin = nullptr;
+  int32_t* rank = nullptr;
+  int32_t* counts = nullptr;
+  int32_t* starts = nullptr;
+  uint32_t* skey = nullptr;
+  double4* spos = nullptr;
+  double* stage = nullptr;        // 3n doubles: x | y | z for host transfers
+  DevStatus* status = nullptr;
+  DevStatus* status_h = nullptr;  // pinned
+  ScanScratch scan{};
+  // graphs: one per buffer parity, each replaying two steps
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  // last error details
+  DevStatus last{};
+};
+
+namespace {
+
+int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return EPI_OK;
+  if (e == cudaErrorMemoryAllocation) return EPI_ERR_OOM;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return EPI_ERR_NO_DEVICE;
+  return EPI_ERR_CUDA;
+}
+
+#define EPI_CUDA(call)                      \
+  do {                                      \
+    const cudaError_t e_ = (call);          \
+    if (e_ != cudaSuccess) return cuda_status(e_); \
+  } while (0)
+
+template <typename T>
+int dev_alloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  return cuda_status(cudaMalloc((void**)p, sizeof(T) * count));
+}
+
+void free_buffers(epi_ctx* c) {
+  for (auto& g : c->graph) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
+  void* ptrs[] = {c->tissues, c->pos[0], c->pos[1], c->attr, c->pair, c->spr, c->dermis,
+                  c->nbr, c->nn, c->sn, c->sm, c->bin, c->rank, c->counts, c->starts,
+                  c->skey, c->spos, c->scan.partial, c->stage};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  c->tissues = nullptr;
+  c->pos[0] = c->pos[1] = nullptr;
+  c->attr = nullptr; c->pair = nullptr; c->spr = nullptr; c->dermis = nullptr;
+  c->nbr = nullptr; c->nn = nullptr; c->sn = nullptr; c->sm = nullptr;
+  c->bin = nullptr; c->rank = nullptr; c->counts = nullptr; c->starts = nullptr;
+  c->skey = nullptr; c->spos = nullptr; c->scan.partial = nullptr; c->stage = nullptr;
+  c->loaded = false;
+}
+
+DevState make_state(epi_ctx* c, int cur) {
+  DevState S;
+  S.tissues = c->tissues;
+  S.pos_cur = c->pos[cur];
+  S.pos_nxt = c->pos[cur ^ 1];
+  S.attr = c->attr;
+  S.pair = c->pair;
+  S.spr = c->spr;
+  S.dermis = c->dermis;
+  S.nbr = c->nbr;
+  S.nn = c->nn;
+  S.sn = c->sn;
+  S.sm = c->sm;
+  S.bin = c->bin;
+  S.rank = c->rank;
+  S.counts = c->counts;
+  S.starts = c->starts;
+  S.skey = c->skey;
+  S.spos = c->spos;
+  S.status = c->status;
+  S.n_total = c->n;
+  S.max_conn = c->cfg.max_conn;
+  return S;
+}
+
+Range whole(const epi_ctx* c) { return Range{0, (int32_t)c->n, 0, c->nbins}; }
+
+Range tissue_range(const epi_ctx* c, int t) {
+  const TissueDev& T = c->tissues_h[t];
+  return Range{T.pbase, T.pbase + T.n, T.binbase, T.binbase + T.anx * T.any * T.anz};
+}
+
+// One reference step over the batch: interact + commit, swap, connect.
+void enqueue_step(epi_ctx* c, int& cur, Timer* tm) {
+  launch_interact_commit(make_state(c, cur), whole(c), c->cfg.precision, c->stream, tm);
+  cur ^= 1;
+  launch_connect(make_state(c, cur), whole(c), c->cfg.precision, c->scan, c->stream, tm);
+}
+
+// Waits for the stream and converts any sticky kernel error to a status.
+int check_status(epi_ctx* c) {
+  EPI_CUDA(cudaMemcpyAsync(c->status_h, c->status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                           c->stream));
+  EPI_CUDA(cudaStreamSynchronize(c->stream));
+  EPI_CUDA(cudaGetLastError());
+  if (c->status_h->code != 0) {
+    c->last = *c->status_h;
+    EPI_CUDA(cudaMemsetAsync(c->status, 0, sizeof(DevStatus), c->stream));
+    EPI_CUDA(cudaStreamSynchronize(c->stream));
+    return c->last.code;
+  }
+  return EPI_OK;
+}
+
+int set_device(const epi_ctx* c) { return cuda_status(cudaSetDevice(c->cfg.device)); }
+
+#define EPI_GUARD_BEGIN try {
+#define EPI_GUARD_END                      \
+  }                                        \
+  catch (const std::bad_alloc&) {          \
+    return EPI_ERR_OOM;                    \
+  }                                        \
+  catch (...) {                            \
+    return EPI_ERR_CUDA;                   \
+  }
+
+int validate_tissue(const epi_tissue_view& v) {
+  if (v.n < 0 || v.nmemb < 0 || v.nder < 0 || v.nmemb + v.nder > v.n) return EPI_ERR_INVALID_ARG;
+  if (v.n > 0 && (!v.x || !v.y || !v.z || !v.radius || !v.state)) return EPI_ERR_INVALID_ARG;
+  if (!(v.lx > 0) || !(v.ly > 0) || !(v.lz > 0)) return EPI_ERR_INVALID_ARG;
+  if (v.nmemb != v.nmx * v.nmy || v.nmx < 3 || v.nmy < 3) return EPI_ERR_UNSUPPORTED;
+  // The 5-bin search window of connect_proc must not wrap onto itself
+  // (cell_connection.cpp:101-109), else the reference double-pushes.
+  const int anx = (int)(v.lx / 2.0 + 0.5), any = (int)(v.ly / 2.0 + 0.5), anz = (int)(v.lz / 2.0);
+  if (anx < 5 || any < 5 || anz < 5) return EPI_ERR_UNSUPPORTED;
+  for (int32_t i = 0; i < v.n; ++i) {
+    const uint8_t s = v.state[i];
+    if (s > ST_MEMB) return EPI_ERR_INVALID_ARG;
+    if ((i < v.nmemb) != (s == ST_MEMB)) return EPI_ERR_INVALID_ARG;
+    if (i >= v.nmemb && i < v.nmemb + v.nder && s != ST_DER) return EPI_ERR_INVALID_ARG;
+    if (i >= v.nmemb + v.nder && s == ST_DER) return EPI_ERR_INVALID_ARG;
+    // every radius must keep each reachable pair inside the reference's
+    // +-2 bin window: LJ_THRESH * (r_i + r_j) < 2 * AREA_GRID
+    if (!(v.radius[i] > 0) || v.radius[i] > 1.6) return EPI_ERR_UNSUPPORTED;
+    if (v.pair) {
+      const int32_t q = v.pair[i];
+      if (q >= v.n || q < -1) return EPI_ERR_INVALID_ARG;
+      if (q >= 0 && (q == i || v.pair[q] != i || q < v.nmemb || i < v.nmemb))
+        return EPI_ERR_INVALID_ARG;
+    }
+  }
+  return EPI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void epi_params_default(epi_params* p) {
+  if (!p) return;
+  p->dt = 0.01;                 // DT_Cell, define.h:86
+  p->eps_m = 0.01;              // cell_interaction.cpp:21
+  p->p_memb = 1. / 4;           // 1 / COMPRESS_FACTOR, :26 and define.h:125
+  p->der_der_const = 0.2;       // :29
+  p->k_total = 3.0;             // :30
+  p->k_desmosome = 3.0 * 0.01;  // K_TOTAL * K_DESMOSOME_RATIO, :31-32
+  p->kspring = 25.0;            // :33
+  p->kspring_d = 5.0;           // :34
+  p->kbend = 0.5;               // :37
+  p->delta_r = 0.4 * 1.4;       // 0.4 * R_der, :42
+  p->para_ljp2 = 0.005;         // :44
+  p->kspring_division = 5.0;    // :45
+  p->lj_thresh = 1.2;           // define.h:135
+  p->thresh_sp = 3.0;           // define.h:132
+}
+
+void epi_config_default(epi_config* c) {
+  if (!c) return;
+  c->device = 0;
+  c->precision = EPI_PREC_MIXED;
+  c->max_conn = 64;
+  c->reserved = 0;
+}
+
+const char* epi_strerror(int s) {
+  switch (s) {
+    case EPI_OK: return "ok";
+    case EPI_ERR_INVALID_ARG: return "invalid argument";
+    case EPI_ERR_NO_DEVICE: return "no usable CUDA device";
+    case EPI_ERR_CUDA: return "CUDA runtime error";
+    case EPI_ERR_OOM: return "device out of memory";
+    case EPI_ERR_BIN_RANGE: return "particle outside the grid (grid_init range assert)";
+    case EPI_ERR_BIN_OVERFLOW: return "grid bin holds more than 199 particles";
+    case EPI_ERR_LIST_OVERFLOW: return "connection list capacity exceeded";
+    case EPI_ERR_COEF_RANGE: return "pair interaction coefficient above 1000 (too strong interaction)";
+    case EPI_ERR_MEMB_COEF_RANGE: return "membrane interaction coefficient above 100";
+    case EPI_ERR_NONFINITE: return "non-finite position";
+    case EPI_ERR_TIMEOUT: return "bounded device wait timed out";
+    case EPI_ERR_STATE: return "call out of order";
+    case EPI_ERR_UNSUPPORTED: return "unsupported geometry";
+    default: return "unknown status";
+  }
+}
+
+int epi_create(epi_ctx** out, const epi_config* cfg) {
+  if (!out) return EPI_ERR_INVALID_ARG;
+  *out = nullptr;
+  EPI_GUARD_BEGIN
+  epi_config c;
+  epi_config_default(&c);
+  if (cfg) c = *cfg;
+  if (c.max_conn <= 0 || c.max_conn > 400) return EPI_ERR_INVALID_ARG;
+  if (c.precision != EPI_PREC_FP64 && c.precision != EPI_PREC_MIXED) return EPI_ERR_INVALID_ARG;
+  int ndev = 0;
+  const cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev <= 0) return EPI_ERR_NO_DEVICE;
+  if (c.device < 0 || c.device >= ndev) return EPI_ERR_INVALID_ARG;
+  EPI_CUDA(cudaSetDevice(c.device));
+  epi_ctx* ctx = new epi_ctx();
+  ctx->cfg = c;
+  int rc = cuda_status(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  if (rc == EPI_OK) rc = dev_alloc(&ctx->status, 1);
+  if (rc == EPI_OK) rc = cuda_status(cudaMallocHost((void**)&ctx->status_h, sizeof(DevStatus)));
+  if (rc == EPI_OK) rc = cuda_status(cudaMemset(ctx->status, 0, sizeof(DevStatus)));
+  if (rc != EPI_OK) {
+    epi_destroy(ctx);
+    return rc;
+  }
+  *out = ctx;
+  return EPI_OK;
+  EPI_GUARD_END
+}
+
+void epi_destroy(epi_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->cfg.device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  free_buffers(ctx);
+  if (ctx->status) cudaFree(ctx->status);
+  if (ctx->status_h) cudaFreeHost(ctx->status_h);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const epi_params* params) {
+  if (!c || ntissues <= 0 || !tv) return EPI_ERR_INVALID_ARG;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  int64_t n = 0;
+  int64_t nbins = 0;
+  for (int t = 0; t < ntissues; ++t) {
+    if ((rc = validate_tissue(tv[t]))) return rc;
+    n += tv[t].n;
+    nbins += (int64_t)((int)(tv[t].lx / 2.0 + 0.5)) * (int)(tv[t].ly / 2.0 + 0.5) *
+             (int)(tv[t].lz / 2.0);
+  }
+  if (n > (int64_t)0x7fffffff || nbins > (int64_t)0x7ffffff0 || ntissues >= (1 << 24))
+    return EPI_ERR_UNSUPPORTED;
+  free_buffers(c);
+  c->ntissues = ntissues;
+  c->n = n;
+  c->nbins = (int32_t)nbins;
+  c->tissues_h.assign(ntissues, TissueDev{});
+  std::vector<double4> pos(n);
+  std::vector<uint32_t> attr(n);
+  std::vector<int32_t> pair(n, -1);
+  std::vector<double> spr(n, 0.0);
+  int32_t pbase = 0, binbase = 0;
+  for (int t = 0; t < ntissues; ++t) {
+    const epi_tissue_view& v = tv[t];
+    epi_params P;
+    if (params) P = params[t];
+    else epi_params_default(&P);
+    TissueDev& T = c->tissues_h[t];
+    T.pbase = pbase;
+    T.n = v.n;
+    T.nmemb = v.nmemb;
+    T.nder = v.nder;
+    T.nmx = v.nmx;
+    T.nmy = v.nmy;
+    T.anx = (int32_t)(v.lx / 2.0 + 0.5);  // ANX / ANY / ANZ, cell_connection.cpp:22-26
+    T.any = (int32_t)(v.ly / 2.0 + 0.5);
+    T.anz = (int32_t)(v.lz / 2.0);
+    T.binbase = binbase;
+    T.lx = v.lx;
+    T.ly = v.ly;
+    T.lz = v.lz;
+    std::memcpy(&T.P, &P, sizeof(Params));
+    double rmax = 0;
+    for (int32_t i = 0; i < v.n; ++i) {
+      const int64_t g = pbase + i;
+      pos[g] = make_double4(v.x[i], v.y[i], v.z[i], v.radius[i]);
+      rmax = std::fmax(rmax, v.radius[i]);
+      const uint32_t st = v.state[i];
+      uint32_t a = st | ((uint32_t)t << 8);
+      if (v.agek && v.agek[i] > P.thresh_sp) a |= 1u << 4;
+      const int32_t q = v.pair ? v.pair[i] : -1;
+      if (st == ST_MUSUME) {
+        // spring_force_to_memb, cell_interaction.cpp:614-620
+        uint32_t code = 0;
+        if (q >= 0 && v.state[q] == ST_FIX) code = 1;
+        else if (v.rest_div_times && v.rest_div_times[i] > 0) code = 2;
+        a |= code << 5;
+      }
+      attr[g] = a;
+      pair[g] = q >= 0 ? pbase + q : -1;
+      spr[g] = v.spr_nat_len ? v.spr_nat_len[i] : 0.0;
+    }
+    T.rmax = rmax;
+    pbase += v.n;
+    binbase += T.anx * T.any * T.anz;
+  }
+  const size_t C = (size_t)c->cfg.max_conn;
+  if ((rc = dev_alloc(&c->tissues, ntissues)) || (rc = dev_alloc(&c->pos[0], n)) ||
+      (rc = dev_alloc(&c->pos[1], n)) || (rc = dev_alloc(&c->attr, n)) ||
+      (rc = dev_alloc(&c->pair, n)) || (rc = dev_alloc(&c->spr, n)) ||
+      (rc = dev_alloc(&c->dermis, n)) || (rc = dev_alloc(&c->nbr, C * n)) ||
+      (rc = dev_alloc(&c->nn, n)) || (rc = dev_alloc(&c->sn, n)) || (rc = dev_alloc(&c->sm, n)) ||
+      (rc = dev_alloc(&c->bin, n)) || (rc = dev_alloc(&c->rank, n)) ||
+      (rc = dev_alloc(&c->counts, nbins)) || (rc = dev_alloc(&c->starts, nbins + 1)) ||
+      (rc = dev_alloc(&c->skey, n)) || (rc = dev_alloc(&c->spos, n)) ||
+      (rc = dev_alloc(&c->stage, 3 * (size_t)n))) {
+    free_buffers(c);
+    return rc;
+  }
+  c->scan.capacity = (int32_t)((std::max<int64_t>(nbins, n) + kScanTile - 1) / kScanTile) + 1;
+  if ((rc = dev_alloc(&c->scan.partial, c->scan.capacity))) {
+    free_buffers(c);
+    return rc;
+  }
+  cudaStream_t s = c->stream;
+  EPI_CUDA(cudaMemcpyAsync(c->tissues, c->tissues_h.data(), sizeof(TissueDev) * ntissues,
+                           cudaMemcpyHostToDevice, s));
+  EPI_CUDA(cudaMemcpyAsync(c->pos[0], pos.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, s));
+  EPI_CUDA(cudaMemcpyAsync(c->pos[1], pos.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, s));
+  EPI_CUDA(cudaMemcpyAsync(c->attr, attr.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s));
+  EPI_CUDA(cudaMemcpyAsync(c->pair, pair.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+  EPI_CUDA(cudaMemcpyAsync(c->spr, spr.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  EPI_CUDA(cudaMemsetAsync(c->counts, 0, sizeof(int32_t) * (size_t)std::max<int64_t>(nbins, 1), s));
+  EPI_CUDA(cudaMemsetAsync(c->nn, 0, sizeof(int32_t) * n, s));
+  EPI_CUDA(cudaMemsetAsync(c->dermis, 0xff, sizeof(int32_t) * n, s));
+  EPI_CUDA(cudaMemsetAsync(c->status, 0, sizeof(DevStatus), s));
+  c->cur = 0;
+  c->loaded = true;
+  launch_connect(make_state(c, c->cur), whole(c), c->cfg.precision, c->scan, s, nullptr);
+  return check_status(c);
+  EPI_GUARD_END
+}
+
+int epi_connect(epi_ctx* c) {
+  if (!c) return EPI_ERR_INVALID_ARG;
+  if (!c->loaded) return EPI_ERR_STATE;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  launch_connect(make_state(c, c->cur), whole(c), c->cfg.precision, c->scan, c->stream, nullptr);
+  return check_status(c);
+  EPI_GUARD_END
+}
+
+int epi_interact_commit(epi_ctx* c) {
+  if (!c) return EPI_ERR_INVALID_ARG;
+  if (!c->loaded) return EPI_ERR_STATE;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  launch_interact_commit(make_state(c, c->cur), whole(c), c->cfg.precision, c->stream, nullptr);
+  c->cur ^= 1;
+  return check_status(c);
+  EPI_GUARD_END
+}
+
+int epi_step(epi_ctx* c, int32_t nsteps) {
+  if (!c || nsteps < 0) return EPI_ERR_INVALID_ARG;
+  if (!c->loaded) return EPI_ERR_STATE;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  for (int32_t k = 0; k < nsteps; ++k) enqueue_step(c, c->cur, nullptr);
+  return check_status(c);
+  EPI_GUARD_END
+}
+
+int epi_step_graph(epi_ctx* c, int32_t nsteps) {
+  if (!c || nsteps < 0) return EPI_ERR_INVALID_ARG;
+  if (!c->loaded) return EPI_ERR_STATE;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  int32_t pairs = nsteps / 2;
+  if (pairs > 0) {
+    cudaGraphExec_t& ge = c->graph[c->cur];
+    if (!ge) {
+      cudaGraph_t g;
+      EPI_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      int cur = c->cur;
+      enqueue_step(c, cur, nullptr);
+      enqueue_step(c, cur, nullptr);
+      EPI_CUDA(cudaStreamEndCapture(c->stream, &g));
+      const cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+      cudaGraphDestroy(g);
+      EPI_CUDA(e);
+    }
+    for (int32_t k = 0; k < pairs; ++k) EPI_CUDA(cudaGraphLaunch(ge, c->stream));
+  }
+  if (nsteps % 2) enqueue_step(c, c->cur, nullptr);
+  return check_status(c);
+  EPI_GUARD_END
+}
+
+int epi_step_per_tissue(epi_ctx* c, int32_t nsteps) {
+  if (!c || nsteps < 0) return EPI_ERR_INVALID_ARG;
+  if (!c->loaded) return EPI_ERR_STATE;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  for (int32_t k = 0; k < nsteps; ++k) {
+    for (int t = 0; t < c->ntissues; ++t) {
+      const Range r = tissue_range(c, t);
+      launch_interact_commit(make_state(c, c->cur), r, c->cfg.precision, c->stream, nullptr);
+      launch_connect(make_state(c, c->cur ^ 1), r, c->cfg.precision, c->scan, c->stream, nullptr);
+    }
+    c->cur ^= 1;
+  }
+  return check_status(c);
+  EPI_GUARD_END
+}
+
+int epi_sync(epi_ctx* c) {
+  if (!c) return EPI_ERR_INVALID_ARG;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  return check_status(c);
+  EPI_GUARD_END
+}
+
+int epi_num_particles(const epi_ctx* c, int64_t* n) {
+  if (!c || !n) return EPI_ERR_INVALID_ARG;
+  *n = c->loaded ? c->n : 0;
+  return EPI_OK;
+}
+
+int epi_download_positions(epi_ctx* c, double* x, double* y, double* z) {
+  if (!c || !x || !y || !z) return EPI_ERR_INVALID_ARG;
+  if (!c->loaded) return EPI_ERR_STATE;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  const int64_t n = c->n;
+  double* d = c->stage;
+  launch_unpack_positions(make_state(c, c->cur), d, d + n, d + 2 * n, (int32_t)n, c->stream);
+  EPI_CUDA(cudaMemcpyAsync(x, d, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+  EPI_CUDA(cudaMemcpyAsync(y, d + n, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+  EPI_CUDA(cudaMemcpyAsync(z, d + 2 * n, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+  return check_status(c);
+  EPI_GUARD_END
+}
+
+int epi_upload_positions(epi_ctx* c, const double* x, const double* y, const double* z) {
+  if (!c || !x || !y || !z) return EPI_ERR_INVALID_ARG;
+  if (!c->loaded) return EPI_ERR_STATE;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  const int64_t n = c->n;
+  double* d = c->stage;
+  EPI_CUDA(cudaMemcpyAsync(d, x, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  EPI_CUDA(cudaMemcpyAsync(d + n, y, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  EPI_CUDA(cudaMemcpyAsync(d + 2 * n, z, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  launch_pack_positions(make_state(c, c->cur), d, d + n, d + 2 * n, (int32_t)n, c->stream);
+  launch_connect(make_state(c, c->cur), whole(c), c->cfg.precision, c->scan, c->stream, nullptr);
+  return check_status(c);
+  EPI_GUARD_END
+}
+
+int epi_get_connections(epi_ctx* c, int32_t* offsets, int32_t* idx, int64_t cap,
+                        int64_t* total) {
+  if (!c || !offsets || cap < 0 || (cap > 0 && !idx)) return EPI_ERR_INVALID_ARG;
+  if (!c->loaded) return EPI_ERR_STATE;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  const int32_t n = (int32_t)c->n;
+  int32_t *rowlen = nullptr, *rowoff = nullptr, *didx = nullptr, *partial = nullptr;
+  if ((rc = dev_alloc(&rowlen, n)) || (rc = dev_alloc(&rowoff, (size_t)n + 1))) {
+    cudaFree(rowlen);
+    return rc;
+  }
+  ScanScratch sc;
+  sc.capacity = (n + kScanTile - 1) / kScanTile + 1;
+  if ((rc = dev_alloc(&partial, sc.capacity))) {
+    cudaFree(rowlen);
+    cudaFree(rowoff);
+    return rc;
+  }
+  sc.partial = partial;
+  const DevState S = make_state(c, c->cur);
+  launch_rowlen(S, rowlen, n, c->stream);
+  launch_scan(rowlen, rowoff, n, 0, sc, c->stream);
+  cudaError_t e = cudaMemcpyAsync(offsets, rowoff, sizeof(int32_t) * ((size_t)n + 1),
+                                  cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  const int64_t tot = e == cudaSuccess ? offsets[n] : 0;
+  if (total) *total = tot;
+  if (e == cudaSuccess && cap >= tot && tot > 0) {
+    e = cudaMalloc((void**)&didx, sizeof(int32_t) * tot);
+    if (e == cudaSuccess) {
+      launch_fill_csr(S, rowoff, didx, n, c->stream);
+      e = cudaMemcpyAsync(idx, didx, sizeof(int32_t) * tot, cudaMemcpyDeviceToHost, c->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    }
+  }
+  cudaFree(rowlen);
+  cudaFree(rowoff);
+  cudaFree(partial);
+  if (didx) cudaFree(didx);
+  EPI_CUDA(e);
+  if (cap < tot && cap > 0) return EPI_ERR_INVALID_ARG;
+  return check_status(c);
+  EPI_GUARD_END
+}
+
+int epi_get_dermis(epi_ctx* c, int32_t* dermis) {
+  if (!c || !dermis) return EPI_ERR_INVALID_ARG;
+  if (!c->loaded) return EPI_ERR_STATE;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  int32_t* d = nullptr;
+  if ((rc = dev_alloc(&d, c->n))) return rc;
+  launch_dermis_local(make_state(c, c->cur), d, (int32_t)c->n, c->stream);
+  cudaError_t e = cudaMemcpyAsync(dermis, d, sizeof(int32_t) * c->n, cudaMemcpyDeviceToHost,
+                                  c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(d);
+  EPI_CUDA(e);
+  return check_status(c);
+  EPI_GUARD_END
+}
+
+int epi_error_info(epi_ctx* c, int32_t* tissue, int32_t* particle, int32_t* other,
+                   double* value) {
+  if (!c) return EPI_ERR_INVALID_ARG;
+  int32_t t = -1, a = c->last.a, b = c->last.b;
+  if (c->last.code != 0 && a >= 0) {
+    for (int k = 0; k < c->ntissues; ++k) {
+      const TissueDev& T = c->tissues_h[k];
+      if (a >= T.pbase && a < T.pbase + T.n) {
+        t = k;
+        a -= T.pbase;
+        if (b >= T.pbase && b < T.pbase + T.n) b -= T.pbase;
+        else if (c->last.code != EPI_ERR_BIN_OVERFLOW) b = -1;
+        break;
+      }
+    }
+  }
+  if (tissue) *tissue = t;
+  if (particle) *particle = a;
+  if (other) *other = b;
+  if (value) *value = c->last.v;
+  return c->last.code;
+}
+
+void* epi_stream(epi_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int epi_time_kernels(epi_ctx* c, int32_t nsteps, int32_t max_classes, double* ms,
+                     int32_t* launches, const char** names, int32_t* nclasses) {
+  if (!c || nsteps < 0 || !ms || !launches || max_classes < KC_COUNT) return EPI_ERR_INVALID_ARG;
+  if (!c->loaded) return EPI_ERR_STATE;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  Timer tm;
+  for (int32_t k = 0; k < nsteps; ++k) enqueue_step(c, c->cur, &tm);
+  rc = check_status(c);
+  for (int k = 0; k < KC_COUNT; ++k) {
+    double sum = 0;
+    for (auto& p : tm.ev[k]) {
+      float f = 0;
+      cudaEventElapsedTime(&f, p.a, p.b);
+      sum += f;
+    }
+    ms[k] = sum;
+    launches[k] = (int32_t)tm.ev[k].size();
+    if (names) names[k] = kKernelClassNames[k];
+  }
+  if (nclasses) *nclasses = KC_COUNT;
+  return rc;
+  EPI_GUARD_END
+}
+
+}  // extern "C"

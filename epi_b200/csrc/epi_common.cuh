@@ -1,0 +1,282 @@
+// Device-side data layout, helpers and force laws of the mechanics step.
+//
+// Layout in HBM (all tissues of a batch concatenated, particle g is particle
+// g - pbase of its tissue):
+//   pos[2][N]  double4 (x, y, z, radius), double-buffered (current / next);
+//              the reference's dual_double d1 / d2 (epi5_MT/DualValue.h:17-55)
+//   attr[N]    u32: bits 0-3 state, bit 4 "agek > THRESH_SP", bits 5-6 the
+//              MUSUME membrane spring selector, bits 8-31 tissue id
+//   pair[N]    i32 global partner index or -1; spr[N] double spring rest length
+//   dermis[N]  i32 global index of the nearest connected MEMB (FIX/MUSUME)
+//   nbr[C][N]  i32 searched neighbours, column-major ("ELL") so that a warp
+//              reading entry k of 32 consecutive particles is coalesced;
+//              nn[N] their count. Membrane lattice links are implicit.
+//   sn/sm[N]   membrane bending scratch (unit vector + length to the right /
+//              upper lattice neighbour), the reference's Memb_data
+//              (epi5_MT/cell.h:42-69)
+//   bins       counting-sort cell list over the reference's 2.0 grid
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace epi {
+
+enum State : uint32_t {
+  ST_ALIVE = 0, ST_DEAD = 1, ST_DISA = 2, ST_UNUSED = 3, ST_FIX = 4, ST_BLANK = 5,
+  ST_DER = 6, ST_MUSUME = 7, ST_AIR = 8, ST_MEMB = 9
+};
+
+enum ErrCode : int32_t {
+  E_OK = 0, E_BIN_RANGE = 5, E_BIN_OVERFLOW = 6, E_LIST_OVERFLOW = 7, E_COEF_RANGE = 8,
+  E_MEMB_COEF_RANGE = 9, E_NONFINITE = 10, E_TIMEOUT = 11
+};
+
+constexpr double kAreaGrid = 2.0 + 1e-7;  // AREA_GRID, cell_connection.cpp:16-19
+constexpr int kBinCap = 200;              // N3, cell_connection.cpp:28
+constexpr int kMembAdj = 4;               // MEMB_ADJ_CONN_NUM (square), define.h:147-153
+
+struct Params {
+  double dt, eps_m, p_memb, der_der_const, k_total, k_desmosome, kspring, kspring_d, kbend,
+      delta_r, para_ljp2, kspring_division, lj_thresh, thresh_sp;
+};
+
+struct TissueDev {
+  int32_t pbase, n, nmemb, nder, nmx, nmy;
+  int32_t anx, any, anz, binbase;  // reference grid (cell_connection.cpp:22-26)
+  double lx, ly, lz, rmax;
+  Params P;
+};
+
+struct DevStatus {
+  int32_t flags;  // bit per ErrCode
+  int32_t code;   // first error recorded
+  int32_t a, b;   // particle / partner (global) of the first error
+  double v;       // offending value
+};
+
+struct DevState {
+  const TissueDev* tissues;
+  double4* pos_cur;
+  double4* pos_nxt;
+  const uint32_t* attr;
+  const int32_t* pair;
+  const double* spr;
+  int32_t* dermis;
+  int32_t* nbr;
+  int32_t* nn;
+  double4* sn;
+  double4* sm;
+  int32_t* bin;
+  int32_t* rank;
+  int32_t* counts;
+  int32_t* starts;
+  uint32_t* skey;   // sorted particles: global index | (is_memb << 31)
+  double4* spos;    // sorted copy of the current positions
+  DevStatus* status;
+  int64_t n_total;  // ELL column stride
+  int32_t max_conn;
+};
+
+__device__ __forceinline__ uint32_t attr_state(uint32_t a) { return a & 15u; }
+__device__ __forceinline__ bool attr_old(uint32_t a) { return (a >> 4) & 1u; }
+__device__ __forceinline__ uint32_t attr_sfm(uint32_t a) { return (a >> 5) & 3u; }
+__device__ __forceinline__ uint32_t attr_tissue(uint32_t a) { return a >> 8; }
+
+__device__ __forceinline__ void raise_error(DevStatus* s, int32_t code, int32_t a, int32_t b,
+                                            double v) {
+  atomicOr(&s->flags, 1 << code);
+  if (atomicCAS(&s->code, 0, code) == 0) {
+    s->a = a;
+    s->b = b;
+    s->v = v;
+  }
+}
+
+// Minimum-image difference, p_diff_x / p_diff_y (epi5_MT/utils.h:25-41).
+// Plain IEEE subtraction and comparison: identical rounding on CPU and GPU.
+__device__ __forceinline__ double pdiff(double a, double b, double L) {
+  const double d = a - b;
+  if (d > 0.5 * L) return d - L;
+  if (d <= -0.5 * L) return d + L;
+  return d;
+}
+
+// |d|^2 exactly as the reference evaluates DIST_SQ / p_dist_sq
+// (utils.h:48-53, cell_connection.cpp:115-119): no fused multiply-add.
+__device__ __forceinline__ double dist_sq_exact(double dx, double dy, double dz) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+
+// Connection predicate of connect_proc (cell_connection.cpp:118-119):
+// |d|^2 <= LJ_THRESH*LJ_THRESH*rad_sum*rad_sum, evaluated left to right.
+__device__ __forceinline__ bool connected_pred(double d2, double lt, double ri, double rj) {
+  const double rs = __dadd_rn(ri, rj);
+  return d2 <= __dmul_rn(__dmul_rn(__dmul_rn(lt, lt), rs), rs);
+}
+
+template <typename R>
+__device__ __forceinline__ R pow6(R v) { return v * v * v * v * v * v; }
+template <typename R>
+__device__ __forceinline__ R pow3(R v) { return v * v * v; }
+
+// Force laws (epi5_MT/cell_interaction.cpp:77-285). Each takes the squared
+// distance d2 and radius sum rs of the pair and returns the coefficient that
+// cell_interaction_apply multiplies by DT and the separation (:48-66).
+template <typename R>
+struct Laws {
+  R eps4, p_memb, der_der_const, k_total, k_desmosome, kspring, kspring_d, delta_r, para_ljp2,
+      kspring_division, lj_thresh, ljt1sq;
+
+  __device__ __forceinline__ explicit Laws(const Params& P)
+      : eps4(R(4.0 * P.eps_m)), p_memb(R(P.p_memb)), der_der_const(R(P.der_der_const)),
+        k_total(R(P.k_total)), k_desmosome(R(P.k_desmosome)), kspring(R(P.kspring)),
+        kspring_d(R(P.kspring_d)), delta_r(R(P.delta_r)), para_ljp2(R(P.para_ljp2)),
+        kspring_division(R(P.kspring_division)), lj_thresh(R(P.lj_thresh)),
+        ljt1sq(R((P.lj_thresh - 1.0) * (P.lj_thresh - 1.0))) {}
+
+  // ljmain, :103-111
+  __device__ __forceinline__ R ljmain(R d2, R rs) const {
+    const R lj6 = pow6(rs) / pow3(d2);
+    return eps4 * lj6 * (lj6 - R(1)) / d2;
+  }
+  // adhesion, :113-124
+  __device__ __forceinline__ R adhesion(R d2, R rs, R k) const {
+    const R d = sqrt(d2);
+    const R m1 = d / rs - R(1);
+    return (m1 + R(1) > lj_thresh) ? R(0) : -(k / d) * m1 * (R(1) - m1 * m1 / ljt1sq);
+  }
+  // is_near, :90-93
+  __device__ __forceinline__ bool near(R d2, R rs) const { return d2 < rs * rs; }
+  // CI_der_to_der, :129-139
+  __device__ __forceinline__ R der_der(R d2, R rs) const {
+    const R d = sqrt(d2);
+    const R dd = d + delta_r;
+    if (dd < rs) {
+      const R lj6 = pow6(rs) / pow6(dd);
+      return eps4 * lj6 * (lj6 - R(1)) / (d * dd) + para_ljp2;
+    }
+    if (near(d2, rs)) return para_ljp2;
+    const R lj6 = pow6(rs) / pow6(dd);
+    return eps4 * lj6 * (lj6 - R(1)) / (d * d) + para_ljp2;
+  }
+  // CI_al_air_de_to_al_air_de_fix_mu, :141-152
+  __device__ __forceinline__ R aad(R d2, R rs, bool both_old) const {
+    if (near(d2, rs)) return ljmain(d2, rs);
+    return adhesion(d2, rs, both_old ? k_total : k_desmosome);
+  }
+  // CI_fix_mu_to_fix_mu, :154-162
+  __device__ __forceinline__ R fixmu(R d2, R rs) const {
+    if (near(d2, rs)) return ljmain(d2, rs);
+    return adhesion(d2, rs, k_desmosome);
+  }
+  // CI_mu_to_memb, :164-172 (spring = the MUSUME's spring_force_to_memb)
+  __device__ __forceinline__ R mu_memb(R d2, R rs, R spring) const {
+    if (near(d2, rs)) return ljmain(d2, rs);
+    return adhesion(d2, rs, spring);
+  }
+  // CI_fix_to_memb, :174-183
+  __device__ __forceinline__ R fix_memb(R d2, R rs) const {
+    if (near(d2, rs)) return ljmain(d2, rs);
+    const R d = sqrt(d2);
+    return -(kspring / d) * (d / rs - R(1));
+  }
+  // CI_memb_to_memb, :185-234; *bad set when |coef| > 100 (the reference aborts)
+  __device__ __forceinline__ R memb_memb(R d2, R rs, bool* bad) const {
+    const R rs2 = rs * rs;
+    const R cr2 = rs2 * p_memb * p_memb;
+    R tmp;
+    if (d2 < cr2) {
+      const R lj6 = pow3(cr2) / pow3(d2);
+      tmp = eps4 * lj6 * (lj6 - R(1)) / d2;
+    } else if (d2 < rs2) {
+      const R d = sqrt(d2);
+      tmp = -(der_der_const / d) * (d / (rs * p_memb) - R(1));
+    } else {
+      const R d = sqrt(d2);
+      const R lam = (R(1) + p_memb) * rs;
+      const R lj6 = pow6(rs * p_memb) / pow6(lam - d);
+      tmp = -(der_der_const / rs) * ((R(1) - p_memb) / p_memb) -
+            eps4 * (lj6 * (lj6 - R(1))) / ((lam - d) * d);
+    }
+    *bad = fabs(tmp) > R(100);
+    return tmp;
+  }
+  // CI_pair, :281-285 (rest = the first cell's spr_nat_len)
+  __device__ __forceinline__ R pair(R d2, R rest) const {
+    const R d = sqrt(d2);
+    return -(kspring_division * (d - rest)) / d;
+  }
+};
+
+// Law selected when cell c iterates its connection o (the per-state bodies
+// of cell_interaction.cpp:549-634). Index order decides double counting
+// (no_double_count, cell.h:293-295).
+enum Law : int { L_NONE = 0, L_OTHER, L_DER_DER, L_AAD, L_FIXMU, L_FIX_MEMB, L_MU_MEMB };
+
+__device__ __forceinline__ bool is_aad_state(uint32_t s) {
+  return s == ST_ALIVE || s == ST_AIR || s == ST_DEAD;
+}
+
+__device__ __forceinline__ int law_of(uint32_t sc, int32_t c, int32_t c_pair, int32_t c_dermis,
+                                      uint32_t so, int32_t o) {
+  switch (sc) {
+    case ST_DER:  // _DER_interaction, :549-561
+      return (so == ST_DER && c > o) ? L_DER_DER : L_OTHER;
+    case ST_ALIVE:
+    case ST_AIR:
+    case ST_DEAD:  // _AL_AIR_DE_interaction, :563-579
+      if (is_aad_state(so)) return c > o ? L_AAD : L_NONE;
+      return so == ST_DER ? L_NONE : L_AAD;
+    case ST_FIX:  // _FIX_interaction, :581-604
+      if (so == ST_FIX) return (c_pair != o && c > o) ? L_FIXMU : L_NONE;
+      if (so == ST_MUSUME) return c_pair != o ? L_FIXMU : L_NONE;
+      if (so == ST_MEMB) return c_dermis == o ? L_FIX_MEMB : L_OTHER;
+      return L_NONE;
+    case ST_MUSUME:  // _MUSUME_interaction, :613-634
+      if (so == ST_MEMB) return c_dermis == o ? L_MU_MEMB : L_OTHER;
+      if (so == ST_MUSUME && c_pair != o && c > o) return L_FIXMU;
+      return L_NONE;
+    default:
+      return L_NONE;
+  }
+}
+
+// spring_force_to_memb of a MUSUME (cell_interaction.cpp:614-620), selected
+// on the host at upload: 0 -> 0, 1 -> Kspring, 2 -> Kspring_d.
+template <typename R>
+__device__ __forceinline__ R sfm_value(uint32_t code, const Laws<R>& L) {
+  return code == 1 ? L.kspring : (code == 2 ? L.kspring_d : R(0));
+}
+
+template <typename R>
+__device__ __forceinline__ R eval_law(int law, const Laws<R>& L, R d2, R rs, bool both_old,
+                                      uint32_t c_sfm) {
+  switch (law) {
+    case L_OTHER: return L.ljmain(d2, rs);
+    case L_DER_DER: return L.der_der(d2, rs);
+    case L_AAD: return L.aad(d2, rs, both_old);
+    case L_FIXMU: return L.fixmu(d2, rs);
+    case L_FIX_MEMB: return L.fix_memb(d2, rs);
+    case L_MU_MEMB: return L.mu_memb(d2, rs, sfm_value(c_sfm, L));
+    default: return R(0);
+  }
+}
+
+// Square membrane lattice neighbours of membrane particle j (tissue-local),
+// _memb_init square branch (epi5_MT/cellmanager.cpp:114-158).
+struct Lattice {
+  int32_t l, ll, r, b, bb, u;
+};
+__device__ __forceinline__ Lattice lattice_of(int32_t j, int32_t NMX, int32_t NMY) {
+  const int32_t jj = j % NMX, kk = j / NMX;
+  Lattice L;
+  L.l = jj == 0 ? j + NMX - 1 : j - 1;
+  L.ll = jj <= 1 ? j + NMX - 2 : j - 2;
+  L.r = jj == NMX - 1 ? j - (NMX - 1) : j + 1;
+  L.b = kk == 0 ? j + NMX * NMY - NMX : j - NMX;
+  L.bb = kk <= 1 ? j + NMX * NMY - 2 * NMX : j - 2 * NMX;
+  L.u = kk == NMY - 1 ? j - (NMX * NMY - NMX) : j + NMX;
+  return L;
+}
+
+}  // namespace epi

@@ -1,0 +1,170 @@
+/* epi_mech.h -- C ABI of the B200 cell-mechanics library (libepi_mech.so).
+ *
+ * The library replaces the per-step mechanics of the epi5_MT epidermis model:
+ *   connect_cell(CellManager&)          epi5_MT/cell_connection.h:3,
+ *                                       epi5_MT/cell_connection.cpp:191-203
+ *   cell_interaction(CellManager&)      epi5_MT/cell_interaction.h:5,
+ *                                       epi5_MT/cell_interaction.cpp:648-685
+ *   pos_copy(CellManager&)              epi5_MT/cellmanager.h:117,
+ *                                       epi5_MT/cellmanager.cpp:19-26
+ *   cell_pos_periodic_fix(CellManager&) epi5_MT/cellmanager.h:111,
+ *                                       epi5_MT/cellmanager.cpp:395-414
+ * for the square-membrane build, on one GPU, for one tissue or a batch of
+ * independent tissues. A tissue is what one epi5_MT CellManager holds:
+ * particles in the reference's index layout (membrane [0,nmemb), dermis
+ * [nmemb,nmemb+nder), every other cell after), a periodic box LX x LY and an
+ * open height LZ.
+ *
+ * Conventions: every call returns an epi_status (0 = EPI_OK); no exception
+ * crosses the ABI. Pointers are host pointers unless stated otherwise. A
+ * context is bound to one device and one stream and must not be used from two
+ * threads at once. Work is stream-ordered; calls that return data to the host
+ * synchronise the context's stream. Errors raised inside kernels are sticky
+ * until the call that reports them returns.
+ */
+#ifndef EPI_MECH_H
+#define EPI_MECH_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. Kernel-side conditions mirror the reference's aborts. */
+typedef enum epi_status {
+  EPI_OK = 0,
+  EPI_ERR_INVALID_ARG = 1,      /* bad pointer, size or tissue description */
+  EPI_ERR_NO_DEVICE = 2,        /* no usable CUDA device */
+  EPI_ERR_CUDA = 3,             /* a CUDA runtime call failed */
+  EPI_ERR_OOM = 4,              /* device allocation failed */
+  EPI_ERR_BIN_RANGE = 5,        /* particle outside the grid: cell_connection.cpp:48-53, :99 */
+  EPI_ERR_BIN_OVERFLOW = 6,     /* more than 199 particles in one 2.0 grid bin: cell_connection.cpp:59 */
+  EPI_ERR_LIST_OVERFLOW = 7,    /* connection list capacity exceeded: cell_connection.cpp:122 */
+  EPI_ERR_COEF_RANGE = 8,       /* |pair coefficient| > 1000: cell_interaction.cpp:51-55 */
+  EPI_ERR_MEMB_COEF_RANGE = 9,  /* |membrane coefficient| > 100: cell_interaction.cpp:200-231 */
+  EPI_ERR_NONFINITE = 10,       /* a position became NaN or infinite */
+  EPI_ERR_TIMEOUT = 11,         /* a bounded device-side wait gave up */
+  EPI_ERR_STATE = 12,           /* call out of order (e.g. step before upload) */
+  EPI_ERR_UNSUPPORTED = 13      /* geometry outside what the library implements */
+} epi_status;
+
+/* Force-law constants of one tissue. Defaults (epi_params_default) are the
+ * reference's compile-time constants: epi5_MT/cell_interaction.cpp:21-45
+ * (eps_m, P_MEMB, DER_DER_CONST, K_TOTAL, K_DESMOSOME, Kspring, Kspring_d,
+ * KBEND, delta_R, para_ljp2, Kspring_division) and epi5_MT/define.h:86,132,135
+ * (DT_Cell, THRESH_SP, LJ_THRESH). */
+typedef struct epi_params {
+  double dt;
+  double eps_m;
+  double p_memb;
+  double der_der_const;
+  double k_total;
+  double k_desmosome;
+  double kspring;
+  double kspring_d;
+  double kbend;
+  double delta_r;
+  double para_ljp2;
+  double kspring_division;
+  double lj_thresh;
+  double thresh_sp;
+} epi_params;
+
+/* One tissue in structure-of-arrays form: what epi5_MT's Cell objects hold for
+ * the mechanics (epi5_MT/cell.h:101-247). Indices (pair) are tissue-local,
+ * -1 for none; pairs must be mutual. nmemb must equal nmx * nmy (square
+ * membrane wired as epi5_MT/cellmanager.cpp:114-166). */
+typedef struct epi_tissue_view {
+  int32_t n, nmemb, nder;
+  int32_t nmx, nmy;
+  double lx, ly, lz;
+  const double* x;
+  const double* y;
+  const double* z;
+  const double* radius;
+  const double* agek;
+  const double* spr_nat_len;
+  const uint8_t* state;          /* CELL_STATE, epi5_MT/define.h:36-47 */
+  const int32_t* pair;
+  const int32_t* rest_div_times;
+} epi_tissue_view;
+
+typedef enum epi_precision {
+  EPI_PREC_FP64 = 0,  /* every force in FP64 */
+  EPI_PREC_MIXED = 1  /* pair and bending forces in FP32, sums and positions in FP64 */
+} epi_precision;
+
+typedef struct epi_config {
+  int32_t device;     /* CUDA device ordinal */
+  int32_t precision;  /* epi_precision */
+  int32_t max_conn;   /* searched connections per particle (membrane lattice links
+                         are extra); the reference allows 400 (define.h:80) */
+  int32_t reserved;
+} epi_config;
+
+typedef struct epi_ctx epi_ctx;
+
+void epi_params_default(epi_params* p);
+void epi_config_default(epi_config* c);
+const char* epi_strerror(int status);
+
+/* Context lifetime. */
+int epi_create(epi_ctx** out, const epi_config* cfg);
+void epi_destroy(epi_ctx* ctx);
+
+/* Loads ntissues tissues (one CellManager each) and their constants, then runs
+ * the first connect, as cman_init does (epi5_MT/cell_init.cpp:132-137).
+ * Replaces any previous contents. params may be NULL (defaults). */
+int epi_upload(epi_ctx* ctx, int32_t ntissues, const epi_tissue_view* tissues,
+               const epi_params* params);
+
+/* connect_cell over every tissue: bins, connection lists, dermis. */
+int epi_connect(epi_ctx* ctx);
+/* cell_interaction + pos_copy + cell_pos_periodic_fix over every tissue,
+ * using the lists of the last connect. */
+int epi_interact_commit(epi_ctx* ctx);
+/* nsteps of the reference's cell_dynamics mechanics (epi5_MT/proc.cpp:22-32
+ * without cell_state_renew): interact+commit, then connect. */
+int epi_step(epi_ctx* ctx, int32_t nsteps);
+/* Same as epi_step, replayed from a CUDA graph captured on first use. */
+int epi_step_graph(epi_ctx* ctx, int32_t nsteps);
+/* Same as epi_step, but one kernel sequence per tissue and no graph: the
+ * unbatched launch pattern, kept as the comparison point for batching. */
+int epi_step_per_tissue(epi_ctx* ctx, int32_t nsteps);
+/* Waits for queued work and reports any kernel-side error. */
+int epi_sync(epi_ctx* ctx);
+
+/* Total particles over all tissues (positions are concatenated by tissue). */
+int epi_num_particles(const epi_ctx* ctx, int64_t* n);
+int epi_download_positions(epi_ctx* ctx, double* x, double* y, double* z);
+/* Overwrites positions (both buffers, like dual_double::_set) and re-connects. */
+int epi_upload_positions(epi_ctx* ctx, const double* x, const double* y, const double* z);
+/* Connection lists as CSR over all particles (offsets has n+1 entries). Each
+ * row holds tissue-local indices sorted ascending; membrane rows include their
+ * four lattice links, as connected_cell does (epi5_MT/cell.h:132). Writes at
+ * most cap indices and always the exact total to *total. */
+int epi_get_connections(epi_ctx* ctx, int32_t* offsets, int32_t* idx, int64_t cap,
+                        int64_t* total);
+/* Nearest connected membrane particle of each FIX / MUSUME cell
+ * (find_dermis, epi5_MT/cell_connection.cpp:158-172), tissue-local, -1 where
+ * none or not applicable. */
+int epi_get_dermis(epi_ctx* ctx, int32_t* dermis);
+/* Details of the last kernel-side error: particle and partner (tissue-local
+ * where known, else -1) and the offending value. */
+int epi_error_info(epi_ctx* ctx, int32_t* tissue, int32_t* particle, int32_t* other,
+                   double* value);
+
+/* The cudaStream_t the context launches on (as void*). */
+void* epi_stream(epi_ctx* ctx);
+/* Per-kernel timing: runs nsteps (not graph-captured) recording CUDA events
+ * around each kernel class on the context stream. ms receives the summed
+ * milliseconds per class, launches the launch count per class, names the
+ * class names; returns the number of classes (<= max_classes). */
+int epi_time_kernels(epi_ctx* ctx, int32_t nsteps, int32_t max_classes, double* ms,
+                     int32_t* launches, const char** names, int32_t* nclasses);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EPI_MECH_H */

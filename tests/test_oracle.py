@@ -1,0 +1,79 @@
+"""The oracle is pinned before it is trusted.
+
+The C restatement (oracle/epi_oracle.c) must reproduce, bit for bit, the
+frames the compiled reference (epi5_MT sources, serial TBB stand-in) wrote
+into tests/golden/ -- positions, sorted connection lists and dermis -- and,
+where the compiled reference is present, fresh runs of it.
+"""
+import numpy as np
+import pytest
+
+from epi_b200 import tissue as T
+from oracle import oracle as O
+from tests.golden.make_golden import load
+from tests.helpers import lists_equal
+
+
+@pytest.mark.parametrize("name,factory", [("c1", T.config1), ("mixed", T.mixed_state_tissue)])
+def test_oracle_reproduces_reference_golden_frames(built, name, factory):
+    frames = load(name)
+    t = factory()
+    ora = O.OracleTissue(t)
+    done = 0
+    fix_mu = (t.state == T.FIX) | (t.state == T.MUSUME)
+    for f in frames:
+        assert ora.step(f["step"] - done) == 0, ora.error()
+        done = f["step"]
+        x, y, z = ora.positions()
+        assert np.array_equal(x, f["x"]) and np.array_equal(y, f["y"]) and np.array_equal(z, f["z"])
+        off, idx = ora.connections()
+        assert lists_equal(off, idx, f["conn_off"], f["conn_idx"])
+        assert np.array_equal(ora.dermis()[fix_mu], f["dermis"][fix_mu])
+
+
+def _ref_available(t):
+    return O.reference_binary(t) is not None
+
+
+@pytest.mark.parametrize("factory,steps", [
+    (lambda: T.layered_tissue(24, 3, 11), 40),
+    (lambda: T.layered_tissue(64, 8, 1), 3),
+    (lambda: T.config1(5), 200),
+])
+def test_oracle_matches_compiled_reference_live(built, factory, steps):
+    t = factory()
+    if not _ref_available(t):
+        pytest.skip("compiled reference not built here (no reference checkout)")
+    frames = O.run_reference(t, steps, steps)
+    ora = O.OracleTissue(t)
+    assert ora.step(steps) == 0
+    x, y, z = ora.positions()
+    f = frames[-1]
+    assert np.array_equal(x, f["x"]) and np.array_equal(y, f["y"]) and np.array_equal(z, f["z"])
+    off, idx = ora.connections()
+    assert lists_equal(off, idx, f["conn_off"], f["conn_idx"])
+
+
+def test_oracle_raw_lists_start_with_lattice_links(built):
+    t = T.config1()
+    ora = O.OracleTissue(t)
+    off, idx = ora.connections(raw=True)
+    # _memb_init pushes l, r, b, u first (cellmanager.cpp:160-163)
+    row = idx[off[17]:off[18]]
+    assert row[:4].tolist() == [16, 18, 1, 33]
+
+
+def test_oracle_flags_too_strong_interaction(built):
+    t = T.config1()
+    k = t.nmemb
+    t.x[k + 1], t.y[k + 1], t.z[k + 1] = t.x[k] + 0.3, t.y[k], t.z[k]
+    ora = O.OracleTissue(t)
+    code = ora.step(1)
+    assert code == 8  # EPI_ERR_COEF_RANGE: the reference prints "Too strong interaction" and exits
+
+
+def test_oracle_flags_out_of_grid(built):
+    t = T.config1()
+    t.z[t.nmemb + 3] = 40.0  # above LZ = 32: grid_init's range assert
+    ora = O.OracleTissue(t)
+    assert ora.error()[0] == 5
