@@ -41,11 +41,16 @@ from epi_b200.ensemble import shard_tissues  # noqa: E402
 
 METRIC = "cell-updates/s: FP32/batched vs plain FP64 GPU @≤1e-5 rel pos err; grad err"
 UNIT = "cell-updates/s"
-KERNEL_LAUNCHES_PER_STEP = 8  # force_commit, bin, 3 x scan, scatter, binsort, search
+# per step: rebuild (bin, 3 x scan, scatter, binsort, candidate search, gate
+# clear; each exits at once unless a tissue needs a rebuild), prepass, step
+KERNEL_LAUNCHES_PER_STEP = 10
 
 
-def workload(name: str):
+def workload(name: str, tissues: int = 512):
     if name == "ensemble":
+        if tissues != 512:
+            return (T.config4()[:tissues],
+                    f"first {tissues} tissues of the batched ensemble (config 4)")
         return T.config4(), "batched ensemble: 512 tissues, side {16..64}, 2-8 layers (config 4)"
     if name == "c2":
         return [T.config2()], "single tissue 64x64 membrane + 32,768 cells (config 2)"
@@ -149,7 +154,7 @@ def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    tissues, desc = workload(args.workload)
+    tissues, desc = workload(args.workload, args.tissues)
     sample = reference_sample(tissues, args.ref_particles)
     try:
         v, d = time_reference_cpu(sample, max(1, args.warmup), max(1, args.steps))
@@ -203,6 +208,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="ensemble", choices=["ensemble", "c1", "c2", "c3"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--skin", type=float, default=None)
+    ap.add_argument("--tissues", type=int, default=512, help="ensemble size (profiling)")
+    ap.add_argument("--mode", default="graph", choices=["graph", "eager"])
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--ref-particles", type=int, default=120000)
@@ -227,14 +235,14 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    tissues, desc = workload(args.workload)
+    tissues, desc = workload(args.workload, args.tissues)
     shards = shard_tissues([t.n for t in tissues], world)
     mine = [tissues[i] for i in shards[rank]]
     n_mine = sum(t.n for t in mine)
     n_all = sum(t.n for t in tissues)
     prec = capi.EPI_PREC_MIXED if args.precision == "mixed" else capi.EPI_PREC_FP64
 
-    ctx = capi.Context(precision=prec, max_conn=64, device=local)
+    ctx = capi.Context(precision=prec, max_conn=64, device=local, skin=args.skin)
     ctx.upload(mine)
     off, _ = ctx.connections()
     kbar = float(off[-1]) / max(n_mine, 1)  # mean connected_cell length incl. lattice links
@@ -248,7 +256,7 @@ def main():
 
     # warm-up (also captures the graph)
     if args.warmup:
-        ctx.step(args.warmup, "graph")
+        ctx.step(args.warmup, args.mode)
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
@@ -256,7 +264,7 @@ def main():
     e1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         e0.record(stream)
-        ctx.step(args.steps, "graph")
+        ctx.step(args.steps, args.mode)
         e1.record(stream)
         e1.synchronize()
     torch.cuda.synchronize()
@@ -275,15 +283,18 @@ def main():
         dom = max(tk, key=lambda k: tk[k][0])
         dom_ms = tk[dom][0] / max(tk[dom][1], 1)
         hbm, peak_kind = measured_peaks()
-        # algorithmic bytes per particle of each kernel class
-        kb = kbar_searched
+        # Algorithmic bytes per particle of each kernel class. The
+        # step kernel does the whole per-step work of the reference (exact
+        # predicate = connect, forces, commit): B = 52 + 8 k (24 B xyz read,
+        # 24 B xyz write, 4 B state, 4k B list write + 4k B list read).
         per_particle = {
-            "force_commit": 32 + 4 + 4 + 4 * kb + 32,   # own pos+radius, attr, count, list, new pos
-            "search": 32 + 4 + 4 * kb + 4 + 4,          # sorted pos, key, list, count, dermis
-            "bin": 32 + 4 + 8,                          # pos, attr, bin + rank
-            "binsort": 4 + 32 + 4 + 32,                 # key in/out, pos gather, sorted copy
-            "scatter": 8 + 4,
-            "scan": 0,
+            "step": 52 + 8 * kbar,
+            "prepass": 32 * 3 + 64,
+            "rebuild_bin": 32 + 4 + 8,
+            "rebuild_scan": 0,
+            "rebuild_sort": 4 + 32 + 4 + 32,
+            "rebuild_search": 32 + 4 + 4 * 2 * kbar + 4,
+            "gate": 0,
         }
         alg = per_particle[dom] * n_mine
         achieved = alg / (dom_ms * 1e-3) / 1e9
@@ -297,8 +308,7 @@ def main():
             "step_alg_bytes_per_particle": 52 + 8 * kbar,
             "step_frac": (52 + 8 * kbar) * value / max(world, 1) / 1e9 / hbm,
         }
-        extras["kernel_ms_per_step"] = {k: v[0] / max(v[1], 1) * (3 if k == "scan" else 1)
-                                        for k, v in tk.items()}
+        extras["kernel_ms_per_step"] = {k: v[0] / max(v[1], 1) for k, v in tk.items()}
 
         # e2e through the C ABI with host buffers: the drop-in's data flow per
         # step (interaction+commit on device, positions to the host for the

@@ -77,7 +77,8 @@ class TissueViewC(ctypes.Structure):
 
 class ConfigC(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("precision", ctypes.c_int32),
-                ("max_conn", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("max_conn", ctypes.c_int32), ("max_cand", ctypes.c_int32),
+                ("skin", ctypes.c_double)]
 
 
 _lib = None
@@ -150,12 +151,16 @@ def default_params() -> ParamsC:
 class Context:
     """One epi_ctx: a batch of tissues resident on one GPU."""
 
-    def __init__(self, precision: int = EPI_PREC_MIXED, max_conn: int = 64, device: int = 0):
+    def __init__(self, precision: int = EPI_PREC_MIXED, max_conn: int = 64, device: int = 0,
+                 max_cand: Optional[int] = None, skin: Optional[float] = None):
         L = lib()
         cfg = ConfigC()
         L.epi_config_default(ctypes.byref(cfg))
         cfg.precision = precision
         cfg.max_conn = max_conn
+        cfg.max_cand = max(max_cand if max_cand is not None else cfg.max_cand, max_conn)
+        if skin is not None:
+            cfg.skin = skin
         cfg.device = device
         h = ctypes.c_void_p()
         _check(L.epi_create(ctypes.byref(h), ctypes.byref(cfg)), "epi_create")

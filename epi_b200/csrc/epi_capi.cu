@@ -7,6 +7,7 @@
 #include "epi_mech.h"
 #include "epi_kernels.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -48,14 +49,29 @@ void timer_end(Timer* tm, int cls, cudaStream_t s) {
 
 }  // namespace epi
 
+namespace {
+
+// Host-side bookkeeping of one tissue in the batch.
+struct TissueHost {
+  int32_t prep_m;  // offset of its membrane particles in the prep list
+  int32_t prep_f;  // offset of its FIX / MUSUME cells in the FIX/MUSUME block
+  int32_t nfm;     // number of FIX / MUSUME cells
+};
+
+}  // namespace
+
 struct epi_ctx {
   epi_config cfg{};
   cudaStream_t stream = nullptr;
+  LaunchCfg lc{148, 256, 0, 0};
   bool loaded = false;
+  bool lists_fresh = false;  // nbr / nn / dermis match the current positions
   int32_t ntissues = 0;
   int64_t n = 0;
   int32_t nbins = 0;
+  int32_t nprep = 0, nprep_memb = 0;
   std::vector<TissueDev> tissues_h;
+  std::vector<TissueHost> thost;
   // device buffers
   TissueDev* tissues = nullptr;
   double4* pos[2] = {nullptr, nullptr};
@@ -64,16 +80,22 @@ struct epi_ctx {
   int32_t* pair = nullptr;
   double* spr = nullptr;
   int32_t* dermis = nullptr;
+  int32_t* cand = nullptr;
+  int32_t* ncand = nullptr;
+  float4* bpos = nullptr;
   int32_t* nbr = nullptr;
   int32_t* nn = nullptr;
   double4* sn = nullptr;
   double4* sm = nullptr;
+  double4* fmemb = nullptr;
   int32_t* bin = nullptr;
   int32_t* rank = nullptr;
   int32_t* counts = nullptr;
   int32_t* starts = nullptr;
   uint32_t* skey = nullptr;
   double4* spos = nullptr;
+  int32_t* gate = nullptr;
+  int32_t* prep = nullptr;
   double* stage = nullptr;        // 3n doubles: x | y | z for host transfers
   DevStatus* status = nullptr;
   DevStatus* status_h = nullptr;  // pinned
@@ -93,9 +115,9 @@ int cuda_status(cudaError_t e) {
   return EPI_ERR_CUDA;
 }
 
-#define EPI_CUDA(call)                      \
-  do {                                      \
-    const cudaError_t e_ = (call);          \
+#define EPI_CUDA(call)                             \
+  do {                                             \
+    const cudaError_t e_ = (call);                 \
     if (e_ != cudaSuccess) return cuda_status(e_); \
   } while (0)
 
@@ -112,17 +134,21 @@ void free_buffers(epi_ctx* c) {
     g = nullptr;
   }
   void* ptrs[] = {c->tissues, c->pos[0], c->pos[1], c->attr, c->pair, c->spr, c->dermis,
-                  c->nbr, c->nn, c->sn, c->sm, c->bin, c->rank, c->counts, c->starts,
-                  c->skey, c->spos, c->scan.partial, c->stage};
+                  c->cand, c->ncand, c->bpos, c->nbr, c->nn, c->sn, c->sm, c->fmemb, c->bin,
+                  c->rank, c->counts, c->starts, c->skey, c->spos, c->gate, c->prep,
+                  c->scan.partial, c->stage};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   c->tissues = nullptr;
   c->pos[0] = c->pos[1] = nullptr;
   c->attr = nullptr; c->pair = nullptr; c->spr = nullptr; c->dermis = nullptr;
-  c->nbr = nullptr; c->nn = nullptr; c->sn = nullptr; c->sm = nullptr;
+  c->cand = nullptr; c->ncand = nullptr; c->bpos = nullptr;
+  c->nbr = nullptr; c->nn = nullptr; c->sn = nullptr; c->sm = nullptr; c->fmemb = nullptr;
   c->bin = nullptr; c->rank = nullptr; c->counts = nullptr; c->starts = nullptr;
-  c->skey = nullptr; c->spos = nullptr; c->scan.partial = nullptr; c->stage = nullptr;
+  c->skey = nullptr; c->spos = nullptr; c->gate = nullptr; c->prep = nullptr;
+  c->scan.partial = nullptr; c->stage = nullptr;
   c->loaded = false;
+  c->lists_fresh = false;
 }
 
 DevState make_state(epi_ctx* c, int cur) {
@@ -134,34 +160,66 @@ DevState make_state(epi_ctx* c, int cur) {
   S.pair = c->pair;
   S.spr = c->spr;
   S.dermis = c->dermis;
+  S.cand = c->cand;
+  S.ncand = c->ncand;
+  S.bpos = c->bpos;
   S.nbr = c->nbr;
   S.nn = c->nn;
   S.sn = c->sn;
   S.sm = c->sm;
+  S.fmemb = c->fmemb;
   S.bin = c->bin;
   S.rank = c->rank;
   S.counts = c->counts;
   S.starts = c->starts;
   S.skey = c->skey;
   S.spos = c->spos;
+  S.gate = c->gate;
+  S.prep = c->prep;
+  S.nprep = c->nprep;
+  S.nprep_memb = c->nprep_memb;
   S.status = c->status;
   S.n_total = c->n;
   S.max_conn = c->cfg.max_conn;
+  S.max_cand = c->cfg.max_cand;
+  S.skin = c->cfg.skin;
   return S;
 }
 
-Range whole(const epi_ctx* c) { return Range{0, (int32_t)c->n, 0, c->nbins}; }
+Range whole(const epi_ctx* c) { return Range{0, (int32_t)c->n, 0, c->nbins, 0, c->ntissues}; }
 
 Range tissue_range(const epi_ctx* c, int t) {
   const TissueDev& T = c->tissues_h[t];
-  return Range{T.pbase, T.pbase + T.n, T.binbase, T.binbase + T.anx * T.any * T.anz};
+  return Range{T.pbase, T.pbase + T.n, T.binbase, T.binbase + T.anx * T.any * T.anz, t, t + 1};
 }
 
-// One reference step over the batch: interact + commit, swap, connect.
+void prepass_all(epi_ctx* c, int cur, Timer* tm) {
+  launch_prepass(make_state(c, cur), 0, c->nprep_memb, c->nprep_memb, c->nprep,
+                 c->cfg.precision, c->lc, c->stream, tm);
+}
+
+void prepass_tissue(epi_ctx* c, int cur, int t) {
+  const TissueDev& T = c->tissues_h[t];
+  const TissueHost& H = c->thost[t];
+  const int32_t f0 = c->nprep_memb + H.prep_f;
+  launch_prepass(make_state(c, cur), H.prep_m, H.prep_m + T.nmemb, f0, f0 + H.nfm,
+                 c->cfg.precision, c->lc, c->stream, nullptr);
+}
+
+// One reference step over the batch: [rebuild] -> prepass -> fused step.
 void enqueue_step(epi_ctx* c, int& cur, Timer* tm) {
-  launch_interact_commit(make_state(c, cur), whole(c), c->cfg.precision, c->stream, tm);
+  launch_rebuild(make_state(c, cur), whole(c), c->scan, c->lc, c->stream, tm);
+  prepass_all(c, cur, tm);
+  launch_step(make_state(c, cur), whole(c), c->cfg.precision, c->lc, c->stream, tm);
   cur ^= 1;
-  launch_connect(make_state(c, cur), whole(c), c->cfg.precision, c->scan, c->stream, tm);
+}
+
+// connect_cell's results for the current positions: lists and dermis.
+void enqueue_materialize(epi_ctx* c) {
+  const DevState S = make_state(c, c->cur);
+  launch_rebuild(S, whole(c), c->scan, c->lc, c->stream, nullptr);
+  prepass_all(c, c->cur, nullptr);
+  launch_exact_lists(S, whole(c), c->lc, c->stream);
 }
 
 // Waits for the stream and converts any sticky kernel error to a status.
@@ -179,36 +237,92 @@ int check_status(epi_ctx* c) {
   return EPI_OK;
 }
 
+int materialize(epi_ctx* c) {
+  if (c->lists_fresh) return EPI_OK;
+  enqueue_materialize(c);
+  const int rc = check_status(c);
+  if (rc == EPI_OK) c->lists_fresh = true;
+  return rc;
+}
+
 int set_device(const epi_ctx* c) { return cuda_status(cudaSetDevice(c->cfg.device)); }
 
 #define EPI_GUARD_BEGIN try {
-#define EPI_GUARD_END                      \
-  }                                        \
-  catch (const std::bad_alloc&) {          \
-    return EPI_ERR_OOM;                    \
-  }                                        \
-  catch (...) {                            \
-    return EPI_ERR_CUDA;                   \
+#define EPI_GUARD_END             \
+  }                               \
+  catch (const std::bad_alloc&) { \
+    return EPI_ERR_OOM;           \
+  }                               \
+  catch (...) {                   \
+    return EPI_ERR_CUDA;          \
   }
 
-int validate_tissue(const epi_tissue_view& v) {
+// Smallest non-negative double x <= hi with pred(x) true, for a predicate that
+// is false then true as x grows; +inf when pred(hi) is false. Non-negative
+// doubles order like their bit patterns, so this bisects on the bits.
+template <class F>
+double first_true(double hi, F pred) {
+  if (!pred(hi)) return INFINITY;
+  if (pred(0.0)) return 0.0;
+  uint64_t lo_b = 0, hi_b;
+  std::memcpy(&hi_b, &hi, 8);
+  while (hi_b - lo_b > 1) {
+    const uint64_t mid = lo_b + (hi_b - lo_b) / 2;
+    double m;
+    std::memcpy(&m, &mid, 8);
+    if (pred(m)) hi_b = mid;
+    else lo_b = mid;
+  }
+  double r;
+  std::memcpy(&r, &hi_b, 8);
+  return r;
+}
+
+double host_pdiff(double a, double b, double L) {
+  const double d = a - b;
+  if (d > 0.5 * L) return d - L;
+  if (d <= -0.5 * L) return d + L;
+  return d;
+}
+
+// Range-assert thresholds of grid_init / connect_proc for a wrapped position
+// (cell_connection.cpp:44-53, :95-99), evaluated with the same IEEE double
+// operations the reference uses.
+void range_thresholds(TissueDev& T) {
+  const double AG = kAreaGrid;
+  auto grid_fails = [&](double v, double L, int32_t an) {
+    const int32_t k = (int32_t)((0.5 * L - host_pdiff(0.5 * L, v, L)) / AG);
+    return k >= an || k < 0;
+  };
+  const double below_lx = std::nextafter(T.lx, 0.0), below_ly = std::nextafter(T.ly, 0.0);
+  T.gx_hi = first_true(below_lx, [&](double v) { return grid_fails(v, T.lx, T.anx); });
+  T.gy_hi = first_true(below_ly, [&](double v) { return grid_fails(v, T.ly, T.any); });
+  T.cx_hi = first_true(T.lx, [&](double v) { return (int32_t)(v / AG) >= T.anx; });
+  T.cy_hi = first_true(T.ly, [&](double v) { return (int32_t)(v / AG) >= T.any; });
+  const double zbig = 4.0 * (T.lz + 4.0);
+  T.gz_hi = first_true(zbig, [&](double v) { return (int32_t)(v / AG) >= T.anz; });
+  T.cz_hi = T.gz_hi;
+  T.cz_lo = -first_true(zbig, [&](double w) { return (int32_t)(w / AG) >= 1; });
+}
+
+int validate_tissue(const epi_tissue_view& v, const epi_params& P) {
   if (v.n < 0 || v.nmemb < 0 || v.nder < 0 || v.nmemb + v.nder > v.n) return EPI_ERR_INVALID_ARG;
   if (v.n > 0 && (!v.x || !v.y || !v.z || !v.radius || !v.state)) return EPI_ERR_INVALID_ARG;
   if (!(v.lx > 0) || !(v.ly > 0) || !(v.lz > 0)) return EPI_ERR_INVALID_ARG;
   if (v.nmemb != v.nmx * v.nmy || v.nmx < 3 || v.nmy < 3) return EPI_ERR_UNSUPPORTED;
   // The 5-bin search window of connect_proc must not wrap onto itself
-  // (cell_connection.cpp:101-109), else the reference double-pushes.
+  // (cell_connection.cpp:101-109), else the reference pushes pairs twice.
   const int anx = (int)(v.lx / 2.0 + 0.5), any = (int)(v.ly / 2.0 + 0.5), anz = (int)(v.lz / 2.0);
   if (anx < 5 || any < 5 || anz < 5) return EPI_ERR_UNSUPPORTED;
+  double rmax = 0;
   for (int32_t i = 0; i < v.n; ++i) {
     const uint8_t s = v.state[i];
     if (s > ST_MEMB) return EPI_ERR_INVALID_ARG;
     if ((i < v.nmemb) != (s == ST_MEMB)) return EPI_ERR_INVALID_ARG;
     if (i >= v.nmemb && i < v.nmemb + v.nder && s != ST_DER) return EPI_ERR_INVALID_ARG;
     if (i >= v.nmemb + v.nder && s == ST_DER) return EPI_ERR_INVALID_ARG;
-    // every radius must keep each reachable pair inside the reference's
-    // +-2 bin window: LJ_THRESH * (r_i + r_j) < 2 * AREA_GRID
-    if (!(v.radius[i] > 0) || v.radius[i] > 1.6) return EPI_ERR_UNSUPPORTED;
+    if (!(v.radius[i] > 0)) return EPI_ERR_INVALID_ARG;
+    rmax = std::max(rmax, v.radius[i]);
     if (v.pair) {
       const int32_t q = v.pair[i];
       if (q >= v.n || q < -1) return EPI_ERR_INVALID_ARG;
@@ -216,6 +330,9 @@ int validate_tissue(const epi_tissue_view& v) {
         return EPI_ERR_INVALID_ARG;
     }
   }
+  // Every pair the reference can connect must lie inside its +-2 bin window:
+  // LJ_THRESH * (r_i + r_j) < 2 * AREA_GRID (cell_connection.cpp:92-109).
+  if (!(P.lj_thresh > 0) || P.lj_thresh * 2.0 * rmax >= 4.0 - 1e-6) return EPI_ERR_UNSUPPORTED;
   return EPI_OK;
 }
 
@@ -246,7 +363,8 @@ void epi_config_default(epi_config* c) {
   c->device = 0;
   c->precision = EPI_PREC_MIXED;
   c->max_conn = 64;
-  c->reserved = 0;
+  c->max_cand = 96;
+  c->skin = 0.3;
 }
 
 const char* epi_strerror(int s) {
@@ -258,7 +376,7 @@ const char* epi_strerror(int s) {
     case EPI_ERR_OOM: return "device out of memory";
     case EPI_ERR_BIN_RANGE: return "particle outside the grid (grid_init range assert)";
     case EPI_ERR_BIN_OVERFLOW: return "grid bin holds more than 199 particles";
-    case EPI_ERR_LIST_OVERFLOW: return "connection list capacity exceeded";
+    case EPI_ERR_LIST_OVERFLOW: return "connection or candidate list capacity exceeded";
     case EPI_ERR_COEF_RANGE: return "pair interaction coefficient above 1000 (too strong interaction)";
     case EPI_ERR_MEMB_COEF_RANGE: return "membrane interaction coefficient above 100";
     case EPI_ERR_NONFINITE: return "non-finite position";
@@ -276,7 +394,9 @@ int epi_create(epi_ctx** out, const epi_config* cfg) {
   epi_config c;
   epi_config_default(&c);
   if (cfg) c = *cfg;
-  if (c.max_conn <= 0 || c.max_conn > 400) return EPI_ERR_INVALID_ARG;
+  if (c.max_conn <= 0 || c.max_conn > 400 || c.max_cand < c.max_conn || c.max_cand > 1024)
+    return EPI_ERR_INVALID_ARG;
+  if (!(c.skin > 0) || c.skin > 2.0) return EPI_ERR_INVALID_ARG;
   if (c.precision != EPI_PREC_FP64 && c.precision != EPI_PREC_MIXED) return EPI_ERR_INVALID_ARG;
   int ndev = 0;
   const cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -285,6 +405,10 @@ int epi_create(epi_ctx** out, const epi_config* cfg) {
   EPI_CUDA(cudaSetDevice(c.device));
   epi_ctx* ctx = new epi_ctx();
   ctx->cfg = c;
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device) == cudaSuccess &&
+      sms > 0)
+    ctx->lc.num_sms = sms;
   int rc = cuda_status(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
   if (rc == EPI_OK) rc = dev_alloc(&ctx->status, 1);
   if (rc == EPI_OK) rc = cuda_status(cudaMallocHost((void**)&ctx->status_h, sizeof(DevStatus)));
@@ -317,7 +441,10 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
   int64_t n = 0;
   int64_t nbins = 0;
   for (int t = 0; t < ntissues; ++t) {
-    if ((rc = validate_tissue(tv[t]))) return rc;
+    epi_params P;
+    if (params) P = params[t];
+    else epi_params_default(&P);
+    if ((rc = validate_tissue(tv[t], P))) return rc;
     n += tv[t].n;
     nbins += (int64_t)((int)(tv[t].lx / 2.0 + 0.5)) * (int)(tv[t].ly / 2.0 + 0.5) *
              (int)(tv[t].lz / 2.0);
@@ -329,17 +456,21 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
   c->n = n;
   c->nbins = (int32_t)nbins;
   c->tissues_h.assign(ntissues, TissueDev{});
+  c->thost.assign(ntissues, TissueHost{});
   std::vector<double4> pos(n);
   std::vector<uint32_t> attr(n);
   std::vector<int32_t> pair(n, -1);
   std::vector<double> spr(n, 0.0);
+  std::vector<int32_t> prep_m, prep_f;
   int32_t pbase = 0, binbase = 0;
+  bool simple = true, any_old = false;
   for (int t = 0; t < ntissues; ++t) {
     const epi_tissue_view& v = tv[t];
     epi_params P;
     if (params) P = params[t];
     else epi_params_default(&P);
     TissueDev& T = c->tissues_h[t];
+    TissueHost& H = c->thost[t];
     T.pbase = pbase;
     T.n = v.n;
     T.nmemb = v.nmemb;
@@ -353,15 +484,27 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
     T.lx = v.lx;
     T.ly = v.ly;
     T.lz = v.lz;
+    T.hlx = 0.5 * v.lx;
+    T.hly = 0.5 * v.ly;
     std::memcpy(&T.P, &P, sizeof(Params));
-    double rmax = 0;
+    T.lawf = make_laws<float>(T.P);
+    T.lawd = make_laws<double>(T.P);
+    range_thresholds(T);
+    H.prep_m = (int32_t)prep_m.size();
+    H.prep_f = (int32_t)prep_f.size();
+    double rmax = 0, rmax_nm = 0;
     for (int32_t i = 0; i < v.n; ++i) {
       const int64_t g = pbase + i;
       pos[g] = make_double4(v.x[i], v.y[i], v.z[i], v.radius[i]);
-      rmax = std::fmax(rmax, v.radius[i]);
       const uint32_t st = v.state[i];
+      rmax = std::max(rmax, v.radius[i]);
+      if (st != ST_MEMB) rmax_nm = std::max(rmax_nm, v.radius[i]);
       uint32_t a = st | ((uint32_t)t << 8);
-      if (v.agek && v.agek[i] > P.thresh_sp) a |= 1u << 4;
+      if (v.agek && v.agek[i] > P.thresh_sp) {
+        a |= 1u << 4;
+        any_old = true;
+      }
+      if (st != ST_MEMB && st != ST_ALIVE && st != ST_DEAD && st != ST_AIR) simple = false;
       const int32_t q = v.pair ? v.pair[i] : -1;
       if (st == ST_MUSUME) {
         // spring_force_to_memb, cell_interaction.cpp:614-620
@@ -372,22 +515,37 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
       }
       attr[g] = a;
       pair[g] = q >= 0 ? pbase + q : -1;
+      if (q >= 0) simple = false;
       spr[g] = v.spr_nat_len ? v.spr_nat_len[i] : 0.0;
+      if (st == ST_MEMB) prep_m.push_back((int32_t)g);
+      if (st == ST_FIX || st == ST_MUSUME) prep_f.push_back((int32_t)g);
     }
     T.rmax = rmax;
+    T.rmax_nm = rmax_nm;
+    H.nfm = (int32_t)prep_f.size() - H.prep_f;
     pbase += v.n;
     binbase += T.anx * T.any * T.anz;
   }
-  const size_t C = (size_t)c->cfg.max_conn;
+  c->lc.simple = simple ? 1 : 0;
+  c->lc.any_old = any_old ? 1 : 0;
+  c->nprep_memb = (int32_t)prep_m.size();
+  c->nprep = c->nprep_memb + (int32_t)prep_f.size();
+  std::vector<int32_t> prep(prep_m);
+  prep.insert(prep.end(), prep_f.begin(), prep_f.end());
+  const size_t C = (size_t)c->cfg.max_conn, CC = (size_t)c->cfg.max_cand;
   if ((rc = dev_alloc(&c->tissues, ntissues)) || (rc = dev_alloc(&c->pos[0], n)) ||
       (rc = dev_alloc(&c->pos[1], n)) || (rc = dev_alloc(&c->attr, n)) ||
       (rc = dev_alloc(&c->pair, n)) || (rc = dev_alloc(&c->spr, n)) ||
-      (rc = dev_alloc(&c->dermis, n)) || (rc = dev_alloc(&c->nbr, C * n)) ||
-      (rc = dev_alloc(&c->nn, n)) || (rc = dev_alloc(&c->sn, n)) || (rc = dev_alloc(&c->sm, n)) ||
+      (rc = dev_alloc(&c->dermis, n)) || (rc = dev_alloc(&c->cand, CC * n)) ||
+      (rc = dev_alloc(&c->ncand, n)) || (rc = dev_alloc(&c->bpos, n)) ||
+      (rc = dev_alloc(&c->nbr, C * n)) || (rc = dev_alloc(&c->nn, n)) ||
+      (rc = dev_alloc(&c->sn, n)) || (rc = dev_alloc(&c->sm, n)) ||
+      (rc = dev_alloc(&c->fmemb, n)) ||
       (rc = dev_alloc(&c->bin, n)) || (rc = dev_alloc(&c->rank, n)) ||
       (rc = dev_alloc(&c->counts, nbins)) || (rc = dev_alloc(&c->starts, nbins + 1)) ||
       (rc = dev_alloc(&c->skey, n)) || (rc = dev_alloc(&c->spos, n)) ||
-      (rc = dev_alloc(&c->stage, 3 * (size_t)n))) {
+      (rc = dev_alloc(&c->gate, (size_t)ntissues + 1)) ||
+      (rc = dev_alloc(&c->prep, prep.size())) || (rc = dev_alloc(&c->stage, 3 * (size_t)n))) {
     free_buffers(c);
     return rc;
   }
@@ -404,14 +562,19 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
   EPI_CUDA(cudaMemcpyAsync(c->attr, attr.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s));
   EPI_CUDA(cudaMemcpyAsync(c->pair, pair.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
   EPI_CUDA(cudaMemcpyAsync(c->spr, spr.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  if (!prep.empty())
+    EPI_CUDA(cudaMemcpyAsync(c->prep, prep.data(), sizeof(int32_t) * prep.size(),
+                             cudaMemcpyHostToDevice, s));
   EPI_CUDA(cudaMemsetAsync(c->counts, 0, sizeof(int32_t) * (size_t)std::max<int64_t>(nbins, 1), s));
   EPI_CUDA(cudaMemsetAsync(c->nn, 0, sizeof(int32_t) * n, s));
+  EPI_CUDA(cudaMemsetAsync(c->ncand, 0, sizeof(int32_t) * n, s));
   EPI_CUDA(cudaMemsetAsync(c->dermis, 0xff, sizeof(int32_t) * n, s));
   EPI_CUDA(cudaMemsetAsync(c->status, 0, sizeof(DevStatus), s));
   c->cur = 0;
   c->loaded = true;
-  launch_connect(make_state(c, c->cur), whole(c), c->cfg.precision, c->scan, s, nullptr);
-  return check_status(c);
+  launch_set_gates(make_state(c, c->cur), ntissues, s);
+  // all pending host copies read std::vector storage: finish before return
+  return materialize(c);
   EPI_GUARD_END
 }
 
@@ -421,8 +584,7 @@ int epi_connect(epi_ctx* c) {
   EPI_GUARD_BEGIN
   int rc = set_device(c);
   if (rc) return rc;
-  launch_connect(make_state(c, c->cur), whole(c), c->cfg.precision, c->scan, c->stream, nullptr);
-  return check_status(c);
+  return materialize(c);
   EPI_GUARD_END
 }
 
@@ -432,8 +594,8 @@ int epi_interact_commit(epi_ctx* c) {
   EPI_GUARD_BEGIN
   int rc = set_device(c);
   if (rc) return rc;
-  launch_interact_commit(make_state(c, c->cur), whole(c), c->cfg.precision, c->stream, nullptr);
-  c->cur ^= 1;
+  enqueue_step(c, c->cur, nullptr);
+  c->lists_fresh = false;
   return check_status(c);
   EPI_GUARD_END
 }
@@ -445,6 +607,7 @@ int epi_step(epi_ctx* c, int32_t nsteps) {
   int rc = set_device(c);
   if (rc) return rc;
   for (int32_t k = 0; k < nsteps; ++k) enqueue_step(c, c->cur, nullptr);
+  if (nsteps > 0) c->lists_fresh = false;
   return check_status(c);
   EPI_GUARD_END
 }
@@ -455,7 +618,7 @@ int epi_step_graph(epi_ctx* c, int32_t nsteps) {
   EPI_GUARD_BEGIN
   int rc = set_device(c);
   if (rc) return rc;
-  int32_t pairs = nsteps / 2;
+  const int32_t pairs = nsteps / 2;
   if (pairs > 0) {
     cudaGraphExec_t& ge = c->graph[c->cur];
     if (!ge) {
@@ -472,6 +635,7 @@ int epi_step_graph(epi_ctx* c, int32_t nsteps) {
     for (int32_t k = 0; k < pairs; ++k) EPI_CUDA(cudaGraphLaunch(ge, c->stream));
   }
   if (nsteps % 2) enqueue_step(c, c->cur, nullptr);
+  if (nsteps > 0) c->lists_fresh = false;
   return check_status(c);
   EPI_GUARD_END
 }
@@ -485,11 +649,14 @@ int epi_step_per_tissue(epi_ctx* c, int32_t nsteps) {
   for (int32_t k = 0; k < nsteps; ++k) {
     for (int t = 0; t < c->ntissues; ++t) {
       const Range r = tissue_range(c, t);
-      launch_interact_commit(make_state(c, c->cur), r, c->cfg.precision, c->stream, nullptr);
-      launch_connect(make_state(c, c->cur ^ 1), r, c->cfg.precision, c->scan, c->stream, nullptr);
+      const DevState S = make_state(c, c->cur);
+      launch_rebuild(S, r, c->scan, c->lc, c->stream, nullptr);
+      prepass_tissue(c, c->cur, t);
+      launch_step(S, r, c->cfg.precision, c->lc, c->stream, nullptr);
     }
     c->cur ^= 1;
   }
+  if (nsteps > 0) c->lists_fresh = false;
   return check_status(c);
   EPI_GUARD_END
 }
@@ -536,8 +703,12 @@ int epi_upload_positions(epi_ctx* c, const double* x, const double* y, const dou
   EPI_CUDA(cudaMemcpyAsync(d, x, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
   EPI_CUDA(cudaMemcpyAsync(d + n, y, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
   EPI_CUDA(cudaMemcpyAsync(d + 2 * n, z, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
-  launch_pack_positions(make_state(c, c->cur), d, d + n, d + 2 * n, (int32_t)n, c->stream);
-  launch_connect(make_state(c, c->cur), whole(c), c->cfg.precision, c->scan, c->stream, nullptr);
+  const DevState S = make_state(c, c->cur);
+  launch_pack_positions(S, d, d + n, d + 2 * n, (int32_t)n, c->stream);
+  // positions may have jumped anywhere: every tissue re-derives its candidates
+  launch_set_gates(S, c->ntissues, c->stream);
+  c->lists_fresh = false;
+  launch_rebuild(S, whole(c), c->scan, c->lc, c->stream, nullptr);
   return check_status(c);
   EPI_GUARD_END
 }
@@ -549,6 +720,7 @@ int epi_get_connections(epi_ctx* c, int32_t* offsets, int32_t* idx, int64_t cap,
   EPI_GUARD_BEGIN
   int rc = set_device(c);
   if (rc) return rc;
+  if ((rc = materialize(c))) return rc;
   const int32_t n = (int32_t)c->n;
   int32_t *rowlen = nullptr, *rowoff = nullptr, *didx = nullptr, *partial = nullptr;
   if ((rc = dev_alloc(&rowlen, n)) || (rc = dev_alloc(&rowoff, (size_t)n + 1))) {
@@ -565,7 +737,7 @@ int epi_get_connections(epi_ctx* c, int32_t* offsets, int32_t* idx, int64_t cap,
   sc.partial = partial;
   const DevState S = make_state(c, c->cur);
   launch_rowlen(S, rowlen, n, c->stream);
-  launch_scan(rowlen, rowoff, n, 0, sc, c->stream);
+  launch_scan(rowlen, rowoff, n, 0, sc, nullptr, c->lc, c->stream);
   cudaError_t e = cudaMemcpyAsync(offsets, rowoff, sizeof(int32_t) * ((size_t)n + 1),
                                   cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
@@ -595,6 +767,7 @@ int epi_get_dermis(epi_ctx* c, int32_t* dermis) {
   EPI_GUARD_BEGIN
   int rc = set_device(c);
   if (rc) return rc;
+  if ((rc = materialize(c))) return rc;
   int32_t* d = nullptr;
   if ((rc = dev_alloc(&d, c->n))) return rc;
   launch_dermis_local(make_state(c, c->cur), d, (int32_t)c->n, c->stream);
@@ -641,6 +814,7 @@ int epi_time_kernels(epi_ctx* c, int32_t nsteps, int32_t max_classes, double* ms
   if (rc) return rc;
   Timer tm;
   for (int32_t k = 0; k < nsteps; ++k) enqueue_step(c, c->cur, &tm);
+  if (nsteps > 0) c->lists_fresh = false;
   rc = check_status(c);
   for (int k = 0; k < KC_COUNT; ++k) {
     double sum = 0;

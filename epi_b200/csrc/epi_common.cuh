@@ -8,9 +8,12 @@
 //              MUSUME membrane spring selector, bits 8-31 tissue id
 //   pair[N]    i32 global partner index or -1; spr[N] double spring rest length
 //   dermis[N]  i32 global index of the nearest connected MEMB (FIX/MUSUME)
-//   nbr[C][N]  i32 searched neighbours, column-major ("ELL") so that a warp
-//              reading entry k of 32 consecutive particles is coalesced;
-//              nn[N] their count. Membrane lattice links are implicit.
+//   cand[N][C] i32 Verlet candidates (all partners within reach + skin at
+//              the last rebuild), one row per particle so that the G lanes
+//              sharing a particle in the step kernel read consecutive
+//              entries; ncand[N]
+//   nbr[N][C]  i32 exact connection lists, materialised on request; nn[N].
+//              Membrane lattice links are implicit in both.
 //   sn/sm[N]   membrane bending scratch (unit vector + length to the right /
 //              upper lattice neighbour), the reference's Memb_data
 //              (epi5_MT/cell.h:42-69)
@@ -40,12 +43,7 @@ struct Params {
       delta_r, para_ljp2, kspring_division, lj_thresh, thresh_sp;
 };
 
-struct TissueDev {
-  int32_t pbase, n, nmemb, nder, nmx, nmy;
-  int32_t anx, any, anz, binbase;  // reference grid (cell_connection.cpp:22-26)
-  double lx, ly, lz, rmax;
-  Params P;
-};
+struct TissueDev;
 
 struct DevStatus {
   int32_t flags;  // bit per ErrCode
@@ -62,19 +60,29 @@ struct DevState {
   const int32_t* pair;
   const double* spr;
   int32_t* dermis;
-  int32_t* nbr;
+  // Verlet candidates: every partner within LJ_THRESH*(r_i+r_j) + skin at
+  // the last rebuild, column-major like nbr.
+  int32_t* cand;
+  int32_t* ncand;
+  float4* bpos;     // positions at the last rebuild (displacement check)
+  int32_t* nbr;     // exact connection lists (materialised on request)
   int32_t* nn;
   double4* sn;
   double4* sm;
+  double4* fmemb;   // membrane bending + lattice spring + wall displacement
   int32_t* bin;
   int32_t* rank;
   int32_t* counts;
   int32_t* starts;
   uint32_t* skey;   // sorted particles: global index | (is_memb << 31)
-  double4* spos;    // sorted copy of the current positions
+  double4* spos;    // sorted copy of the positions at rebuild
+  int32_t* gate;    // [0]: some tissue needs a rebuild, [1 + t]: tissue t does
+  const int32_t* prep;  // membrane particles, then FIX/MUSUME cells
+  int32_t nprep, nprep_memb;
   DevStatus* status;
-  int64_t n_total;  // ELL column stride
-  int32_t max_conn;
+  int64_t n_total;  // column stride of cand / nbr
+  int32_t max_conn, max_cand;
+  double skin;
 };
 
 __device__ __forceinline__ uint32_t attr_state(uint32_t a) { return a & 15u; }
@@ -126,13 +134,6 @@ template <typename R>
 struct Laws {
   R eps4, p_memb, der_der_const, k_total, k_desmosome, kspring, kspring_d, delta_r, para_ljp2,
       kspring_division, lj_thresh, ljt1sq;
-
-  __device__ __forceinline__ explicit Laws(const Params& P)
-      : eps4(R(4.0 * P.eps_m)), p_memb(R(P.p_memb)), der_der_const(R(P.der_der_const)),
-        k_total(R(P.k_total)), k_desmosome(R(P.k_desmosome)), kspring(R(P.kspring)),
-        kspring_d(R(P.kspring_d)), delta_r(R(P.delta_r)), para_ljp2(R(P.para_ljp2)),
-        kspring_division(R(P.kspring_division)), lj_thresh(R(P.lj_thresh)),
-        ljt1sq(R((P.lj_thresh - 1.0) * (P.lj_thresh - 1.0))) {}
 
   // ljmain, :103-111
   __device__ __forceinline__ R ljmain(R d2, R rs) const {
@@ -208,6 +209,25 @@ struct Laws {
   }
 };
 
+// Constants of the laws in arithmetic type R, precomputed once per tissue.
+template <typename R>
+__host__ __device__ inline Laws<R> make_laws(const Params& P) {
+  Laws<R> L;
+  L.eps4 = R(4.0 * P.eps_m);
+  L.p_memb = R(P.p_memb);
+  L.der_der_const = R(P.der_der_const);
+  L.k_total = R(P.k_total);
+  L.k_desmosome = R(P.k_desmosome);
+  L.kspring = R(P.kspring);
+  L.kspring_d = R(P.kspring_d);
+  L.delta_r = R(P.delta_r);
+  L.para_ljp2 = R(P.para_ljp2);
+  L.kspring_division = R(P.kspring_division);
+  L.lj_thresh = R(P.lj_thresh);
+  L.ljt1sq = R((P.lj_thresh - 1.0) * (P.lj_thresh - 1.0));
+  return L;
+}
+
 // Law selected when cell c iterates its connection o (the per-state bodies
 // of cell_interaction.cpp:549-634). Index order decides double counting
 // (no_double_count, cell.h:293-295).
@@ -260,6 +280,45 @@ __device__ __forceinline__ R eval_law(int law, const Laws<R>& L, R d2, R rs, boo
     case L_MU_MEMB: return L.mu_memb(d2, rs, sfm_value(c_sfm, L));
     default: return R(0);
   }
+}
+
+struct TissueDev {
+  int32_t pbase, n, nmemb, nder, nmx, nmy;
+  int32_t anx, any, anz, binbase;  // reference grid (cell_connection.cpp:22-26)
+  double lx, ly, lz, hlx, hly;     // box and half box
+  double rmax;     // largest radius in the tissue
+  double rmax_nm;  // largest non-membrane radius (membranes only pair with those)
+  // Range asserts of grid_init / connect_proc (cell_connection.cpp:48-53,
+  // :99) as thresholds on a wrapped position, found on the host with the
+  // same IEEE arithmetic: grid_init fails for gx_hi <= x < lx (x == lx wraps
+  // to bin 0), gy_hi likewise, z >= gz_hi; connect_proc (non-membrane cells)
+  // fails for x >= cx_hi, y >= cy_hi, z >= cz_hi or z <= cz_lo.
+  double gx_hi, gy_hi, gz_hi, cx_hi, cy_hi, cz_hi, cz_lo;
+  Params P;
+  Laws<float> lawf;
+  Laws<double> lawd;
+  template <typename R>
+  __device__ __forceinline__ const Laws<R>& laws() const;
+};
+template <>
+__device__ __forceinline__ const Laws<float>& TissueDev::laws<float>() const { return lawf; }
+template <>
+__device__ __forceinline__ const Laws<double>& TissueDev::laws<double>() const { return lawd; }
+
+// The reference's range asserts for a wrapped position (see TissueDev).
+__device__ __forceinline__ bool range_ok(const TissueDev& T, double x, double y, double z,
+                                         bool memb) {
+  bool ok = (x < T.gx_hi || x >= T.lx) && (y < T.gy_hi || y >= T.ly) && z < T.gz_hi;
+  if (!memb) ok = ok && x < T.cx_hi && y < T.cy_hi && z < T.cz_hi && z > T.cz_lo;
+  return ok;
+}
+
+// Minimum-image difference with a precomputed half box (same result as pdiff).
+__device__ __forceinline__ double pdiff_h(double a, double b, double L, double h) {
+  const double d = a - b;
+  if (d > h) return d - L;
+  if (d <= -h) return d + L;
+  return d;
 }
 
 // Square membrane lattice neighbours of membrane particle j (tissue-local),

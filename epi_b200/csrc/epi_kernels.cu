@@ -1,14 +1,24 @@
-// Mechanics kernels for sm_100a: binning, neighbour search, force + commit.
+// Mechanics kernels for sm_100a.
 //
-// One step of the reference (epi5_MT/proc.cpp:22-32 without state renewal) is
-//   k_force_commit  cell_interaction + pos_copy + cell_pos_periodic_fix
-//   k_bin           grid_init's binning (+ membrane bending scratch)
-//   scan            bin offsets (counting sort)
-//   k_scatter       particles into bin order
-//   k_binsort       deterministic order inside each bin, sorted position copy
-//   k_search        connect_proc's neighbour search + find_dermis
-// Every kernel covers a particle range and a bin range, so the same code runs
-// a whole batch of tissues per launch or one tissue per launch.
+// One step of the reference (epi5_MT/proc.cpp:22-32 without state renewal)
+// runs as
+//   [rebuild]  Verlet candidate rebuild of the tissues that need one
+//              (bin -> scan -> scatter -> per-bin sort -> candidate search);
+//              every kernel of it exits at once when no tissue does
+//   k_prepass  membrane bending scratch (_memb_bend_calc1) and the dermis of
+//              FIX / MUSUME cells (find_dermis)
+//   k_step     connect_proc's exact predicate over the candidates, every
+//              force of cell_interaction, pos_copy and the periodic wrap,
+//              fused; flags tissues whose particles moved more than skin/2
+//              since their last rebuild
+//
+// The reference rebuilds its connection lists from scratch every step
+// (connect_cell, cell_connection.cpp:191-203). Here a tissue's candidate list
+// holds every partner within LJ_THRESH*(r_i+r_j) + skin at the last rebuild;
+// while no particle has moved more than skin/2 since, every pair that can
+// satisfy the reference's predicate is a candidate, and k_step evaluates that
+// predicate exactly (same rounding as the reference) on the current
+// positions. The connection set of every step is therefore the reference's.
 //
 // Forces are gathered, not scattered: each particle sums every interaction it
 // takes part in (the reference adds +d to c1 and -d to c2 with CAS atomics,
@@ -16,18 +26,23 @@
 // deterministic and repeatable bit for bit.
 #include "epi_kernels.h"
 
-#include <cstdio>
-
 namespace epi {
 
-const char* const kKernelClassNames[KC_COUNT] = {"force_commit", "bin", "scan",
-                                                  "scatter", "binsort", "search"};
+const char* const kKernelClassNames[KC_COUNT] = {
+    "step", "prepass", "rebuild_bin", "rebuild_scan", "rebuild_sort", "rebuild_search", "gate"};
 
 namespace {
 
-constexpr int kBlock = 256;
+inline int blocks_for(int64_t n, int b) { return (int)((n + b - 1) / b); }
+inline int stride_blocks(int64_t n, int b, const LaunchCfg& lc) {
+  const int need = blocks_for(n, b);
+  const int cap = lc.num_sms * 8;
+  return need < cap ? (need > 0 ? need : 1) : cap;
+}
 
-inline int blocks_for(int64_t n, int b = kBlock) { return (int)((n + b - 1) / b); }
+#define GRID_STRIDE(i, lo, hi) \
+  for (int64_t i = (lo) + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (hi); \
+       i += (int64_t)gridDim.x * blockDim.x)
 
 // ---------------------------------------------------------------------------
 // Scan (reduce -> top-level scan -> down-sweep). No inter-block waiting.
@@ -65,8 +80,11 @@ __device__ __forceinline__ int32_t block_excl_scan(int32_t v, int32_t* total) {
   return before + incl - v;
 }
 
+__device__ __forceinline__ bool closed(const int32_t* gate) { return gate && *gate == 0; }
+
 __global__ void k_scan_partial(const int32_t* __restrict__ in, int32_t n,
-                               int32_t* __restrict__ partial) {
+                               int32_t* __restrict__ partial, const int32_t* gate) {
+  if (closed(gate)) return;
   const int64_t base = (int64_t)blockIdx.x * kScanTile + threadIdx.x * kScanItems;
   int32_t s = 0;
 #pragma unroll
@@ -77,9 +95,13 @@ __global__ void k_scan_partial(const int32_t* __restrict__ in, int32_t n,
   if (threadIdx.x == 0) partial[blockIdx.x] = tot;
 }
 
-__global__ void k_set1(int32_t* out, int32_t v) { *out = v; }
+__global__ void k_set1(int32_t* out, int32_t v, const int32_t* gate) {
+  if (closed(gate)) return;
+  *out = v;
+}
 
-__global__ void k_scan_top(int32_t* partial, int32_t nb) {
+__global__ void k_scan_top(int32_t* partial, int32_t nb, const int32_t* gate) {
+  if (closed(gate)) return;
   int32_t carry = 0;
   for (int32_t base = 0; base < nb; base += kScanThreads) {
     const int32_t i = base + threadIdx.x;
@@ -92,7 +114,9 @@ __global__ void k_scan_top(int32_t* partial, int32_t nb) {
 }
 
 __global__ void k_scan_final(const int32_t* __restrict__ in, int32_t* __restrict__ out,
-                             int32_t n, const int32_t* __restrict__ partial, int32_t init) {
+                             int32_t n, const int32_t* __restrict__ partial, int32_t init,
+                             const int32_t* gate) {
+  if (closed(gate)) return;
   const int64_t base = (int64_t)blockIdx.x * kScanTile + threadIdx.x * kScanItems;
   int32_t v[kScanItems];
   int32_t s = 0;
@@ -112,85 +136,89 @@ __global__ void k_scan_final(const int32_t* __restrict__ in, int32_t* __restrict
 }
 
 // ---------------------------------------------------------------------------
-// Binning: grid_init (cell_connection.cpp:38-62) plus the range assert of
-// connect_proc (:95-99). Membrane particles also compute their bending
-// scratch, _memb_bend_calc1 (cell_interaction.cpp:296-324).
+// Reference grid checks: grid_init's bin (cell_connection.cpp:44-53) and the
+// range assert of connect_proc (:95-99). Returns the tissue-local bin or -1.
 // ---------------------------------------------------------------------------
-template <typename R>
-__global__ void k_bin(DevState S, Range r) {
-  const int32_t i = r.p0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= r.p1) return;
-  const uint32_t a = S.attr[i];
-  const TissueDev& T = S.tissues[attr_tissue(a)];
-  const double4 p = S.pos_cur[i];
-  const uint32_t st = attr_state(a);
-  if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z)) {
-    raise_error(S.status, E_NONFINITE, i, -1, p.x);
-    S.bin[i] = -1;
-    return;
-  }
-  const int32_t aix = (int32_t)((0.5 * T.lx - pdiff(0.5 * T.lx, p.x, T.lx)) / kAreaGrid);
-  const int32_t aiy = (int32_t)((0.5 * T.ly - pdiff(0.5 * T.ly, p.y, T.ly)) / kAreaGrid);
-  const int32_t aiz = (int32_t)(fmax(p.z, 0.0) / kAreaGrid);  // min0, utils.h:55-57
+__device__ __forceinline__ int32_t ref_bin(const TissueDev& T, double x, double y, double z,
+                                           bool memb) {
+  const int32_t aix = (int32_t)((0.5 * T.lx - pdiff(0.5 * T.lx, x, T.lx)) / kAreaGrid);
+  const int32_t aiy = (int32_t)((0.5 * T.ly - pdiff(0.5 * T.ly, y, T.ly)) / kAreaGrid);
+  const int32_t aiz = (int32_t)(fmax(z, 0.0) / kAreaGrid);  // min0, utils.h:55-57
   bool bad = aix >= T.anx || aiy >= T.any || aiz >= T.anz || aix < 0 || aiy < 0 || aiz < 0;
-  if (st != ST_MEMB) {
-    const int32_t cx = (int32_t)(p.x / kAreaGrid), cy = (int32_t)(p.y / kAreaGrid),
-                  cz = (int32_t)(p.z / kAreaGrid);
+  if (!memb) {
+    const int32_t cx = (int32_t)(x / kAreaGrid), cy = (int32_t)(y / kAreaGrid),
+                  cz = (int32_t)(z / kAreaGrid);
     bad |= cx >= T.anx || cy >= T.any || cz >= T.anz || cx < 0 || cy < 0 || cz < 0;
   }
-  if (bad) {
-    raise_error(S.status, E_BIN_RANGE, i, -1, p.z);
-    S.bin[i] = -1;
-    return;
-  }
-  const int32_t b = T.binbase + (aix * T.any + aiy) * T.anz + aiz;
-  const int32_t rk = atomicAdd(&S.counts[b], 1);
-  if (rk + 1 >= kBinCap) raise_error(S.status, E_BIN_OVERFLOW, i, b, (double)(rk + 1));
-  S.bin[i] = b;
-  S.rank[i] = rk;
-  if (st == ST_MEMB) {
-    const int32_t j = i - T.pbase;
-    const Lattice L = lattice_of(j, T.nmx, T.nmy);
-    const double4 pr = S.pos_cur[T.pbase + L.r];
-    const double4 pu = S.pos_cur[T.pbase + L.u];
-    const R nx = R(pdiff(pr.x, p.x, T.lx)), ny = R(pdiff(pr.y, p.y, T.ly)), nz = R(pr.z - p.z);
-    const R dn = sqrt(nx * nx + ny * ny + nz * nz);
-    S.sn[i] = make_double4(nx / dn, ny / dn, nz / dn, dn);
-    const R mx = R(pdiff(pu.x, p.x, T.lx)), my = R(pdiff(pu.y, p.y, T.ly)), mz = R(pu.z - p.z);
-    const R dm = sqrt(mx * mx + my * my + mz * mz);
-    S.sm[i] = make_double4(mx / dm, my / dm, mz / dm, dm);
+  return bad ? -1 : (aix * T.any + aiy) * T.anz + aiz;
+}
+
+// ---------------------------------------------------------------------------
+// Rebuild: binning on the reference's 2.0 grid of every particle of a gated
+// tissue.
+// ---------------------------------------------------------------------------
+__global__ void k_bin(DevState S, Range r) {
+  if (S.gate[0] == 0) return;
+  GRID_STRIDE(i, r.p0, r.p1) {
+    const uint32_t a = S.attr[i];
+    const uint32_t t = attr_tissue(a);
+    if (S.gate[1 + t] == 0) continue;
+    const TissueDev& T = S.tissues[t];
+    const double4 p = S.pos_cur[i];
+    if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z)) {
+      raise_error(S.status, E_NONFINITE, (int32_t)i, -1, p.x);
+      S.bin[i] = -1;
+      continue;
+    }
+    const int32_t lb = ref_bin(T, p.x, p.y, p.z, attr_state(a) == ST_MEMB);
+    if (lb < 0) {
+      raise_error(S.status, E_BIN_RANGE, (int32_t)i, -1, p.z);
+      S.bin[i] = -1;
+      continue;
+    }
+    const int32_t b = T.binbase + lb;
+    const int32_t rk = atomicAdd(&S.counts[b], 1);
+    if (rk + 1 >= kBinCap) raise_error(S.status, E_BIN_OVERFLOW, (int32_t)i, b, (double)(rk + 1));
+    S.bin[i] = b;
+    S.rank[i] = rk;
   }
 }
 
 __global__ void k_scatter(DevState S, Range r) {
-  const int32_t i = r.p0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= r.p1) return;
-  const int32_t b = S.bin[i];
-  if (b < 0) return;
-  S.skey[S.starts[b] + S.rank[i]] = (uint32_t)i;
+  if (S.gate[0] == 0) return;
+  GRID_STRIDE(i, r.p0, r.p1) {
+    const uint32_t t = attr_tissue(S.attr[i]);
+    if (S.gate[1 + t] == 0) continue;
+    const int32_t b = S.bin[i];
+    if (b < 0) continue;
+    S.skey[S.starts[b] + S.rank[i]] = (uint32_t)i;
+  }
 }
 
 // Per-bin insertion sort by particle index (bins hold a few to a few dozen
 // particles), then the sorted position copy the search streams through.
+// Bins of tissues that are not rebuilt are empty.
 __global__ void k_binsort(DevState S, Range r) {
-  const int32_t b = r.b0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= r.b1) return;
-  const int32_t s0 = S.starts[b], s1 = S.starts[b + 1];
-  S.counts[b] = 0;  // ready for the next binning
-  for (int32_t s = s0 + 1; s < s1; ++s) {
-    const uint32_t v = S.skey[s];
-    int32_t k = s - 1;
-    while (k >= s0 && S.skey[k] > v) {
-      S.skey[k + 1] = S.skey[k];
-      --k;
+  if (S.gate[0] == 0) return;
+  GRID_STRIDE(b, r.b0, r.b1) {
+    const int32_t s0 = S.starts[b], s1 = S.starts[b + 1];
+    if (s1 <= s0) continue;
+    S.counts[b] = 0;  // ready for the next binning
+    for (int32_t s = s0 + 1; s < s1; ++s) {
+      const uint32_t v = S.skey[s];
+      int32_t k = s - 1;
+      while (k >= s0 && S.skey[k] > v) {
+        S.skey[k + 1] = S.skey[k];
+        --k;
+      }
+      S.skey[k + 1] = v;
     }
-    S.skey[k + 1] = v;
-  }
-  for (int32_t s = s0; s < s1; ++s) {
-    const uint32_t g = S.skey[s];
-    const bool memb = attr_state(S.attr[g]) == ST_MEMB;
-    S.skey[s] = g | (memb ? 0x80000000u : 0u);
-    S.spos[s] = S.pos_cur[g];
+    for (int32_t s = s0; s < s1; ++s) {
+      const uint32_t g = S.skey[s];
+      const bool memb = attr_state(S.attr[g]) == ST_MEMB;
+      S.skey[s] = g | (memb ? 0x80000000u : 0u);
+      S.spos[s] = S.pos_cur[g];
+    }
   }
 }
 
@@ -226,77 +254,126 @@ __device__ __forceinline__ int window_ranges(double x, double R, double L, int32
   return 1;
 }
 
-// ---------------------------------------------------------------------------
-// Neighbour search, connect_proc (cell_connection.cpp:70-129) + find_dermis
-// (:158-172). Every particle collects all partners within
-// LJ_THRESH*(r_i+r_j), except membrane-membrane pairs, which the reference
-// never searches (only non-membrane cells iterate, and their partners include
-// membranes). The predicate is symmetric and evaluated with the reference's
-// exact rounding, so the sets equal the reference's two-sided pushes. The
-// window covers every bin that can hold a partner within reach (radius bound
-// rmax of the tissue); the reference's fixed 5x5x5 window is a superset for
-// every reachable pair (reach <= 1.2 * 2.8 < 2 * AREA_GRID).
-// ---------------------------------------------------------------------------
-__global__ void k_search(DevState S, Range r) {
-  const int32_t i = r.p0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= r.p1) return;
-  const uint32_t a = S.attr[i];
-  const TissueDev& T = S.tissues[attr_tissue(a)];
-  const uint32_t st = attr_state(a);
-  const bool memb_i = st == ST_MEMB;
-  const bool wants_dermis = st == ST_FIX || st == ST_MUSUME;
-  const double4 p = S.pos_cur[i];
-  const double lt = T.P.lj_thresh;
-  const double R = lt * (p.w + T.rmax) + 1e-6;
-  int32_t xlo[2], xhi[2], ylo[2], yhi[2];
-  const int nxr = window_ranges(p.x, R, T.lx, T.anx, xlo, xhi);
-  const int nyr = window_ranges(p.y, R, T.ly, T.any, ylo, yhi);
-  int32_t z0 = (int32_t)floor((p.z - R) / kAreaGrid);
-  int32_t z1 = (int32_t)floor((p.z + R) / kAreaGrid);
-  z0 = z0 < 0 ? 0 : (z0 > T.anz - 1 ? T.anz - 1 : z0);
-  z1 = z1 < 0 ? 0 : (z1 > T.anz - 1 ? T.anz - 1 : z1);
-  const int64_t N = S.n_total;
-  const int32_t cap = S.max_conn;
-  int32_t count = 0;
-  int32_t best = -1;
-  double bestd = T.lx * T.lx;  // find_dermis starts from LX*LX
-  for (int xr = 0; xr < nxr; ++xr) {
-    for (int32_t bx = xlo[xr]; bx <= xhi[xr]; ++bx) {
-      for (int yr = 0; yr < nyr; ++yr) {
-        for (int32_t by = ylo[yr]; by <= yhi[yr]; ++by) {
-          const int32_t col = T.binbase + (bx * T.any + by) * T.anz;
-          const int32_t s_lo = S.starts[col + z0], s_hi = S.starts[col + z1 + 1];
-          for (int32_t s = s_lo; s < s_hi; ++s) {
-            const uint32_t key = S.skey[s];
-            const int32_t j = (int32_t)(key & 0x7fffffffu);
-            if (j == i || (memb_i && (key >> 31))) continue;
-            const double4 q = S.spos[s];
-            const double dx = pdiff(p.x, q.x, T.lx);
-            const double dy = pdiff(p.y, q.y, T.ly);
-            const double dz = p.z - q.z;
-            const double d2 = dist_sq_exact(dx, dy, dz);
-            if (!connected_pred(d2, lt, p.w, q.w)) continue;
-            if (count < cap) S.nbr[(int64_t)count * N + i] = j;
-            ++count;
-            if (wants_dermis && (key >> 31) && (d2 < bestd || (d2 == bestd && j < best))) {
-              bestd = d2;
-              best = j;
+// Candidate search of a gated tissue: every partner within
+// LJ_THRESH*(r_i+r_j) + skin (membrane pairs excluded: connect_proc only
+// iterates non-membrane cells, cell_connection.cpp:93). The window covers
+// every bin that can hold such a partner; the reference's fixed 5x5x5 window
+// is a superset for every pair it can connect (reach <= 1.2 * 3.2 < 2 * 2.0).
+// Candidates come out in bin order, deterministic after k_binsort.
+__global__ void k_cand_search(DevState S, Range r) {
+  if (S.gate[0] == 0) return;
+  GRID_STRIDE(i, r.p0, r.p1) {
+    const uint32_t a = S.attr[i];
+    const uint32_t t = attr_tissue(a);
+    if (S.gate[1 + t] == 0) continue;
+    const TissueDev& T = S.tissues[t];
+    const bool memb_i = attr_state(a) == ST_MEMB;
+    const double4 p = S.pos_cur[i];
+    const double lt = T.P.lj_thresh;
+    const double skin = S.skin;
+    const double R = lt * (p.w + (memb_i ? T.rmax_nm : T.rmax)) + skin + 1e-6;
+    int32_t xlo[2], xhi[2], ylo[2], yhi[2];
+    const int nxr = window_ranges(p.x, R, T.lx, T.anx, xlo, xhi);
+    const int nyr = window_ranges(p.y, R, T.ly, T.any, ylo, yhi);
+    int32_t z0 = (int32_t)floor((p.z - R) / kAreaGrid);
+    int32_t z1 = (int32_t)floor((p.z + R) / kAreaGrid);
+    z0 = z0 < 0 ? 0 : (z0 > T.anz - 1 ? T.anz - 1 : z0);
+    z1 = z1 < 0 ? 0 : (z1 > T.anz - 1 ? T.anz - 1 : z1);
+    const int32_t cap = S.max_cand;
+    int32_t count = 0;
+    for (int xr = 0; xr < nxr; ++xr) {
+      for (int32_t bx = xlo[xr]; bx <= xhi[xr]; ++bx) {
+        for (int yr = 0; yr < nyr; ++yr) {
+          for (int32_t by = ylo[yr]; by <= yhi[yr]; ++by) {
+            const int32_t col = T.binbase + (bx * T.any + by) * T.anz;
+            const int32_t s_lo = S.starts[col + z0], s_hi = S.starts[col + z1 + 1];
+            for (int32_t s = s_lo; s < s_hi; ++s) {
+              const uint32_t key = S.skey[s];
+              const int32_t j = (int32_t)(key & 0x7fffffffu);
+              if (j == i || (memb_i && (key >> 31))) continue;
+              const double4 q = S.spos[s];
+              const double dx = pdiff(p.x, q.x, T.lx);
+              const double dy = pdiff(p.y, q.y, T.ly);
+              const double dz = p.z - q.z;
+              const double reach = lt * (p.w + q.w) + skin;
+              if (dx * dx + dy * dy + dz * dz > reach * reach * (1.0 + 1e-12)) continue;
+              if (count < cap) S.cand[(int64_t)count * S.n_total + i] = j;
+              ++count;
             }
           }
         }
       }
     }
+    if (count > cap) raise_error(S.status, E_LIST_OVERFLOW, (int32_t)i, -1, (double)count);
+    S.ncand[i] = count < cap ? count : cap;
+    S.bpos[i] = make_float4((float)p.x, (float)p.y, (float)p.z, 0.f);
   }
-  if (count > cap) raise_error(S.status, E_LIST_OVERFLOW, i, -1, (double)count);
-  S.nn[i] = count < cap ? count : cap;
-  S.dermis[i] = wants_dermis ? best : -1;
+}
+
+__global__ void k_gate_clear(DevState S, Range r, int32_t clear_any) {
+  GRID_STRIDE(t, r.t0, r.t1) S.gate[1 + t] = 0;
+  if (clear_any && blockIdx.x == 0 && threadIdx.x == 0) S.gate[0] = 0;
+}
+
+__global__ void k_gate_set_all(DevState S, int32_t ntissues) {
+  GRID_STRIDE(t, 0, ntissues) S.gate[1 + t] = 1;
+  if (blockIdx.x == 0 && threadIdx.x == 0) S.gate[0] = 1;
 }
 
 // ---------------------------------------------------------------------------
-// Force + commit: cell_interaction (cell_interaction.cpp:648-685) gathered per
-// particle, then pos_copy (cellmanager.cpp:19-26) and the single periodic
-// wrap of cell_pos_periodic_fix (:395-414). R is the arithmetic type of the
-// force laws (double: FP64 path; float: mixed path). Sums stay in double.
+// Prepass: _memb_bend_calc1 (cell_interaction.cpp:296-324) for every
+// membrane particle, find_dermis (cell_connection.cpp:158-172) for every
+// FIX / MUSUME cell, from the current positions. prep holds the membrane
+// particles of all tissues, then the FIX / MUSUME cells; [m0, m1) and
+// [f0, f1) select the entries of this launch.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void k_prepass(DevState S, int32_t m0, int32_t m1, int32_t f0, int32_t f1) {
+  const int64_t nm = m1 - m0;
+  GRID_STRIDE(e, 0, nm + (f1 - f0)) {
+    const int32_t i = e < nm ? S.prep[m0 + e] : S.prep[f0 + (e - nm)];
+    const uint32_t a = S.attr[i];
+    const TissueDev& T = S.tissues[attr_tissue(a)];
+    const double4 p = S.pos_cur[i];
+    if (e < nm) {
+      const Lattice L = lattice_of(i - T.pbase, T.nmx, T.nmy);
+      const double4 pr = S.pos_cur[T.pbase + L.r];
+      const double4 pu = S.pos_cur[T.pbase + L.u];
+      const R nx = R(pdiff(pr.x, p.x, T.lx)), ny = R(pdiff(pr.y, p.y, T.ly)), nz = R(pr.z - p.z);
+      const R dn = sqrt(nx * nx + ny * ny + nz * nz);
+      S.sn[i] = make_double4(nx / dn, ny / dn, nz / dn, dn);
+      const R mx = R(pdiff(pu.x, p.x, T.lx)), my = R(pdiff(pu.y, p.y, T.ly)), mz = R(pu.z - p.z);
+      const R dm = sqrt(mx * mx + my * my + mz * mz);
+      S.sm[i] = make_double4(mx / dm, my / dm, mz / dm, dm);
+    } else {
+      const int32_t nc = S.ncand[i];
+      const double lt = T.P.lj_thresh;
+      int32_t best = -1;
+      double bestd = T.lx * T.lx;  // find_dermis starts from LX*LX
+      for (int32_t k = 0; k < nc; ++k) {
+        const int32_t q = S.cand[(int64_t)k * S.n_total + i];
+        if (attr_state(S.attr[q]) != ST_MEMB) continue;
+        const double4 pq = S.pos_cur[q];
+        const double d2 =
+            dist_sq_exact(pdiff(p.x, pq.x, T.lx), pdiff(p.y, pq.y, T.ly), p.z - pq.z);
+        if (!connected_pred(d2, lt, p.w, pq.w)) continue;
+        // strict <, as the reference; on exact ties the lowest index wins
+        if (d2 < bestd || (d2 == bestd && q < best)) {
+          bestd = d2;
+          best = q;
+        }
+      }
+      S.dermis[i] = best;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Step: cell_interaction (cell_interaction.cpp:648-685) gathered per
+// particle, pos_copy (cellmanager.cpp:19-26), the single periodic wrap of
+// cell_pos_periodic_fix (:395-414), and the range checks the next
+// connect_cell would make. R is the arithmetic type of the force laws
+// (double: FP64 path; float: mixed path). Sums and positions stay double.
 // ---------------------------------------------------------------------------
 template <typename R>
 __device__ __forceinline__ R dot3(const double4& a, const double4& b) {
@@ -314,23 +391,37 @@ __device__ __forceinline__ R comp(const double4& v, int k) {
   return R(k == 0 ? v.x : (k == 1 ? v.y : v.z));
 }
 
-template <typename R>
-__global__ void k_force_commit(DevState S, Range r) {
-  const int32_t i = r.p0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= r.p1) return;
-  const uint32_t a = S.attr[i];
-  const TissueDev& T = S.tissues[attr_tissue(a)];
-  const Laws<R> L(T.P);
-  const uint32_t st = attr_state(a);
-  const double4 p = S.pos_cur[i];
-  const double dt = T.P.dt;
-  double ax = 0.0, ay = 0.0, az = 0.0;
+// Separation of a pair as cell_interaction_apply computes it for its c1
+// (:56-58), seen from particle i: the reference adds +d to c1, -d to c2.
+__device__ __forceinline__ void pair_sep(const double4& p, const double4& pq, bool i_is_c1,
+                                         const TissueDev& T, double& dx, double& dy, double& dz) {
+  if (i_is_c1) {
+    dx = pdiff(p.x, pq.x, T.lx);
+    dy = pdiff(p.y, pq.y, T.ly);
+    dz = p.z - pq.z;
+  } else {
+    dx = -pdiff(pq.x, p.x, T.lx);
+    dy = -pdiff(pq.y, p.y, T.ly);
+    dz = -(pq.z - p.z);
+  }
+}
 
-  if (st == ST_MEMB) {
-    const int32_t j = i - T.pbase;
-    const Lattice Lt = lattice_of(j, T.nmx, T.nmy);
+// Membrane particles: bending (_memb_bend_calc2 + _memb_bend_calc3,
+// :326-449, from calc1's scratch), the four lattice springs of
+// _MEMB_interaction (:529-547, each applied once by the higher index) and
+// the wall (:287-294). The sum goes to S.fmemb; k_step adds it.
+template <typename R>
+__global__ void k_memb_force(DevState S, int32_t m0, int32_t m1) {
+  GRID_STRIDE(e, m0, m1) {
+    const int32_t i = S.prep[e];
+    const uint32_t a = S.attr[i];
+    const TissueDev& T = S.tissues[attr_tissue(a)];
+    const Laws<R>& L = T.laws<R>();
+    const double4 p = S.pos_cur[i];
+    const double dt = T.P.dt;
     const int32_t pb = T.pbase;
-    // _memb_bend_calc2 + _memb_bend_calc3 (:326-449) from calc1's scratch.
+    const Lattice Lt = lattice_of(i - pb, T.nmx, T.nmy);
+    double ax = 0.0, ay = 0.0, az = 0.0;
     {
       const double4 nv = S.sn[i], nvr = S.sn[pb + Lt.r], nvl = S.sn[pb + Lt.l];
       const double4 nvll = S.sn[pb + Lt.ll], nvbb = S.sn[pb + Lt.bb];
@@ -343,26 +434,24 @@ __global__ void k_force_commit(DevState S, Range r) {
       const R dn = R(nv.w), dnl = R(nvl.w), dm = R(mv.w), dmb = R(mvb.w);
       const R fn = bend_factor(ipn), fnl = bend_factor(ipnl), fnll = bend_factor(ipnll);
       const R fm = bend_factor(ipm), fmb = bend_factor(ipmb), fmbb = bend_factor(ipmbb);
-      R f[3];
+      const R s = R(dt * T.P.kbend);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         const R n0 = comp<R>(nv, k), nr = comp<R>(nvr, k), nl = comp<R>(nvl, k),
                 nll = comp<R>(nvll, k);
         const R m0 = comp<R>(mv, k), mu = comp<R>(mvu, k), mb = comp<R>(mvb, k),
                 mbb = comp<R>(mvbb, k);
-        f[k] = -fn * (nr - ipn * n0) / dn +
-               fnl * ((n0 - ipnl * nl) / dnl - (nl - ipnl * n0) / dn) +
-               fnll * (nll - ipnll * nl) / dnl - fm * (mu - ipm * m0) / dm +
-               fmb * ((m0 - ipmb * mb) / dmb - (mb - ipmb * m0) / dm) +
-               fmbb * (mbb - ipmbb * mb) / dmb;
+        const R f = -fn * (nr - ipn * n0) / dn +
+                    fnl * ((n0 - ipnl * nl) / dnl - (nl - ipnl * n0) / dn) +
+                    fnll * (nll - ipnll * nl) / dnl - fm * (mu - ipm * m0) / dm +
+                    fmb * ((m0 - ipmb * mb) / dmb - (mb - ipmb * m0) / dm) +
+                    fmbb * (mbb - ipmbb * mb) / dmb;
+        const double d = double(s * f);
+        if (k == 0) ax += d;
+        else if (k == 1) ay += d;
+        else az += d;
       }
-      const R s = R(dt * T.P.kbend);
-      ax += double(s * f[0]);
-      ay += double(s * f[1]);
-      az += double(s * f[2]);
     }
-    // _MEMB_interaction (:529-547): the four lattice links, each applied once
-    // by the higher index.
     const int32_t links[4] = {Lt.l, Lt.r, Lt.b, Lt.u};
 #pragma unroll
     for (int k = 0; k < kMembAdj; ++k) {
@@ -370,108 +459,188 @@ __global__ void k_force_commit(DevState S, Range r) {
       const double4 pq = S.pos_cur[q];
       const bool hi = i > q;
       double dx, dy, dz;
-      if (hi) {
-        dx = pdiff(p.x, pq.x, T.lx); dy = pdiff(p.y, pq.y, T.ly); dz = p.z - pq.z;
-      } else {
-        dx = -pdiff(pq.x, p.x, T.lx); dy = -pdiff(pq.y, p.y, T.ly); dz = -(pq.z - p.z);
-      }
-      const R rdx = R(dx), rdy = R(dy), rdz = R(dz);
-      const R d2 = rdx * rdx + rdy * rdy + rdz * rdz;
+      pair_sep(p, pq, hi, T, dx, dy, dz);
+      const R d2 = R(dist_sq_exact(dx, dy, dz));
       bool bad;
       const R c = L.memb_memb(d2, R(p.w + pq.w), &bad);
       if (bad) raise_error(S.status, E_MEMB_COEF_RANGE, hi ? i : q, hi ? q : i, double(c));
       const R sdt = R(dt) * c;
-      ax += double(sdt * rdx);
-      ay += double(sdt * rdy);
-      az += double(sdt * rdz);
+      ax += double(sdt * R(dx));
+      ay += double(sdt * R(dy));
+      az += double(sdt * R(dz));
     }
+    if (p.z < p.w) {
+      const R z = R(p.z), rad = R(p.w);
+      const R distlj = R(2) * z;
+      const R lj6 = pow6(rad) / pow6(z);
+      const R ljm = L.eps4 * lj6 * (lj6 - R(1)) / (distlj * distlj);
+      az += double(R(dt) * ljm * R(2) * z);
+    }
+    S.fmemb[i] = make_double4(ax, ay, az, 0.0);
   }
-  // wall_interaction (:287-294) for MEMB and DER below their radius
-  if ((st == ST_MEMB || st == ST_DER) && p.z < p.w) {
-    const R z = R(p.z), rad = R(p.w);
-    const R distlj = R(2) * z;
-    const R lj6 = pow6(rad) / pow6(z);
-    const R ljm = L.eps4 * lj6 * (lj6 - R(1)) / (distlj * distlj);
-    az += double(R(dt) * ljm * R(2) * z);
+}
+
+// The step proper, one thread per particle. kSimple: every cell of the batch
+// is ALIVE, DEAD or AIR (or a membrane particle) and none is paired; then
+// each connected pair receives exactly one application of
+// CI_al_air_de_to_al_air_de_fix_mu (:141-152): from the higher index when
+// both cells are ALIVE/DEAD/AIR (:566-570), from the cell's side when the
+// partner is a membrane particle (:573-575). kOld: some cell is older than
+// THRESH_SP, so the adhesion constant depends on both cells' ages.
+template <typename R, bool kSimple, bool kOld>
+__global__ void __launch_bounds__(256) k_step(DevState S, Range r) {
+  const int64_t i = r.p0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= r.p1) return;
+  const int64_t N = S.n_total;
+  const uint32_t a = __ldg(&S.attr[i]);
+  const uint32_t t = attr_tissue(a);
+  const TissueDev& T = S.tissues[t];
+  const Laws<R>& L = T.laws<R>();
+  const uint32_t st = attr_state(a);
+  const double4 p = S.pos_cur[i];
+  const double lx = T.lx, ly = T.ly, hlx = T.hlx, hly = T.hly;
+  const double lt2 = T.P.lj_thresh * T.P.lj_thresh;  // LJ_THRESH*LJ_THRESH, folded as the reference
+  const R dt = R(T.P.dt);
+  int32_t pair_i = -1, dermis_i = -1;
+  if (!kSimple && st != ST_MEMB) {
+    pair_i = __ldg(&S.pair[i]);
+    if (st == ST_FIX || st == ST_MUSUME) dermis_i = __ldg(&S.dermis[i]);
+  }
+  const bool old_i = attr_old(a);
+  double ax = 0.0, ay = 0.0, az = 0.0;
+
+  // Candidates: connect_proc's exact predicate (cell_connection.cpp:115-119),
+  // then the law(s) the reference applies to the pair.
+  const int32_t nc = __ldg(&S.ncand[i]);
+  for (int32_t k = 0; k < nc; ++k) {
+    const int32_t q = __ldg(&S.cand[(int64_t)k * N + i]);
+    const double4 pq = S.pos_cur[q];
+    const double dx = pdiff_h(p.x, pq.x, lx, hlx), dy = pdiff_h(p.y, pq.y, ly, hly);
+    const double dz = p.z - pq.z;
+    const double d2e = dist_sq_exact(dx, dy, dz);
+    const double rse = __dadd_rn(p.w, pq.w);
+    if (!(d2e <= __dmul_rn(__dmul_rn(lt2, rse), rse))) continue;
+    const R d2 = R(d2e);
+    const R rs = R(rse);
+    R coef;
+    if (kSimple) {
+      const bool both_old = kOld && old_i && attr_old(__ldg(&S.attr[q]));
+      coef = L.aad(d2, rs, both_old);
+      if (fabs(coef) > R(1000)) raise_error(S.status, E_COEF_RANGE, (int32_t)i, q, double(coef));
+    } else {
+      const uint32_t aq = __ldg(&S.attr[q]);
+      const uint32_t sq = attr_state(aq);
+      const bool both_old = old_i && attr_old(aq);
+      coef = R(0);
+      // the law i applies while iterating q (if i is not a membrane particle)
+      if (st != ST_MEMB) {
+        const int law = law_of(st, (int32_t)i, pair_i, dermis_i, sq, q);
+        if (law != L_NONE) {
+          const R c = eval_law<R>(law, L, d2, rs, both_old, attr_sfm(a));
+          if (fabs(c) > R(1000)) raise_error(S.status, E_COEF_RANGE, (int32_t)i, q, double(c));
+          coef += c;
+        }
+      }
+      // ... and the law q applies while iterating i (if q is not)
+      if (sq != ST_MEMB) {
+        int32_t pair_q = -1, dermis_q = -1;
+        if (sq == ST_FIX || sq == ST_MUSUME) {
+          pair_q = __ldg(&S.pair[q]);
+          dermis_q = __ldg(&S.dermis[q]);
+        }
+        const int law = law_of(sq, q, pair_q, dermis_q, st, (int32_t)i);
+        if (law != L_NONE) {
+          const R c = eval_law<R>(law, L, d2, rs, both_old, attr_sfm(aq));
+          if (fabs(c) > R(1000)) raise_error(S.status, E_COEF_RANGE, q, (int32_t)i, double(c));
+          coef += c;
+        }
+      }
+    }
+    const R sdt = dt * coef;
+    ax += double(sdt * R(dx));
+    ay += double(sdt * R(dy));
+    az += double(sdt * R(dz));
   }
 
-  int32_t pair_i = -1, dermis_i = -1;
-  if (st != ST_MEMB) {
-    pair_i = S.pair[i];
-    if (st == ST_FIX || st == ST_MUSUME) dermis_i = S.dermis[i];
-    // _pair_interaction (:637-641), from whichever side has the higher index
+  if (st == ST_MEMB) {
+    const double4 f = S.fmemb[i];
+    ax += f.x;
+    ay += f.y;
+    az += f.z;
+  } else if (!kSimple) {
+    // wall_interaction (:287-294) for DER below its radius
+    if (st == ST_DER && p.z < p.w) {
+      const R z = R(p.z), rad = R(p.w);
+      const R distlj = R(2) * z;
+      const R lj6 = pow6(rad) / pow6(z);
+      const R ljm = L.eps4 * lj6 * (lj6 - R(1)) / (distlj * distlj);
+      az += double(dt * ljm * R(2) * z);
+    }
+    // _pair_interaction (:637-641), applied by the higher index of the pair
     if (pair_i >= 0) {
       const double4 pq = S.pos_cur[pair_i];
       const bool hi = i > pair_i;
       double dx, dy, dz;
-      if (hi) {
-        dx = pdiff(p.x, pq.x, T.lx); dy = pdiff(p.y, pq.y, T.ly); dz = p.z - pq.z;
-      } else {
-        dx = -pdiff(pq.x, p.x, T.lx); dy = -pdiff(pq.y, p.y, T.ly); dz = -(pq.z - p.z);
-      }
-      const R rdx = R(dx), rdy = R(dy), rdz = R(dz);
-      const R d2 = rdx * rdx + rdy * rdy + rdz * rdz;
+      pair_sep(p, pq, hi, T, dx, dy, dz);
+      const R d2 = R(dist_sq_exact(dx, dy, dz));
       const R c = L.pair(d2, R(hi ? S.spr[i] : S.spr[pair_i]));
-      if (fabs(c) > R(1000)) raise_error(S.status, E_COEF_RANGE, i, pair_i, double(c));
-      const R sdt = R(dt) * c;
-      ax += double(sdt * rdx);
-      ay += double(sdt * rdy);
-      az += double(sdt * rdz);
+      if (fabs(c) > R(1000)) raise_error(S.status, E_COEF_RANGE, (int32_t)i, pair_i, double(c));
+      const R sdt = dt * c;
+      ax += double(sdt * R(dx));
+      ay += double(sdt * R(dy));
+      az += double(sdt * R(dz));
     }
   }
 
-  // Searched connections: the law i applies while iterating q (if i is not a
-  // membrane particle) and the law q applies while iterating i (if q is not).
-  const int64_t N = S.n_total;
-  const int32_t nn = S.nn[i];
-  const bool old_i = attr_old(a);
-  for (int32_t k = 0; k < nn; ++k) {
-    const int32_t q = S.nbr[(int64_t)k * N + i];
-    const uint32_t aq = S.attr[q];
-    const uint32_t sq = attr_state(aq);
-    const double4 pq = S.pos_cur[q];
-    const double dx = pdiff(p.x, pq.x, T.lx), dy = pdiff(p.y, pq.y, T.ly), dz = p.z - pq.z;
-    const R rdx = R(dx), rdy = R(dy), rdz = R(dz);
-    const R d2 = rdx * rdx + rdy * rdy + rdz * rdz;
-    const R rs = R(p.w + pq.w);
-    const bool both_old = old_i && attr_old(aq);
-    R coef = R(0);
-    if (st != ST_MEMB) {
-      const int law = law_of(st, i, pair_i, dermis_i, sq, q);
-      if (law != L_NONE) {
-        const R c = eval_law<R>(law, L, d2, rs, both_old, attr_sfm(a));
-        if (fabs(c) > R(1000)) raise_error(S.status, E_COEF_RANGE, i, q, double(c));
-        coef += c;
-      }
-    }
-    if (sq != ST_MEMB) {
-      int32_t pair_q = -1, dermis_q = -1;
-      if (sq == ST_FIX || sq == ST_MUSUME) {
-        pair_q = S.pair[q];
-        dermis_q = S.dermis[q];
-      }
-      const int law = law_of(sq, q, pair_q, dermis_q, st, i);
-      if (law != L_NONE) {
-        const R c = eval_law<R>(law, L, d2, rs, both_old, attr_sfm(aq));
-        if (fabs(c) > R(1000)) raise_error(S.status, E_COEF_RANGE, q, i, double(c));
-        coef += c;
-      }
-    }
-    const R sdt = R(dt) * coef;
-    ax += double(sdt * rdx);
-    ay += double(sdt * rdy);
-    az += double(sdt * rdz);
-  }
-
+  // pos_copy + the single wrap of cell_pos_periodic_fix
   double nx = p.x + ax, ny = p.y + ay;
   const double nz = p.z + az;
-  if (nx > T.lx) nx -= T.lx;
-  else if (nx < 0) nx += T.lx;
-  if (ny > T.ly) ny -= T.ly;
-  else if (ny < 0) ny += T.ly;
-  if (!isfinite(nx) || !isfinite(ny) || !isfinite(nz))
-    raise_error(S.status, E_NONFINITE, i, -1, nz);
+  if (nx > lx) nx -= lx;
+  else if (nx < 0) nx += lx;
+  if (ny > ly) ny -= ly;
+  else if (ny < 0) ny += ly;
+  if (!isfinite(nx) || !isfinite(ny) || !isfinite(nz)) {
+    raise_error(S.status, E_NONFINITE, (int32_t)i, -1, nz);
+  } else if (!range_ok(T, nx, ny, nz, st == ST_MEMB)) {
+    raise_error(S.status, E_BIN_RANGE, (int32_t)i, -1, nz);
+  }
   S.pos_nxt[i] = make_double4(nx, ny, nz, p.w);
+  // Candidate validity: rebuild the tissue once a particle moved skin/2.
+  const float4 b = S.bpos[i];
+  double ex = nx - (double)b.x, ey = ny - (double)b.y;
+  if (ex > hlx) ex -= lx;
+  else if (ex < -hlx) ex += lx;
+  if (ey > hly) ey -= ly;
+  else if (ey < -hly) ey += ly;
+  const double ez = nz - (double)b.z;
+  const double lim = 0.5 * S.skin - 1e-3;  // margin covers the float rounding of bpos
+  if (!(ex * ex + ey * ey + ez * ez <= lim * lim)) {
+    S.gate[1 + t] = 1;
+    S.gate[0] = 1;
+  }
+}
+
+// connect_cell's lists (for export): the exact predicate over the candidates.
+__global__ void k_exact_lists(DevState S, Range r) {
+  GRID_STRIDE(i, r.p0, r.p1) {
+    const uint32_t a = S.attr[i];
+    const TissueDev& T = S.tissues[attr_tissue(a)];
+    const double4 p = S.pos_cur[i];
+    const int32_t nc = S.ncand[i];
+    const double lt = T.P.lj_thresh;
+    int32_t count = 0;
+    for (int32_t k = 0; k < nc; ++k) {
+      const int32_t q = S.cand[(int64_t)k * S.n_total + i];
+      const double4 pq = S.pos_cur[q];
+      const double d2 =
+          dist_sq_exact(pdiff(p.x, pq.x, T.lx), pdiff(p.y, pq.y, T.ly), p.z - pq.z);
+      if (!connected_pred(d2, lt, p.w, pq.w)) continue;
+      if (count < S.max_conn) S.nbr[(int64_t)count * S.n_total + i] = q;
+      ++count;
+    }
+    if (count > S.max_conn) raise_error(S.status, E_LIST_OVERFLOW, (int32_t)i, -1, (double)count);
+    S.nn[i] = count < S.max_conn ? count : S.max_conn;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -514,7 +683,8 @@ __global__ void k_dermis_local(DevState S, int32_t* out, int32_t n) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t a = S.attr[i];
-  const int32_t d = S.dermis[i];
+  const uint32_t st = attr_state(a);
+  const int32_t d = (st == ST_FIX || st == ST_MUSUME) ? S.dermis[i] : -1;
   out[i] = d < 0 ? -1 : d - S.tissues[attr_tissue(a)].pbase;
 }
 
@@ -540,70 +710,112 @@ __global__ void k_pack(DevState S, const double* x, const double* y, const doubl
 }  // namespace
 
 void launch_scan(const int32_t* in, int32_t* out, int32_t n, int32_t init,
-                 const ScanScratch& sc, cudaStream_t s) {
+                 const ScanScratch& sc, const int32_t* gate, const LaunchCfg&,
+                 cudaStream_t s) {
   const int32_t nb = (n + kScanTile - 1) / kScanTile;
   if (nb == 0) {
-    k_set1<<<1, 1, 0, s>>>(out, init);
+    k_set1<<<1, 1, 0, s>>>(out, init, gate);
     return;
   }
-  k_scan_partial<<<nb, kScanThreads, 0, s>>>(in, n, sc.partial);
-  k_scan_top<<<1, kScanThreads, 0, s>>>(sc.partial, nb);
-  k_scan_final<<<nb, kScanThreads, 0, s>>>(in, out, n, sc.partial, init);
+  k_scan_partial<<<nb, kScanThreads, 0, s>>>(in, n, sc.partial, gate);
+  k_scan_top<<<1, kScanThreads, 0, s>>>(sc.partial, nb, gate);
+  k_scan_final<<<nb, kScanThreads, 0, s>>>(in, out, n, sc.partial, init, gate);
 }
 
-void launch_connect(const DevState& S, const Range& r, int precision, const ScanScratch& sc,
-                    cudaStream_t s, Timer* tm) {
+void launch_rebuild(const DevState& S, const Range& r, const ScanScratch& sc,
+                    const LaunchCfg& lc, cudaStream_t s, Timer* tm) {
   const int32_t np = r.p1 - r.p0, nbins = r.b1 - r.b0;
-  if (np <= 0) return;
-  timer_begin(tm, KC_BIN, s);
-  if (precision == 1)
-    k_bin<float><<<blocks_for(np), kBlock, 0, s>>>(S, r);
-  else
-    k_bin<double><<<blocks_for(np), kBlock, 0, s>>>(S, r);
-  timer_end(tm, KC_BIN, s);
-  timer_begin(tm, KC_SCAN, s);
-  launch_scan(S.counts + r.b0, S.starts + r.b0, nbins, r.p0, sc, s);
-  timer_end(tm, KC_SCAN, s);
-  timer_begin(tm, KC_SCATTER, s);
-  k_scatter<<<blocks_for(np), kBlock, 0, s>>>(S, r);
-  timer_end(tm, KC_SCATTER, s);
-  timer_begin(tm, KC_BINSORT, s);
-  k_binsort<<<blocks_for(nbins), kBlock, 0, s>>>(S, r);
-  timer_end(tm, KC_BINSORT, s);
-  timer_begin(tm, KC_SEARCH, s);
-  k_search<<<blocks_for(np), kBlock, 0, s>>>(S, r);
-  timer_end(tm, KC_SEARCH, s);
+  const int B = lc.block;
+  timer_begin(tm, KC_REBUILD_BIN, s);
+  k_bin<<<stride_blocks(np, B, lc), B, 0, s>>>(S, r);
+  timer_end(tm, KC_REBUILD_BIN, s);
+  timer_begin(tm, KC_REBUILD_SCAN, s);
+  launch_scan(S.counts + r.b0, S.starts + r.b0, nbins, r.p0, sc, S.gate, lc, s);
+  timer_end(tm, KC_REBUILD_SCAN, s);
+  timer_begin(tm, KC_REBUILD_SORT, s);
+  k_scatter<<<stride_blocks(np, B, lc), B, 0, s>>>(S, r);
+  k_binsort<<<stride_blocks(nbins, B, lc), B, 0, s>>>(S, r);
+  timer_end(tm, KC_REBUILD_SORT, s);
+  timer_begin(tm, KC_REBUILD_SEARCH, s);
+  k_cand_search<<<stride_blocks(np, B, lc), B, 0, s>>>(S, r);
+  timer_end(tm, KC_REBUILD_SEARCH, s);
+  timer_begin(tm, KC_GATE, s);
+  const int32_t nt = r.t1 - r.t0;
+  const bool whole = r.p0 == 0 && (int64_t)r.p1 == S.n_total;
+  k_gate_clear<<<stride_blocks(nt, B, lc), B, 0, s>>>(S, r, whole ? 1 : 0);
+  timer_end(tm, KC_GATE, s);
 }
 
-void launch_interact_commit(const DevState& S, const Range& r, int precision, cudaStream_t s,
-                            Timer* tm) {
+void launch_prepass(const DevState& S, int32_t m0, int32_t m1, int32_t f0, int32_t f1,
+                    int precision, const LaunchCfg& lc, cudaStream_t s, Timer* tm) {
+  const int64_t n = (int64_t)(m1 - m0) + (f1 - f0);
+  if (n <= 0) return;
+  timer_begin(tm, KC_PREPASS, s);
+  const int g = stride_blocks(n, lc.block, lc);
+  if (precision == 1)
+    k_prepass<float><<<g, lc.block, 0, s>>>(S, m0, m1, f0, f1);
+  else
+    k_prepass<double><<<g, lc.block, 0, s>>>(S, m0, m1, f0, f1);
+  if (m1 > m0) {
+    const int gm = stride_blocks(m1 - m0, lc.block, lc);
+    if (precision == 1)
+      k_memb_force<float><<<gm, lc.block, 0, s>>>(S, m0, m1);
+    else
+      k_memb_force<double><<<gm, lc.block, 0, s>>>(S, m0, m1);
+  }
+  timer_end(tm, KC_PREPASS, s);
+}
+
+template <typename R>
+void launch_step_r(const DevState& S, const Range& r, const LaunchCfg& lc, cudaStream_t s) {
+  const int grid = blocks_for(r.p1 - r.p0, 256);
+  if (lc.simple && lc.any_old)
+    k_step<R, true, true><<<grid, 256, 0, s>>>(S, r);
+  else if (lc.simple)
+    k_step<R, true, false><<<grid, 256, 0, s>>>(S, r);
+  else
+    k_step<R, false, true><<<grid, 256, 0, s>>>(S, r);
+}
+
+void launch_step(const DevState& S, const Range& r, int precision, const LaunchCfg& lc,
+                 cudaStream_t s, Timer* tm) {
   const int32_t np = r.p1 - r.p0;
   if (np <= 0) return;
-  timer_begin(tm, KC_FORCE, s);
+  timer_begin(tm, KC_STEP, s);
   if (precision == 1)
-    k_force_commit<float><<<blocks_for(np), kBlock, 0, s>>>(S, r);
+    launch_step_r<float>(S, r, lc, s);
   else
-    k_force_commit<double><<<blocks_for(np), kBlock, 0, s>>>(S, r);
-  timer_end(tm, KC_FORCE, s);
+    launch_step_r<double>(S, r, lc, s);
+  timer_end(tm, KC_STEP, s);
+}
+
+void launch_exact_lists(const DevState& S, const Range& r, const LaunchCfg& lc,
+                        cudaStream_t s) {
+  const int32_t np = r.p1 - r.p0;
+  if (np > 0) k_exact_lists<<<stride_blocks(np, lc.block, lc), lc.block, 0, s>>>(S, r);
+}
+
+void launch_set_gates(const DevState& S, int32_t ntissues, cudaStream_t s) {
+  k_gate_set_all<<<(ntissues + 255) / 256 + 1, 256, 0, s>>>(S, ntissues);
 }
 
 void launch_rowlen(const DevState& S, int32_t* rowlen, int32_t n, cudaStream_t s) {
-  if (n > 0) k_rowlen<<<blocks_for(n), kBlock, 0, s>>>(S, rowlen, n);
+  if (n > 0) k_rowlen<<<blocks_for(n, 256), 256, 0, s>>>(S, rowlen, n);
 }
 void launch_fill_csr(const DevState& S, const int32_t* rowoff, int32_t* idx, int32_t n,
                      cudaStream_t s) {
-  if (n > 0) k_fill_csr<<<blocks_for(n), kBlock, 0, s>>>(S, rowoff, idx, n);
+  if (n > 0) k_fill_csr<<<blocks_for(n, 256), 256, 0, s>>>(S, rowoff, idx, n);
 }
 void launch_dermis_local(const DevState& S, int32_t* out, int32_t n, cudaStream_t s) {
-  if (n > 0) k_dermis_local<<<blocks_for(n), kBlock, 0, s>>>(S, out, n);
+  if (n > 0) k_dermis_local<<<blocks_for(n, 256), 256, 0, s>>>(S, out, n);
 }
 void launch_unpack_positions(const DevState& S, double* x, double* y, double* z, int32_t n,
                              cudaStream_t s) {
-  if (n > 0) k_unpack<<<blocks_for(n), kBlock, 0, s>>>(S, x, y, z, n);
+  if (n > 0) k_unpack<<<blocks_for(n, 256), 256, 0, s>>>(S, x, y, z, n);
 }
 void launch_pack_positions(const DevState& S, const double* x, const double* y,
                            const double* z, int32_t n, cudaStream_t s) {
-  if (n > 0) k_pack<<<blocks_for(n), kBlock, 0, s>>>(S, x, y, z, n);
+  if (n > 0) k_pack<<<blocks_for(n, 256), 256, 0, s>>>(S, x, y, z, n);
 }
 
 }  // namespace epi

@@ -4,11 +4,12 @@
 
 namespace epi {
 
-// Half-open particle and bin ranges a launch covers: the whole batch, or one
-// tissue for the unbatched launch pattern.
+// Half-open particle, bin and tissue ranges a launch covers: the whole batch,
+// or one tissue for the unbatched launch pattern.
 struct Range {
-  int32_t p0, p1;  // particles [p0, p1)
-  int32_t b0, b1;  // bins [b0, b1)
+  int32_t p0, p1;  // particles
+  int32_t b0, b1;  // bins
+  int32_t t0, t1;  // tissues
 };
 
 struct ScanScratch {
@@ -17,24 +18,48 @@ struct ScanScratch {
 };
 constexpr int kScanTile = 2048;
 
+struct LaunchCfg {
+  int num_sms;      // grid-stride kernels use a few blocks per SM
+  int block;        // threads per block of the grid-stride kernels
+  int simple;       // batch holds only ALIVE / DEAD / AIR / MEMB, no pairs
+  int any_old;      // some cell is older than THRESH_SP
+};
+
 // Kernel classes, for per-class timing.
-enum KernelClass : int { KC_FORCE = 0, KC_BIN, KC_SCAN, KC_SCATTER, KC_BINSORT, KC_SEARCH, KC_COUNT };
+enum KernelClass : int {
+  KC_STEP = 0, KC_PREPASS, KC_REBUILD_BIN, KC_REBUILD_SCAN, KC_REBUILD_SORT,
+  KC_REBUILD_SEARCH, KC_GATE, KC_COUNT
+};
 extern const char* const kKernelClassNames[KC_COUNT];
 
 struct Timer;  // optional per-class CUDA-event recorder (host side)
 void timer_begin(Timer* tm, int cls, cudaStream_t s);
 void timer_end(Timer* tm, int cls, cudaStream_t s);
 
-// Exclusive scan: out[k] = init + sum(in[0..k)) for k in [0, n], out[n] the total.
+// Exclusive scan: out[k] = init + sum(in[0..k)) for k in [0, n], out[n] the
+// total. When gate is non-null the kernels do nothing unless *gate != 0.
 void launch_scan(const int32_t* in, int32_t* out, int32_t n, int32_t init,
-                 const ScanScratch& sc, cudaStream_t s);
+                 const ScanScratch& sc, const int32_t* gate, const LaunchCfg& lc,
+                 cudaStream_t s);
 
-// connect_cell: bin -> scan -> scatter -> per-bin sort -> neighbour search.
-void launch_connect(const DevState& S, const Range& r, int precision, const ScanScratch& sc,
-                    cudaStream_t s, Timer* tm);
-// cell_interaction + pos_copy + cell_pos_periodic_fix (writes S.pos_nxt).
-void launch_interact_commit(const DevState& S, const Range& r, int precision, cudaStream_t s,
-                            Timer* tm);
+// Verlet candidate rebuild of every tissue whose gate is set (all kernels
+// exit at once when no gate is set): bin -> scan -> scatter -> per-bin sort
+// -> candidate search -> gate reset.
+void launch_rebuild(const DevState& S, const Range& r, const ScanScratch& sc,
+                    const LaunchCfg& lc, cudaStream_t s, Timer* tm);
+// Membrane bending scratch (_memb_bend_calc1) and dermis (find_dermis) for
+// prep entries [m0, m1) (membrane role) and [f0, f1) (FIX / MUSUME role).
+void launch_prepass(const DevState& S, int32_t m0, int32_t m1, int32_t f0, int32_t f1,
+                    int precision, const LaunchCfg& lc, cudaStream_t s, Timer* tm);
+// cell_interaction + pos_copy + cell_pos_periodic_fix from the current
+// positions into S.pos_nxt; flags tissues whose particles moved more than
+// skin/2 since their last rebuild.
+void launch_step(const DevState& S, const Range& r, int precision, const LaunchCfg& lc,
+                 cudaStream_t s, Timer* tm);
+// Exact connection lists (connect_cell's result) into S.nbr / S.nn.
+void launch_exact_lists(const DevState& S, const Range& r, const LaunchCfg& lc,
+                        cudaStream_t s);
+void launch_set_gates(const DevState& S, int32_t ntissues, cudaStream_t s);
 
 // CSR export of the connection lists (tissue-local indices, rows sorted).
 void launch_rowlen(const DevState& S, int32_t* rowlen, int32_t n, cudaStream_t s);

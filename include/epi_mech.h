@@ -95,12 +95,19 @@ typedef enum epi_precision {
   EPI_PREC_MIXED = 1  /* pair and bending forces in FP32, sums and positions in FP64 */
 } epi_precision;
 
+/* Connection lists are exact every step, as connect_cell's are. Internally a
+ * tissue keeps a candidate list of every partner within
+ * LJ_THRESH*(r_i+r_j) + skin, rebuilt once any of its particles has moved
+ * skin/2 since the last rebuild; the reference's predicate is evaluated on
+ * the candidates at every step. skin trades rebuild frequency for candidate
+ * count and never changes results. */
 typedef struct epi_config {
   int32_t device;     /* CUDA device ordinal */
   int32_t precision;  /* epi_precision */
-  int32_t max_conn;   /* searched connections per particle (membrane lattice links
-                         are extra); the reference allows 400 (define.h:80) */
-  int32_t reserved;
+  int32_t max_conn;   /* connections per particle (membrane lattice links are
+                         extra); the reference allows 400 (define.h:80) */
+  int32_t max_cand;   /* candidates per particle (>= max_conn) */
+  double skin;        /* candidate margin, > 0 (default 0.3) */
 } epi_config;
 
 typedef struct epi_ctx epi_ctx;
