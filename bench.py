@@ -210,6 +210,7 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--skin", type=float, default=None)
     ap.add_argument("--tissues", type=int, default=512, help="ensemble size (profiling)")
+    ap.add_argument("--variant", type=int, default=None, help="step-kernel tuning variant")
     ap.add_argument("--mode", default="graph", choices=["graph", "eager"])
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--plain-steps", type=int, default=3)
@@ -242,7 +243,8 @@ def main():
     n_all = sum(t.n for t in tissues)
     prec = capi.EPI_PREC_MIXED if args.precision == "mixed" else capi.EPI_PREC_FP64
 
-    ctx = capi.Context(precision=prec, max_conn=64, device=local, skin=args.skin)
+    ctx = capi.Context(precision=prec, max_conn=64, device=local, skin=args.skin,
+                       variant=args.variant)
     ctx.upload(mine)
     off, _ = ctx.connections()
     kbar = float(off[-1]) / max(n_mine, 1)  # mean connected_cell length incl. lattice links
@@ -257,6 +259,7 @@ def main():
     # warm-up (also captures the graph)
     if args.warmup:
         ctx.step(args.warmup, args.mode)
+    rebuilds0 = ctx.rebuild_count()
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
@@ -270,6 +273,7 @@ def main():
     torch.cuda.synchronize()
     barrier()
     ms = e0.elapsed_time(e1)
+    rebuilds_timed = ctx.rebuild_count() - rebuilds0
     if dist is not None:
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -368,6 +372,8 @@ def main():
     if rank == 0:
         cfg = {"workload": desc, "tissues": len(tissues), "particles": n_all,
                "mean_connections": kbar, "precision": args.precision,
+               "skin": args.skin if args.skin is not None else 0.1,
+               "tissue_rebuilds_per_step": rebuilds_timed / max(args.steps, 1) / len(mine),
                "launch": "one CUDA graph per 2 steps over the whole batch",
                "l2": "inputs larger than L2 (working set >> 126 MB)"
                if n_all * 200 > 126e6 else "working set fits in L2 (no flush)",

@@ -40,7 +40,7 @@ EXPORTED = [
     "epi_upload", "epi_connect", "epi_interact_commit", "epi_step", "epi_step_graph",
     "epi_step_per_tissue", "epi_sync", "epi_num_particles", "epi_download_positions",
     "epi_upload_positions", "epi_get_connections", "epi_get_dermis", "epi_error_info",
-    "epi_stream", "epi_time_kernels",
+    "epi_stream", "epi_rebuild_count", "epi_time_kernels",
 ]
 
 
@@ -78,7 +78,8 @@ class TissueViewC(ctypes.Structure):
 class ConfigC(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("precision", ctypes.c_int32),
                 ("max_conn", ctypes.c_int32), ("max_cand", ctypes.c_int32),
-                ("skin", ctypes.c_double)]
+                ("skin", ctypes.c_double), ("variant", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
 
 _lib = None
@@ -114,6 +115,7 @@ def lib():
                                           ctypes.POINTER(ctypes.c_int64)]
         L.epi_get_dermis.argtypes = [vp, _ip]
         L.epi_error_info.argtypes = [vp, _ip, _ip, _ip, _dp]
+        L.epi_rebuild_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         L.epi_stream.argtypes = [vp]
         L.epi_stream.restype = vp
         L.epi_time_kernels.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, _dp, _ip,
@@ -152,7 +154,8 @@ class Context:
     """One epi_ctx: a batch of tissues resident on one GPU."""
 
     def __init__(self, precision: int = EPI_PREC_MIXED, max_conn: int = 64, device: int = 0,
-                 max_cand: Optional[int] = None, skin: Optional[float] = None):
+                 max_cand: Optional[int] = None, skin: Optional[float] = None,
+                 variant: Optional[int] = None):
         L = lib()
         cfg = ConfigC()
         L.epi_config_default(ctypes.byref(cfg))
@@ -161,6 +164,8 @@ class Context:
         cfg.max_cand = max(max_cand if max_cand is not None else cfg.max_cand, max_conn)
         if skin is not None:
             cfg.skin = skin
+        if variant is not None:
+            cfg.variant = variant
         cfg.device = device
         h = ctypes.c_void_p()
         _check(L.epi_create(ctypes.byref(h), ctypes.byref(cfg)), "epi_create")
@@ -282,6 +287,11 @@ class Context:
         code = lib().epi_error_info(self._h, ctypes.byref(t), ctypes.byref(a), ctypes.byref(b),
                                     ctypes.byref(v))
         return dict(code=code, tissue=t.value, particle=a.value, other=b.value, value=v.value)
+
+    def rebuild_count(self) -> int:
+        v = ctypes.c_int64()
+        _check(lib().epi_rebuild_count(self._h, ctypes.byref(v)), "epi_rebuild_count")
+        return int(v.value)
 
     def stream_handle(self) -> int:
         return int(lib().epi_stream(self._h) or 0)

@@ -63,7 +63,7 @@ struct TissueHost {
 struct epi_ctx {
   epi_config cfg{};
   cudaStream_t stream = nullptr;
-  LaunchCfg lc{148, 256, 0, 0};
+  LaunchCfg lc{148, 256, 0, 0, 0};
   bool loaded = false;
   bool lists_fresh = false;  // nbr / nn / dermis match the current positions
   int32_t ntissues = 0;
@@ -85,20 +85,20 @@ struct epi_ctx {
   float4* bpos = nullptr;
   int32_t* nbr = nullptr;
   int32_t* nn = nullptr;
-  double4* sn = nullptr;
-  double4* sm = nullptr;
   double4* fmemb = nullptr;
   int32_t* bin = nullptr;
   int32_t* rank = nullptr;
   int32_t* counts = nullptr;
   int32_t* starts = nullptr;
   uint32_t* skey = nullptr;
-  double4* spos = nullptr;
+  float4* spos = nullptr;
   int32_t* gate = nullptr;
+  int32_t* rl = nullptr;    // rebuild work list: [count | list (T) | ppre (T+1) | bpre (T+1)]
   int32_t* prep = nullptr;
   double* stage = nullptr;        // 3n doubles: x | y | z for host transfers
   DevStatus* status = nullptr;
   DevStatus* status_h = nullptr;  // pinned
+  unsigned long long* rebuilds = nullptr;
   ScanScratch scan{};
   // graphs: one per buffer parity, each replaying two steps
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -134,8 +134,8 @@ void free_buffers(epi_ctx* c) {
     g = nullptr;
   }
   void* ptrs[] = {c->tissues, c->pos[0], c->pos[1], c->attr, c->pair, c->spr, c->dermis,
-                  c->cand, c->ncand, c->bpos, c->nbr, c->nn, c->sn, c->sm, c->fmemb, c->bin,
-                  c->rank, c->counts, c->starts, c->skey, c->spos, c->gate, c->prep,
+                  c->cand, c->ncand, c->bpos, c->nbr, c->nn, c->fmemb, c->bin,
+                  c->rank, c->counts, c->starts, c->skey, c->spos, c->gate, c->rl, c->prep,
                   c->scan.partial, c->stage};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -143,9 +143,9 @@ void free_buffers(epi_ctx* c) {
   c->pos[0] = c->pos[1] = nullptr;
   c->attr = nullptr; c->pair = nullptr; c->spr = nullptr; c->dermis = nullptr;
   c->cand = nullptr; c->ncand = nullptr; c->bpos = nullptr;
-  c->nbr = nullptr; c->nn = nullptr; c->sn = nullptr; c->sm = nullptr; c->fmemb = nullptr;
+  c->nbr = nullptr; c->nn = nullptr; c->fmemb = nullptr;
   c->bin = nullptr; c->rank = nullptr; c->counts = nullptr; c->starts = nullptr;
-  c->skey = nullptr; c->spos = nullptr; c->gate = nullptr; c->prep = nullptr;
+  c->skey = nullptr; c->spos = nullptr; c->gate = nullptr; c->rl = nullptr; c->prep = nullptr;
   c->scan.partial = nullptr; c->stage = nullptr;
   c->loaded = false;
   c->lists_fresh = false;
@@ -165,8 +165,6 @@ DevState make_state(epi_ctx* c, int cur) {
   S.bpos = c->bpos;
   S.nbr = c->nbr;
   S.nn = c->nn;
-  S.sn = c->sn;
-  S.sm = c->sm;
   S.fmemb = c->fmemb;
   S.bin = c->bin;
   S.rank = c->rank;
@@ -175,10 +173,16 @@ DevState make_state(epi_ctx* c, int cur) {
   S.skey = c->skey;
   S.spos = c->spos;
   S.gate = c->gate;
+  S.rl_count = c->rl;
+  S.rl_list = c->rl ? c->rl + 1 : nullptr;
+  S.rl_ppre = c->rl ? c->rl + 1 + c->ntissues : nullptr;
+  S.rl_bpre = c->rl ? c->rl + 2 + 2 * c->ntissues : nullptr;
+  S.ntissues = c->ntissues;
   S.prep = c->prep;
   S.nprep = c->nprep;
   S.nprep_memb = c->nprep_memb;
   S.status = c->status;
+  S.rebuilds = c->rebuilds;
   S.n_total = c->n;
   S.max_conn = c->cfg.max_conn;
   S.max_cand = c->cfg.max_cand;
@@ -190,7 +194,7 @@ Range whole(const epi_ctx* c) { return Range{0, (int32_t)c->n, 0, c->nbins, 0, c
 
 Range tissue_range(const epi_ctx* c, int t) {
   const TissueDev& T = c->tissues_h[t];
-  return Range{T.pbase, T.pbase + T.n, T.binbase, T.binbase + T.anx * T.any * T.anz, t, t + 1};
+  return Range{T.pbase, T.pbase + T.n, T.binbase, T.binbase + T.anx * T.any * T.anz + 1, t, t + 1};
 }
 
 void prepass_all(epi_ctx* c, int cur, Timer* tm) {
@@ -364,7 +368,9 @@ void epi_config_default(epi_config* c) {
   c->precision = EPI_PREC_MIXED;
   c->max_conn = 64;
   c->max_cand = 96;
-  c->skin = 0.3;
+  c->skin = 0.1;
+  c->variant = 0;
+  c->reserved = 0;
 }
 
 const char* epi_strerror(int s) {
@@ -397,6 +403,7 @@ int epi_create(epi_ctx** out, const epi_config* cfg) {
   if (c.max_conn <= 0 || c.max_conn > 400 || c.max_cand < c.max_conn || c.max_cand > 1024)
     return EPI_ERR_INVALID_ARG;
   if (!(c.skin > 0) || c.skin > 2.0) return EPI_ERR_INVALID_ARG;
+  if (c.variant < 0 || c.variant > 4) return EPI_ERR_INVALID_ARG;
   if (c.precision != EPI_PREC_FP64 && c.precision != EPI_PREC_MIXED) return EPI_ERR_INVALID_ARG;
   int ndev = 0;
   const cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -405,6 +412,7 @@ int epi_create(epi_ctx** out, const epi_config* cfg) {
   EPI_CUDA(cudaSetDevice(c.device));
   epi_ctx* ctx = new epi_ctx();
   ctx->cfg = c;
+  ctx->lc.variant = c.variant;
   int sms = 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device) == cudaSuccess &&
       sms > 0)
@@ -413,6 +421,8 @@ int epi_create(epi_ctx** out, const epi_config* cfg) {
   if (rc == EPI_OK) rc = dev_alloc(&ctx->status, 1);
   if (rc == EPI_OK) rc = cuda_status(cudaMallocHost((void**)&ctx->status_h, sizeof(DevStatus)));
   if (rc == EPI_OK) rc = cuda_status(cudaMemset(ctx->status, 0, sizeof(DevStatus)));
+  if (rc == EPI_OK) rc = dev_alloc(&ctx->rebuilds, 1);
+  if (rc == EPI_OK) rc = cuda_status(cudaMemset(ctx->rebuilds, 0, sizeof(unsigned long long)));
   if (rc != EPI_OK) {
     epi_destroy(ctx);
     return rc;
@@ -428,6 +438,7 @@ void epi_destroy(epi_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   free_buffers(ctx);
   if (ctx->status) cudaFree(ctx->status);
+  if (ctx->rebuilds) cudaFree(ctx->rebuilds);
   if (ctx->status_h) cudaFreeHost(ctx->status_h);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -447,7 +458,7 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
     if ((rc = validate_tissue(tv[t], P))) return rc;
     n += tv[t].n;
     nbins += (int64_t)((int)(tv[t].lx / 2.0 + 0.5)) * (int)(tv[t].ly / 2.0 + 0.5) *
-             (int)(tv[t].lz / 2.0);
+                 (int)(tv[t].lz / 2.0) + 1;
   }
   if (n > (int64_t)0x7fffffff || nbins > (int64_t)0x7ffffff0 || ntissues >= (1 << 24))
     return EPI_ERR_UNSUPPORTED;
@@ -524,7 +535,7 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
     T.rmax_nm = rmax_nm;
     H.nfm = (int32_t)prep_f.size() - H.prep_f;
     pbase += v.n;
-    binbase += T.anx * T.any * T.anz;
+    binbase += T.anx * T.any * T.anz + 1;  // + sentinel (end offset of the tissue)
   }
   c->lc.simple = simple ? 1 : 0;
   c->lc.any_old = any_old ? 1 : 0;
@@ -539,12 +550,12 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
       (rc = dev_alloc(&c->dermis, n)) || (rc = dev_alloc(&c->cand, CC * n)) ||
       (rc = dev_alloc(&c->ncand, n)) || (rc = dev_alloc(&c->bpos, n)) ||
       (rc = dev_alloc(&c->nbr, C * n)) || (rc = dev_alloc(&c->nn, n)) ||
-      (rc = dev_alloc(&c->sn, n)) || (rc = dev_alloc(&c->sm, n)) ||
       (rc = dev_alloc(&c->fmemb, n)) ||
       (rc = dev_alloc(&c->bin, n)) || (rc = dev_alloc(&c->rank, n)) ||
       (rc = dev_alloc(&c->counts, nbins)) || (rc = dev_alloc(&c->starts, nbins + 1)) ||
       (rc = dev_alloc(&c->skey, n)) || (rc = dev_alloc(&c->spos, n)) ||
       (rc = dev_alloc(&c->gate, (size_t)ntissues + 1)) ||
+      (rc = dev_alloc(&c->rl, 3 + 3 * (size_t)ntissues)) ||
       (rc = dev_alloc(&c->prep, prep.size())) || (rc = dev_alloc(&c->stage, 3 * (size_t)n))) {
     free_buffers(c);
     return rc;
@@ -804,6 +815,19 @@ int epi_error_info(epi_ctx* c, int32_t* tissue, int32_t* particle, int32_t* othe
 }
 
 void* epi_stream(epi_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int epi_rebuild_count(epi_ctx* c, int64_t* count) {
+  if (!c || !count) return EPI_ERR_INVALID_ARG;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  unsigned long long v = 0;
+  EPI_CUDA(cudaMemcpyAsync(&v, c->rebuilds, sizeof(v), cudaMemcpyDeviceToHost, c->stream));
+  EPI_CUDA(cudaStreamSynchronize(c->stream));
+  *count = (int64_t)v;
+  return EPI_OK;
+  EPI_GUARD_END
+}
 
 int epi_time_kernels(epi_ctx* c, int32_t nsteps, int32_t max_classes, double* ms,
                      int32_t* launches, const char** names, int32_t* nclasses) {

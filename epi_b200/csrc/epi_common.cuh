@@ -67,19 +67,23 @@ struct DevState {
   float4* bpos;     // positions at the last rebuild (displacement check)
   int32_t* nbr;     // exact connection lists (materialised on request)
   int32_t* nn;
-  double4* sn;
-  double4* sm;
   double4* fmemb;   // membrane bending + lattice spring + wall displacement
   int32_t* bin;
   int32_t* rank;
   int32_t* counts;
   int32_t* starts;
   uint32_t* skey;   // sorted particles: global index | (is_memb << 31)
-  double4* spos;    // sorted copy of the positions at rebuild
+  float4* spos;     // sorted copy of the positions (and radii) at rebuild
   int32_t* gate;    // [0]: some tissue needs a rebuild, [1 + t]: tissue t does
+  int32_t* rl_count;  // rebuild work list: number of gated tissues
+  int32_t* rl_list;   // their ids
+  int32_t* rl_ppre;   // prefix sums of their particle counts (count + 1 entries)
+  int32_t* rl_bpre;   // prefix sums of their bin counts
+  int32_t ntissues;
   const int32_t* prep;  // membrane particles, then FIX/MUSUME cells
   int32_t nprep, nprep_memb;
   DevStatus* status;
+  unsigned long long* rebuilds;  // tissue candidate rebuilds so far
   int64_t n_total;  // column stride of cand / nbr
   int32_t max_conn, max_cand;
   double skin;
@@ -122,6 +126,14 @@ __device__ __forceinline__ bool connected_pred(double d2, double lt, double ri, 
   return d2 <= __dmul_rn(__dmul_rn(__dmul_rn(lt, lt), rs), rs);
 }
 
+// Division and square root of the force laws: IEEE in the FP64 path, the
+// hardware approximations (MUFU reciprocal / reciprocal square root, about
+// 2 ulp) in the FP32 path.
+__device__ __forceinline__ double ldiv(double a, double b) { return a / b; }
+__device__ __forceinline__ float ldiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double lsqrt(double v) { return sqrt(v); }
+__device__ __forceinline__ float lsqrt(float v) { return v * rsqrtf(v); }
+
 template <typename R>
 __device__ __forceinline__ R pow6(R v) { return v * v * v * v * v * v; }
 template <typename R>
@@ -137,28 +149,28 @@ struct Laws {
 
   // ljmain, :103-111
   __device__ __forceinline__ R ljmain(R d2, R rs) const {
-    const R lj6 = pow6(rs) / pow3(d2);
-    return eps4 * lj6 * (lj6 - R(1)) / d2;
+    const R lj6 = ldiv(pow6(rs), pow3(d2));
+    return ldiv(eps4 * lj6 * (lj6 - R(1)), d2);
   }
   // adhesion, :113-124
   __device__ __forceinline__ R adhesion(R d2, R rs, R k) const {
-    const R d = sqrt(d2);
-    const R m1 = d / rs - R(1);
-    return (m1 + R(1) > lj_thresh) ? R(0) : -(k / d) * m1 * (R(1) - m1 * m1 / ljt1sq);
+    const R d = lsqrt(d2);
+    const R m1 = ldiv(d, rs) - R(1);
+    return (m1 + R(1) > lj_thresh) ? R(0) : -ldiv(k, d) * m1 * (R(1) - ldiv(m1 * m1, ljt1sq));
   }
   // is_near, :90-93
   __device__ __forceinline__ bool near(R d2, R rs) const { return d2 < rs * rs; }
   // CI_der_to_der, :129-139
   __device__ __forceinline__ R der_der(R d2, R rs) const {
-    const R d = sqrt(d2);
+    const R d = lsqrt(d2);
     const R dd = d + delta_r;
     if (dd < rs) {
-      const R lj6 = pow6(rs) / pow6(dd);
-      return eps4 * lj6 * (lj6 - R(1)) / (d * dd) + para_ljp2;
+      const R lj6 = ldiv(pow6(rs), pow6(dd));
+      return ldiv(eps4 * lj6 * (lj6 - R(1)), d * dd) + para_ljp2;
     }
     if (near(d2, rs)) return para_ljp2;
-    const R lj6 = pow6(rs) / pow6(dd);
-    return eps4 * lj6 * (lj6 - R(1)) / (d * d) + para_ljp2;
+    const R lj6 = ldiv(pow6(rs), pow6(dd));
+    return ldiv(eps4 * lj6 * (lj6 - R(1)), d * d) + para_ljp2;
   }
   // CI_al_air_de_to_al_air_de_fix_mu, :141-152
   __device__ __forceinline__ R aad(R d2, R rs, bool both_old) const {
@@ -178,8 +190,8 @@ struct Laws {
   // CI_fix_to_memb, :174-183
   __device__ __forceinline__ R fix_memb(R d2, R rs) const {
     if (near(d2, rs)) return ljmain(d2, rs);
-    const R d = sqrt(d2);
-    return -(kspring / d) * (d / rs - R(1));
+    const R d = lsqrt(d2);
+    return -ldiv(kspring, d) * (ldiv(d, rs) - R(1));
   }
   // CI_memb_to_memb, :185-234; *bad set when |coef| > 100 (the reference aborts)
   __device__ __forceinline__ R memb_memb(R d2, R rs, bool* bad) const {
@@ -187,25 +199,25 @@ struct Laws {
     const R cr2 = rs2 * p_memb * p_memb;
     R tmp;
     if (d2 < cr2) {
-      const R lj6 = pow3(cr2) / pow3(d2);
-      tmp = eps4 * lj6 * (lj6 - R(1)) / d2;
+      const R lj6 = ldiv(pow3(cr2), pow3(d2));
+      tmp = ldiv(eps4 * lj6 * (lj6 - R(1)), d2);
     } else if (d2 < rs2) {
-      const R d = sqrt(d2);
-      tmp = -(der_der_const / d) * (d / (rs * p_memb) - R(1));
+      const R d = lsqrt(d2);
+      tmp = -ldiv(der_der_const, d) * (ldiv(d, rs * p_memb) - R(1));
     } else {
-      const R d = sqrt(d2);
+      const R d = lsqrt(d2);
       const R lam = (R(1) + p_memb) * rs;
-      const R lj6 = pow6(rs * p_memb) / pow6(lam - d);
-      tmp = -(der_der_const / rs) * ((R(1) - p_memb) / p_memb) -
-            eps4 * (lj6 * (lj6 - R(1))) / ((lam - d) * d);
+      const R lj6 = ldiv(pow6(rs * p_memb), pow6(lam - d));
+      tmp = -ldiv(der_der_const, rs) * ldiv(R(1) - p_memb, p_memb) -
+            ldiv(eps4 * (lj6 * (lj6 - R(1))), (lam - d) * d);
     }
     *bad = fabs(tmp) > R(100);
     return tmp;
   }
   // CI_pair, :281-285 (rest = the first cell's spr_nat_len)
   __device__ __forceinline__ R pair(R d2, R rest) const {
-    const R d = sqrt(d2);
-    return -(kspring_division * (d - rest)) / d;
+    const R d = lsqrt(d2);
+    return ldiv(-(kspring_division * (d - rest)), d);
   }
 };
 
@@ -284,7 +296,8 @@ __device__ __forceinline__ R eval_law(int law, const Laws<R>& L, R d2, R rs, boo
 
 struct TissueDev {
   int32_t pbase, n, nmemb, nder, nmx, nmy;
-  int32_t anx, any, anz, binbase;  // reference grid (cell_connection.cpp:22-26)
+  int32_t anx, any, anz;  // reference grid (cell_connection.cpp:22-26)
+  int32_t binbase;        // first bin; a tissue owns anx*any*anz bins + 1 sentinel
   double lx, ly, lz, hlx, hly;     // box and half box
   double rmax;     // largest radius in the tissue
   double rmax_nm;  // largest non-membrane radius (membranes only pair with those)

@@ -154,41 +154,143 @@ __device__ __forceinline__ int32_t ref_bin(const TissueDev& T, double x, double 
 }
 
 // ---------------------------------------------------------------------------
-// Rebuild: binning on the reference's 2.0 grid of every particle of a gated
-// tissue.
+// Rebuild work list. k_gate_compact lists the gated tissues of [t0, t1) with
+// prefix sums of their particle and bin counts; every other rebuild kernel
+// then strides over the gated particles (or bins) only, mapping a running
+// index back to (tissue, local index) by binary search in the prefix sums.
+// With nothing gated the list is empty and each kernel exits at once.
 // ---------------------------------------------------------------------------
-__global__ void k_bin(DevState S, Range r) {
-  if (S.gate[0] == 0) return;
-  GRID_STRIDE(i, r.p0, r.p1) {
-    const uint32_t a = S.attr[i];
-    const uint32_t t = attr_tissue(a);
-    if (S.gate[1 + t] == 0) continue;
+__global__ void k_gate_compact(DevState S, int32_t t0, int32_t t1) {
+  if (S.gate[0] == 0) {
+    if (threadIdx.x == 0) {
+      S.rl_count[0] = 0;
+      S.rl_ppre[0] = 0;
+      S.rl_bpre[0] = 0;
+    }
+    return;
+  }
+  int32_t cc = 0, cp = 0, cb = 0;
+  for (int32_t base = t0; base < t1; base += kScanThreads) {
+    const int32_t t = base + threadIdx.x;
+    const bool g = t < t1 && S.gate[1 + t] != 0;
+    int32_t np = 0, nb = 0;
+    if (g) {
+      const TissueDev& T = S.tissues[t];
+      np = T.n;
+      nb = T.anx * T.any * T.anz;
+    }
+    int32_t tc, tp, tb;
+    const int32_t oc = block_excl_scan(g ? 1 : 0, &tc);
+    const int32_t op = block_excl_scan(np, &tp);
+    const int32_t ob = block_excl_scan(nb, &tb);
+    if (g) {
+      S.rl_list[cc + oc] = t;
+      S.rl_ppre[cc + oc] = cp + op;
+      S.rl_bpre[cc + oc] = cb + ob;
+    }
+    cc += tc;
+    cp += tp;
+    cb += tb;
+  }
+  if (threadIdx.x == 0) {
+    S.rl_count[0] = cc;
+    S.rl_ppre[cc] = cp;
+    S.rl_bpre[cc] = cb;
+  }
+}
+
+// index k of the last prefix entry <= g (pre[0] = 0, non-decreasing, n+1 entries)
+__device__ __forceinline__ int32_t locate(const int32_t* pre, int32_t n, int32_t g) {
+  int32_t lo = 0, hi = n;  // answer in [lo, hi)
+  while (hi - lo > 1) {
+    const int32_t mid = (lo + hi) >> 1;
+    if (pre[mid] <= g) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Gated particle g -> global particle index (and its tissue).
+__device__ __forceinline__ int32_t gated_particle(const DevState& S, int32_t cnt, int32_t g,
+                                                  int32_t* tissue) {
+  const int32_t k = locate(S.rl_ppre, cnt, g);
+  const int32_t t = S.rl_list[k];
+  *tissue = t;
+  return S.tissues[t].pbase + (g - S.rl_ppre[k]);
+}
+
+#define GATED_PARTICLES(g, cnt)                                                        \
+  const int32_t cnt = S.rl_count[0];                                                   \
+  if (cnt == 0) return;                                                                \
+  const int32_t ngated_ = S.rl_ppre[cnt];                                              \
+  for (int32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ngated_;                 \
+       g += gridDim.x * blockDim.x)
+
+// Binning on the reference's 2.0 grid (grid_init, cell_connection.cpp:38-62).
+__global__ void k_bin(DevState S) {
+  GATED_PARTICLES(g, cnt) {
+    int32_t t;
+    const int32_t i = gated_particle(S, cnt, g, &t);
     const TissueDev& T = S.tissues[t];
     const double4 p = S.pos_cur[i];
     if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z)) {
-      raise_error(S.status, E_NONFINITE, (int32_t)i, -1, p.x);
+      raise_error(S.status, E_NONFINITE, i, -1, p.x);
       S.bin[i] = -1;
       continue;
     }
-    const int32_t lb = ref_bin(T, p.x, p.y, p.z, attr_state(a) == ST_MEMB);
+    const int32_t lb = ref_bin(T, p.x, p.y, p.z, attr_state(S.attr[i]) == ST_MEMB);
     if (lb < 0) {
-      raise_error(S.status, E_BIN_RANGE, (int32_t)i, -1, p.z);
+      raise_error(S.status, E_BIN_RANGE, i, -1, p.z);
       S.bin[i] = -1;
       continue;
     }
     const int32_t b = T.binbase + lb;
     const int32_t rk = atomicAdd(&S.counts[b], 1);
-    if (rk + 1 >= kBinCap) raise_error(S.status, E_BIN_OVERFLOW, (int32_t)i, b, (double)(rk + 1));
+    if (rk + 1 >= kBinCap) raise_error(S.status, E_BIN_OVERFLOW, i, b, (double)(rk + 1));
     S.bin[i] = b;
     S.rank[i] = rk;
   }
 }
 
-__global__ void k_scatter(DevState S, Range r) {
-  if (S.gate[0] == 0) return;
-  GRID_STRIDE(i, r.p0, r.p1) {
-    const uint32_t t = attr_tissue(S.attr[i]);
-    if (S.gate[1 + t] == 0) continue;
+// Per gated tissue, one block: exclusive scan of its bin counts into
+// starts, offset by the tissue's first particle, so each tissue's sorted
+// particles occupy its own slots [pbase, pbase + n). Each tissue's bins end
+// with a sentinel entry that receives the end offset.
+__global__ void k_scan_tissue(DevState S) {
+  const int32_t cnt = S.rl_count[0];
+  for (int32_t k = blockIdx.x; k < cnt; k += gridDim.x) {
+    const TissueDev& T = S.tissues[S.rl_list[k]];
+    const int32_t nb = T.anx * T.any * T.anz;
+    const int32_t* in = S.counts + T.binbase;
+    int32_t* out = S.starts + T.binbase;
+    int32_t carry = T.pbase;
+    for (int32_t base = 0; base < nb; base += kScanTile) {
+      const int32_t b0 = base + threadIdx.x * kScanItems;
+      int32_t v[kScanItems];
+      int32_t sum = 0;
+#pragma unroll
+      for (int q = 0; q < kScanItems; ++q) {
+        v[q] = b0 + q < nb ? in[b0 + q] : 0;
+        sum += v[q];
+      }
+      int32_t tot;
+      int32_t run = carry + block_excl_scan(sum, &tot);
+#pragma unroll
+      for (int q = 0; q < kScanItems; ++q) {
+        if (b0 + q < nb) out[b0 + q] = run;
+        run += v[q];
+      }
+      carry += tot;
+    }
+    if (threadIdx.x == 0) out[nb] = carry;
+    __syncthreads();
+  }
+}
+
+__global__ void k_scatter(DevState S) {
+  GATED_PARTICLES(g, cnt) {
+    int32_t t;
+    const int32_t i = gated_particle(S, cnt, g, &t);
     const int32_t b = S.bin[i];
     if (b < 0) continue;
     S.skey[S.starts[b] + S.rank[i]] = (uint32_t)i;
@@ -197,27 +299,31 @@ __global__ void k_scatter(DevState S, Range r) {
 
 // Per-bin insertion sort by particle index (bins hold a few to a few dozen
 // particles), then the sorted position copy the search streams through.
-// Bins of tissues that are not rebuilt are empty.
-__global__ void k_binsort(DevState S, Range r) {
-  if (S.gate[0] == 0) return;
-  GRID_STRIDE(b, r.b0, r.b1) {
+__global__ void k_binsort(DevState S) {
+  const int32_t cnt = S.rl_count[0];
+  if (cnt == 0) return;
+  const int32_t nbg = S.rl_bpre[cnt];
+  for (int32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < nbg; g += gridDim.x * blockDim.x) {
+    const int32_t k = locate(S.rl_bpre, cnt, g);
+    const int32_t b = S.tissues[S.rl_list[k]].binbase + (g - S.rl_bpre[k]);
     const int32_t s0 = S.starts[b], s1 = S.starts[b + 1];
     if (s1 <= s0) continue;
     S.counts[b] = 0;  // ready for the next binning
     for (int32_t s = s0 + 1; s < s1; ++s) {
       const uint32_t v = S.skey[s];
-      int32_t k = s - 1;
-      while (k >= s0 && S.skey[k] > v) {
-        S.skey[k + 1] = S.skey[k];
-        --k;
+      int32_t q = s - 1;
+      while (q >= s0 && S.skey[q] > v) {
+        S.skey[q + 1] = S.skey[q];
+        --q;
       }
-      S.skey[k + 1] = v;
+      S.skey[q + 1] = v;
     }
     for (int32_t s = s0; s < s1; ++s) {
-      const uint32_t g = S.skey[s];
-      const bool memb = attr_state(S.attr[g]) == ST_MEMB;
-      S.skey[s] = g | (memb ? 0x80000000u : 0u);
-      S.spos[s] = S.pos_cur[g];
+      const uint32_t gi = S.skey[s];
+      const bool memb = attr_state(S.attr[gi]) == ST_MEMB;
+      S.skey[s] = gi | (memb ? 0x80000000u : 0u);
+      const double4 pg = S.pos_cur[gi];
+      S.spos[s] = make_float4((float)pg.x, (float)pg.y, (float)pg.z, (float)pg.w);
     }
   }
 }
@@ -232,8 +338,10 @@ __device__ __forceinline__ int window_ranges(double x, double R, double L, int32
     hi[0] = an - 1;
     return 1;
   }
+  // floor(v / AG) through a multiply; the caller's window already carries a
+  // margin far wider than the rounding difference.
   auto bin_of = [&](double v) {
-    int32_t k = (int32_t)floor(v / kAreaGrid);
+    int32_t k = (int32_t)floor(v * (1.0 / kAreaGrid));
     return k < 0 ? 0 : (k > an - 1 ? an - 1 : k);
   };
   const double a = x - R, b = x + R;
@@ -260,26 +368,41 @@ __device__ __forceinline__ int window_ranges(double x, double R, double L, int32
 // every bin that can hold such a partner; the reference's fixed 5x5x5 window
 // is a superset for every pair it can connect (reach <= 1.2 * 3.2 < 2 * 2.0).
 // Candidates come out in bin order, deterministic after k_binsort.
-__global__ void k_cand_search(DevState S, Range r) {
-  if (S.gate[0] == 0) return;
-  GRID_STRIDE(i, r.p0, r.p1) {
+__global__ void k_cand_search(DevState S) {
+  // One warp per gated particle: the lanes stride the contiguous slots of
+  // each bin column, and ballots keep the candidates in slot order.
+  constexpr double kInvAG = 1.0 / kAreaGrid;
+  const int32_t cnt = S.rl_count[0];
+  if (cnt == 0) return;
+  const int32_t ngated = S.rl_ppre[cnt];
+  const int lane = threadIdx.x & 31;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  const int32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (int32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ngated; g += warps) {
+    int32_t t;
+    const int32_t i = gated_particle(S, cnt, g, &t);
     const uint32_t a = S.attr[i];
-    const uint32_t t = attr_tissue(a);
-    if (S.gate[1 + t] == 0) continue;
     const TissueDev& T = S.tissues[t];
     const bool memb_i = attr_state(a) == ST_MEMB;
     const double4 p = S.pos_cur[i];
     const double lt = T.P.lj_thresh;
     const double skin = S.skin;
-    const double R = lt * (p.w + (memb_i ? T.rmax_nm : T.rmax)) + skin + 1e-6;
+    // Candidates are compared in float: the margin covers the rounding of
+    // float coordinates up to the box size (and the window widens with it).
+    const double margin = 1e-4 + 5e-7 * (T.lx > T.ly ? T.lx : T.ly) + 5e-7 * T.lz;
+    const double R = lt * (p.w + (memb_i ? T.rmax_nm : T.rmax)) + skin + margin + 1e-6;
     int32_t xlo[2], xhi[2], ylo[2], yhi[2];
     const int nxr = window_ranges(p.x, R, T.lx, T.anx, xlo, xhi);
     const int nyr = window_ranges(p.y, R, T.ly, T.any, ylo, yhi);
-    int32_t z0 = (int32_t)floor((p.z - R) / kAreaGrid);
-    int32_t z1 = (int32_t)floor((p.z + R) / kAreaGrid);
+    int32_t z0 = (int32_t)floor((p.z - R) * kInvAG) - 1;
+    int32_t z1 = (int32_t)floor((p.z + R) * kInvAG) + 1;
     z0 = z0 < 0 ? 0 : (z0 > T.anz - 1 ? T.anz - 1 : z0);
     z1 = z1 < 0 ? 0 : (z1 > T.anz - 1 ? T.anz - 1 : z1);
+    const float px = (float)p.x, py = (float)p.y, pz = (float)p.z, pw = (float)p.w;
+    const float flx = (float)T.lx, fly = (float)T.ly, fhx = 0.5f * flx, fhy = 0.5f * fly;
+    const float flt = (float)lt, fskin = (float)(skin + margin);
     const int32_t cap = S.max_cand;
+    const int64_t N = S.n_total;
     int32_t count = 0;
     for (int xr = 0; xr < nxr; ++xr) {
       for (int32_t bx = xlo[xr]; bx <= xhi[xr]; ++bx) {
@@ -287,32 +410,50 @@ __global__ void k_cand_search(DevState S, Range r) {
           for (int32_t by = ylo[yr]; by <= yhi[yr]; ++by) {
             const int32_t col = T.binbase + (bx * T.any + by) * T.anz;
             const int32_t s_lo = S.starts[col + z0], s_hi = S.starts[col + z1 + 1];
-            for (int32_t s = s_lo; s < s_hi; ++s) {
-              const uint32_t key = S.skey[s];
-              const int32_t j = (int32_t)(key & 0x7fffffffu);
-              if (j == i || (memb_i && (key >> 31))) continue;
-              const double4 q = S.spos[s];
-              const double dx = pdiff(p.x, q.x, T.lx);
-              const double dy = pdiff(p.y, q.y, T.ly);
-              const double dz = p.z - q.z;
-              const double reach = lt * (p.w + q.w) + skin;
-              if (dx * dx + dy * dy + dz * dz > reach * reach * (1.0 + 1e-12)) continue;
-              if (count < cap) S.cand[(int64_t)count * S.n_total + i] = j;
-              ++count;
+            for (int32_t base = s_lo; base < s_hi; base += 32) {
+              const int32_t s = base + lane;
+              bool hit = false;
+              int32_t j = 0;
+              if (s < s_hi) {
+                const uint32_t key = S.skey[s];
+                j = (int32_t)(key & 0x7fffffffu);
+                if (j != i && !(memb_i && (key >> 31))) {
+                  const float4 q = S.spos[s];
+                  float dx = px - q.x, dy = py - q.y;
+                  dx = dx > fhx ? dx - flx : (dx <= -fhx ? dx + flx : dx);
+                  dy = dy > fhy ? dy - fly : (dy <= -fhy ? dy + fly : dy);
+                  const float dz = pz - q.z;
+                  const float reach = flt * (pw + q.w) + fskin;
+                  hit = dx * dx + dy * dy + dz * dz <= reach * reach;
+                }
+              }
+              const unsigned m = __ballot_sync(0xffffffffu, hit);
+              if (hit) {
+                const int32_t k = count + __popc(m & lt_mask);
+                if (k < cap) S.cand[(int64_t)k * N + i] = j;
+              }
+              count += __popc(m);
             }
           }
         }
       }
     }
-    if (count > cap) raise_error(S.status, E_LIST_OVERFLOW, (int32_t)i, -1, (double)count);
-    S.ncand[i] = count < cap ? count : cap;
-    S.bpos[i] = make_float4((float)p.x, (float)p.y, (float)p.z, 0.f);
+    if (lane == 0) {
+      if (count > cap) raise_error(S.status, E_LIST_OVERFLOW, i, -1, (double)count);
+      S.ncand[i] = count < cap ? count : cap;
+      S.bpos[i] = make_float4((float)p.x, (float)p.y, (float)p.z, 0.f);
+    }
   }
 }
 
-__global__ void k_gate_clear(DevState S, Range r, int32_t clear_any) {
-  GRID_STRIDE(t, r.t0, r.t1) S.gate[1 + t] = 0;
-  if (clear_any && blockIdx.x == 0 && threadIdx.x == 0) S.gate[0] = 0;
+__global__ void k_gate_clear(DevState S, int32_t clear_any) {
+  const int32_t cnt = S.rl_count[0];
+  for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x)
+    S.gate[1 + S.rl_list[k]] = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (cnt) atomicAdd(S.rebuilds, (unsigned long long)cnt);
+    if (clear_any) S.gate[0] = 0;
+  }
 }
 
 __global__ void k_gate_set_all(DevState S, int32_t ntissues) {
@@ -321,50 +462,33 @@ __global__ void k_gate_set_all(DevState S, int32_t ntissues) {
 }
 
 // ---------------------------------------------------------------------------
-// Prepass: _memb_bend_calc1 (cell_interaction.cpp:296-324) for every
-// membrane particle, find_dermis (cell_connection.cpp:158-172) for every
-// FIX / MUSUME cell, from the current positions. prep holds the membrane
-// particles of all tissues, then the FIX / MUSUME cells; [m0, m1) and
-// [f0, f1) select the entries of this launch.
+// find_dermis (cell_connection.cpp:158-172) for the FIX / MUSUME cells in
+// prep[f0, f1), from the current positions: the nearest connected membrane
+// particle, strict <, starting from LX*LX.
 // ---------------------------------------------------------------------------
-template <typename R>
-__global__ void k_prepass(DevState S, int32_t m0, int32_t m1, int32_t f0, int32_t f1) {
-  const int64_t nm = m1 - m0;
-  GRID_STRIDE(e, 0, nm + (f1 - f0)) {
-    const int32_t i = e < nm ? S.prep[m0 + e] : S.prep[f0 + (e - nm)];
-    const uint32_t a = S.attr[i];
-    const TissueDev& T = S.tissues[attr_tissue(a)];
+__global__ void k_dermis(DevState S, int32_t f0, int32_t f1) {
+  GRID_STRIDE(e, f0, f1) {
+    const int32_t i = S.prep[e];
+    const TissueDev& T = S.tissues[attr_tissue(S.attr[i])];
     const double4 p = S.pos_cur[i];
-    if (e < nm) {
-      const Lattice L = lattice_of(i - T.pbase, T.nmx, T.nmy);
-      const double4 pr = S.pos_cur[T.pbase + L.r];
-      const double4 pu = S.pos_cur[T.pbase + L.u];
-      const R nx = R(pdiff(pr.x, p.x, T.lx)), ny = R(pdiff(pr.y, p.y, T.ly)), nz = R(pr.z - p.z);
-      const R dn = sqrt(nx * nx + ny * ny + nz * nz);
-      S.sn[i] = make_double4(nx / dn, ny / dn, nz / dn, dn);
-      const R mx = R(pdiff(pu.x, p.x, T.lx)), my = R(pdiff(pu.y, p.y, T.ly)), mz = R(pu.z - p.z);
-      const R dm = sqrt(mx * mx + my * my + mz * mz);
-      S.sm[i] = make_double4(mx / dm, my / dm, mz / dm, dm);
-    } else {
-      const int32_t nc = S.ncand[i];
-      const double lt = T.P.lj_thresh;
-      int32_t best = -1;
-      double bestd = T.lx * T.lx;  // find_dermis starts from LX*LX
-      for (int32_t k = 0; k < nc; ++k) {
-        const int32_t q = S.cand[(int64_t)k * S.n_total + i];
-        if (attr_state(S.attr[q]) != ST_MEMB) continue;
-        const double4 pq = S.pos_cur[q];
-        const double d2 =
-            dist_sq_exact(pdiff(p.x, pq.x, T.lx), pdiff(p.y, pq.y, T.ly), p.z - pq.z);
-        if (!connected_pred(d2, lt, p.w, pq.w)) continue;
-        // strict <, as the reference; on exact ties the lowest index wins
-        if (d2 < bestd || (d2 == bestd && q < best)) {
-          bestd = d2;
-          best = q;
-        }
+    const int32_t nc = S.ncand[i];
+    const double lt = T.P.lj_thresh;
+    int32_t best = -1;
+    double bestd = T.lx * T.lx;
+    for (int32_t k = 0; k < nc; ++k) {
+      const int32_t q = S.cand[(int64_t)k * S.n_total + i];
+      if (attr_state(S.attr[q]) != ST_MEMB) continue;
+      const double4 pq = S.pos_cur[q];
+      const double d2 =
+          dist_sq_exact(pdiff(p.x, pq.x, T.lx), pdiff(p.y, pq.y, T.ly), p.z - pq.z);
+      if (!connected_pred(d2, lt, p.w, pq.w)) continue;
+      // on exact ties the lowest index wins (the reference: first in list order)
+      if (d2 < bestd || (d2 == bestd && q < best)) {
+        bestd = d2;
+        best = q;
       }
-      S.dermis[i] = best;
     }
+    S.dermis[i] = best;
   }
 }
 
@@ -375,20 +499,10 @@ __global__ void k_prepass(DevState S, int32_t m0, int32_t m1, int32_t f0, int32_
 // connect_cell would make. R is the arithmetic type of the force laws
 // (double: FP64 path; float: mixed path). Sums and positions stay double.
 // ---------------------------------------------------------------------------
-template <typename R>
-__device__ __forceinline__ R dot3(const double4& a, const double4& b) {
-  return R(a.x) * R(b.x) + R(a.y) * R(b.y) + R(a.z) * R(b.z);
-}
-
 // _memb_bend_diff_factor with NEW_BEND_POT (cell_interaction.cpp:349-360)
 template <typename R>
 __device__ __forceinline__ R bend_factor(R c) {
   return c >= R(0) ? (R(1) - c) : R(1) / ((R(1) + c) * (R(1) + c));
-}
-
-template <typename R>
-__device__ __forceinline__ R comp(const double4& v, int k) {
-  return R(k == 0 ? v.x : (k == 1 ? v.y : v.z));
 }
 
 // Separation of a pair as cell_interaction_apply computes it for its c1
@@ -406,56 +520,119 @@ __device__ __forceinline__ void pair_sep(const double4& p, const double4& pq, bo
   }
 }
 
-// Membrane particles: bending (_memb_bend_calc2 + _memb_bend_calc3,
-// :326-449, from calc1's scratch), the four lattice springs of
+// Reciprocal square root and division: correctly rounded in the FP64 path,
+// the hardware approximations (about 2 ulp) in the FP32 path.
+__device__ __forceinline__ float frsqrt(float v) { return rsqrtf(v); }
+__device__ __forceinline__ double frsqrt(double v) { return 1.0 / sqrt(v); }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
+
+template <typename R>
+struct Vec3 {
+  R x, y, z;
+};
+// Offset of a lattice neighbour from the particle (minimum image).
+template <typename R>
+__device__ __forceinline__ Vec3<R> offset_of(const double4& q, const double4& p,
+                                             const TissueDev& T) {
+  return Vec3<R>{R(pdiff_h(q.x, p.x, T.lx, T.hlx)), R(pdiff_h(q.y, p.y, T.ly, T.hly)),
+                 R(q.z - p.z)};
+}
+// Unit vector and length of b - a: the nv / dn (or mv / dm) that
+// _memb_bend_calc1 stores for a membrane particle (cell_interaction.cpp:296-309).
+template <typename R>
+struct Unit {
+  R x, y, z, d;
+};
+template <typename R>
+__device__ __forceinline__ Unit<R> unit_of(R x, R y, R z) {
+  const R s = x * x + y * y + z * z;
+  const R inv = frsqrt(s);
+  return Unit<R>{x * inv, y * inv, z * inv, s * inv};
+}
+template <typename R>
+__device__ __forceinline__ Unit<R> unit_ab(const Vec3<R>& a, const Vec3<R>& b) {
+  return unit_of(b.x - a.x, b.y - a.y, b.z - a.z);
+}
+template <typename R>
+__device__ __forceinline__ R dotu(const Unit<R>& a, const Unit<R>& b) {
+  return a.x * b.x + a.y * b.y + a.z * b.z;
+}
+template <typename R>
+__device__ __forceinline__ R cmp(const Unit<R>& v, int k) {
+  return k == 0 ? v.x : (k == 1 ? v.y : v.z);
+}
+
+// Membrane particles: bending (_memb_bend_calc1..3, :296-449; the unit
+// vectors of calc1 are recomputed from the eleven lattice positions the
+// stencil reaches instead of being stored), the four lattice springs of
 // _MEMB_interaction (:529-547, each applied once by the higher index) and
 // the wall (:287-294). The sum goes to S.fmemb; k_step adds it.
 template <typename R>
-__global__ void k_memb_force(DevState S, int32_t m0, int32_t m1) {
+__global__ void __launch_bounds__(256) k_memb_force(DevState S, int32_t m0, int32_t m1) {
   GRID_STRIDE(e, m0, m1) {
     const int32_t i = S.prep[e];
-    const uint32_t a = S.attr[i];
-    const TissueDev& T = S.tissues[attr_tissue(a)];
+    const TissueDev& T = S.tissues[attr_tissue(S.attr[i])];
     const Laws<R>& L = T.laws<R>();
-    const double4 p = S.pos_cur[i];
     const double dt = T.P.dt;
-    const int32_t pb = T.pbase;
-    const Lattice Lt = lattice_of(i - pb, T.nmx, T.nmy);
+    const int32_t pb = T.pbase, NMX = T.nmx, NMY = T.nmy;
+    const int32_t j = i - pb, jj = j % NMX, kk = j / NMX;
+    // lattice site at column jj+dj, row kk+dk with periodic wrap; the same
+    // wiring as _memb_init (cellmanager.cpp:114-158)
+    auto site = [&](int dj, int dk) {
+      int32_t c = jj + dj, w = kk + dk;
+      c += c < 0 ? NMX : 0;
+      c -= c >= NMX ? NMX : 0;
+      w += w < 0 ? NMY : 0;
+      w -= w >= NMY ? NMY : 0;
+      return pb + w * NMX + c;
+    };
+    const double4 p = S.pos_cur[i];
     double ax = 0.0, ay = 0.0, az = 0.0;
     {
-      const double4 nv = S.sn[i], nvr = S.sn[pb + Lt.r], nvl = S.sn[pb + Lt.l];
-      const double4 nvll = S.sn[pb + Lt.ll], nvbb = S.sn[pb + Lt.bb];
-      const double4 nvbbr = S.sn[pb + lattice_of(Lt.bb, T.nmx, T.nmy).r];
-      const double4 mv = S.sm[i], mvu = S.sm[pb + Lt.u], mvb = S.sm[pb + Lt.b];
-      const double4 mvbb = S.sm[pb + Lt.bb];
-      const R ipn = dot3<R>(nv, nvr), ipnl = dot3<R>(nvl, nv), ipnll = dot3<R>(nvll, nvl);
-      const R ipm = dot3<R>(mv, mvu), ipmb = dot3<R>(mvb, mv);
-      const R ipmbb = dot3<R>(nvbb, nvbbr);  // the reference reads memb_bb's ipn (:380)
-      const R dn = R(nv.w), dnl = R(nvl.w), dm = R(mv.w), dmb = R(mvb.w);
+      const Vec3<R> o_r = offset_of<R>(S.pos_cur[site(1, 0)], p, T);
+      const Vec3<R> o_rr = offset_of<R>(S.pos_cur[site(2, 0)], p, T);
+      const Vec3<R> o_l = offset_of<R>(S.pos_cur[site(-1, 0)], p, T);
+      const Vec3<R> o_ll = offset_of<R>(S.pos_cur[site(-2, 0)], p, T);
+      const Vec3<R> o_u = offset_of<R>(S.pos_cur[site(0, 1)], p, T);
+      const Vec3<R> o_uu = offset_of<R>(S.pos_cur[site(0, 2)], p, T);
+      const Vec3<R> o_b = offset_of<R>(S.pos_cur[site(0, -1)], p, T);
+      const Vec3<R> o_bb = offset_of<R>(S.pos_cur[site(0, -2)], p, T);
+      const Vec3<R> o_bbr = offset_of<R>(S.pos_cur[site(1, -2)], p, T);
+      const Vec3<R> o_bbrr = offset_of<R>(S.pos_cur[site(2, -2)], p, T);
+      const Vec3<R> o0{R(0), R(0), R(0)};
+      const Unit<R> nv = unit_ab(o0, o_r), nvr = unit_ab(o_r, o_rr);
+      const Unit<R> nvl = unit_ab(o_l, o0), nvll = unit_ab(o_ll, o_l);
+      const Unit<R> nvbb = unit_ab(o_bb, o_bbr), nvbbr = unit_ab(o_bbr, o_bbrr);
+      const Unit<R> mv = unit_ab(o0, o_u), mvu = unit_ab(o_u, o_uu);
+      const Unit<R> mvb = unit_ab(o_b, o0), mvbb = unit_ab(o_bb, o_b);
+      const R ipn = dotu(nv, nvr), ipnl = dotu(nvl, nv), ipnll = dotu(nvll, nvl);
+      const R ipm = dotu(mv, mvu), ipmb = dotu(mvb, mv);
+      const R ipmbb = dotu(nvbb, nvbbr);  // the reference reads memb_bb's ipn (:380)
       const R fn = bend_factor(ipn), fnl = bend_factor(ipnl), fnll = bend_factor(ipnll);
       const R fm = bend_factor(ipm), fmb = bend_factor(ipmb), fmbb = bend_factor(ipmbb);
       const R s = R(dt * T.P.kbend);
+      const R idn = fdiv(R(1), nv.d), idnl = fdiv(R(1), nvl.d);
+      const R idm = fdiv(R(1), mv.d), idmb = fdiv(R(1), mvb.d);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        const R n0 = comp<R>(nv, k), nr = comp<R>(nvr, k), nl = comp<R>(nvl, k),
-                nll = comp<R>(nvll, k);
-        const R m0 = comp<R>(mv, k), mu = comp<R>(mvu, k), mb = comp<R>(mvb, k),
-                mbb = comp<R>(mvbb, k);
-        const R f = -fn * (nr - ipn * n0) / dn +
-                    fnl * ((n0 - ipnl * nl) / dnl - (nl - ipnl * n0) / dn) +
-                    fnll * (nll - ipnll * nl) / dnl - fm * (mu - ipm * m0) / dm +
-                    fmb * ((m0 - ipmb * mb) / dmb - (mb - ipmb * m0) / dm) +
-                    fmbb * (mbb - ipmbb * mb) / dmb;
+        const R n0 = cmp(nv, k), nr = cmp(nvr, k), nl = cmp(nvl, k), nll = cmp(nvll, k);
+        const R m0 = cmp(mv, k), mu = cmp(mvu, k), mb = cmp(mvb, k), mbb = cmp(mvbb, k);
+        const R f = -fn * (nr - ipn * n0) * idn +
+                    fnl * ((n0 - ipnl * nl) * idnl - (nl - ipnl * n0) * idn) +
+                    fnll * (nll - ipnll * nl) * idnl - fm * (mu - ipm * m0) * idm +
+                    fmb * ((m0 - ipmb * mb) * idmb - (mb - ipmb * m0) * idm) +
+                    fmbb * (mbb - ipmbb * mb) * idmb;
         const double d = double(s * f);
         if (k == 0) ax += d;
         else if (k == 1) ay += d;
         else az += d;
       }
     }
-    const int32_t links[4] = {Lt.l, Lt.r, Lt.b, Lt.u};
+    const int32_t links[4] = {site(-1, 0), site(1, 0), site(0, -1), site(0, 1)};
 #pragma unroll
     for (int k = 0; k < kMembAdj; ++k) {
-      const int32_t q = pb + links[k];
+      const int32_t q = links[k];
       const double4 pq = S.pos_cur[q];
       const bool hi = i > q;
       double dx, dy, dz;
@@ -480,64 +657,67 @@ __global__ void k_memb_force(DevState S, int32_t m0, int32_t m1) {
   }
 }
 
-// The step proper, one thread per particle. kSimple: every cell of the batch
-// is ALIVE, DEAD or AIR (or a membrane particle) and none is paired; then
-// each connected pair receives exactly one application of
-// CI_al_air_de_to_al_air_de_fix_mu (:141-152): from the higher index when
-// both cells are ALIVE/DEAD/AIR (:566-570), from the cell's side when the
-// partner is a membrane particle (:573-575). kOld: some cell is older than
-// THRESH_SP, so the adhesion constant depends on both cells' ages.
+// The step proper. Per particle: connect_proc's exact predicate
+// (cell_connection.cpp:115-119) on every candidate, the law(s) the reference
+// applies to each connected pair, the particle's own terms, then pos_copy and
+// the single wrap of cell_pos_periodic_fix.
+//
+// kSimple: every cell of the batch is ALIVE, DEAD or AIR (or a membrane
+// particle) and none is paired; then each connected pair receives exactly
+// one application of CI_al_air_de_to_al_air_de_fix_mu (:141-152): from the
+// higher index when both cells are ALIVE/DEAD/AIR (:566-570), from the
+// cell's side when the partner is a membrane particle (:573-575). kOld: some
+// cell is older than THRESH_SP, so the adhesion constant depends on both
+// cells' ages.
 template <typename R, bool kSimple, bool kOld>
-__global__ void __launch_bounds__(256) k_step(DevState S, Range r) {
-  const int64_t i = r.p0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= r.p1) return;
-  const int64_t N = S.n_total;
-  const uint32_t a = __ldg(&S.attr[i]);
-  const uint32_t t = attr_tissue(a);
-  const TissueDev& T = S.tissues[t];
-  const Laws<R>& L = T.laws<R>();
-  const uint32_t st = attr_state(a);
-  const double4 p = S.pos_cur[i];
-  const double lx = T.lx, ly = T.ly, hlx = T.hlx, hly = T.hly;
-  const double lt2 = T.P.lj_thresh * T.P.lj_thresh;  // LJ_THRESH*LJ_THRESH, folded as the reference
-  const R dt = R(T.P.dt);
+struct Particle {
+  const DevState& S;
+  const int32_t i;
+  const uint32_t a;
+  const uint32_t t;
+  const uint32_t st;
+  const TissueDev& T;
+  const Laws<R>& L;
+  const double4 p;
+  const double lt2;  // LJ_THRESH * LJ_THRESH, folded as the reference does
+  const R dt;
   int32_t pair_i = -1, dermis_i = -1;
-  if (!kSimple && st != ST_MEMB) {
-    pair_i = __ldg(&S.pair[i]);
-    if (st == ST_FIX || st == ST_MUSUME) dermis_i = __ldg(&S.dermis[i]);
-  }
-  const bool old_i = attr_old(a);
   double ax = 0.0, ay = 0.0, az = 0.0;
 
-  // Candidates: connect_proc's exact predicate (cell_connection.cpp:115-119),
-  // then the law(s) the reference applies to the pair.
-  const int32_t nc = __ldg(&S.ncand[i]);
-  for (int32_t k = 0; k < nc; ++k) {
-    const int32_t q = __ldg(&S.cand[(int64_t)k * N + i]);
-    const double4 pq = S.pos_cur[q];
-    const double dx = pdiff_h(p.x, pq.x, lx, hlx), dy = pdiff_h(p.y, pq.y, ly, hly);
+  __device__ __forceinline__ Particle(const DevState& S_, int32_t i_)
+      : S(S_), i(i_), a(__ldg(&S_.attr[i_])), t(attr_tissue(a)), st(attr_state(a)),
+        T(S_.tissues[t]), L(T.laws<R>()), p(S_.pos_cur[i_]),
+        lt2(T.P.lj_thresh * T.P.lj_thresh), dt(R(T.P.dt)) {
+    if (!kSimple && st != ST_MEMB) {
+      pair_i = __ldg(&S.pair[i]);
+      if (st == ST_FIX || st == ST_MUSUME) dermis_i = __ldg(&S.dermis[i]);
+    }
+  }
+
+  __device__ __forceinline__ void candidate(int32_t q, const double4& pq) {
+    const double dx = pdiff_h(p.x, pq.x, T.lx, T.hlx), dy = pdiff_h(p.y, pq.y, T.ly, T.hly);
     const double dz = p.z - pq.z;
     const double d2e = dist_sq_exact(dx, dy, dz);
     const double rse = __dadd_rn(p.w, pq.w);
-    if (!(d2e <= __dmul_rn(__dmul_rn(lt2, rse), rse))) continue;
+    if (!(d2e <= __dmul_rn(__dmul_rn(lt2, rse), rse))) return;
     const R d2 = R(d2e);
     const R rs = R(rse);
     R coef;
     if (kSimple) {
-      const bool both_old = kOld && old_i && attr_old(__ldg(&S.attr[q]));
+      const bool both_old = kOld && attr_old(a) && attr_old(__ldg(&S.attr[q]));
       coef = L.aad(d2, rs, both_old);
-      if (fabs(coef) > R(1000)) raise_error(S.status, E_COEF_RANGE, (int32_t)i, q, double(coef));
+      if (fabs(coef) > R(1000)) raise_error(S.status, E_COEF_RANGE, i, q, double(coef));
     } else {
       const uint32_t aq = __ldg(&S.attr[q]);
       const uint32_t sq = attr_state(aq);
-      const bool both_old = old_i && attr_old(aq);
+      const bool both_old = attr_old(a) && attr_old(aq);
       coef = R(0);
       // the law i applies while iterating q (if i is not a membrane particle)
       if (st != ST_MEMB) {
-        const int law = law_of(st, (int32_t)i, pair_i, dermis_i, sq, q);
+        const int law = law_of(st, i, pair_i, dermis_i, sq, q);
         if (law != L_NONE) {
           const R c = eval_law<R>(law, L, d2, rs, both_old, attr_sfm(a));
-          if (fabs(c) > R(1000)) raise_error(S.status, E_COEF_RANGE, (int32_t)i, q, double(c));
+          if (fabs(c) > R(1000)) raise_error(S.status, E_COEF_RANGE, i, q, double(c));
           coef += c;
         }
       }
@@ -548,76 +728,112 @@ __global__ void __launch_bounds__(256) k_step(DevState S, Range r) {
           pair_q = __ldg(&S.pair[q]);
           dermis_q = __ldg(&S.dermis[q]);
         }
-        const int law = law_of(sq, q, pair_q, dermis_q, st, (int32_t)i);
+        const int law = law_of(sq, q, pair_q, dermis_q, st, i);
         if (law != L_NONE) {
           const R c = eval_law<R>(law, L, d2, rs, both_old, attr_sfm(aq));
-          if (fabs(c) > R(1000)) raise_error(S.status, E_COEF_RANGE, q, (int32_t)i, double(c));
+          if (fabs(c) > R(1000)) raise_error(S.status, E_COEF_RANGE, q, i, double(c));
           coef += c;
         }
       }
     }
-    const R sdt = dt * coef;
-    ax += double(sdt * R(dx));
-    ay += double(sdt * R(dy));
-    az += double(sdt * R(dz));
+    // DT * coef * separation (cell_interaction_apply, :56-58), summed in FP64
+    const double sdt = double(dt * coef);
+    ax = fma(sdt, dx, ax);
+    ay = fma(sdt, dy, ay);
+    az = fma(sdt, dz, az);
   }
 
-  if (st == ST_MEMB) {
-    const double4 f = S.fmemb[i];
-    ax += f.x;
-    ay += f.y;
-    az += f.z;
-  } else if (!kSimple) {
-    // wall_interaction (:287-294) for DER below its radius
-    if (st == ST_DER && p.z < p.w) {
-      const R z = R(p.z), rad = R(p.w);
-      const R distlj = R(2) * z;
-      const R lj6 = pow6(rad) / pow6(z);
-      const R ljm = L.eps4 * lj6 * (lj6 - R(1)) / (distlj * distlj);
-      az += double(dt * ljm * R(2) * z);
+  __device__ __forceinline__ void finish() {
+    if (st == ST_MEMB) {
+      const double4 f = S.fmemb[i];
+      ax += f.x;
+      ay += f.y;
+      az += f.z;
+    } else if (!kSimple) {
+      // wall_interaction (:287-294) for DER below its radius
+      if (st == ST_DER && p.z < p.w) {
+        const R z = R(p.z), rad = R(p.w);
+        const R distlj = R(2) * z;
+        const R lj6 = pow6(rad) / pow6(z);
+        const R ljm = L.eps4 * lj6 * (lj6 - R(1)) / (distlj * distlj);
+        az += double(dt * ljm * R(2) * z);
+      }
+      // _pair_interaction (:637-641), applied by the higher index of the pair
+      if (pair_i >= 0) {
+        const double4 pq = S.pos_cur[pair_i];
+        const bool hi = i > pair_i;
+        double dx, dy, dz;
+        pair_sep(p, pq, hi, T, dx, dy, dz);
+        const R d2 = R(dist_sq_exact(dx, dy, dz));
+        const R c = L.pair(d2, R(hi ? S.spr[i] : S.spr[pair_i]));
+        if (fabs(c) > R(1000)) raise_error(S.status, E_COEF_RANGE, i, pair_i, double(c));
+        const R sdt = dt * c;
+        ax += double(sdt * R(dx));
+        ay += double(sdt * R(dy));
+        az += double(sdt * R(dz));
+      }
     }
-    // _pair_interaction (:637-641), applied by the higher index of the pair
-    if (pair_i >= 0) {
-      const double4 pq = S.pos_cur[pair_i];
-      const bool hi = i > pair_i;
-      double dx, dy, dz;
-      pair_sep(p, pq, hi, T, dx, dy, dz);
-      const R d2 = R(dist_sq_exact(dx, dy, dz));
-      const R c = L.pair(d2, R(hi ? S.spr[i] : S.spr[pair_i]));
-      if (fabs(c) > R(1000)) raise_error(S.status, E_COEF_RANGE, (int32_t)i, pair_i, double(c));
-      const R sdt = dt * c;
-      ax += double(sdt * R(dx));
-      ay += double(sdt * R(dy));
-      az += double(sdt * R(dz));
+    // pos_copy + the single wrap of cell_pos_periodic_fix
+    const double lx = T.lx, ly = T.ly, hlx = T.hlx, hly = T.hly;
+    double nx = p.x + ax, ny = p.y + ay;
+    const double nz = p.z + az;
+    if (nx > lx) nx -= lx;
+    else if (nx < 0) nx += lx;
+    if (ny > ly) ny -= ly;
+    else if (ny < 0) ny += ly;
+    if (!isfinite(nx) || !isfinite(ny) || !isfinite(nz)) {
+      raise_error(S.status, E_NONFINITE, i, -1, nz);
+    } else if (!range_ok(T, nx, ny, nz, st == ST_MEMB)) {
+      raise_error(S.status, E_BIN_RANGE, i, -1, nz);
+    }
+    S.pos_nxt[i] = make_double4(nx, ny, nz, p.w);
+    // Candidate validity: rebuild the tissue once a particle moved skin/2.
+    const float4 b = S.bpos[i];
+    double ex = nx - (double)b.x, ey = ny - (double)b.y;
+    if (ex > hlx) ex -= lx;
+    else if (ex < -hlx) ex += lx;
+    if (ey > hly) ey -= ly;
+    else if (ey < -hly) ey += ly;
+    const double ez = nz - (double)b.z;
+    const double lim = 0.5 * S.skin - 1e-3;  // margin covers the float rounding of bpos
+    if (!(ex * ex + ey * ey + ez * ez <= lim * lim)) {
+      S.gate[1 + t] = 1;
+      S.gate[0] = 1;
     }
   }
+};
 
-  // pos_copy + the single wrap of cell_pos_periodic_fix
-  double nx = p.x + ax, ny = p.y + ay;
-  const double nz = p.z + az;
-  if (nx > lx) nx -= lx;
-  else if (nx < 0) nx += lx;
-  if (ny > ly) ny -= ly;
-  else if (ny < 0) ny += ly;
-  if (!isfinite(nx) || !isfinite(ny) || !isfinite(nz)) {
-    raise_error(S.status, E_NONFINITE, (int32_t)i, -1, nz);
-  } else if (!range_ok(T, nx, ny, nz, st == ST_MEMB)) {
-    raise_error(S.status, E_BIN_RANGE, (int32_t)i, -1, nz);
+// One thread per particle. The candidate chain index -> position is
+// software-pipelined: indices are loaded two candidates ahead (they stream
+// from HBM), positions one ahead (gathers from L1/L2), so neither latency is
+// paid serially per candidate. kMinBlocks bounds the registers so that that
+// many 256-thread blocks stay resident per SM.
+template <typename R, bool kSimple, bool kOld, int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) k_step(DevState S, Range r) {
+  const int64_t i = r.p0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= r.p1) return;
+  const int64_t N = S.n_total;
+  const int32_t nc = __ldg(&S.ncand[i]);
+  const int32_t* cp = S.cand + i;  // column-major: entry k at cp[k * N]
+  int32_t q1 = nc > 1 ? __ldg(cp + N) : 0;
+  int32_t q2 = nc > 2 ? __ldg(cp + 2 * N) : 0;
+  Particle<R, kSimple, kOld> P(S, (int32_t)i);
+  int32_t q0 = nc > 0 ? __ldg(cp) : 0;
+  double4 p0 = nc > 0 ? S.pos_cur[q0] : P.p;
+  cp += 3 * N;
+  for (int32_t k = 0; k < nc; ++k) {
+    const int32_t q = q0;
+    const double4 pq = p0;
+    q0 = q1;
+    q1 = q2;
+    if (k + 3 < nc) {
+      q2 = __ldg(cp);
+      cp += N;
+    }
+    if (k + 1 < nc) p0 = S.pos_cur[q0];
+    P.candidate(q, pq);
   }
-  S.pos_nxt[i] = make_double4(nx, ny, nz, p.w);
-  // Candidate validity: rebuild the tissue once a particle moved skin/2.
-  const float4 b = S.bpos[i];
-  double ex = nx - (double)b.x, ey = ny - (double)b.y;
-  if (ex > hlx) ex -= lx;
-  else if (ex < -hlx) ex += lx;
-  if (ey > hly) ey -= ly;
-  else if (ey < -hly) ey += ly;
-  const double ez = nz - (double)b.z;
-  const double lim = 0.5 * S.skin - 1e-3;  // margin covers the float rounding of bpos
-  if (!(ex * ex + ey * ey + ez * ez <= lim * lim)) {
-    S.gate[1 + t] = 1;
-    S.gate[0] = 1;
-  }
+  P.finish();
 }
 
 // connect_cell's lists (for export): the exact predicate over the candidates.
@@ -722,40 +938,35 @@ void launch_scan(const int32_t* in, int32_t* out, int32_t n, int32_t init,
   k_scan_final<<<nb, kScanThreads, 0, s>>>(in, out, n, sc.partial, init, gate);
 }
 
-void launch_rebuild(const DevState& S, const Range& r, const ScanScratch& sc,
+void launch_rebuild(const DevState& S, const Range& r, const ScanScratch&,
                     const LaunchCfg& lc, cudaStream_t s, Timer* tm) {
-  const int32_t np = r.p1 - r.p0, nbins = r.b1 - r.b0;
   const int B = lc.block;
+  const int grid = lc.num_sms * 8;
   timer_begin(tm, KC_REBUILD_BIN, s);
-  k_bin<<<stride_blocks(np, B, lc), B, 0, s>>>(S, r);
+  k_gate_compact<<<1, kScanThreads, 0, s>>>(S, r.t0, r.t1);
+  k_bin<<<grid, B, 0, s>>>(S);
   timer_end(tm, KC_REBUILD_BIN, s);
   timer_begin(tm, KC_REBUILD_SCAN, s);
-  launch_scan(S.counts + r.b0, S.starts + r.b0, nbins, r.p0, sc, S.gate, lc, s);
+  const int nt = r.t1 - r.t0;
+  k_scan_tissue<<<nt < lc.num_sms * 4 ? (nt > 0 ? nt : 1) : lc.num_sms * 4, kScanThreads, 0, s>>>(S);
   timer_end(tm, KC_REBUILD_SCAN, s);
   timer_begin(tm, KC_REBUILD_SORT, s);
-  k_scatter<<<stride_blocks(np, B, lc), B, 0, s>>>(S, r);
-  k_binsort<<<stride_blocks(nbins, B, lc), B, 0, s>>>(S, r);
+  k_scatter<<<grid, B, 0, s>>>(S);
+  k_binsort<<<grid, B, 0, s>>>(S);
   timer_end(tm, KC_REBUILD_SORT, s);
   timer_begin(tm, KC_REBUILD_SEARCH, s);
-  k_cand_search<<<stride_blocks(np, B, lc), B, 0, s>>>(S, r);
+  k_cand_search<<<grid, B, 0, s>>>(S);
   timer_end(tm, KC_REBUILD_SEARCH, s);
   timer_begin(tm, KC_GATE, s);
-  const int32_t nt = r.t1 - r.t0;
-  const bool whole = r.p0 == 0 && (int64_t)r.p1 == S.n_total;
-  k_gate_clear<<<stride_blocks(nt, B, lc), B, 0, s>>>(S, r, whole ? 1 : 0);
+  const bool whole = r.t0 == 0 && r.t1 == S.ntissues;
+  k_gate_clear<<<1, B, 0, s>>>(S, whole ? 1 : 0);
   timer_end(tm, KC_GATE, s);
 }
 
 void launch_prepass(const DevState& S, int32_t m0, int32_t m1, int32_t f0, int32_t f1,
                     int precision, const LaunchCfg& lc, cudaStream_t s, Timer* tm) {
-  const int64_t n = (int64_t)(m1 - m0) + (f1 - f0);
-  if (n <= 0) return;
+  if (m1 <= m0 && f1 <= f0) return;
   timer_begin(tm, KC_PREPASS, s);
-  const int g = stride_blocks(n, lc.block, lc);
-  if (precision == 1)
-    k_prepass<float><<<g, lc.block, 0, s>>>(S, m0, m1, f0, f1);
-  else
-    k_prepass<double><<<g, lc.block, 0, s>>>(S, m0, m1, f0, f1);
   if (m1 > m0) {
     const int gm = stride_blocks(m1 - m0, lc.block, lc);
     if (precision == 1)
@@ -763,18 +974,29 @@ void launch_prepass(const DevState& S, int32_t m0, int32_t m1, int32_t f0, int32
     else
       k_memb_force<double><<<gm, lc.block, 0, s>>>(S, m0, m1);
   }
+  if (f1 > f0) k_dermis<<<stride_blocks(f1 - f0, lc.block, lc), lc.block, 0, s>>>(S, f0, f1);
   timer_end(tm, KC_PREPASS, s);
+}
+
+template <typename R, bool kSimple, bool kOld>
+void launch_step_v(const DevState& S, const Range& r, const LaunchCfg& lc, cudaStream_t s) {
+  const int grid = blocks_for(r.p1 - r.p0, 256);
+  switch (lc.variant) {
+    case 2: k_step<R, kSimple, kOld, 5><<<grid, 256, 0, s>>>(S, r); break;
+    case 3: k_step<R, kSimple, kOld, 6><<<grid, 256, 0, s>>>(S, r); break;
+    case 4: k_step<R, kSimple, kOld, 3><<<grid, 256, 0, s>>>(S, r); break;
+    default: k_step<R, kSimple, kOld, 4><<<grid, 256, 0, s>>>(S, r); break;
+  }
 }
 
 template <typename R>
 void launch_step_r(const DevState& S, const Range& r, const LaunchCfg& lc, cudaStream_t s) {
-  const int grid = blocks_for(r.p1 - r.p0, 256);
   if (lc.simple && lc.any_old)
-    k_step<R, true, true><<<grid, 256, 0, s>>>(S, r);
+    launch_step_v<R, true, true>(S, r, lc, s);
   else if (lc.simple)
-    k_step<R, true, false><<<grid, 256, 0, s>>>(S, r);
+    launch_step_v<R, true, false>(S, r, lc, s);
   else
-    k_step<R, false, true><<<grid, 256, 0, s>>>(S, r);
+    launch_step_v<R, false, true>(S, r, lc, s);
 }
 
 void launch_step(const DevState& S, const Range& r, int precision, const LaunchCfg& lc,

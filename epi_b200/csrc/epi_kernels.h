@@ -23,6 +23,7 @@ struct LaunchCfg {
   int block;        // threads per block of the grid-stride kernels
   int simple;       // batch holds only ALIVE / DEAD / AIR / MEMB, no pairs
   int any_old;      // some cell is older than THRESH_SP
+  int variant;      // step-kernel instantiation (pipeline depth / residency), see epi_config
 };
 
 // Kernel classes, for per-class timing.

@@ -107,7 +107,12 @@ typedef struct epi_config {
   int32_t max_conn;   /* connections per particle (membrane lattice links are
                          extra); the reference allows 400 (define.h:80) */
   int32_t max_cand;   /* candidates per particle (>= max_conn) */
-  double skin;        /* candidate margin, > 0 (default 0.3) */
+  double skin;        /* candidate margin, > 0 (default 0.1) */
+  int32_t variant;    /* step-kernel register budget: 0 = default (1);
+                         1..4 = 4, 5, 6, 3 resident 256-thread blocks per SM.
+                         Same formulas; the compiler may fuse multiply-adds
+                         differently, so results agree to rounding. */
+  int32_t reserved;   /* must be 0 */
 } epi_config;
 
 typedef struct epi_ctx epi_ctx;
@@ -164,6 +169,9 @@ int epi_error_info(epi_ctx* ctx, int32_t* tissue, int32_t* particle, int32_t* ot
 
 /* The cudaStream_t the context launches on (as void*). */
 void* epi_stream(epi_ctx* ctx);
+/* Tissue candidate-list rebuilds since the context was created (the count
+ * the skin trades against candidate-list length). */
+int epi_rebuild_count(epi_ctx* ctx, int64_t* count);
 /* Per-kernel timing: runs nsteps (not graph-captured) recording CUDA events
  * around each kernel class on the context stream. ms receives the summed
  * milliseconds per class, launches the launch count per class, names the

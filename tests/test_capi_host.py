@@ -44,14 +44,17 @@ def test_default_params_equal_reference_constants(built):
 def test_create_rejects_bad_arguments(built):
     L = capi.lib()
     assert L.epi_create(None, None) == capi.EPI_ERR_INVALID_ARG
-    cfg = capi.ConfigC(0, 7, 64, 96, 0.3)  # unknown precision
+    cfg = capi.ConfigC(0, 7, 64, 96, 0.3, 0, 0)  # unknown precision
     h = ctypes.c_void_p()
     assert L.epi_create(ctypes.byref(h), ctypes.byref(cfg)) in (
         capi.EPI_ERR_INVALID_ARG, capi.EPI_ERR_NO_DEVICE)
-    cfg = capi.ConfigC(0, 1, 64, 32, 0.3)  # fewer candidates than connections
+    cfg = capi.ConfigC(0, 1, 64, 32, 0.3, 0, 0)  # fewer candidates than connections
     assert L.epi_create(ctypes.byref(h), ctypes.byref(cfg)) in (
         capi.EPI_ERR_INVALID_ARG, capi.EPI_ERR_NO_DEVICE)
-    cfg = capi.ConfigC(0, 1, 64, 96, -1.0)  # negative skin
+    cfg = capi.ConfigC(0, 1, 64, 96, -1.0, 0, 0)  # negative skin
+    assert L.epi_create(ctypes.byref(h), ctypes.byref(cfg)) in (
+        capi.EPI_ERR_INVALID_ARG, capi.EPI_ERR_NO_DEVICE)
+    cfg = capi.ConfigC(0, 1, 64, 96, 0.1, 9, 0)  # unknown step-kernel variant
     assert L.epi_create(ctypes.byref(h), ctypes.byref(cfg)) in (
         capi.EPI_ERR_INVALID_ARG, capi.EPI_ERR_NO_DEVICE)
     assert L.epi_step(None, 1) == capi.EPI_ERR_INVALID_ARG

@@ -24,9 +24,9 @@ TOL_FP64 = 1e-10
 TOL_MIXED = 1e-5
 
 
-def run_gpu(tissues, steps, precision=FP64, mode="eager", max_conn=64, skin=None):
+def run_gpu(tissues, steps, precision=FP64, mode="eager", max_conn=64, skin=None, variant=None):
     with capi.Context(precision=precision, max_conn=max_conn, max_cand=2 * max_conn,
-                      skin=skin) as ctx:
+                      skin=skin, variant=variant) as ctx:
         ctx.upload(tissues)
         if steps:
             ctx.step(steps, mode)
@@ -193,6 +193,22 @@ def test_simple_and_general_step_kernels_agree(built):
     assert rel_pos_err(tuple(a[sl] for a in pos_b), pos_s, t.lx, t.ly) <= 1e-13
     assert np.array_equal(off_b[: t.n + 1], off_s)
     assert np.array_equal(idx_b[: off_s[-1]], idx_s)
+
+
+@pytest.mark.parametrize("variant", [1, 2, 3, 4])
+def test_step_kernel_variants_agree(built, variant):
+    """Register-budget variants run the same formulas in the same order; only
+    the compiler's multiply-add fusion may differ (FP64: rounding level)."""
+    ts = [T.mixed_state_tissue(), T.config1(6)]
+    ref = run_gpu(ts, 40, FP64, max_conn=96, variant=0)
+    got = run_gpu(ts, 40, FP64, max_conn=96, variant=variant)
+    base = 0
+    for t in ts:
+        sl = slice(base, base + t.n)
+        assert rel_pos_err(tuple(a[sl] for a in got[0]), tuple(a[sl] for a in ref[0]),
+                           t.lx, t.ly) <= 1e-13
+        base += t.n
+    assert np.array_equal(ref[1], got[1]) and np.array_equal(ref[2], got[2])
 
 
 def test_repeat_runs_are_deterministic(built):
