@@ -40,7 +40,7 @@ EXPORTED = [
     "epi_upload", "epi_connect", "epi_interact_commit", "epi_step", "epi_step_graph",
     "epi_step_per_tissue", "epi_sync", "epi_num_particles", "epi_download_positions",
     "epi_upload_positions", "epi_get_connections", "epi_get_dermis", "epi_error_info",
-    "epi_stream", "epi_rebuild_count", "epi_time_kernels",
+    "epi_stream", "epi_rebuild_count", "epi_time_kernels", "epi_connect_noalloc",
 ]
 
 

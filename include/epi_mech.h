@@ -179,6 +179,42 @@ int epi_rebuild_count(epi_ctx* ctx, int64_t* count);
 int epi_time_kernels(epi_ctx* ctx, int32_t nsteps, int32_t max_classes, double* ms,
                      int32_t* launches, const char** names, int32_t* nclasses);
 
+/* ---- connect_cell of one tissue without any device allocation ------------
+ * No counterpart in the reference: it exists for callers that cannot let this
+ * library call cudaMalloc — applications whose device memory all belongs to
+ * another allocator (a framework's caching allocator, or a pool sized once at
+ * start-up against a fixed memory budget) and loops that must not allocate
+ * once they run. The caller owns every buffer; the working storage is one
+ * fixed file-scope device array (about 0.75 MB) that exists on every GPU
+ * that loads the library until the process exits.
+ *
+ * Inputs x, y, z, radius (n doubles each) and outputs conn (n * max_conn
+ * int32, row i at conn + i * max_conn) and count (n int32) are device memory.
+ * Particles [0, nmemb) are the square membrane (nmemb = nmx * nmy). On return
+ * the work is queued on `stream` (a cudaStream_t; NULL = the default stream)
+ * and nothing is synchronised. When the stream reaches it: count[i] is the
+ * length of connected_cell for particle i (membrane rows include their four
+ * lattice links) and row i holds the first min(count[i], max_conn) partner
+ * indices sorted ascending; count[i] > max_conn means the row overflowed;
+ * count[i] = -1 means particle i is outside the grid (the reference's range
+ * assert). The connection set is connect_proc's (cell_connection.cpp:70-129).
+ *
+ * Limits: n <= EPI_NOALLOC_MAX_PARTICLES and ANX*ANY*ANZ <=
+ * EPI_NOALLOC_MAX_BINS (ANX = (int)(lx/2 + 0.5), ANY likewise, ANZ =
+ * (int)(lz/2)); larger calls return EPI_ERR_INVALID_ARG and queue nothing.
+ * It calls no allocating routine. The first call on each device looks up the
+ * device address of the working array (cudaGetSymbolAddress); make that first
+ * call before any stream capture. Every call on a device shares the array and
+ * it keeps the last call's contents (each call clears what it needs); calls
+ * whose work overlaps on the GPU — on different streams or from different
+ * host threads — race on it. */
+#define EPI_NOALLOC_MAX_PARTICLES 40960
+#define EPI_NOALLOC_MAX_BINS 32768
+int epi_connect_noalloc(const double* x, const double* y, const double* z,
+                        const double* radius, int32_t n, int32_t nmemb, int32_t nmx,
+                        int32_t nmy, double lx, double ly, double lz, double lj_thresh,
+                        int32_t max_conn, int32_t* conn, int32_t* count, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
