@@ -128,11 +128,15 @@ int dev_alloc(T** p, size_t count) {
   return cuda_status(cudaMalloc((void**)p, sizeof(T) * count));
 }
 
-void free_buffers(epi_ctx* c) {
+void destroy_graphs(epi_ctx* c) {
   for (auto& g : c->graph) {
     if (g) cudaGraphExecDestroy(g);
     g = nullptr;
   }
+}
+
+void free_buffers(epi_ctx* c) {
+  destroy_graphs(c);
   void* ptrs[] = {c->tissues, c->pos[0], c->pos[1], c->attr, c->pair, c->spr, c->dermis,
                   c->cand, c->ncand, c->bpos, c->nbr, c->nn, c->fmemb, c->bin,
                   c->rank, c->counts, c->starts, c->skey, c->spos, c->gate, c->rl, c->prep,
@@ -462,7 +466,13 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
   }
   if (n > (int64_t)0x7fffffff || nbins > (int64_t)0x7ffffff0 || ntissues >= (1 << 24))
     return EPI_ERR_UNSUPPORTED;
-  free_buffers(c);
+  // A re-upload of the same shape (the per-step connect of an application
+  // that renews cell state on the host) keeps the device buffers.
+  const bool reuse = c->loaded && c->ntissues == ntissues && c->n == n && c->nbins == nbins;
+  const int32_t old_nprep = c->nprep;
+  destroy_graphs(c);
+  if (!reuse) free_buffers(c);
+  c->loaded = false;
   c->ntissues = ntissues;
   c->n = n;
   c->nbins = (int32_t)nbins;
@@ -544,7 +554,15 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
   std::vector<int32_t> prep(prep_m);
   prep.insert(prep.end(), prep_f.begin(), prep_f.end());
   const size_t C = (size_t)c->cfg.max_conn, CC = (size_t)c->cfg.max_cand;
-  if ((rc = dev_alloc(&c->tissues, ntissues)) || (rc = dev_alloc(&c->pos[0], n)) ||
+  if (reuse && (int32_t)prep.size() > old_nprep) {
+    cudaFree(c->prep);
+    c->prep = nullptr;
+    if ((rc = dev_alloc(&c->prep, prep.size()))) {
+      free_buffers(c);
+      return rc;
+    }
+  }
+  if (!reuse && ((rc = dev_alloc(&c->tissues, ntissues)) || (rc = dev_alloc(&c->pos[0], n)) ||
       (rc = dev_alloc(&c->pos[1], n)) || (rc = dev_alloc(&c->attr, n)) ||
       (rc = dev_alloc(&c->pair, n)) || (rc = dev_alloc(&c->spr, n)) ||
       (rc = dev_alloc(&c->dermis, n)) || (rc = dev_alloc(&c->cand, CC * n)) ||
@@ -556,14 +574,16 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
       (rc = dev_alloc(&c->skey, n)) || (rc = dev_alloc(&c->spos, n)) ||
       (rc = dev_alloc(&c->gate, (size_t)ntissues + 1)) ||
       (rc = dev_alloc(&c->rl, 3 + 3 * (size_t)ntissues)) ||
-      (rc = dev_alloc(&c->prep, prep.size())) || (rc = dev_alloc(&c->stage, 3 * (size_t)n))) {
+      (rc = dev_alloc(&c->prep, prep.size())) || (rc = dev_alloc(&c->stage, 3 * (size_t)n)))) {
     free_buffers(c);
     return rc;
   }
-  c->scan.capacity = (int32_t)((std::max<int64_t>(nbins, n) + kScanTile - 1) / kScanTile) + 1;
-  if ((rc = dev_alloc(&c->scan.partial, c->scan.capacity))) {
-    free_buffers(c);
-    return rc;
+  if (!reuse) {
+    c->scan.capacity = (int32_t)((std::max<int64_t>(nbins, n) + kScanTile - 1) / kScanTile) + 1;
+    if ((rc = dev_alloc(&c->scan.partial, c->scan.capacity))) {
+      free_buffers(c);
+      return rc;
+    }
   }
   cudaStream_t s = c->stream;
   EPI_CUDA(cudaMemcpyAsync(c->tissues, c->tissues_h.data(), sizeof(TissueDev) * ntissues,

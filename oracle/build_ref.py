@@ -20,7 +20,14 @@ Two variants per geometry:
            timed CPU baseline (AVX2/FMA level so the binary runs on any
            current x86 host).
 
-Usage: python oracle/build_ref.py [geometry ...]   (default: all known)
+A third variant, built on request (it needs epi_b200/libepi_mech.so):
+  dropin : the same harness with the reference's cell_connection.cpp and
+           cell_interaction.cpp replaced by the drop-in GPU mechanics
+           (epi_b200/shim/epi5_gpu_mechanics.cpp) and linked to the library;
+           every other translation unit is the reference's own. This is how
+           epi5_MT itself would be built against the library.
+
+Usage: python oracle/build_ref.py [--dropin] [geometry ...]   (default: all known)
 """
 from __future__ import annotations
 
@@ -32,6 +39,7 @@ from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent
 REF_DIR = Path(os.environ.get("EPI_REFERENCE_DIR", "/root/reference")) / "epi5_MT"
 OUT = HERE / "_ref"
 
@@ -136,20 +144,35 @@ def binary_path(name: str, variant: str) -> Path:
     return OUT / name / f"ref_harness_{variant}"
 
 
+DROPIN_SHIM = ROOT / "epi_b200" / "shim" / "epi5_gpu_mechanics.cpp"
+DROPIN_LIB = ROOT / "epi_b200" / "libepi_mech.so"
+# the two translation units the drop-in replaces
+DROPIN_REPLACED = ("cell_connection.cpp", "cell_interaction.cpp")
+
+
 def build(name: str, variant: str, jobs: int = 8) -> Path:
     overlay = write_overlay(name)
     odir = OUT / name / variant
     odir.mkdir(parents=True, exist_ok=True)
+    inc = ["-I", str(HERE / "tbb_shim"), "-I", str(REF_DIR), "-include", str(overlay)]
+    srcs = [REF_DIR / s for s in SOURCES] + [HERE / "ref_harness.cpp"]
+    libs = []
+    deps = []
     if variant == "serial":
         flags = ["-O2", "-ffp-contract=off"]
     elif variant == "omp":
         flags = ["-O3", "-march=x86-64-v3", "-fopenmp", "-DEPI_TBB_SHIM_OPENMP"]
+    elif variant == "dropin":
+        flags = ["-O2", "-ffp-contract=off"]
+        inc += ["-I", str(ROOT / "include")]
+        srcs = [s for s in srcs if s.name not in DROPIN_REPLACED] + [DROPIN_SHIM]
+        # relative rpath: the binary sits three levels below the repository root
+        libs = [f"-L{DROPIN_LIB.parent}", "-lepi_mech", "-Wl,-rpath,$ORIGIN/../../../epi_b200"]
+        deps = [DROPIN_LIB, ROOT / "include" / "epi_mech.h"]
     else:
         raise ValueError(variant)
-    inc = ["-I", str(HERE / "tbb_shim"), "-I", str(REF_DIR), "-include", str(overlay)]
-    srcs = [REF_DIR / s for s in SOURCES] + [HERE / "ref_harness.cpp"]
     out = binary_path(name, variant)
-    newest_src = max(p.stat().st_mtime for p in srcs + [overlay, Path(__file__)])
+    newest_src = max(p.stat().st_mtime for p in srcs + deps + [overlay, Path(__file__)])
     if out.exists() and out.stat().st_mtime > newest_src:
         return out
     work = []
@@ -158,7 +181,7 @@ def build(name: str, variant: str, jobs: int = 8) -> Path:
         work.append((["g++", *COMMON_FLAGS, *flags, *inc, "-c", str(s), "-o", str(obj)], obj))
     with ThreadPoolExecutor(max_workers=jobs) as ex:
         objs = list(ex.map(_compile, work))
-    link = ["g++", *flags, *[str(o) for o in objs], "-o", str(out)]
+    link = ["g++", *flags, *[str(o) for o in objs], *libs, "-o", str(out)]
     r = subprocess.run(link, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed: {r.stderr[-4000:]}")
@@ -170,12 +193,16 @@ def available() -> bool:
 
 
 def main(argv):
+    variants = ["serial", "omp"]
+    if "--dropin" in argv:
+        argv = [a for a in argv if a != "--dropin"]
+        variants.append("dropin")
     names = argv or list(GEOMETRIES)
     if not available():
         print(f"reference sources not found under {REF_DIR}; nothing built")
         return 0
     for name in names:
-        for variant in ("serial", "omp"):
+        for variant in variants:
             p = build(name, variant)
             print(p)
     return 0

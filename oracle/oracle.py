@@ -154,19 +154,23 @@ def reference_binary(t, variant: str = "serial") -> Optional[Path]:
     return p if p.exists() else None
 
 
-def run_reference(t, nsteps: int, every: int, variant: str = "serial"):
+def run_reference(t, nsteps: int, every: int, variant: str = "serial",
+                  env: Optional[dict] = None):
     """Run the compiled reference on `t` (default parameters only: the reference
-    fixes its constants at compile time). Returns the parsed frames."""
+    fixes its constants at compile time). Returns the parsed frames. `env`
+    adds environment variables (the dropin variant reads EPI_MECH_*)."""
     from epi_b200.tissue import read_reference_frames
     exe = reference_binary(t, variant)
     if exe is None:
         raise FileNotFoundError("compiled reference harness not built for this geometry")
+    full_env = dict(os.environ)
+    full_env.update(env or {})
     with tempfile.TemporaryDirectory() as d:
         cells = os.path.join(d, "cells.dat")
         out = os.path.join(d, "frames.bin")
         t.write_reference_file(cells)
         r = subprocess.run([str(exe), "run", cells, str(nsteps), out, str(every)],
-                           capture_output=True, text=True)
+                           capture_output=True, text=True, env=full_env)
         if r.returncode != 0:
             raise RuntimeError(f"reference harness failed ({r.returncode}): {r.stderr[-2000:]}")
         return read_reference_frames(out)

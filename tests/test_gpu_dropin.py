@@ -1,0 +1,61 @@
+"""The drop-in: epi5_MT's own step loop with connect_cell and cell_interaction
+replaced by epi_b200/shim/epi5_gpu_mechanics.cpp over the C ABI.
+
+The binary (oracle/_ref/<geometry>/ref_harness_dropin, built by
+`python oracle/build_ref.py --dropin` where the reference sources are) is the
+reference's harness compiled from the reference's own cellmanager, cell,
+cell_init, utils ... translation units; only the two mechanics files differ.
+Its frames must match the reference's golden frames to the library's FP64
+bars: lists and dermis bit-exact, positions within 1e-10 of L_x after 1000
+steps. In the default (mixed) precision the positions stay within 1e-5.
+"""
+import numpy as np
+import pytest
+
+from epi_b200 import tissue as T
+from oracle import oracle as O
+from tests.golden.make_golden import load
+from tests.helpers import lists_equal, list_diff_summary, rel_pos_err
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64 = 1e-10
+TOL_MIXED = 1e-5
+
+
+def _dropin_frames(t, steps, every, precision):
+    if O.reference_binary(t, "dropin") is None:
+        pytest.skip("drop-in harness not built (python oracle/build_ref.py --dropin)")
+    return O.run_reference(t, steps, every, variant="dropin",
+                           env={"EPI_MECH_PRECISION": precision})
+
+
+@pytest.mark.parametrize("name,factory,steps,every", [
+    ("c1", T.config1, 1000, 100),
+    ("mixed", T.mixed_state_tissue, 300, 50),
+])
+def test_dropin_fp64_matches_reference_frames(built, name, factory, steps, every):
+    t = factory()
+    golden = {f["step"]: f for f in load(name)}
+    frames = {f["step"]: f for f in _dropin_frames(t, steps, every, "fp64")}
+    fm = (t.state == T.FIX) | (t.state == T.MUSUME)
+    for s, g in golden.items():
+        f = frames[s]
+        err = rel_pos_err((f["x"], f["y"], f["z"]), (g["x"], g["y"], g["z"]), t.lx, t.ly)
+        assert err <= TOL_FP64, (name, s, err)
+        assert lists_equal(f["conn_off"], f["conn_idx"], g["conn_off"], g["conn_idx"]), \
+            list_diff_summary(f["conn_off"], f["conn_idx"], g["conn_off"], g["conn_idx"])
+        assert np.array_equal(f["dermis"][fm], g["dermis"][fm]), (name, s)
+        # positions come back wrapped into the box by the host's periodic fix
+        assert (f["x"] >= 0).all() and (f["x"] <= t.lx).all()
+        assert (f["y"] >= 0).all() and (f["y"] <= t.ly).all()
+
+
+def test_dropin_mixed_precision_within_bar(built):
+    t = T.config1()
+    golden = {f["step"]: f for f in load("c1")}
+    frames = {f["step"]: f for f in _dropin_frames(t, 1000, 100, "mixed")}
+    for s, g in golden.items():
+        f = frames[s]
+        err = rel_pos_err((f["x"], f["y"], f["z"]), (g["x"], g["y"], g["z"]), t.lx, t.ly)
+        assert err <= TOL_MIXED, (s, err)
