@@ -40,7 +40,8 @@ EXPORTED = [
     "epi_upload", "epi_connect", "epi_interact_commit", "epi_step", "epi_step_graph",
     "epi_step_per_tissue", "epi_sync", "epi_num_particles", "epi_download_positions",
     "epi_upload_positions", "epi_get_connections", "epi_get_dermis", "epi_error_info",
-    "epi_stream", "epi_rebuild_count", "epi_time_kernels", "epi_connect_noalloc",
+    "epi_stream", "epi_rebuild_count", "epi_time_kernels", "epi_adjoint",
+    "epi_connect_noalloc",
 ]
 
 
@@ -73,6 +74,13 @@ class TissueViewC(ctypes.Structure):
                 ("x", _dp), ("y", _dp), ("z", _dp), ("radius", _dp), ("agek", _dp),
                 ("spr_nat_len", _dp), ("state", _up), ("pair", _ip),
                 ("rest_div_times", _ip)]
+
+
+class LossC(ctypes.Structure):
+    _fields_ = [("target_x", ctypes.POINTER(ctypes.c_double)),
+                ("target_y", ctypes.POINTER(ctypes.c_double)),
+                ("target_z", ctypes.POINTER(ctypes.c_double)),
+                ("cells_only", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class ConfigC(ctypes.Structure):
@@ -120,6 +128,8 @@ def lib():
         L.epi_stream.restype = vp
         L.epi_time_kernels.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, _dp, _ip,
                                        ctypes.POINTER(ctypes.c_char_p), _ip]
+        L.epi_adjoint.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(LossC),
+                                  _dp, _dp]
         for f in EXPORTED:
             if f not in ("epi_params_default", "epi_config_default", "epi_strerror",
                          "epi_destroy", "epi_stream"):
@@ -227,6 +237,10 @@ class Context:
         _check(rc, "epi_upload")
 
     @property
+    def ntissues(self) -> int:
+        return len(self.tissues)
+
+    @property
     def n(self) -> int:
         v = ctypes.c_int64()
         _check(lib().epi_num_particles(self._h, ctypes.byref(v)), "epi_num_particles")
@@ -306,3 +320,19 @@ class Context:
                                       _ptr(launches, ctypes.c_int32), names,
                                       ctypes.byref(ncls)), "epi_time_kernels")
         return {names[k].decode(): (float(ms[k]), int(launches[k])) for k in range(ncls.value)}
+
+    def adjoint(self, nsteps: int, target, checkpoint_every: int = 20, cells_only: bool = True):
+        """epi_adjoint: runs nsteps steps and returns (loss per tissue, gradient
+        per tissue as an array (ntissues, 3): d loss / d (s_spring, s_eps,
+        s_bend)). `target` is (x, y, z) over all particles."""
+        tx, ty, tz = (np.ascontiguousarray(a, np.float64) for a in target)
+        assert len(tx) == len(ty) == len(tz) == self.n
+        spec = LossC(_ptr(tx, ctypes.c_double), _ptr(ty, ctypes.c_double),
+                     _ptr(tz, ctypes.c_double), 1 if cells_only else 0, 0)
+        nt = self.ntissues
+        loss = np.zeros(nt)
+        grad = np.zeros(3 * nt)
+        _check(lib().epi_adjoint(self._h, nsteps, checkpoint_every, ctypes.byref(spec),
+                                 _ptr(loss, ctypes.c_double), _ptr(grad, ctypes.c_double)),
+               "epi_adjoint")
+        return loss, grad.reshape(nt, 3)

@@ -1,0 +1,451 @@
+// Reverse-mode adjoint of the mechanics step, FP64.
+//
+// The step maps positions X_t to X_{t+1} = wrap(X_t + D(X_t; s)), where D is
+// the displacement cell_interaction accumulates (epi5_MT/cell_interaction.cpp
+// :648-685) and s = (s_spring, s_eps, s_bend) multiplies every spring
+// constant, eps_m and KBEND. The wrap is a translation by a box length, so
+// its derivative is the identity. Given lambda = dL/dX_{t+1}, one backward
+// step returns
+//   dL/dX_t = lambda + (dD/dX_t)^T lambda     and adds   (dD/ds)^T lambda
+// to the parameter gradient. The connection set of step t is the exact
+// predicate of connect_proc at X_t (piecewise constant in X), evaluated on
+// the Verlet candidates like the forward step.
+//
+// Terms of D for membrane particles and ALIVE / DEAD / AIR cells (the state
+// set the adjoint supports):
+//   pairs     D_i += DT c(r2) d_ij, c the law of the pair (ljmain below the
+//             radius sum, adhesion above, :103-152); J = c I + 2 c'(r2) d d^T
+//             and D_j gets -DT c d_ij, so (dD/dX)^T lambda at i is
+//             DT sum_j J (lambda_i - lambda_j): a gather over the same lists.
+//   lattice   the four lattice springs of _MEMB_interaction (CI_memb_to_memb,
+//             :185-234), the same gather over fixed partners.
+//   wall      z += DT W(z) for z < r (:287-294).
+//   bending   D_k += DT KBEND B_k(eleven lattice sites) (:296-449). Its
+//             vector-Jacobian product is derived by hand below; each
+//             membrane particle writes the products for the eleven sites of
+//             its stencil and every site gathers the eleven entries that
+//             name it, so no atomics are needed and results are
+//             deterministic.
+#include "epi_kernels.h"
+#include "epi_device.cuh"
+
+namespace epi {
+namespace {
+
+struct D3 {
+  double x, y, z;
+};
+__device__ __forceinline__ D3 d3(double x, double y, double z) { return D3{x, y, z}; }
+__device__ __forceinline__ D3 operator+(D3 a, D3 b) { return D3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ D3 operator-(D3 a, D3 b) { return D3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ D3 operator*(double s, D3 a) { return D3{s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ D3& operator+=(D3& a, D3 b) { return a = a + b; }
+__device__ __forceinline__ D3& operator-=(D3& a, D3 b) { return a = a - b; }
+__device__ __forceinline__ double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ D3 xyz(double4 v) { return D3{v.x, v.y, v.z}; }
+
+// A pair coefficient with its derivatives: c, dc/d(r2), and the parts of c
+// that scale with s_spring and with s_eps (each law is linear in them).
+struct LawD {
+  double c, dc_dr2, c_spring, c_eps;
+};
+
+// ljmain (:103-111): c = eps4 u (u - 1) / r2 with u = rs^6 / r2^3.
+__device__ __forceinline__ LawD ljmain_d(const Laws<double>& L, double r2, double rs) {
+  const double rs2 = rs * rs;
+  const double u = rs2 * rs2 * rs2 / (r2 * r2 * r2);
+  const double c = L.eps4 * u * (u - 1.0) / r2;
+  const double dc = -L.eps4 * u * (7.0 * u - 4.0) / (r2 * r2);
+  return LawD{c, dc, 0.0, c};
+}
+
+// CI_al_air_de_to_al_air_de_fix_mu (:141-152) with adhesion (:113-124).
+__device__ __forceinline__ LawD aad_d(const Laws<double>& L, double r2, double rs,
+                                      bool both_old) {
+  if (r2 < rs * rs) return ljmain_d(L, r2, rs);
+  const double k = both_old ? L.k_total : L.k_desmosome;
+  const double r = sqrt(r2);
+  const double y = r / rs - 1.0;
+  if (y + 1.0 > L.lj_thresh) return LawD{0.0, 0.0, 0.0, 0.0};
+  const double h = 1.0 - y * y / L.ljt1sq;
+  const double c = -(k / r) * y * h;
+  // dc/dr = k y h / r^2 - (k / r) (1 - 3 y^2 / a^2) / rs
+  const double dcdr = k * y * h / r2 - (k / r) * (1.0 - 3.0 * y * y / L.ljt1sq) / rs;
+  return LawD{c, dcdr / (2.0 * r), c, 0.0};
+}
+
+// CI_memb_to_memb (:185-234), three branches.
+__device__ __forceinline__ LawD memb_memb_d(const Laws<double>& L, double r2, double rs) {
+  const double P = L.p_memb;
+  const double rs2 = rs * rs;
+  const double cr2 = rs2 * P * P;
+  if (r2 < cr2) {
+    const double u = cr2 * cr2 * cr2 / (r2 * r2 * r2);
+    const double c = L.eps4 * u * (u - 1.0) / r2;
+    return LawD{c, -L.eps4 * u * (7.0 * u - 4.0) / (r2 * r2), 0.0, c};
+  }
+  const double r = sqrt(r2);
+  if (r2 < rs2) {
+    const double c = -(L.der_der_const / r) * (r / (rs * P) - 1.0);
+    return LawD{c, -L.der_der_const / (2.0 * r2 * r), c, 0.0};
+  }
+  const double lam = (1.0 + P) * rs;
+  const double v = lam - r;
+  const double cr = rs * P;
+  const double cr2v = cr * cr / (v * v);
+  const double u = cr2v * cr2v * cr2v;
+  const double c_spring = -(L.der_der_const / rs) * ((1.0 - P) / P);
+  const double vr = v * r;
+  const double c_eps = -L.eps4 * u * (u - 1.0) / vr;
+  // d/dr of u (u - 1) / (v r), with du/dr = 6 u / v and d(v r)/dr = v - r
+  const double dh = 6.0 * u * (2.0 * u - 1.0) / (v * vr) - u * (u - 1.0) * (v - r) / (vr * vr);
+  return LawD{c_spring + c_eps, -L.eps4 * dh / (2.0 * r), c_spring, c_eps};
+}
+
+// _memb_bend_diff_factor (:349-360) and its derivative.
+__device__ __forceinline__ double bf(double c) {
+  return c >= 0.0 ? 1.0 - c : 1.0 / ((1.0 + c) * (1.0 + c));
+}
+__device__ __forceinline__ double bf_d(double c) {
+  if (c >= 0.0) return -1.0;
+  const double e = 1.0 + c;
+  return -2.0 / (e * e * e);
+}
+
+// Unit vector of b - a with its length.
+struct U3 {
+  D3 v;
+  double len;
+};
+__device__ __forceinline__ U3 unit3(D3 a, D3 b) {
+  const D3 w = b - a;
+  const double len = sqrt(dot(w, w));
+  return U3{(1.0 / len) * w, len};
+}
+// Adjoint of w = b - a from the adjoints of the unit vector (ub) and of the
+// length (lb): w_bar = (ub - (ub . u) u) / len + lb u; b += w_bar, a -= w_bar.
+__device__ __forceinline__ void unit3_back(const U3& u, D3 ub, double lb, D3& abar, D3& bbar) {
+  const D3 w = (1.0 / u.len) * (ub - dot(ub, u.v) * u.v) + lb * u.v;
+  bbar += w;
+  abar -= w;
+}
+
+// Stencil slots of the bending term of particle k, as lattice offsets:
+// k, r, rr, l, ll, u, uu, b, bb, r of bb, rr of bb.
+constexpr int kSlots = 11;
+__constant__ int kSlotDj[kSlots] = {0, 1, 2, -1, -2, 0, 0, 0, 0, 1, 2};
+__constant__ int kSlotDk[kSlots] = {0, 0, 0, 0, 0, 1, 2, -1, -2, -2, -2};
+
+// One half of BCALC (:396-404) and its adjoint. With n, a (the right /
+// upper neighbour's vector), l, m (the left / lower ones), the lengths D, E
+// and the cosines p = n.a, q = l.n, w:
+//   T = -g(p) (a - p n) / D + g(q) ((n - q l) / E - (l - q n) / D)
+//       + g(w) (m - w l) / E.
+// Given ybar, returns y . T and accumulates the adjoints of n, a, l, m, D, E
+// and w (w's inputs differ between the two halves).
+struct HalfBar {
+  D3 n, a, l, m;
+  double D, E, w;
+};
+__device__ __forceinline__ double half_back(D3 yb, D3 n, D3 a, D3 l, D3 m, double D, double E,
+                                            double w, HalfBar& hb) {
+  const double p = dot(n, a), q = dot(l, n);
+  const double gp = bf(p), gq = bf(q), gw = bf(w);
+  const double yn = dot(yb, n), ya = dot(yb, a), yl = dot(yb, l), ym = dot(yb, m);
+  const double iD = 1.0 / D, iE = 1.0 / E;
+  const double val = -gp * (ya - p * yn) * iD + gq * ((yn - q * yl) * iE - (yl - q * yn) * iD) +
+                     gw * (ym - w * yl) * iE;
+  const double pb = (-bf_d(p) * (ya - p * yn) + gp * yn) * iD;
+  const double qb = bf_d(q) * ((yn - q * yl) * iE - (yl - q * yn) * iD) + gq * (yn * iD - yl * iE);
+  hb.w = bf_d(w) * (ym - w * yl) * iE - gw * yl * iE;
+  hb.a = (-gp * iD) * yb + pb * n;
+  hb.n = (gp * p * iD + gq * iE + gq * q * iD) * yb + pb * a + qb * l;
+  hb.l = (-gq * q * iE - gq * iD - gw * w * iE) * yb + qb * n;
+  hb.m = (gw * iE) * yb;
+  hb.D = (gp * (ya - p * yn) + gq * (yl - q * yn)) * iD * iD;
+  hb.E = -(gq * (yn - q * yl) + gw * (ym - w * yl)) * iE * iE;
+  return val;
+}
+
+// Membrane particles: bending, lattice-spring and wall adjoints. Writes the
+// bending products for the eleven stencil sites to bend[e * 11 + slot], the
+// lattice + wall product at the particle itself to madj[e], and the
+// parameter partials to gmemb[e].
+__global__ void __launch_bounds__(256) k_adj_memb(DevState S, const double4* __restrict__ lam,
+                                                  double4* __restrict__ bend,
+                                                  double4* __restrict__ madj,
+                                                  double4* __restrict__ gmemb) {
+  GRID_STRIDE(e, 0, S.nprep_memb) {
+    const int32_t i = S.prep[e];
+    const TissueDev& T = S.tissues[attr_tissue(S.attr[i])];
+    const Laws<double>& L = T.lawd;
+    const double dt = T.P.dt;
+    const int32_t pb = T.pbase, NMX = T.nmx, NMY = T.nmy;
+    const int32_t j = i - pb, jj = j % NMX, kk = j / NMX;
+    auto site = [&](int dj, int dk) {
+      int32_t c = jj + dj, w = kk + dk;
+      c += c < 0 ? NMX : 0;
+      c -= c >= NMX ? NMX : 0;
+      w += w < 0 ? NMY : 0;
+      w -= w >= NMY ? NMY : 0;
+      return pb + w * NMX + c;
+    };
+    const double4 p = S.pos_cur[i];
+    const D3 li = xyz(lam[i]);
+    double g_spring = 0.0, g_eps = 0.0, g_bend = 0.0;
+    // --- bending: forward recompute of the stencil, then its adjoint
+    D3 o[kSlots];
+    o[0] = d3(0.0, 0.0, 0.0);
+#pragma unroll
+    for (int s = 1; s < kSlots; ++s) {
+      const Vec3<double> v = offset_of<double>(S.pos_cur[site(kSlotDj[s], kSlotDk[s])], p, T);
+      o[s] = d3(v.x, v.y, v.z);
+    }
+    const U3 nv = unit3(o[0], o[1]), nvr = unit3(o[1], o[2]);
+    const U3 nvl = unit3(o[3], o[0]), nvll = unit3(o[4], o[3]);
+    const U3 mv = unit3(o[0], o[5]), mvu = unit3(o[5], o[6]);
+    const U3 mvb = unit3(o[7], o[0]), mvbb = unit3(o[8], o[7]);
+    const U3 nvbb = unit3(o[8], o[9]), nvbbr = unit3(o[9], o[10]);
+    const double sb = dt * T.P.kbend;
+    const D3 yb = sb * li;
+    HalfBar hn, hm;
+    const double ipnll = dot(nvll.v, nvl.v);
+    const double ipmbb = dot(nvbb.v, nvbbr.v);  // memb_bb's ipn (:380)
+    const double fn = half_back(yb, nv.v, nvr.v, nvl.v, nvll.v, nv.len, nvl.len, ipnll, hn);
+    const double fm = half_back(yb, mv.v, mvu.v, mvb.v, mvbb.v, mv.len, mvb.len, ipmbb, hm);
+    g_bend = fn + fm;  // lambda . (dt kbend BCALC): d/ds_bend of the bending term
+    D3 ob[kSlots];
+#pragma unroll
+    for (int s = 0; s < kSlots; ++s) ob[s] = d3(0.0, 0.0, 0.0);
+    // ipnll = nvll . nvl
+    hn.m += hn.w * nvl.v;
+    hn.l += hn.w * nvll.v;
+    unit3_back(nv, hn.n, hn.D, ob[0], ob[1]);
+    unit3_back(nvr, hn.a, 0.0, ob[1], ob[2]);
+    unit3_back(nvl, hn.l, hn.E, ob[3], ob[0]);
+    unit3_back(nvll, hn.m, 0.0, ob[4], ob[3]);
+    unit3_back(mv, hm.n, hm.D, ob[0], ob[5]);
+    unit3_back(mvu, hm.a, 0.0, ob[5], ob[6]);
+    unit3_back(mvb, hm.l, hm.E, ob[7], ob[0]);
+    unit3_back(mvbb, hm.m, 0.0, ob[8], ob[7]);
+    // ipmbb = nvbb . nvbbr
+    unit3_back(nvbb, hm.w * nvbbr.v, 0.0, ob[8], ob[9]);
+    unit3_back(nvbbr, hm.w * nvbb.v, 0.0, ob[9], ob[10]);
+    // o[s] = x_site - x_k: the particle itself receives minus every offset's
+    // adjoint (o[0] is the constant zero)
+    D3 self = d3(0.0, 0.0, 0.0);
+#pragma unroll
+    for (int s = 1; s < kSlots; ++s) {
+      self -= ob[s];
+      bend[e * kSlots + s] = make_double4(ob[s].x, ob[s].y, ob[s].z, 0.0);
+    }
+    bend[e * kSlots] = make_double4(self.x, self.y, self.z, 0.0);
+    // --- lattice springs (each pair from both sides: gather)
+    D3 mu = d3(0.0, 0.0, 0.0);
+    const int32_t links[4] = {site(-1, 0), site(1, 0), site(0, -1), site(0, 1)};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int32_t q = links[k];
+      const double4 pq = S.pos_cur[q];
+      double dx, dy, dz;
+      pair_sep(p, pq, i > q, T, dx, dy, dz);
+      const D3 d = d3(dx, dy, dz);
+      const LawD w = memb_memb_d(L, dist_sq_exact(dx, dy, dz), p.w + pq.w);
+      const D3 dl = li - xyz(lam[q]);
+      mu += dt * (w.c * dl + (2.0 * w.dc_dr2 * dot(d, dl)) * d);
+      const double ld = dot(li, d);
+      g_spring += dt * w.c_spring * ld;
+      g_eps += dt * w.c_eps * ld;
+    }
+    // --- wall: dz = dt eps4 u (u - 1) / (2 z), u = (r / z)^6
+    if (p.z < p.w) {
+      const double z = p.z;
+      const double rz = p.w / z;
+      const double rz2 = rz * rz;
+      const double u = rz2 * rz2 * rz2;
+      const double W = dt * L.eps4 * u * (u - 1.0) / (2.0 * z);
+      const double dW = -dt * L.eps4 * u * (13.0 * u - 7.0) / (2.0 * z * z);
+      mu.z += dW * li.z;
+      g_eps += W * li.z;
+    }
+    madj[e] = make_double4(mu.x, mu.y, mu.z, 0.0);
+    gmemb[e] = make_double4(g_spring, g_eps, g_bend, 0.0);
+  }
+}
+
+// Every particle: pair adjoint over the exact connections at X_t, plus the
+// membrane terms, into lam_out; parameter partials into gpart.
+__global__ void __launch_bounds__(256) k_adj_pairs(DevState S, const double4* __restrict__ lam,
+                                                   double4* __restrict__ lam_out,
+                                                   const double4* __restrict__ bend,
+                                                   const double4* __restrict__ madj,
+                                                   const double4* __restrict__ gmemb,
+                                                   double4* __restrict__ gpart) {
+  const int64_t N = S.n_total;
+  GRID_STRIDE(i, 0, N) {
+    const uint32_t a = S.attr[i];
+    const TissueDev& T = S.tissues[attr_tissue(a)];
+    const Laws<double>& L = T.lawd;
+    const double dt = T.P.dt;
+    const double lt2 = T.P.lj_thresh * T.P.lj_thresh;
+    const double4 p = S.pos_cur[i];
+    const D3 li = xyz(lam[i]);
+    D3 mu = li;
+    double g_spring = 0.0, g_eps = 0.0, g_bend = 0.0;
+    const int32_t nc = S.ncand[i];
+    for (int32_t k = 0; k < nc; ++k) {
+      const int32_t q = S.cand[(int64_t)k * N + i];
+      const double4 pq = S.pos_cur[q];
+      const double dx = pdiff_h(p.x, pq.x, T.lx, T.hlx), dy = pdiff_h(p.y, pq.y, T.ly, T.hly);
+      const double dz = p.z - pq.z;
+      const double r2 = dist_sq_exact(dx, dy, dz);
+      const double rs = __dadd_rn(p.w, pq.w);
+      if (!(r2 <= __dmul_rn(__dmul_rn(lt2, rs), rs))) continue;  // connect_proc :115-119
+      const bool both_old = attr_old(a) && attr_old(S.attr[q]);
+      const LawD w = aad_d(L, r2, rs, both_old);
+      const D3 d = d3(dx, dy, dz);
+      const D3 dl = li - xyz(lam[q]);
+      mu += dt * (w.c * dl + (2.0 * w.dc_dr2 * dot(d, dl)) * d);
+      const double ld = dot(li, d);
+      g_spring += dt * w.c_spring * ld;
+      g_eps += dt * w.c_eps * ld;
+    }
+    if (attr_state(a) == ST_MEMB) {
+      const int32_t j = (int32_t)i - T.pbase;
+      const int32_t e = T.mbase + j;
+      const int32_t NMX = T.nmx, NMY = T.nmy, jj = j % NMX, kk = j / NMX;
+      mu += xyz(madj[e]);
+      const double4 gm = gmemb[e];
+      g_spring += gm.x;
+      g_eps += gm.y;
+      g_bend += gm.z;
+      // bending products naming this site: slot s of the particle at
+      // (jj - dj_s, kk - dk_s)
+#pragma unroll
+      for (int s = 0; s < kSlots; ++s) {
+        int32_t c = jj - kSlotDj[s], w = kk - kSlotDk[s];
+        c += c < 0 ? NMX : 0;
+        c -= c >= NMX ? NMX : 0;
+        w += w < 0 ? NMY : 0;
+        w -= w >= NMY ? NMY : 0;
+        mu += xyz(bend[(int64_t)(T.mbase + w * NMX + c) * kSlots + s]);
+      }
+    }
+    lam_out[i] = make_double4(mu.x, mu.y, mu.z, 0.0);
+    gpart[i] = make_double4(g_spring, g_eps, g_bend, 0.0);
+  }
+}
+
+// lambda at the last step: dL/dX_T of L_t = inv_cnt[t] sum |X_T - X*|^2 over
+// the loss set (minimum image in x and y); the loss terms go to gpart.w.
+__global__ void k_adj_seed(DevState S, const double* __restrict__ target, int32_t cells_only,
+                           const double* __restrict__ inv_cnt, double4* __restrict__ lam,
+                           double4* __restrict__ gpart) {
+  const int64_t N = S.n_total;
+  GRID_STRIDE(i, 0, N) {
+    const uint32_t a = S.attr[i];
+    const uint32_t t = attr_tissue(a);
+    const TissueDev& T = S.tissues[t];
+    const double4 p = S.pos_cur[i];
+    const bool in = !(cells_only && attr_state(a) == ST_MEMB);
+    const double w = in ? inv_cnt[t] : 0.0;
+    const double dx = pdiff(p.x, target[i], T.lx);
+    const double dy = pdiff(p.y, target[N + i], T.ly);
+    const double dz = p.z - target[2 * N + i];
+    lam[i] = make_double4(2.0 * w * dx, 2.0 * w * dy, 2.0 * w * dz, 0.0);
+    gpart[i] = make_double4(0.0, 0.0, 0.0, w * (dx * dx + dy * dy + dz * dz));
+  }
+}
+
+// Per tissue, in a fixed order: acc[4 t + c] += sum over its particles of
+// gpart[i].{x, y, z, w}.
+__global__ void __launch_bounds__(256) k_tissue_sum(DevState S, const double4* __restrict__ gpart,
+                                                    double* __restrict__ acc) {
+  __shared__ double4 sh[256];
+  for (int32_t t = blockIdx.x; t < S.ntissues; t += gridDim.x) {
+    const TissueDev& T = S.tissues[t];
+    double4 s = make_double4(0.0, 0.0, 0.0, 0.0);
+    for (int32_t k = threadIdx.x; k < T.n; k += blockDim.x) {
+      const double4 g = gpart[T.pbase + k];
+      s.x += g.x;
+      s.y += g.y;
+      s.z += g.z;
+      s.w += g.w;
+    }
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+      if ((int)threadIdx.x < h) {
+        const double4 o = sh[threadIdx.x + h];
+        sh[threadIdx.x].x += o.x;
+        sh[threadIdx.x].y += o.y;
+        sh[threadIdx.x].z += o.z;
+        sh[threadIdx.x].w += o.w;
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      acc[4 * t + 0] += sh[0].x;
+      acc[4 * t + 1] += sh[0].y;
+      acc[4 * t + 2] += sh[0].z;
+      acc[4 * t + 3] += sh[0].w;
+    }
+    __syncthreads();
+  }
+}
+
+// Flags the tissues whose particles moved more than skin/2 from the
+// positions of their last candidate rebuild (the forward step's test, for
+// positions loaded from a checkpoint or a stored step).
+__global__ void k_gate_check(DevState S) {
+  GRID_STRIDE(i, 0, S.n_total) {
+    const uint32_t t = attr_tissue(S.attr[i]);
+    const TissueDev& T = S.tissues[t];
+    const double4 p = S.pos_cur[i];
+    const float4 b = S.bpos[i];
+    double ex = p.x - (double)b.x, ey = p.y - (double)b.y;
+    if (ex > T.hlx) ex -= T.lx;
+    else if (ex < -T.hlx) ex += T.lx;
+    if (ey > T.hly) ey -= T.ly;
+    else if (ey < -T.hly) ey += T.ly;
+    const double ez = p.z - (double)b.z;
+    const double lim = 0.5 * S.skin - 1e-3;
+    if (!(ex * ex + ey * ey + ez * ez <= lim * lim)) {
+      S.gate[1 + t] = 1;
+      S.gate[0] = 1;
+    }
+  }
+}
+
+}  // namespace
+
+void launch_gate_check(const DevState& S, const LaunchCfg& lc, cudaStream_t s) {
+  if (S.n_total > 0)
+    k_gate_check<<<stride_blocks(S.n_total, lc.block, lc), lc.block, 0, s>>>(S);
+}
+
+void launch_adjoint_seed(const DevState& S, const double* target, int32_t cells_only,
+                         const double* inv_cnt, double4* lam, double4* gpart,
+                         const LaunchCfg& lc, cudaStream_t s) {
+  if (S.n_total > 0)
+    k_adj_seed<<<stride_blocks(S.n_total, lc.block, lc), lc.block, 0, s>>>(
+        S, target, cells_only, inv_cnt, lam, gpart);
+}
+
+void launch_adjoint_step(const DevState& S, const AdjointBuffers& B, const LaunchCfg& lc,
+                         cudaStream_t s) {
+  if (S.nprep_memb > 0)
+    k_adj_memb<<<stride_blocks(S.nprep_memb, 256, lc), 256, 0, s>>>(S, B.lam_in, B.bend, B.madj,
+                                                                     B.gmemb);
+  if (S.n_total > 0)
+    k_adj_pairs<<<blocks_for(S.n_total, 256), 256, 0, s>>>(S, B.lam_in, B.lam_out, B.bend, B.madj,
+                                                           B.gmemb, B.gpart);
+}
+
+void launch_tissue_sum(const DevState& S, const double4* gpart, double* acc, const LaunchCfg& lc,
+                       cudaStream_t s) {
+  const int grid = S.ntissues < lc.num_sms * 8 ? S.ntissues : lc.num_sms * 8;
+  if (grid > 0) k_tissue_sum<<<grid, 256, 0, s>>>(S, gpart, acc);
+}
+
+}  // namespace epi

@@ -346,6 +346,22 @@ int validate_tissue(const epi_tissue_view& v, const epi_params& P) {
 
 }  // namespace
 
+namespace {
+// Device allocations released when the call returns.
+struct ScopedDeviceMemory {
+  std::vector<void*> ptrs;
+  ~ScopedDeviceMemory() {
+    for (void* p : ptrs) cudaFree(p);
+  }
+  template <typename T>
+  int get(T** p, size_t count) {
+    const int rc = dev_alloc(p, count);
+    if (rc == EPI_OK) ptrs.push_back(*p);
+    return rc;
+  }
+};
+}  // namespace
+
 extern "C" {
 
 void epi_params_default(epi_params* p) {
@@ -502,6 +518,7 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
     T.any = (int32_t)(v.ly / 2.0 + 0.5);
     T.anz = (int32_t)(v.lz / 2.0);
     T.binbase = binbase;
+    T.mbase = (int32_t)prep_m.size();
     T.lx = v.lx;
     T.ly = v.ly;
     T.lz = v.lz;
@@ -606,6 +623,96 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
   launch_set_gates(make_state(c, c->cur), ntissues, s);
   // all pending host copies read std::vector storage: finish before return
   return materialize(c);
+  EPI_GUARD_END
+}
+
+int epi_adjoint(epi_ctx* c, int32_t nsteps, int32_t K, const epi_loss* loss, double* loss_out,
+                double* grad) {
+  if (!c || nsteps < 0 || K < 1 || !loss || !loss->target_x || !loss->target_y ||
+      !loss->target_z || loss->reserved != 0 || (loss->cells_only != 0 && loss->cells_only != 1))
+    return EPI_ERR_INVALID_ARG;
+  if (!c->loaded) return EPI_ERR_STATE;
+  if (!c->lc.simple) return EPI_ERR_UNSUPPORTED;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  const size_t n = (size_t)c->n;
+  const int32_t nt = c->ntissues;
+  const int32_t nseg = (nsteps + K - 1) / K;
+  const size_t hist_len = (size_t)std::max(1, std::min(K, nsteps));
+  cudaStream_t s = c->stream;
+  ScopedDeviceMemory mem;
+  double4 *lam0, *lam1, *bend, *madj, *gmemb, *gpart, *ckpt, *hist, *xT;
+  double *acc, *target, *inv_cnt;
+  const size_t nm = (size_t)std::max(c->nprep_memb, 1);
+  if ((rc = mem.get(&lam0, n)) || (rc = mem.get(&lam1, n)) || (rc = mem.get(&gpart, n)) ||
+      (rc = mem.get(&bend, 11 * nm)) || (rc = mem.get(&madj, nm)) || (rc = mem.get(&gmemb, nm)) ||
+      (rc = mem.get(&ckpt, n * (size_t)std::max(nseg, 1))) || (rc = mem.get(&hist, n * hist_len)) ||
+      (rc = mem.get(&xT, n)) || (rc = mem.get(&acc, 4 * (size_t)nt)) ||
+      (rc = mem.get(&target, 3 * n)) || (rc = mem.get(&inv_cnt, (size_t)nt)))
+    return rc;
+  const size_t pbytes = sizeof(double4) * n;
+  EPI_CUDA(cudaMemcpyAsync(target, loss->target_x, 8 * n, cudaMemcpyHostToDevice, s));
+  EPI_CUDA(cudaMemcpyAsync(target + n, loss->target_y, 8 * n, cudaMemcpyHostToDevice, s));
+  EPI_CUDA(cudaMemcpyAsync(target + 2 * n, loss->target_z, 8 * n, cudaMemcpyHostToDevice, s));
+  std::vector<double> inv(nt);
+  for (int32_t t = 0; t < nt; ++t) {
+    const int32_t cnt = c->tissues_h[t].n - (loss->cells_only ? c->tissues_h[t].nmemb : 0);
+    inv[t] = cnt > 0 ? 1.0 / cnt : 0.0;
+  }
+  EPI_CUDA(cudaMemcpyAsync(inv_cnt, inv.data(), 8 * (size_t)nt, cudaMemcpyHostToDevice, s));
+  EPI_CUDA(cudaMemsetAsync(acc, 0, 32 * (size_t)nt, s));
+  // forward, keeping a checkpoint every K steps
+  for (int32_t t = 0; t < nsteps; ++t) {
+    if (t % K == 0)
+      EPI_CUDA(cudaMemcpyAsync(ckpt + (size_t)(t / K) * n, c->pos[c->cur], pbytes,
+                               cudaMemcpyDeviceToDevice, s));
+    enqueue_step(c, c->cur, nullptr);
+  }
+  c->lists_fresh = false;
+  if ((rc = check_status(c))) return rc;
+  EPI_CUDA(cudaMemcpyAsync(xT, c->pos[c->cur], pbytes, cudaMemcpyDeviceToDevice, s));
+  launch_adjoint_seed(make_state(c, c->cur), target, loss->cells_only, inv_cnt, lam0,
+                      gpart, c->lc, s);
+  launch_tissue_sum(make_state(c, c->cur), gpart, acc, c->lc, s);
+  double4* lam[2] = {lam0, lam1};
+  int a = 0;
+  for (int32_t seg = nseg - 1; seg >= 0; --seg) {
+    const int32_t t0 = seg * K, t1 = std::min(t0 + K, nsteps);
+    // recompute X_t0 .. X_{t1-1} from the checkpoint
+    EPI_CUDA(cudaMemcpyAsync(c->pos[c->cur], ckpt + (size_t)seg * n, pbytes,
+                             cudaMemcpyDeviceToDevice, s));
+    launch_gate_check(make_state(c, c->cur), c->lc, s);
+    for (int32_t t = t0; t < t1; ++t) {
+      EPI_CUDA(cudaMemcpyAsync(hist + (size_t)(t - t0) * n, c->pos[c->cur], pbytes,
+                               cudaMemcpyDeviceToDevice, s));
+      if (t + 1 < t1) enqueue_step(c, c->cur, nullptr);
+    }
+    // and differentiate them in reverse
+    for (int32_t t = t1 - 1; t >= t0; --t) {
+      DevState St = make_state(c, c->cur);
+      St.pos_cur = hist + (size_t)(t - t0) * n;
+      launch_gate_check(St, c->lc, s);
+      launch_rebuild(St, whole(c), c->scan, c->lc, s, nullptr);
+      const AdjointBuffers B{lam[a], lam[a ^ 1], bend, madj, gmemb, gpart};
+      launch_adjoint_step(St, B, c->lc, s);
+      launch_tissue_sum(St, gpart, acc, c->lc, s);
+      a ^= 1;
+    }
+    if ((rc = check_status(c))) return rc;
+  }
+  // the context ends at X_T; its candidates are rebuilt before the next step
+  EPI_CUDA(cudaMemcpyAsync(c->pos[c->cur], xT, pbytes, cudaMemcpyDeviceToDevice, s));
+  launch_set_gates(make_state(c, c->cur), nt, s);
+  std::vector<double> h(4 * (size_t)nt);
+  EPI_CUDA(cudaMemcpyAsync(h.data(), acc, 32 * (size_t)nt, cudaMemcpyDeviceToHost, s));
+  if ((rc = check_status(c))) return rc;
+  for (int32_t t = 0; t < nt; ++t) {
+    if (loss_out) loss_out[t] = h[4 * t + 3];
+    if (grad)
+      for (int k = 0; k < 3; ++k) grad[3 * t + k] = h[4 * t + k];
+  }
+  return EPI_OK;
   EPI_GUARD_END
 }
 

@@ -298,6 +298,7 @@ struct TissueDev {
   int32_t pbase, n, nmemb, nder, nmx, nmy;
   int32_t anx, any, anz;  // reference grid (cell_connection.cpp:22-26)
   int32_t binbase;        // first bin; a tissue owns anx*any*anz bins + 1 sentinel
+  int32_t mbase;          // index in prep of the tissue's first membrane particle
   double lx, ly, lz, hlx, hly;     // box and half box
   double rmax;     // largest radius in the tissue
   double rmax_nm;  // largest non-membrane radius (membranes only pair with those)

@@ -25,6 +25,7 @@
 // cell_interaction.cpp:48-66). No atomics touch positions, so a step is
 // deterministic and repeatable bit for bit.
 #include "epi_kernels.h"
+#include "epi_device.cuh"
 
 namespace epi {
 
@@ -32,17 +33,6 @@ const char* const kKernelClassNames[KC_COUNT] = {
     "step", "prepass", "rebuild_bin", "rebuild_scan", "rebuild_sort", "rebuild_search", "gate"};
 
 namespace {
-
-inline int blocks_for(int64_t n, int b) { return (int)((n + b - 1) / b); }
-inline int stride_blocks(int64_t n, int b, const LaunchCfg& lc) {
-  const int need = blocks_for(n, b);
-  const int cap = lc.num_sms * 8;
-  return need < cap ? (need > 0 ? need : 1) : cap;
-}
-
-#define GRID_STRIDE(i, lo, hi) \
-  for (int64_t i = (lo) + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (hi); \
-       i += (int64_t)gridDim.x * blockDim.x)
 
 // ---------------------------------------------------------------------------
 // Scan (reduce -> top-level scan -> down-sweep). No inter-block waiting.
@@ -499,69 +489,6 @@ __global__ void k_dermis(DevState S, int32_t f0, int32_t f1) {
 // connect_cell would make. R is the arithmetic type of the force laws
 // (double: FP64 path; float: mixed path). Sums and positions stay double.
 // ---------------------------------------------------------------------------
-// _memb_bend_diff_factor with NEW_BEND_POT (cell_interaction.cpp:349-360)
-template <typename R>
-__device__ __forceinline__ R bend_factor(R c) {
-  return c >= R(0) ? (R(1) - c) : R(1) / ((R(1) + c) * (R(1) + c));
-}
-
-// Separation of a pair as cell_interaction_apply computes it for its c1
-// (:56-58), seen from particle i: the reference adds +d to c1, -d to c2.
-__device__ __forceinline__ void pair_sep(const double4& p, const double4& pq, bool i_is_c1,
-                                         const TissueDev& T, double& dx, double& dy, double& dz) {
-  if (i_is_c1) {
-    dx = pdiff(p.x, pq.x, T.lx);
-    dy = pdiff(p.y, pq.y, T.ly);
-    dz = p.z - pq.z;
-  } else {
-    dx = -pdiff(pq.x, p.x, T.lx);
-    dy = -pdiff(pq.y, p.y, T.ly);
-    dz = -(pq.z - p.z);
-  }
-}
-
-// Reciprocal square root and division: correctly rounded in the FP64 path,
-// the hardware approximations (about 2 ulp) in the FP32 path.
-__device__ __forceinline__ float frsqrt(float v) { return rsqrtf(v); }
-__device__ __forceinline__ double frsqrt(double v) { return 1.0 / sqrt(v); }
-__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
-__device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
-
-template <typename R>
-struct Vec3 {
-  R x, y, z;
-};
-// Offset of a lattice neighbour from the particle (minimum image).
-template <typename R>
-__device__ __forceinline__ Vec3<R> offset_of(const double4& q, const double4& p,
-                                             const TissueDev& T) {
-  return Vec3<R>{R(pdiff_h(q.x, p.x, T.lx, T.hlx)), R(pdiff_h(q.y, p.y, T.ly, T.hly)),
-                 R(q.z - p.z)};
-}
-// Unit vector and length of b - a: the nv / dn (or mv / dm) that
-// _memb_bend_calc1 stores for a membrane particle (cell_interaction.cpp:296-309).
-template <typename R>
-struct Unit {
-  R x, y, z, d;
-};
-template <typename R>
-__device__ __forceinline__ Unit<R> unit_of(R x, R y, R z) {
-  const R s = x * x + y * y + z * z;
-  const R inv = frsqrt(s);
-  return Unit<R>{x * inv, y * inv, z * inv, s * inv};
-}
-template <typename R>
-__device__ __forceinline__ Unit<R> unit_ab(const Vec3<R>& a, const Vec3<R>& b) {
-  return unit_of(b.x - a.x, b.y - a.y, b.z - a.z);
-}
-template <typename R>
-__device__ __forceinline__ R dotu(const Unit<R>& a, const Unit<R>& b) {
-  return a.x * b.x + a.y * b.y + a.z * b.z;
-}
-template <typename R>
-__device__ __forceinline__ R cmp(const Unit<R>& v, int k) {
-  return k == 0 ? v.x : (k == 1 ? v.y : v.z);
-}
 
 // Membrane particles: bending (_memb_bend_calc1..3, :296-449; the unit
 // vectors of calc1 are recomputed from the eleven lattice positions the

@@ -72,4 +72,29 @@ void launch_unpack_positions(const DevState& S, double* x, double* y, double* z,
 void launch_pack_positions(const DevState& S, const double* x, const double* y,
                            const double* z, int32_t n, cudaStream_t s);
 
+// ---- reverse-mode adjoint (FP64), membrane + ALIVE / DEAD / AIR tissues ----
+struct AdjointBuffers {
+  const double4* lam_in;  // dL/dX_{t+1}
+  double4* lam_out;       // dL/dX_t
+  double4* bend;          // 11 bending products per membrane particle
+  double4* madj;          // lattice + wall product per membrane particle
+  double4* gmemb;         // membrane parameter partials
+  double4* gpart;         // per-particle parameter partials (spring, eps, bend, loss)
+};
+// Sets the gate of every tissue with a particle farther than skin/2 from
+// its last rebuild position.
+void launch_gate_check(const DevState& S, const LaunchCfg& lc, cudaStream_t s);
+// lambda_T and the loss terms (gpart.w) of L_t = inv_cnt[t] sum |X - X*|^2;
+// target holds x | y | z (3 n doubles).
+void launch_adjoint_seed(const DevState& S, const double* target, int32_t cells_only,
+                         const double* inv_cnt, double4* lam, double4* gpart,
+                         const LaunchCfg& lc, cudaStream_t s);
+// One backward step at positions S.pos_cur (lists: exact predicate over the
+// current candidates, which must be valid for S.pos_cur).
+void launch_adjoint_step(const DevState& S, const AdjointBuffers& B, const LaunchCfg& lc,
+                         cudaStream_t s);
+// acc[4 t + c] += per-tissue sums of gpart (fixed order: deterministic).
+void launch_tissue_sum(const DevState& S, const double4* gpart, double* acc, const LaunchCfg& lc,
+                       cudaStream_t s);
+
 }  // namespace epi

@@ -179,6 +179,37 @@ int epi_rebuild_count(epi_ctx* ctx, int64_t* count);
 int epi_time_kernels(epi_ctx* ctx, int32_t nsteps, int32_t max_classes, double* ms,
                      int32_t* launches, const char** names, int32_t* nclasses);
 
+/* ---- gradients: reverse-mode adjoint of the step --------------------------
+ * No counterpart in the reference, which has no gradients. The loss of
+ * tissue t is L_t = mean over its loss set of |x_i(T) - x*_i|^2, x_i(T) the
+ * positions after nsteps steps from the current state (minimum image in x
+ * and y); the loss set is every particle (cells_only = 0) or every
+ * non-membrane particle (cells_only = 1). Targets are n_total doubles each,
+ * concatenated by tissue like the positions. */
+typedef struct epi_loss {
+  const double* target_x;
+  const double* target_y;
+  const double* target_z;
+  int32_t cells_only;
+  int32_t reserved;  /* must be 0 */
+} epi_loss;
+/* Runs nsteps steps (the context ends at the positions epi_step(ctx, nsteps)
+ * reaches) and returns, per tissue t, loss[t] and the gradient of L_t with
+ * respect to three multipliers of the tissue's force constants, at 1:
+ *   grad[3t + 0]  every spring constant (der_der_const, k_total,
+ *                 k_desmosome, kspring, kspring_d, kspring_division),
+ *   grad[3t + 1]  eps_m (Lennard-Jones depth),
+ *   grad[3t + 2]  kbend (membrane bending).
+ * d L_t / d eps_m is grad[3t + 1] / eps_m, and so on. Reverse mode: the
+ * positions are checkpointed every `checkpoint_every` steps and each segment
+ * is recomputed before it is differentiated, so the device holds
+ * ceil(nsteps / checkpoint_every) + checkpoint_every position sets.
+ * Derivatives are evaluated in FP64 along the trajectory of the context's
+ * precision. Tissues must hold only membrane and ALIVE / DEAD / AIR cells
+ * without pairs (else EPI_ERR_UNSUPPORTED). loss or grad may be NULL. */
+int epi_adjoint(epi_ctx* ctx, int32_t nsteps, int32_t checkpoint_every, const epi_loss* loss,
+                double* loss_out, double* grad);
+
 /* ---- connect_cell of one tissue without any device allocation ------------
  * No counterpart in the reference: it exists for callers that cannot let this
  * library call cudaMalloc — applications whose device memory all belongs to

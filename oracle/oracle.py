@@ -8,6 +8,10 @@ bench.py's CPU-baseline leg:
 * run_reference -- runs the compiled reference harness (oracle/_ref, built by
   oracle/build_ref.py from the reference sources) on a tissue and returns its
   frames.
+* tangent_gradient -- the FP64 forward-mode gradient of a final-state loss
+  with respect to the spring / LJ-epsilon / bending multipliers
+  (oracle/epi_oracle_tangent.cpp, same library), the reference gradient of
+  the adjoint tests.
 
 Nothing in the product package imports this module.
 """
@@ -30,14 +34,24 @@ _lib = None
 
 
 def build_oracle(force: bool = False) -> Path:
-    src = [HERE / "epi_oracle.c"]
+    c_src = HERE / "epi_oracle.c"
+    cpp_src = HERE / "epi_oracle_tangent.cpp"
     hdr = HERE / "epi_oracle.h"
+    deps = [c_src, cpp_src, hdr, Path(__file__)]
     if (not force and LIB_PATH.exists()
-            and LIB_PATH.stat().st_mtime > max(p.stat().st_mtime for p in src + [hdr])):
+            and LIB_PATH.stat().st_mtime > max(p.stat().st_mtime for p in deps)):
         return LIB_PATH
-    cmd = ["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-std=c11",
-           "-o", str(LIB_PATH), *map(str, src), "-lm"]
-    subprocess.run(cmd, check=True)
+    # -ffp-contract=off: the restatement evaluates the reference's arithmetic
+    # operation by operation (no fused multiply-adds)
+    flags = ["-O2", "-ffp-contract=off", "-fPIC"]
+    with tempfile.TemporaryDirectory() as d:
+        c_obj, cpp_obj = os.path.join(d, "oracle.o"), os.path.join(d, "tangent.o")
+        subprocess.run(["gcc", *flags, "-std=c11", "-c", str(c_src), "-o", c_obj], check=True)
+        subprocess.run(["g++", *flags, "-std=c++17", "-c", str(cpp_src), "-o", cpp_obj],
+                       check=True)
+        tmp = str(LIB_PATH) + ".tmp"
+        subprocess.run(["g++", "-shared", "-o", tmp, c_obj, cpp_obj, "-lm"], check=True)
+        os.replace(tmp, LIB_PATH)
     return LIB_PATH
 
 
@@ -69,6 +83,10 @@ def lib():
         L.ora_get_dermis.argtypes = [P, i32]
         L.ora_error_info.argtypes = [P, i32, i32, d]
         L.ora_error_info.restype = ctypes.c_int
+        L.ora_tangent_gradient.argtypes = (
+            [ctypes.c_int32] * 5 + [ctypes.c_double] * 3 + [d] * 7 + [u8, i32, i32] +
+            [ctypes.c_int32, d, d, d, ctypes.c_int32, ctypes.c_int32, d, d, d, d, d])
+        L.ora_tangent_gradient.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -193,3 +211,38 @@ def time_reference(t, warmup: int, steps: int, threads: Optional[int] = None):
         if r.returncode != 0:
             raise RuntimeError(f"reference harness failed ({r.returncode}): {r.stderr[-2000:]}")
         return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def tangent_gradient(t, nsteps: int, target=None, cells_only: bool = True, dual: bool = True,
+                     params=None):
+    """Forward-mode FP64 gradient (oracle/epi_oracle_tangent.cpp).
+
+    Runs `nsteps` steps of tissue `t` and returns (loss, grad, positions):
+    loss = mean over the loss set (non-membrane particles when `cells_only`)
+    of the squared minimum-image distance to `target` (x, y, z arrays), and
+    grad = d loss / d (s_spring, s_eps, s_bend), the multipliers of every
+    spring constant, of eps_m and of kbend, at 1. With dual=False the
+    plain-double instantiation runs (no gradient: grad is None).
+    """
+    L = lib()
+    p = np.array((params or t.params).as_tuple(), dtype=np.float64)
+    keep = [np.ascontiguousarray(a, dtype=np.float64) for a in (
+        t.x, t.y, t.z, t.radius, t.agek, t.spr_nat_len)]
+    st = np.ascontiguousarray(t.state, dtype=np.uint8)
+    pr = np.ascontiguousarray(t.pair, dtype=np.int32)
+    rd = np.ascontiguousarray(t.rest_div_times, dtype=np.int32)
+    tgt = [np.ascontiguousarray(a, dtype=np.float64) for a in target] if target is not None \
+        else [None] * 3
+    loss = ctypes.c_double(0.0)
+    grad = np.zeros(3)
+    out = [np.empty(t.n) for _ in range(3)]
+    rc = L.ora_tangent_gradient(
+        t.n, t.nmemb, t.nder, t.nmx, t.nmy, t.lx, t.ly, t.lz, _p(p, ctypes.c_double),
+        *[_p(a, ctypes.c_double) for a in keep], _p(st, ctypes.c_uint8),
+        _p(pr, ctypes.c_int32), _p(rd, ctypes.c_int32), nsteps,
+        *[(_p(a, ctypes.c_double) if a is not None else None) for a in tgt],
+        1 if cells_only else 0, 1 if dual else 0, ctypes.byref(loss),
+        _p(grad, ctypes.c_double), *[_p(a, ctypes.c_double) for a in out])
+    if rc != 0:
+        raise RuntimeError(f"oracle tangent failed with code {rc}")
+    return loss.value, (grad if dual else None), tuple(out)

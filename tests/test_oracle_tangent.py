@@ -1,0 +1,75 @@
+"""The reference gradient is pinned before it is trusted.
+
+oracle/epi_oracle_tangent.cpp restates the step as a template: its plain
+double instantiation must reproduce the C oracle (itself pinned to the
+compiled reference) bit for bit, the dual-number instantiation must carry
+the same values, and its gradient must match central finite differences of
+the oracle's own step (h = 1e-4 relative).
+"""
+import numpy as np
+import pytest
+
+from epi_b200 import tissue as T
+from oracle import oracle as O
+
+STEPS = 200
+H = 1e-4
+
+
+def aged_tissue():
+    """C1 with every other cell older than THRESH_SP and some DEAD / AIR cells,
+    so that both adhesion constants (K_TOTAL for two old cells) take part."""
+    t = T.config1(3).copy()
+    cells = np.arange(t.nmemb, t.n)
+    t.agek[cells[::2]] = 5.0
+    t.agek[cells[::5]] = 4.0
+    t.state[cells[3::7]] = T.DEAD
+    t.state[cells[5::11]] = T.AIR
+    t.validate()
+    return t
+
+
+def min_image_loss(t, pos, target):
+    d = [pos[k] - target[k] for k in range(3)]
+    for k, L in ((0, t.lx), (1, t.ly)):
+        d[k] = np.where(d[k] > 0.5 * L, d[k] - L, np.where(d[k] <= -0.5 * L, d[k] + L, d[k]))
+    m = slice(t.nmemb, t.n)
+    return float(np.mean(d[0][m] ** 2 + d[1][m] ** 2 + d[2][m] ** 2))
+
+
+def oracle_positions(t, steps, params=None):
+    ora = O.OracleTissue(t, params=params)
+    assert ora.step(steps) == 0, ora.error()
+    return ora.positions()
+
+
+@pytest.mark.parametrize("factory", [T.config1, aged_tissue])
+def test_tangent_value_path_is_the_oracle_bit_for_bit(built, factory):
+    t = factory()
+    ref = oracle_positions(t, STEPS)
+    _, _, plain = O.tangent_gradient(t, STEPS, dual=False)
+    _, _, dual = O.tangent_gradient(t, STEPS, target=ref)
+    for k in range(3):
+        assert np.array_equal(plain[k], ref[k])
+        assert np.array_equal(dual[k], ref[k])
+
+
+@pytest.mark.parametrize("factory", [T.config1, aged_tissue])
+def test_tangent_gradient_matches_central_differences(built, factory):
+    t = factory()
+    target = oracle_positions(t, STEPS, t.params.scaled(1.1, 1.1, 1.1))
+    loss, grad, pos = O.tangent_gradient(t, STEPS, target=target)
+    assert loss == pytest.approx(min_image_loss(t, pos, target), rel=1e-12)
+    for k in range(3):
+        e = [1.0, 1.0, 1.0]
+        e[k] = 1.0 + H
+        lp = min_image_loss(t, oracle_positions(t, STEPS, t.params.scaled(*e)), target)
+        e[k] = 1.0 - H
+        lm = min_image_loss(t, oracle_positions(t, STEPS, t.params.scaled(*e)), target)
+        fd = (lp - lm) / (2 * H)
+        assert abs(fd - grad[k]) <= 1e-5 * abs(grad[k]), (k, fd, grad[k])
+
+
+def test_tangent_rejects_states_outside_its_scope(built):
+    with pytest.raises(RuntimeError):
+        O.tangent_gradient(T.mixed_state_tissue(), 1)
