@@ -41,9 +41,11 @@ from epi_b200.ensemble import shard_tissues  # noqa: E402
 
 METRIC = "cell-updates/s: FP32/batched vs plain FP64 GPU @≤1e-5 rel pos err; grad err"
 UNIT = "cell-updates/s"
-# per step: rebuild (bin, 3 x scan, scatter, binsort, candidate search, gate
-# clear; each exits at once unless a tissue needs a rebuild), prepass, step
-KERNEL_LAUNCHES_PER_STEP = 10
+# per step: rebuild (gate compaction, bin, per-tissue scan, scatter, binsort,
+# candidate search, gate clear; each exits at once unless a tissue needs a
+# rebuild), membrane prepass, step; plus the dermis kernel when a tissue holds
+# FIX / MUSUME cells
+KERNEL_LAUNCHES_PER_STEP = 9
 
 
 def workload(name: str, tissues: int = 512):
@@ -192,6 +194,78 @@ def load_traffic(kernel: str, workload_name: str):
         return None
 
 
+def min_image_err(t, a, b):
+    """max over particles of the minimum-image |a - b| / L_x."""
+    d = [a[k] - b[k] for k in range(3)]
+    for k, L in ((0, t.lx), (1, t.ly)):
+        d[k] = np.where(d[k] > 0.5 * L, d[k] - L, np.where(d[k] <= -0.5 * L, d[k] + L, d[k]))
+    return float(np.sqrt(d[0] ** 2 + d[1] ** 2 + d[2] ** 2).max() / t.lx)
+
+
+def mean_sq_loss(t, pos, target):
+    d = [pos[k] - target[k] for k in range(3)]
+    for k, L in ((0, t.lx), (1, t.ly)):
+        d[k] = np.where(d[k] > 0.5 * L, d[k] - L, np.where(d[k] <= -0.5 * L, d[k] + L, d[k]))
+    m = slice(t.nmemb, t.n)
+    return float(np.mean(d[0][m] ** 2 + d[1][m] ** 2 + d[2][m] ** 2))
+
+
+def accuracy_check(capi, device: int, steps: int):
+    """Mixed (FP32 forces) against FP64 positions on the 64x64, 32,768-cell
+    tissue after `steps` steps (the FP64 path is pinned to the oracle by the
+    parity tests)."""
+    t = T.config2()
+    pos = {}
+    for name, prec in (("fp64", capi.EPI_PREC_FP64), ("mixed", capi.EPI_PREC_MIXED)):
+        with capi.Context(precision=prec, device=device) as c:
+            c.upload([t])
+            c.step(steps, "graph")
+            pos[name] = c.positions()
+    return {"workload": "64x64 membrane + 32,768 cells (seed 1)", "steps": steps,
+            "max_rel_pos_err_mixed_vs_fp64": min_image_err(t, pos["mixed"], pos["fp64"]),
+            "bar": 1e-5}
+
+
+def adjoint_check(capi, device: int, steps: int, every: int = 20, h: float = 1e-4):
+    """The adjoint workload: 64x64 membrane + 32,768 cells, loss = mean squared
+    distance of the final cell positions to a run with every force constant
+    +10%; gradient w.r.t. the spring / LJ-epsilon / bending multipliers by
+    epi_adjoint (FP64, checkpoint every `every` steps), against central
+    differences of the FP64 step (h relative)."""
+    import torch
+    t = T.config5()
+
+    def run(params):
+        with capi.Context(precision=capi.EPI_PREC_FP64, device=device) as c:
+            c.upload([t], [params])
+            c.step(steps, "graph")
+            return c.positions()
+
+    target = run(t.params.scaled(1.1, 1.1, 1.1))
+    with capi.Context(precision=capi.EPI_PREC_FP64, device=device) as c:
+        c.upload([t])
+        c.adjoint(steps, target, checkpoint_every=every)  # warm-up
+        c.upload([t])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        loss, grad = c.adjoint(steps, target, checkpoint_every=every)
+        adj_s = time.perf_counter() - t0
+    fd = []
+    for k in range(3):
+        e = [1.0, 1.0, 1.0]
+        e[k] = 1.0 + h
+        lp = mean_sq_loss(t, run(t.params.scaled(*e)), target)
+        e[k] = 1.0 - h
+        lm = mean_sq_loss(t, run(t.params.scaled(*e)), target)
+        fd.append((lp - lm) / (2 * h))
+    rel = [abs(grad[0, k] - fd[k]) / abs(fd[k]) for k in range(3)]
+    return {"workload": "64x64 membrane + 32,768 cells (seed 4), target from +10% constants",
+            "steps": steps, "checkpoint_every": every, "loss": float(loss[0]),
+            "grad": [float(g) for g in grad[0]], "fd": fd, "fd_h": h,
+            "max_rel_err_vs_fd": max(rel), "bar": 1e-4, "seconds": adj_s,
+            "grad_order": ["s_spring", "s_eps", "s_bend"]}
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -217,6 +291,10 @@ def main():
     ap.add_argument("--ref-particles", type=int, default=120000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="timed region only (profiling)")
+    ap.add_argument("--adjoint-steps", type=int, default=200,
+                    help="steps of the adjoint workload (0: skip)")
+    ap.add_argument("--accuracy-steps", type=int, default=1000,
+                    help="steps of the mixed-vs-FP64 position error check (0: skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 0)
 
@@ -369,6 +447,12 @@ def main():
             extras["fp64_plain"] = {"value": plain, "unit": UNIT, "steps": args.plain_steps,
                                     "speedup": value / plain}
 
+    if world == 1 and not args.no_extras:
+        if args.accuracy_steps > 0:
+            extras["accuracy"] = accuracy_check(capi, local, args.accuracy_steps)
+        if args.adjoint_steps > 0:
+            extras["adjoint"] = adjoint_check(capi, local, args.adjoint_steps)
+
     if rank == 0:
         cfg = {"workload": desc, "tissues": len(tissues), "particles": n_all,
                "mean_connections": kbar, "precision": args.precision,
@@ -383,7 +467,9 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32-force/f64-sum" if args.precision == "mixed" else "f64",
                 "data": "synthetic (seeded splitmix64 jittered lattices)", "config": cfg,
-                "gpu_launches": KERNEL_LAUNCHES_PER_STEP * args.steps,
+                "gpu_launches": (KERNEL_LAUNCHES_PER_STEP + int(any(
+                    ((t.state == T.FIX) | (t.state == T.MUSUME)).any() for t in mine)))
+                * args.steps,
                 "clocks": clk.summary()}
         line.update(extras)
         if world == 1 and not args.no_cpu_baseline and not args.no_extras:
