@@ -282,10 +282,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="ensemble", choices=["ensemble", "c1", "c2", "c3"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
-    ap.add_argument("--skin", type=float, default=None)
+    ap.add_argument("--skin", type=float, default=None,
+                    help="candidate skin (default: chosen by the autotuner)")
     ap.add_argument("--tissues", type=int, default=512, help="ensemble size (profiling)")
     ap.add_argument("--variant", type=int, default=None, help="step-kernel tuning variant")
     ap.add_argument("--mode", default="graph", choices=["graph", "eager"])
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default skin / variant instead of epi_autotune's choice")
+    ap.add_argument("--tune-steps", type=int, default=64, help="timed steps per autotuner trial")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--ref-particles", type=int, default=120000)
@@ -324,6 +328,12 @@ def main():
     ctx = capi.Context(precision=prec, max_conn=64, device=local, skin=args.skin,
                        variant=args.variant)
     ctx.upload(mine)
+    tuned = None
+    if args.skin is None and args.variant is None and not args.no_autotune:
+        skin, variant, trial_ms = ctx.autotune(args.tune_steps)
+        tuned = {"skin": skin, "variant": variant, "trial_ms_per_step": trial_ms,
+                 "trial_steps": args.tune_steps,
+                 "grid": "skin {0.05,0.08,0.1,0.15,0.2,0.3} x step-kernel variant 1..4"}
     off, _ = ctx.connections()
     kbar = float(off[-1]) / max(n_mine, 1)  # mean connected_cell length incl. lattice links
     nmemb_mine = sum(t.nmemb for t in mine)
@@ -456,7 +466,10 @@ def main():
     if rank == 0:
         cfg = {"workload": desc, "tissues": len(tissues), "particles": n_all,
                "mean_connections": kbar, "precision": args.precision,
-               "skin": args.skin if args.skin is not None else 0.1,
+               "skin": (tuned["skin"] if tuned else
+                        (args.skin if args.skin is not None else 0.1)),
+               "variant": tuned["variant"] if tuned else (args.variant or 1),
+               "autotune": tuned,
                "tissue_rebuilds_per_step": rebuilds_timed / max(args.steps, 1) / len(mine),
                "launch": "one CUDA graph per 2 steps over the whole batch",
                "l2": "inputs larger than L2 (working set >> 126 MB)"

@@ -40,7 +40,7 @@ EXPORTED = [
     "epi_upload", "epi_connect", "epi_interact_commit", "epi_step", "epi_step_graph",
     "epi_step_per_tissue", "epi_sync", "epi_num_particles", "epi_download_positions",
     "epi_upload_positions", "epi_get_connections", "epi_get_dermis", "epi_error_info",
-    "epi_stream", "epi_rebuild_count", "epi_time_kernels", "epi_adjoint",
+    "epi_stream", "epi_rebuild_count", "epi_time_kernels", "epi_autotune", "epi_adjoint",
     "epi_connect_noalloc",
 ]
 
@@ -128,6 +128,7 @@ def lib():
         L.epi_stream.restype = vp
         L.epi_time_kernels.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, _dp, _ip,
                                        ctypes.POINTER(ctypes.c_char_p), _ip]
+        L.epi_autotune.argtypes = [vp, ctypes.c_int32, _dp, _ip, _dp]
         L.epi_adjoint.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(LossC),
                                   _dp, _dp]
         for f in EXPORTED:
@@ -336,3 +337,13 @@ class Context:
                                  _ptr(loss, ctypes.c_double), _ptr(grad, ctypes.c_double)),
                "epi_adjoint")
         return loss, grad.reshape(nt, 3)
+
+    def autotune(self, trial_steps: int = 64):
+        """epi_autotune: returns (skin, variant, ms per step of the best trial)
+        and keeps that pair in the context."""
+        skin = ctypes.c_double()
+        variant = ctypes.c_int32()
+        ms = ctypes.c_double()
+        _check(lib().epi_autotune(self._h, trial_steps, ctypes.byref(skin), ctypes.byref(variant),
+                                  ctypes.byref(ms)), "epi_autotune")
+        return float(skin.value), int(variant.value), float(ms.value)

@@ -245,6 +245,30 @@ int check_status(epi_ctx* c) {
   return EPI_OK;
 }
 
+// nsteps steps replayed from the two-step graph of the current parity
+// (captured on first use), plus one eager step for an odd count.
+int enqueue_graph_steps(epi_ctx* c, int32_t nsteps) {
+  const int32_t pairs = nsteps / 2;
+  if (pairs > 0) {
+    cudaGraphExec_t& ge = c->graph[c->cur];
+    if (!ge) {
+      cudaGraph_t g;
+      EPI_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      int cur = c->cur;
+      enqueue_step(c, cur, nullptr);
+      enqueue_step(c, cur, nullptr);
+      EPI_CUDA(cudaStreamEndCapture(c->stream, &g));
+      const cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+      cudaGraphDestroy(g);
+      EPI_CUDA(e);
+    }
+    for (int32_t k = 0; k < pairs; ++k) EPI_CUDA(cudaGraphLaunch(ge, c->stream));
+  }
+  if (nsteps % 2) enqueue_step(c, c->cur, nullptr);
+  if (nsteps > 0) c->lists_fresh = false;
+  return EPI_OK;
+}
+
 int materialize(epi_ctx* c) {
   if (c->lists_fresh) return EPI_OK;
   enqueue_materialize(c);
@@ -756,25 +780,80 @@ int epi_step_graph(epi_ctx* c, int32_t nsteps) {
   EPI_GUARD_BEGIN
   int rc = set_device(c);
   if (rc) return rc;
-  const int32_t pairs = nsteps / 2;
-  if (pairs > 0) {
-    cudaGraphExec_t& ge = c->graph[c->cur];
-    if (!ge) {
-      cudaGraph_t g;
-      EPI_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-      int cur = c->cur;
-      enqueue_step(c, cur, nullptr);
-      enqueue_step(c, cur, nullptr);
-      EPI_CUDA(cudaStreamEndCapture(c->stream, &g));
-      const cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
-      cudaGraphDestroy(g);
-      EPI_CUDA(e);
-    }
-    for (int32_t k = 0; k < pairs; ++k) EPI_CUDA(cudaGraphLaunch(ge, c->stream));
-  }
-  if (nsteps % 2) enqueue_step(c, c->cur, nullptr);
-  if (nsteps > 0) c->lists_fresh = false;
+  if ((rc = enqueue_graph_steps(c, nsteps))) return rc;
   return check_status(c);
+  EPI_GUARD_END
+}
+
+int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* variant_out,
+                 double* ms_out) {
+  if (!c || trial_steps < 2) return EPI_ERR_INVALID_ARG;
+  if (!c->loaded) return EPI_ERR_STATE;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  static const double kSkins[] = {0.05, 0.08, 0.1, 0.15, 0.2, 0.3};
+  static const int32_t kVariants[] = {1, 2, 3, 4};
+  constexpr int32_t kWarm = 4;  // the first step after a restore rebuilds every tissue
+  const size_t pbytes = sizeof(double4) * (size_t)c->n;
+  cudaStream_t s = c->stream;
+  ScopedDeviceMemory mem;
+  double4* saved = nullptr;
+  if ((rc = mem.get(&saved, (size_t)c->n))) return rc;
+  const int cur0 = c->cur;
+  EPI_CUDA(cudaMemcpyAsync(saved, c->pos[cur0], pbytes, cudaMemcpyDeviceToDevice, s));
+  cudaEvent_t ev[2];
+  EPI_CUDA(cudaEventCreate(&ev[0]));
+  EPI_CUDA(cudaEventCreate(&ev[1]));
+  struct Events {
+    cudaEvent_t* e;
+    ~Events() {
+      cudaEventDestroy(e[0]);
+      cudaEventDestroy(e[1]);
+    }
+  } ev_guard{ev};
+  // every trial starts from the saved positions with fresh candidates
+  auto restore = [&]() -> int {
+    EPI_CUDA(cudaMemcpyAsync(c->pos[cur0], saved, pbytes, cudaMemcpyDeviceToDevice, s));
+    c->cur = cur0;
+    launch_set_gates(make_state(c, c->cur), c->ntissues, s);
+    c->lists_fresh = false;
+    return EPI_OK;
+  };
+  auto apply = [&](double skin, int32_t variant) {
+    c->cfg.skin = skin;
+    c->cfg.variant = variant;
+    c->lc.variant = variant;
+    destroy_graphs(c);  // the graphs hold the skin and the kernel instantiation
+  };
+  double best = INFINITY, best_skin = c->cfg.skin;
+  int32_t best_variant = c->cfg.variant;
+  for (double skin : kSkins) {
+    for (int32_t variant : kVariants) {
+      apply(skin, variant);
+      if ((rc = restore())) return rc;
+      if ((rc = enqueue_graph_steps(c, kWarm))) return rc;
+      EPI_CUDA(cudaEventRecord(ev[0], s));
+      if ((rc = enqueue_graph_steps(c, trial_steps))) return rc;
+      EPI_CUDA(cudaEventRecord(ev[1], s));
+      // a skin whose candidate rows overflow max_cand fails here: skip it
+      if (check_status(c) != EPI_OK) continue;
+      float ms = 0;
+      EPI_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+      if (ms < best) {
+        best = ms;
+        best_skin = skin;
+        best_variant = variant;
+      }
+    }
+  }
+  apply(best_skin, best_variant);
+  if ((rc = restore())) return rc;
+  if ((rc = check_status(c))) return rc;
+  if (skin_out) *skin_out = best_skin;
+  if (variant_out) *variant_out = best_variant;
+  if (ms_out) *ms_out = std::isfinite(best) ? best / trial_steps : -1.0;
+  return std::isfinite(best) ? EPI_OK : EPI_ERR_LIST_OVERFLOW;
   EPI_GUARD_END
 }
 

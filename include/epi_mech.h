@@ -179,6 +179,18 @@ int epi_rebuild_count(epi_ctx* ctx, int64_t* count);
 int epi_time_kernels(epi_ctx* ctx, int32_t nsteps, int32_t max_classes, double* ms,
                      int32_t* launches, const char** names, int32_t* nclasses);
 
+/* Autotuner. Times short graph-replayed trials of the uploaded batch for
+ * every candidate skin in {0.05, 0.08, 0.1, 0.15, 0.2, 0.3} and step-kernel
+ * variant 1..4 (4 warm-up steps, then trial_steps timed with CUDA events),
+ * and keeps the fastest pair in the context's configuration. Skins whose
+ * candidate rows would overflow max_cand are skipped. The simulation state
+ * is left as it was (positions are restored after every trial), and neither
+ * choice changes results beyond multiply-add rounding (connection sets are
+ * exact for every skin). Writes the choice and the best trial's time per
+ * step; any output may be NULL. No counterpart in the reference. */
+int epi_autotune(epi_ctx* ctx, int32_t trial_steps, double* skin, int32_t* variant,
+                 double* ms_per_step);
+
 /* ---- gradients: reverse-mode adjoint of the step --------------------------
  * No counterpart in the reference, which has no gradients. The loss of
  * tissue t is L_t = mean over its loss set of |x_i(T) - x*_i|^2, x_i(T) the
