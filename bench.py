@@ -43,8 +43,8 @@ METRIC = "cell-updates/s: FP32/batched vs plain FP64 GPU @≤1e-5 rel pos err; g
 UNIT = "cell-updates/s"
 # per step: rebuild (gate compaction, bin, per-tissue scan, scatter, binsort,
 # candidate search, gate clear; each exits at once unless a tissue needs a
-# rebuild), the cell step and the membrane step; plus the dermis kernel when a
-# tissue holds FIX / MUSUME cells
+# rebuild), membrane prepass, step; plus the dermis kernel when a tissue holds
+# FIX / MUSUME cells
 KERNEL_LAUNCHES_PER_STEP = 9
 
 
@@ -289,7 +289,7 @@ def main():
     ap.add_argument("--mode", default="graph", choices=["graph", "eager"])
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default skin / variant instead of epi_autotune's choice")
-    ap.add_argument("--tune-steps", type=int, default=128, help="timed steps per autotuner trial")
+    ap.add_argument("--tune-steps", type=int, default=64, help="timed steps per autotuner trial")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--ref-particles", type=int, default=120000)
@@ -330,10 +330,6 @@ def main():
     ctx.upload(mine)
     tuned = None
     if args.skin is None and args.variant is None and not args.no_autotune:
-        # tune on the state the timed region starts from (after the warm-up's
-        # relaxation of the jittered start), then warm up again below
-        if args.warmup:
-            ctx.step(args.warmup, args.mode)
         skin, variant, trial_ms = ctx.autotune(args.tune_steps)
         tuned = {"skin": skin, "variant": variant, "trial_ms_per_step": trial_ms,
                  "trial_steps": args.tune_steps,
@@ -341,11 +337,7 @@ def main():
     off, _ = ctx.connections()
     kbar = float(off[-1]) / max(n_mine, 1)  # mean connected_cell length incl. lattice links
     nmemb_mine = sum(t.nmemb for t in mine)
-    n_cells = n_mine - nmemb_mine
-    rows = np.diff(off)
-    is_memb = np.concatenate([t.state == T.MEMB for t in mine])
-    kbar_cells = float(rows[~is_memb].mean()) if n_cells else 0.0
-    kbar_memb = float(rows[is_memb].mean()) if nmemb_mine else 0.0
+    kbar_searched = (float(off[-1]) - 4 * nmemb_mine) / max(n_mine, 1)
     stream = torch.cuda.ExternalStream(ctx.stream_handle())
 
     def barrier():
@@ -383,20 +375,20 @@ def main():
         dom = max(tk, key=lambda k: tk[k][0])
         dom_ms = tk[dom][0] / max(tk[dom][1], 1)
         hbm, peak_kind = measured_peaks()
-        # Algorithmic bytes per launch of the step kernels: the per-step work
-        # of the reference for a particle (exact predicate = connect, forces,
-        # commit) is B = 52 + 8 k (24 B xyz read, 24 B xyz write, 4 B state,
-        # 4k B list write + 4k B list read), times the particles the kernel
-        # processes: the cells (k_step) or the membrane particles
-        # (k_step_memb, whose k includes the four lattice links).
-        alg_per_launch = {
-            "step": (52 + 8 * kbar_cells) * n_cells,
-            "step_memb": (52 + 8 * kbar_memb) * nmemb_mine,
+        # Algorithmic bytes per particle of each kernel class. The
+        # step kernel does the whole per-step work of the reference (exact
+        # predicate = connect, forces, commit): B = 52 + 8 k (24 B xyz read,
+        # 24 B xyz write, 4 B state, 4k B list write + 4k B list read).
+        per_particle = {
+            "step": 52 + 8 * kbar,
+            "prepass": 32 * 3 + 64,
+            "rebuild_bin": 32 + 4 + 8,
+            "rebuild_scan": 0,
+            "rebuild_sort": 4 + 32 + 4 + 32,
+            "rebuild_search": 32 + 4 + 4 * 2 * kbar + 4,
+            "gate": 0,
         }
-        if dom not in alg_per_launch:
-            dom = "step"
-            dom_ms = tk[dom][0] / max(tk[dom][1], 1)
-        alg = alg_per_launch[dom]
+        alg = per_particle[dom] * n_mine
         achieved = alg / (dom_ms * 1e-3) / 1e9
         traffic = load_traffic(dom, args.workload)
         extras["roofline"] = {
@@ -404,8 +396,7 @@ def main():
             "frac": achieved / hbm, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
             if peak_kind == "measured" else "fallback",
             "traffic": traffic, "alg_bytes_per_launch": alg,
-            "launch_ms": dom_ms, "units_per_launch": n_cells if dom == "step" else nmemb_mine,
-            "mean_connections_cells": kbar_cells, "mean_connections_memb": kbar_memb,
+            "launch_ms": dom_ms,
             "step_alg_bytes_per_particle": 52 + 8 * kbar,
             "step_frac": (52 + 8 * kbar) * value / max(world, 1) / 1e9 / hbm,
         }

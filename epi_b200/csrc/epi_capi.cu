@@ -63,10 +63,6 @@ struct TissueHost {
 struct epi_ctx {
   epi_config cfg{};
   cudaStream_t stream = nullptr;
-  // second stream: the membrane step runs on it concurrently with the cell
-  // step (fork / join events; also inside the captured graphs)
-  cudaStream_t stream2 = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   LaunchCfg lc{148, 256, 0, 0, 0};
   bool loaded = false;
   bool lists_fresh = false;  // nbr / nn / dermis match the current positions
@@ -89,6 +85,7 @@ struct epi_ctx {
   float4* bpos = nullptr;
   int32_t* nbr = nullptr;
   int32_t* nn = nullptr;
+  double4* fmemb = nullptr;
   int32_t* bin = nullptr;
   int32_t* rank = nullptr;
   int32_t* counts = nullptr;
@@ -141,7 +138,7 @@ void destroy_graphs(epi_ctx* c) {
 void free_buffers(epi_ctx* c) {
   destroy_graphs(c);
   void* ptrs[] = {c->tissues, c->pos[0], c->pos[1], c->attr, c->pair, c->spr, c->dermis,
-                  c->cand, c->ncand, c->bpos, c->nbr, c->nn, c->bin,
+                  c->cand, c->ncand, c->bpos, c->nbr, c->nn, c->fmemb, c->bin,
                   c->rank, c->counts, c->starts, c->skey, c->spos, c->gate, c->rl, c->prep,
                   c->scan.partial, c->stage};
   for (void* p : ptrs)
@@ -150,7 +147,7 @@ void free_buffers(epi_ctx* c) {
   c->pos[0] = c->pos[1] = nullptr;
   c->attr = nullptr; c->pair = nullptr; c->spr = nullptr; c->dermis = nullptr;
   c->cand = nullptr; c->ncand = nullptr; c->bpos = nullptr;
-  c->nbr = nullptr; c->nn = nullptr;
+  c->nbr = nullptr; c->nn = nullptr; c->fmemb = nullptr;
   c->bin = nullptr; c->rank = nullptr; c->counts = nullptr; c->starts = nullptr;
   c->skey = nullptr; c->spos = nullptr; c->gate = nullptr; c->rl = nullptr; c->prep = nullptr;
   c->scan.partial = nullptr; c->stage = nullptr;
@@ -172,6 +169,7 @@ DevState make_state(epi_ctx* c, int cur) {
   S.bpos = c->bpos;
   S.nbr = c->nbr;
   S.nn = c->nn;
+  S.fmemb = c->fmemb;
   S.bin = c->bin;
   S.rank = c->rank;
   S.counts = c->counts;
@@ -203,28 +201,24 @@ Range tissue_range(const epi_ctx* c, int t) {
   return Range{T.pbase, T.pbase + T.n, T.binbase, T.binbase + T.anx * T.any * T.anz + 1, t, t + 1};
 }
 
-void dermis_all(epi_ctx* c, int cur, Timer* tm) {
-  launch_dermis(make_state(c, cur), c->nprep_memb, c->nprep, c->lc, c->stream, tm);
+void prepass_all(epi_ctx* c, int cur, Timer* tm) {
+  launch_prepass(make_state(c, cur), 0, c->nprep_memb, c->nprep_memb, c->nprep,
+                 c->cfg.precision, c->lc, c->stream, tm);
 }
 
-// One reference step over the batch: [rebuild] -> dermis -> the cell step
-// and the membrane step, concurrently on two streams (sequentially when
-// kernel classes are being timed).
+void prepass_tissue(epi_ctx* c, int cur, int t) {
+  const TissueDev& T = c->tissues_h[t];
+  const TissueHost& H = c->thost[t];
+  const int32_t f0 = c->nprep_memb + H.prep_f;
+  launch_prepass(make_state(c, cur), H.prep_m, H.prep_m + T.nmemb, f0, f0 + H.nfm,
+                 c->cfg.precision, c->lc, c->stream, nullptr);
+}
+
+// One reference step over the batch: [rebuild] -> prepass -> fused step.
 void enqueue_step(epi_ctx* c, int& cur, Timer* tm) {
-  const DevState S = make_state(c, cur);
-  launch_rebuild(S, whole(c), c->scan, c->lc, c->stream, tm);
-  dermis_all(c, cur, tm);
-  if (tm) {
-    launch_step(S, whole(c), c->cfg.precision, c->lc, c->stream, tm);
-    launch_step_memb(S, 0, c->nprep_memb, c->cfg.precision, c->lc, c->stream, tm);
-  } else {
-    cudaEventRecord(c->ev_fork, c->stream);
-    cudaStreamWaitEvent(c->stream2, c->ev_fork, 0);
-    launch_step_memb(S, 0, c->nprep_memb, c->cfg.precision, c->lc, c->stream2, nullptr);
-    launch_step(S, whole(c), c->cfg.precision, c->lc, c->stream, nullptr);
-    cudaEventRecord(c->ev_join, c->stream2);
-    cudaStreamWaitEvent(c->stream, c->ev_join, 0);
-  }
+  launch_rebuild(make_state(c, cur), whole(c), c->scan, c->lc, c->stream, tm);
+  prepass_all(c, cur, tm);
+  launch_step(make_state(c, cur), whole(c), c->cfg.precision, c->lc, c->stream, tm);
   cur ^= 1;
 }
 
@@ -232,7 +226,7 @@ void enqueue_step(epi_ctx* c, int& cur, Timer* tm) {
 void enqueue_materialize(epi_ctx* c) {
   const DevState S = make_state(c, c->cur);
   launch_rebuild(S, whole(c), c->scan, c->lc, c->stream, nullptr);
-  dermis_all(c, c->cur, nullptr);
+  prepass_all(c, c->cur, nullptr);
   launch_exact_lists(S, whole(c), c->lc, c->stream);
 }
 
@@ -468,11 +462,6 @@ int epi_create(epi_ctx** out, const epi_config* cfg) {
       sms > 0)
     ctx->lc.num_sms = sms;
   int rc = cuda_status(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-  if (rc == EPI_OK) rc = cuda_status(cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking));
-  if (rc == EPI_OK)
-    rc = cuda_status(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
-  if (rc == EPI_OK)
-    rc = cuda_status(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
   if (rc == EPI_OK) rc = dev_alloc(&ctx->status, 1);
   if (rc == EPI_OK) rc = cuda_status(cudaMallocHost((void**)&ctx->status_h, sizeof(DevStatus)));
   if (rc == EPI_OK) rc = cuda_status(cudaMemset(ctx->status, 0, sizeof(DevStatus)));
@@ -495,10 +484,6 @@ void epi_destroy(epi_ctx* ctx) {
   if (ctx->status) cudaFree(ctx->status);
   if (ctx->rebuilds) cudaFree(ctx->rebuilds);
   if (ctx->status_h) cudaFreeHost(ctx->status_h);
-  if (ctx->stream2) cudaStreamSynchronize(ctx->stream2);
-  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
-  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
-  if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -624,6 +609,7 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
       (rc = dev_alloc(&c->dermis, n)) || (rc = dev_alloc(&c->cand, CC * n)) ||
       (rc = dev_alloc(&c->ncand, n)) || (rc = dev_alloc(&c->bpos, n)) ||
       (rc = dev_alloc(&c->nbr, C * n)) || (rc = dev_alloc(&c->nn, n)) ||
+      (rc = dev_alloc(&c->fmemb, n)) ||
       (rc = dev_alloc(&c->bin, n)) || (rc = dev_alloc(&c->rank, n)) ||
       (rc = dev_alloc(&c->counts, nbins)) || (rc = dev_alloc(&c->starts, nbins + 1)) ||
       (rc = dev_alloc(&c->skey, n)) || (rc = dev_alloc(&c->spos, n)) ||
@@ -881,13 +867,9 @@ int epi_step_per_tissue(epi_ctx* c, int32_t nsteps) {
     for (int t = 0; t < c->ntissues; ++t) {
       const Range r = tissue_range(c, t);
       const DevState S = make_state(c, c->cur);
-      const TissueHost& H = c->thost[t];
-      const int32_t f0 = c->nprep_memb + H.prep_f;
       launch_rebuild(S, r, c->scan, c->lc, c->stream, nullptr);
-      launch_dermis(S, f0, f0 + H.nfm, c->lc, c->stream, nullptr);
+      prepass_tissue(c, c->cur, t);
       launch_step(S, r, c->cfg.precision, c->lc, c->stream, nullptr);
-      launch_step_memb(S, H.prep_m, H.prep_m + c->tissues_h[t].nmemb, c->cfg.precision, c->lc,
-                       c->stream, nullptr);
     }
     c->cur ^= 1;
   }

@@ -67,6 +67,7 @@ struct DevState {
   float4* bpos;     // positions at the last rebuild (displacement check)
   int32_t* nbr;     // exact connection lists (materialised on request)
   int32_t* nn;
+  double4* fmemb;   // membrane bending + lattice spring + wall displacement
   int32_t* bin;
   int32_t* rank;
   int32_t* counts;

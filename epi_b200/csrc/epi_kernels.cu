@@ -30,8 +30,7 @@
 namespace epi {
 
 const char* const kKernelClassNames[KC_COUNT] = {
-    "step", "step_memb", "dermis", "rebuild_bin", "rebuild_scan", "rebuild_sort",
-    "rebuild_search", "gate"};
+    "step", "prepass", "rebuild_bin", "rebuild_scan", "rebuild_sort", "rebuild_search", "gate"};
 
 namespace {
 
@@ -491,15 +490,16 @@ __global__ void k_dermis(DevState S, int32_t f0, int32_t f1) {
 // (double: FP64 path; float: mixed path). Sums and positions stay double.
 // ---------------------------------------------------------------------------
 
-// Membrane particle i's own terms: bending (_memb_bend_calc1..3, :296-449;
-// the unit vectors of calc1 are recomputed from the eleven lattice positions
-// the stencil reaches instead of being stored), the four lattice springs of
+// Membrane particles: bending (_memb_bend_calc1..3, :296-449; the unit
+// vectors of calc1 are recomputed from the eleven lattice positions the
+// stencil reaches instead of being stored), the four lattice springs of
 // _MEMB_interaction (:529-547, each applied once by the higher index) and
-// the wall (:287-294), summed in that order into (fx, fy, fz).
+// the wall (:287-294). The sum goes to S.fmemb; k_step adds it.
 template <typename R>
-__device__ __forceinline__ void memb_forces(const DevState& S, int32_t i, const TissueDev& T,
-                                            double& fx, double& fy, double& fz) {
-  {
+__global__ void __launch_bounds__(256) k_memb_force(DevState S, int32_t m0, int32_t m1) {
+  GRID_STRIDE(e, m0, m1) {
+    const int32_t i = S.prep[e];
+    const TissueDev& T = S.tissues[attr_tissue(S.attr[i])];
     const Laws<R>& L = T.laws<R>();
     const double dt = T.P.dt;
     const int32_t pb = T.pbase, NMX = T.nmx, NMY = T.nmy;
@@ -580,9 +580,7 @@ __device__ __forceinline__ void memb_forces(const DevState& S, int32_t i, const 
       const R ljm = L.eps4 * lj6 * (lj6 - R(1)) / (distlj * distlj);
       az += double(R(dt) * ljm * R(2) * z);
     }
-    fx = ax;
-    fy = ay;
-    fz = az;
+    S.fmemb[i] = make_double4(ax, ay, az, 0.0);
   }
 }
 
@@ -672,13 +670,12 @@ struct Particle {
     az = fma(sdt, dz, az);
   }
 
-  // fx, fy, fz: a membrane particle's own terms (memb_forces), added after
-  // its pair terms; ignored for cells.
-  __device__ __forceinline__ void finish(double fx, double fy, double fz) {
+  __device__ __forceinline__ void finish() {
     if (st == ST_MEMB) {
-      ax += fx;
-      ay += fy;
-      az += fz;
+      const double4 f = S.fmemb[i];
+      ax += f.x;
+      ay += f.y;
+      az += f.z;
     } else if (!kSimple) {
       // wall_interaction (:287-294) for DER below its radius
       if (st == ST_DER && p.z < p.w) {
@@ -733,19 +730,22 @@ struct Particle {
   }
 };
 
-// The candidate loop of one particle. The chain candidate index -> position
-// is software-pipelined: indices are loaded two candidates ahead (they
-// stream from HBM), positions one ahead (gathers from L1/L2), so neither
-// latency is paid serially per candidate.
-template <typename R, bool kSimple, bool kOld>
-__device__ __forceinline__ void candidate_loop(const DevState& S, int64_t i,
-                                               Particle<R, kSimple, kOld>& P) {
+// One thread per particle. The candidate chain index -> position is
+// software-pipelined: indices are loaded two candidates ahead (they stream
+// from HBM), positions one ahead (gathers from L1/L2), so neither latency is
+// paid serially per candidate. kMinBlocks bounds the registers so that that
+// many 256-thread blocks stay resident per SM.
+template <typename R, bool kSimple, bool kOld, int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) k_step(DevState S, Range r) {
+  const int64_t i = r.p0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= r.p1) return;
   const int64_t N = S.n_total;
   const int32_t nc = __ldg(&S.ncand[i]);
   const int32_t* cp = S.cand + i;  // column-major: entry k at cp[k * N]
-  int32_t q0 = nc > 0 ? __ldg(cp) : 0;
   int32_t q1 = nc > 1 ? __ldg(cp + N) : 0;
   int32_t q2 = nc > 2 ? __ldg(cp + 2 * N) : 0;
+  Particle<R, kSimple, kOld> P(S, (int32_t)i);
+  int32_t q0 = nc > 0 ? __ldg(cp) : 0;
   double4 p0 = nc > 0 ? S.pos_cur[q0] : P.p;
   cp += 3 * N;
   for (int32_t k = 0; k < nc; ++k) {
@@ -760,33 +760,7 @@ __device__ __forceinline__ void candidate_loop(const DevState& S, int64_t i,
     if (k + 1 < nc) p0 = S.pos_cur[q0];
     P.candidate(q, pq);
   }
-}
-
-// Cells (every particle that is not a membrane particle), one thread each.
-// kMinBlocks bounds the registers so that that many 256-thread blocks stay
-// resident per SM.
-template <typename R, bool kSimple, bool kOld, int kMinBlocks>
-__global__ void __launch_bounds__(256, kMinBlocks) k_step(DevState S, Range r) {
-  const int64_t i = r.p0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= r.p1 || attr_state(__ldg(&S.attr[i])) == ST_MEMB) return;
-  Particle<R, kSimple, kOld> P(S, (int32_t)i);
-  candidate_loop(S, i, P);
-  P.finish(0.0, 0.0, 0.0);
-}
-
-// Membrane particles (prep entries [m0, m1)), one thread each: pairs with
-// cells over the candidates, then the particle's own terms. Independent of
-// k_step (disjoint outputs), so the two may run concurrently.
-template <typename R, bool kSimple, bool kOld>
-__global__ void __launch_bounds__(256) k_step_memb(DevState S, int32_t m0, int32_t m1) {
-  const int32_t e = m0 + (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
-  if (e >= m1) return;
-  const int32_t i = __ldg(&S.prep[e]);
-  Particle<R, kSimple, kOld> P(S, i);
-  candidate_loop(S, i, P);
-  double fx, fy, fz;
-  memb_forces<R>(S, i, P.T, fx, fy, fz);
-  P.finish(fx, fy, fz);
+  P.finish();
 }
 
 // connect_cell's lists (for export): the exact predicate over the candidates.
@@ -916,12 +890,19 @@ void launch_rebuild(const DevState& S, const Range& r, const ScanScratch&,
   timer_end(tm, KC_GATE, s);
 }
 
-void launch_dermis(const DevState& S, int32_t f0, int32_t f1, const LaunchCfg& lc,
-                   cudaStream_t s, Timer* tm) {
-  if (f1 <= f0) return;
-  timer_begin(tm, KC_DERMIS, s);
-  k_dermis<<<stride_blocks(f1 - f0, lc.block, lc), lc.block, 0, s>>>(S, f0, f1);
-  timer_end(tm, KC_DERMIS, s);
+void launch_prepass(const DevState& S, int32_t m0, int32_t m1, int32_t f0, int32_t f1,
+                    int precision, const LaunchCfg& lc, cudaStream_t s, Timer* tm) {
+  if (m1 <= m0 && f1 <= f0) return;
+  timer_begin(tm, KC_PREPASS, s);
+  if (m1 > m0) {
+    const int gm = stride_blocks(m1 - m0, lc.block, lc);
+    if (precision == 1)
+      k_memb_force<float><<<gm, lc.block, 0, s>>>(S, m0, m1);
+    else
+      k_memb_force<double><<<gm, lc.block, 0, s>>>(S, m0, m1);
+  }
+  if (f1 > f0) k_dermis<<<stride_blocks(f1 - f0, lc.block, lc), lc.block, 0, s>>>(S, f0, f1);
+  timer_end(tm, KC_PREPASS, s);
 }
 
 template <typename R, bool kSimple, bool kOld>
@@ -955,29 +936,6 @@ void launch_step(const DevState& S, const Range& r, int precision, const LaunchC
   else
     launch_step_r<double>(S, r, lc, s);
   timer_end(tm, KC_STEP, s);
-}
-
-template <typename R>
-void launch_step_memb_r(const DevState& S, int32_t m0, int32_t m1, const LaunchCfg& lc,
-                        cudaStream_t s) {
-  const int grid = blocks_for(m1 - m0, 256);
-  if (lc.simple && lc.any_old)
-    k_step_memb<R, true, true><<<grid, 256, 0, s>>>(S, m0, m1);
-  else if (lc.simple)
-    k_step_memb<R, true, false><<<grid, 256, 0, s>>>(S, m0, m1);
-  else
-    k_step_memb<R, false, true><<<grid, 256, 0, s>>>(S, m0, m1);
-}
-
-void launch_step_memb(const DevState& S, int32_t m0, int32_t m1, int precision,
-                      const LaunchCfg& lc, cudaStream_t s, Timer* tm) {
-  if (m1 <= m0) return;
-  timer_begin(tm, KC_STEP_MEMB, s);
-  if (precision == 1)
-    launch_step_memb_r<float>(S, m0, m1, lc, s);
-  else
-    launch_step_memb_r<double>(S, m0, m1, lc, s);
-  timer_end(tm, KC_STEP_MEMB, s);
 }
 
 void launch_exact_lists(const DevState& S, const Range& r, const LaunchCfg& lc,

@@ -28,7 +28,7 @@ struct LaunchCfg {
 
 // Kernel classes, for per-class timing.
 enum KernelClass : int {
-  KC_STEP = 0, KC_STEP_MEMB, KC_DERMIS, KC_REBUILD_BIN, KC_REBUILD_SCAN, KC_REBUILD_SORT,
+  KC_STEP = 0, KC_PREPASS, KC_REBUILD_BIN, KC_REBUILD_SCAN, KC_REBUILD_SORT,
   KC_REBUILD_SEARCH, KC_GATE, KC_COUNT
 };
 extern const char* const kKernelClassNames[KC_COUNT];
@@ -48,19 +48,15 @@ void launch_scan(const int32_t* in, int32_t* out, int32_t n, int32_t init,
 // -> candidate search -> gate reset.
 void launch_rebuild(const DevState& S, const Range& r, const ScanScratch& sc,
                     const LaunchCfg& lc, cudaStream_t s, Timer* tm);
-// find_dermis for the FIX / MUSUME cells of prep entries [f0, f1).
-void launch_dermis(const DevState& S, int32_t f0, int32_t f1, const LaunchCfg& lc,
-                   cudaStream_t s, Timer* tm);
+// Membrane bending scratch (_memb_bend_calc1) and dermis (find_dermis) for
+// prep entries [m0, m1) (membrane role) and [f0, f1) (FIX / MUSUME role).
+void launch_prepass(const DevState& S, int32_t m0, int32_t m1, int32_t f0, int32_t f1,
+                    int precision, const LaunchCfg& lc, cudaStream_t s, Timer* tm);
 // cell_interaction + pos_copy + cell_pos_periodic_fix from the current
-// positions into S.pos_nxt, for the cells of range r (launch_step) and the
-// membrane particles of prep entries [m0, m1) (launch_step_memb); flags
-// tissues whose particles moved more than skin/2 since their last rebuild.
-// The two write disjoint particles and may run concurrently; both need the
-// dermis of the step's positions (launch_dermis) when FIX / MUSUME cells exist.
+// positions into S.pos_nxt; flags tissues whose particles moved more than
+// skin/2 since their last rebuild.
 void launch_step(const DevState& S, const Range& r, int precision, const LaunchCfg& lc,
                  cudaStream_t s, Timer* tm);
-void launch_step_memb(const DevState& S, int32_t m0, int32_t m1, int precision,
-                      const LaunchCfg& lc, cudaStream_t s, Timer* tm);
 // Exact connection lists (connect_cell's result) into S.nbr / S.nn.
 void launch_exact_lists(const DevState& S, const Range& r, const LaunchCfg& lc,
                         cudaStream_t s);
