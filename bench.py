@@ -289,7 +289,7 @@ def main():
     ap.add_argument("--mode", default="graph", choices=["graph", "eager"])
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default skin / variant instead of epi_autotune's choice")
-    ap.add_argument("--tune-steps", type=int, default=64, help="timed steps per autotuner trial")
+    ap.add_argument("--tune-steps", type=int, default=128, help="timed steps per autotuner trial")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--ref-particles", type=int, default=120000)
@@ -330,6 +330,10 @@ def main():
     ctx.upload(mine)
     tuned = None
     if args.skin is None and args.variant is None and not args.no_autotune:
+        # tune on the state the timed region starts from (after the warm-up's
+        # relaxation of the jittered start), then warm up again below
+        if args.warmup:
+            ctx.step(args.warmup, args.mode)
         skin, variant, trial_ms = ctx.autotune(args.tune_steps)
         tuned = {"skin": skin, "variant": variant, "trial_ms_per_step": trial_ms,
                  "trial_steps": args.tune_steps,
