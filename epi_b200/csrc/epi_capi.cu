@@ -75,6 +75,8 @@ struct epi_ctx {
   // device buffers
   TissueDev* tissues = nullptr;
   double4* pos[2] = {nullptr, nullptr};
+  float4* posf[2] = {nullptr, nullptr};
+  bool posf_stale = true;  // pos[cur] was written outside the step kernel
   int cur = 0;
   uint32_t* attr = nullptr;
   int32_t* pair = nullptr;
@@ -137,7 +139,7 @@ void destroy_graphs(epi_ctx* c) {
 
 void free_buffers(epi_ctx* c) {
   destroy_graphs(c);
-  void* ptrs[] = {c->tissues, c->pos[0], c->pos[1], c->attr, c->pair, c->spr, c->dermis,
+  void* ptrs[] = {c->tissues, c->pos[0], c->pos[1], c->posf[0], c->posf[1], c->attr, c->pair, c->spr, c->dermis,
                   c->cand, c->ncand, c->bpos, c->nbr, c->nn, c->fmemb, c->bin,
                   c->rank, c->counts, c->starts, c->skey, c->spos, c->gate, c->rl, c->prep,
                   c->scan.partial, c->stage};
@@ -145,6 +147,7 @@ void free_buffers(epi_ctx* c) {
     if (p) cudaFree(p);
   c->tissues = nullptr;
   c->pos[0] = c->pos[1] = nullptr;
+  c->posf[0] = c->posf[1] = nullptr;
   c->attr = nullptr; c->pair = nullptr; c->spr = nullptr; c->dermis = nullptr;
   c->cand = nullptr; c->ncand = nullptr; c->bpos = nullptr;
   c->nbr = nullptr; c->nn = nullptr; c->fmemb = nullptr;
@@ -160,6 +163,8 @@ DevState make_state(epi_ctx* c, int cur) {
   S.tissues = c->tissues;
   S.pos_cur = c->pos[cur];
   S.pos_nxt = c->pos[cur ^ 1];
+  S.posf_cur = c->posf[cur];
+  S.posf_nxt = c->posf[cur ^ 1];
   S.attr = c->attr;
   S.pair = c->pair;
   S.spr = c->spr;
@@ -214,8 +219,17 @@ void prepass_tissue(epi_ctx* c, int cur, int t) {
                  c->cfg.precision, c->lc, c->stream, nullptr);
 }
 
+// Refreshes the FP32 position copy of the current parity after positions
+// were written by anything but the step kernel (upload, restore, ...).
+void ensure_posf(epi_ctx* c) {
+  if (!c->posf_stale) return;
+  launch_posf(make_state(c, c->cur), c->lc, c->stream);
+  c->posf_stale = false;
+}
+
 // One reference step over the batch: [rebuild] -> prepass -> fused step.
 void enqueue_step(epi_ctx* c, int& cur, Timer* tm) {
+  ensure_posf(c);
   launch_rebuild(make_state(c, cur), whole(c), c->scan, c->lc, c->stream, tm);
   prepass_all(c, cur, tm);
   launch_step(make_state(c, cur), whole(c), c->cfg.precision, c->lc, c->stream, tm);
@@ -248,6 +262,7 @@ int check_status(epi_ctx* c) {
 // nsteps steps replayed from the two-step graph of the current parity
 // (captured on first use), plus one eager step for an odd count.
 int enqueue_graph_steps(epi_ctx* c, int32_t nsteps) {
+  ensure_posf(c);  // never inside the captured graph
   const int32_t pairs = nsteps / 2;
   if (pairs > 0) {
     cudaGraphExec_t& ge = c->graph[c->cur];
@@ -335,6 +350,29 @@ void range_thresholds(TissueDev& T) {
   T.gz_hi = first_true(zbig, [&](double v) { return (int32_t)(v / AG) >= T.anz; });
   T.cz_hi = T.gz_hi;
   T.cz_lo = -first_true(zbig, [&](double w) { return (int32_t)(w / AG) >= 1; });
+}
+
+// FP32 box constants and the band around the connection threshold inside
+// which the mixed path defers to the FP64 predicate. With u = 2^-24 (FP32
+// unit roundoff), M a bound on |coordinate| and D = LJ_THRESH * 2 rmax the
+// longest connection: each coordinate rounds by <= M u, a separation
+// component (difference, then possibly +-L) by <= 4 M u =: e; d2 in FP32
+// then errs by <= 2 sqrt(3) D e + 3 e^2 + 4 D^2 u, and the FP32 threshold
+// LJ_THRESH^2 (r_i + r_j)^2 by <= 9 D^2 u. ftol is twice the sum (plus the
+// FP64 predicate's own rounding, far below).
+void set_fp32_bounds(TissueDev& T) {
+  T.lxf = (float)T.lx;
+  T.lyf = (float)T.ly;
+  T.hlxf = (float)T.hlx;
+  T.hlyf = (float)T.hly;
+  T.lt2f = (float)(T.P.lj_thresh * T.P.lj_thresh);
+  const double u = std::ldexp(1.0, -24);
+  const double M = std::max(std::max(T.lx, T.ly), T.lz) + 8.0;
+  const double e = 4.0 * M * u;
+  const double D = T.P.lj_thresh * 2.0 * T.rmax;
+  const double tol = 2.0 * (2.0 * std::sqrt(3.0) * D * e + 3.0 * e * e + 13.0 * D * D * u) +
+                     1e-14 * D * D;
+  T.ftol = (float)(tol * (1.0 + 1e-3));
 }
 
 int validate_tissue(const epi_tissue_view& v, const epi_params& P) {
@@ -584,6 +622,7 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
     }
     T.rmax = rmax;
     T.rmax_nm = rmax_nm;
+    set_fp32_bounds(T);
     H.nfm = (int32_t)prep_f.size() - H.prep_f;
     pbase += v.n;
     binbase += T.anx * T.any * T.anz + 1;  // + sentinel (end offset of the tissue)
@@ -604,7 +643,8 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
     }
   }
   if (!reuse && ((rc = dev_alloc(&c->tissues, ntissues)) || (rc = dev_alloc(&c->pos[0], n)) ||
-      (rc = dev_alloc(&c->pos[1], n)) || (rc = dev_alloc(&c->attr, n)) ||
+      (rc = dev_alloc(&c->pos[1], n)) || (rc = dev_alloc(&c->posf[0], n)) ||
+      (rc = dev_alloc(&c->posf[1], n)) || (rc = dev_alloc(&c->attr, n)) ||
       (rc = dev_alloc(&c->pair, n)) || (rc = dev_alloc(&c->spr, n)) ||
       (rc = dev_alloc(&c->dermis, n)) || (rc = dev_alloc(&c->cand, CC * n)) ||
       (rc = dev_alloc(&c->ncand, n)) || (rc = dev_alloc(&c->bpos, n)) ||
@@ -631,6 +671,7 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
                            cudaMemcpyHostToDevice, s));
   EPI_CUDA(cudaMemcpyAsync(c->pos[0], pos.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, s));
   EPI_CUDA(cudaMemcpyAsync(c->pos[1], pos.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, s));
+  c->posf_stale = true;
   EPI_CUDA(cudaMemcpyAsync(c->attr, attr.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s));
   EPI_CUDA(cudaMemcpyAsync(c->pair, pair.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
   EPI_CUDA(cudaMemcpyAsync(c->spr, spr.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
@@ -706,6 +747,7 @@ int epi_adjoint(epi_ctx* c, int32_t nsteps, int32_t K, const epi_loss* loss, dou
     // recompute X_t0 .. X_{t1-1} from the checkpoint
     EPI_CUDA(cudaMemcpyAsync(c->pos[c->cur], ckpt + (size_t)seg * n, pbytes,
                              cudaMemcpyDeviceToDevice, s));
+    c->posf_stale = true;
     launch_gate_check(make_state(c, c->cur), c->lc, s);
     for (int32_t t = t0; t < t1; ++t) {
       EPI_CUDA(cudaMemcpyAsync(hist + (size_t)(t - t0) * n, c->pos[c->cur], pbytes,
@@ -727,6 +769,7 @@ int epi_adjoint(epi_ctx* c, int32_t nsteps, int32_t K, const epi_loss* loss, dou
   }
   // the context ends at X_T; its candidates are rebuilt before the next step
   EPI_CUDA(cudaMemcpyAsync(c->pos[c->cur], xT, pbytes, cudaMemcpyDeviceToDevice, s));
+  c->posf_stale = true;
   launch_set_gates(make_state(c, c->cur), nt, s);
   std::vector<double> h(4 * (size_t)nt);
   EPI_CUDA(cudaMemcpyAsync(h.data(), acc, 32 * (size_t)nt, cudaMemcpyDeviceToHost, s));
@@ -816,6 +859,7 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
   auto restore = [&]() -> int {
     EPI_CUDA(cudaMemcpyAsync(c->pos[cur0], saved, pbytes, cudaMemcpyDeviceToDevice, s));
     c->cur = cur0;
+    c->posf_stale = true;
     launch_set_gates(make_state(c, c->cur), c->ntissues, s);
     c->lists_fresh = false;
     return EPI_OK;
@@ -863,6 +907,7 @@ int epi_step_per_tissue(epi_ctx* c, int32_t nsteps) {
   EPI_GUARD_BEGIN
   int rc = set_device(c);
   if (rc) return rc;
+  ensure_posf(c);
   for (int32_t k = 0; k < nsteps; ++k) {
     for (int t = 0; t < c->ntissues; ++t) {
       const Range r = tissue_range(c, t);

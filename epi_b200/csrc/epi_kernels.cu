@@ -25,6 +25,8 @@
 // cell_interaction.cpp:48-66). No atomics touch positions, so a step is
 // deterministic and repeatable bit for bit.
 #include "epi_kernels.h"
+
+#include <type_traits>
 #include "epi_device.cuh"
 
 namespace epi {
@@ -490,6 +492,41 @@ __global__ void k_dermis(DevState S, int32_t f0, int32_t f1) {
 // (double: FP64 path; float: mixed path). Sums and positions stay double.
 // ---------------------------------------------------------------------------
 
+// Offsets of lattice neighbours from membrane particle i (minimum image): from
+// the FP64 positions in the FP64 path, from the FP32 copies in the mixed path.
+template <typename R>
+struct SiteOffsets;
+template <>
+struct SiteOffsets<double> {
+  const DevState& S;
+  const double4 p;
+  const TissueDev& T;
+  __device__ __forceinline__ SiteOffsets(const DevState& S_, int32_t, const double4& p_,
+                                         const TissueDev& T_)
+      : S(S_), p(p_), T(T_) {}
+  __device__ __forceinline__ Vec3<double> operator()(int32_t q) const {
+    return offset_of<double>(S.pos_cur[q], p, T);
+  }
+};
+template <>
+struct SiteOffsets<float> {
+  const DevState& S;
+  const float4 pf;
+  const TissueDev& T;
+  __device__ __forceinline__ SiteOffsets(const DevState& S_, int32_t i, const double4&,
+                                         const TissueDev& T_)
+      : S(S_), pf(S_.posf_cur[i]), T(T_) {}
+  __device__ __forceinline__ Vec3<float> operator()(int32_t q) const {
+    const float4 o = S.posf_cur[q];
+    float dx = o.x - pf.x, dy = o.y - pf.y;
+    if (dx > T.hlxf) dx -= T.lxf;
+    else if (dx <= -T.hlxf) dx += T.lxf;
+    if (dy > T.hlyf) dy -= T.lyf;
+    else if (dy <= -T.hlyf) dy += T.lyf;
+    return Vec3<float>{dx, dy, o.z - pf.z};
+  }
+};
+
 // Membrane particles: bending (_memb_bend_calc1..3, :296-449; the unit
 // vectors of calc1 are recomputed from the eleven lattice positions the
 // stencil reaches instead of being stored), the four lattice springs of
@@ -515,18 +552,19 @@ __global__ void __launch_bounds__(256) k_memb_force(DevState S, int32_t m0, int3
       return pb + w * NMX + c;
     };
     const double4 p = S.pos_cur[i];
+    const SiteOffsets<R> off(S, i, p, T);
     double ax = 0.0, ay = 0.0, az = 0.0;
     {
-      const Vec3<R> o_r = offset_of<R>(S.pos_cur[site(1, 0)], p, T);
-      const Vec3<R> o_rr = offset_of<R>(S.pos_cur[site(2, 0)], p, T);
-      const Vec3<R> o_l = offset_of<R>(S.pos_cur[site(-1, 0)], p, T);
-      const Vec3<R> o_ll = offset_of<R>(S.pos_cur[site(-2, 0)], p, T);
-      const Vec3<R> o_u = offset_of<R>(S.pos_cur[site(0, 1)], p, T);
-      const Vec3<R> o_uu = offset_of<R>(S.pos_cur[site(0, 2)], p, T);
-      const Vec3<R> o_b = offset_of<R>(S.pos_cur[site(0, -1)], p, T);
-      const Vec3<R> o_bb = offset_of<R>(S.pos_cur[site(0, -2)], p, T);
-      const Vec3<R> o_bbr = offset_of<R>(S.pos_cur[site(1, -2)], p, T);
-      const Vec3<R> o_bbrr = offset_of<R>(S.pos_cur[site(2, -2)], p, T);
+      const Vec3<R> o_r = off(site(1, 0));
+      const Vec3<R> o_rr = off(site(2, 0));
+      const Vec3<R> o_l = off(site(-1, 0));
+      const Vec3<R> o_ll = off(site(-2, 0));
+      const Vec3<R> o_u = off(site(0, 1));
+      const Vec3<R> o_uu = off(site(0, 2));
+      const Vec3<R> o_b = off(site(0, -1));
+      const Vec3<R> o_bb = off(site(0, -2));
+      const Vec3<R> o_bbr = off(site(1, -2));
+      const Vec3<R> o_bbrr = off(site(2, -2));
       const Vec3<R> o0{R(0), R(0), R(0)};
       const Unit<R> nv = unit_ab(o0, o_r), nvr = unit_ab(o_r, o_rr);
       const Unit<R> nvl = unit_ab(o_l, o0), nvll = unit_ab(o_ll, o_l);
@@ -598,6 +636,10 @@ __global__ void __launch_bounds__(256) k_memb_force(DevState S, int32_t m0, int3
 // cells' ages.
 template <typename R, bool kSimple, bool kOld>
 struct Particle {
+  // The mixed path gathers candidates' FP32 copies and forms separations in
+  // FP32; the FP64 path gathers the FP64 positions.
+  static constexpr bool kFloatPos = sizeof(R) == 4;
+  using Pos = typename std::conditional<kFloatPos, float4, double4>::type;
   const DevState& S;
   const int32_t i;
   const uint32_t a;
@@ -610,25 +652,70 @@ struct Particle {
   const R dt;
   int32_t pair_i = -1, dermis_i = -1;
   double ax = 0.0, ay = 0.0, az = 0.0;
+  // the particle's FP32 copy (mixed path only)
+  float4 pf = make_float4(0.f, 0.f, 0.f, 0.f);
 
   __device__ __forceinline__ Particle(const DevState& S_, int32_t i_)
       : S(S_), i(i_), a(__ldg(&S_.attr[i_])), t(attr_tissue(a)), st(attr_state(a)),
         T(S_.tissues[t]), L(T.laws<R>()), p(S_.pos_cur[i_]),
         lt2(T.P.lj_thresh * T.P.lj_thresh), dt(R(T.P.dt)) {
+    if (kFloatPos) pf = S.posf_cur[i];
     if (!kSimple && st != ST_MEMB) {
       pair_i = __ldg(&S.pair[i]);
       if (st == ST_FIX || st == ST_MUSUME) dermis_i = __ldg(&S.dermis[i]);
     }
   }
 
-  __device__ __forceinline__ void candidate(int32_t q, const double4& pq) {
-    const double dx = pdiff_h(p.x, pq.x, T.lx, T.hlx), dy = pdiff_h(p.y, pq.y, T.ly, T.hly);
-    const double dz = p.z - pq.z;
-    const double d2e = dist_sq_exact(dx, dy, dz);
+  // Connection test and separation of candidate q. FP64 path: the
+  // reference's predicate (connect_proc :115-119) with its rounding. Mixed
+  // path: the same test in FP32, decided by the FP64 predicate whenever the
+  // FP32 d2 lies within T.ftol of the threshold, so the connection set is
+  // the reference's in both.
+  __device__ __forceinline__ bool connected(int32_t q, const double4& pq, R& dx, R& dy, R& dz,
+                                            R& d2, R& rs) const {
+    const double ddx = pdiff_h(p.x, pq.x, T.lx, T.hlx), ddy = pdiff_h(p.y, pq.y, T.ly, T.hly);
+    const double ddz = p.z - pq.z;
+    const double d2e = dist_sq_exact(ddx, ddy, ddz);
     const double rse = __dadd_rn(p.w, pq.w);
-    if (!(d2e <= __dmul_rn(__dmul_rn(lt2, rse), rse))) return;
-    const R d2 = R(d2e);
-    const R rs = R(rse);
+    if (!(d2e <= __dmul_rn(__dmul_rn(lt2, rse), rse))) return false;
+    dx = R(ddx);
+    dy = R(ddy);
+    dz = R(ddz);
+    d2 = R(d2e);
+    rs = R(rse);
+    return true;
+  }
+  __device__ __forceinline__ bool connected(int32_t q, const float4& qf, R& dx, R& dy, R& dz,
+                                            R& d2, R& rs) const {
+    float fx = pf.x - qf.x, fy = pf.y - qf.y;
+    if (fx > T.hlxf) fx -= T.lxf;
+    else if (fx <= -T.hlxf) fx += T.lxf;
+    if (fy > T.hlyf) fy -= T.lyf;
+    else if (fy <= -T.hlyf) fy += T.lyf;
+    const float fz = pf.z - qf.z;
+    const float f2 = fx * fx + fy * fy + fz * fz;
+    const float frs = pf.w + qf.w;
+    const float thr = T.lt2f * frs * frs;
+    if (f2 > thr + T.ftol) return false;
+    if (f2 >= thr - T.ftol) {
+      // too close to the threshold for FP32: the reference's FP64 predicate
+      const double4 pq = S.pos_cur[q];
+      const double d2e = dist_sq_exact(pdiff_h(p.x, pq.x, T.lx, T.hlx),
+                                       pdiff_h(p.y, pq.y, T.ly, T.hly), p.z - pq.z);
+      const double rse = __dadd_rn(p.w, pq.w);
+      if (!(d2e <= __dmul_rn(__dmul_rn(lt2, rse), rse))) return false;
+    }
+    dx = R(fx);
+    dy = R(fy);
+    dz = R(fz);
+    d2 = R(f2);
+    rs = R(frs);
+    return true;
+  }
+
+  __device__ __forceinline__ void candidate(int32_t q, const Pos& pq) {
+    R dx, dy, dz, d2, rs;
+    if (!connected(q, pq, dx, dy, dz, d2, rs)) return;
     R coef;
     if (kSimple) {
       const bool both_old = kOld && attr_old(a) && attr_old(__ldg(&S.attr[q]));
@@ -664,10 +751,10 @@ struct Particle {
       }
     }
     // DT * coef * separation (cell_interaction_apply, :56-58), summed in FP64
-    const double sdt = double(dt * coef);
-    ax = fma(sdt, dx, ax);
-    ay = fma(sdt, dy, ay);
-    az = fma(sdt, dz, az);
+    const R sdt = dt * coef;
+    ax += double(sdt * dx);
+    ay += double(sdt * dy);
+    az += double(sdt * dz);
   }
 
   __device__ __forceinline__ void finish() {
@@ -714,6 +801,7 @@ struct Particle {
       raise_error(S.status, E_BIN_RANGE, i, -1, nz);
     }
     S.pos_nxt[i] = make_double4(nx, ny, nz, p.w);
+    if (kFloatPos) S.posf_nxt[i] = make_float4((float)nx, (float)ny, (float)nz, (float)p.w);
     // Candidate validity: rebuild the tissue once a particle moved skin/2.
     const float4 b = S.bpos[i];
     double ex = nx - (double)b.x, ey = ny - (double)b.y;
@@ -735,6 +823,17 @@ struct Particle {
 // from HBM), positions one ahead (gathers from L1/L2), so neither latency is
 // paid serially per candidate. kMinBlocks bounds the registers so that that
 // many 256-thread blocks stay resident per SM.
+template <typename Pos>
+__device__ __forceinline__ const Pos* gather_source(const DevState& S);
+template <>
+__device__ __forceinline__ const double4* gather_source<double4>(const DevState& S) {
+  return S.pos_cur;
+}
+template <>
+__device__ __forceinline__ const float4* gather_source<float4>(const DevState& S) {
+  return S.posf_cur;
+}
+
 template <typename R, bool kSimple, bool kOld, int kMinBlocks>
 __global__ void __launch_bounds__(256, kMinBlocks) k_step(DevState S, Range r) {
   const int64_t i = r.p0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -744,20 +843,23 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_step(DevState S, Range r) {
   const int32_t* cp = S.cand + i;  // column-major: entry k at cp[k * N]
   int32_t q1 = nc > 1 ? __ldg(cp + N) : 0;
   int32_t q2 = nc > 2 ? __ldg(cp + 2 * N) : 0;
-  Particle<R, kSimple, kOld> P(S, (int32_t)i);
+  using Part = Particle<R, kSimple, kOld>;
+  using Pos = typename Part::Pos;
+  Part P(S, (int32_t)i);
+  const Pos* src = gather_source<Pos>(S);
   int32_t q0 = nc > 0 ? __ldg(cp) : 0;
-  double4 p0 = nc > 0 ? S.pos_cur[q0] : P.p;
+  Pos p0 = src[q0];
   cp += 3 * N;
   for (int32_t k = 0; k < nc; ++k) {
     const int32_t q = q0;
-    const double4 pq = p0;
+    const Pos pq = p0;
     q0 = q1;
     q1 = q2;
     if (k + 3 < nc) {
       q2 = __ldg(cp);
       cp += N;
     }
-    if (k + 1 < nc) p0 = S.pos_cur[q0];
+    if (k + 1 < nc) p0 = src[q0];
     P.candidate(q, pq);
   }
   P.finish();
@@ -848,9 +950,23 @@ __global__ void k_pack(DevState S, const double* x, const double* y, const doubl
   const double4 p = make_double4(x[i], y[i], z[i], r);
   S.pos_cur[i] = p;
   S.pos_nxt[i] = p;
+  const float4 f = make_float4((float)p.x, (float)p.y, (float)p.z, (float)r);
+  S.posf_cur[i] = f;
+  S.posf_nxt[i] = f;
+}
+
+__global__ void k_posf(DevState S) {
+  GRID_STRIDE(i, 0, S.n_total) {
+    const double4 p = S.pos_cur[i];
+    S.posf_cur[i] = make_float4((float)p.x, (float)p.y, (float)p.z, (float)p.w);
+  }
 }
 
 }  // namespace
+
+void launch_posf(const DevState& S, const LaunchCfg& lc, cudaStream_t s) {
+  if (S.n_total > 0) k_posf<<<stride_blocks(S.n_total, lc.block, lc), lc.block, 0, s>>>(S);
+}
 
 void launch_scan(const int32_t* in, int32_t* out, int32_t n, int32_t init,
                  const ScanScratch& sc, const int32_t* gate, const LaunchCfg&,

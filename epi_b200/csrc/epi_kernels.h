@@ -71,6 +71,8 @@ void launch_unpack_positions(const DevState& S, double* x, double* y, double* z,
                              cudaStream_t s);
 void launch_pack_positions(const DevState& S, const double* x, const double* y,
                            const double* z, int32_t n, cudaStream_t s);
+// FP32 copies of the current positions (S.posf_cur from S.pos_cur).
+void launch_posf(const DevState& S, const LaunchCfg& lc, cudaStream_t s);
 
 // ---- reverse-mode adjoint (FP64), membrane + ALIVE / DEAD / AIR tissues ----
 struct AdjointBuffers {

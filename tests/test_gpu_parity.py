@@ -287,3 +287,66 @@ def test_kernel_timing_reports_every_class(built):
                        "rebuild_search", "gate"}
     assert all(v[1] == 3 for v in tm.values())
     assert tm["step"][0] > 0
+
+
+def threshold_pair_tissue():
+    """A dermis cell with one ALIVE cell at the largest FP64 separation the
+    reference still connects and one at the smallest it does not (same axis,
+    reference rounding), far from everything else. ljmain, which the DER
+    applies to the ALIVE cell (cell_interaction.cpp:549-561), is not zero at
+    the cut-off, so a misjudged pair moves the DER by ~4e-5."""
+    side = 16
+    nm = side * side
+    jj, kk = np.meshgrid(np.arange(side), np.arange(side), indexing="xy")
+    mx, my = (jj.ravel() + 0.5).astype(float), (kk.ravel() + 0.5).astype(float)
+    xd, yd, zd = 8.0, 8.0, 6.0
+    r_der, r_cell = T.R_DER, 0.5
+    lt2 = 1.2 * 1.2
+    rs = r_der + r_cell
+    thr = lt2 * rs * rs
+
+    def connected(xa):
+        dx = xd - xa
+        return dx * dx + 0.0 * 0.0 + 0.0 * 0.0 <= thr
+
+    # largest xa > xd (ALIVE to the right) still connected: walk up from a guess
+    xa = xd + 1.2 * rs
+    while connected(np.nextafter(xa, np.inf)):
+        xa = np.nextafter(xa, np.inf)
+    while not connected(xa):
+        xa = np.nextafter(xa, -np.inf)
+    inside = xa
+    # smallest xb < xd (to the left) not connected
+    xb = xd - 1.2 * rs
+    while connected(xb):
+        xb = np.nextafter(xb, -np.inf)
+    while not connected(np.nextafter(xb, np.inf)):
+        xb = np.nextafter(xb, np.inf)
+    outside = xb
+    x = np.concatenate([mx, [xd, inside, outside]])
+    y = np.concatenate([my, [yd, yd, yd]])
+    z = np.concatenate([np.full(nm, 1.0), [zd, zd, zd]])
+    n = nm + 3
+    t = T.Tissue(nmx=side, nmy=side, lx=16.0, ly=16.0, lz=32.0, x=x, y=y, z=z,
+                 radius=np.concatenate([np.full(nm, T.R_MEMB), [r_der, r_cell, r_cell]]),
+                 state=np.concatenate([np.full(nm, T.MEMB, np.uint8),
+                                       np.array([T.DER, T.ALIVE, T.ALIVE], np.uint8)]),
+                 agek=np.zeros(n), spr_nat_len=np.zeros(n), pair=np.full(n, -1, np.int32),
+                 rest_div_times=np.zeros(n, np.int32), nmemb=nm, nder=1, name="threshold")
+    t.validate()
+    return t
+
+
+def test_mixed_path_decides_threshold_pairs_with_the_fp64_predicate(built):
+    t = threshold_pair_tissue()
+    d = t.nmemb
+    _, off, idx, _ = run_gpu([t], 0, FP64)
+    assert list(idx[off[d]:off[d + 1]]) == [d + 1]  # inside connected, outside not
+    p64, _, _, _ = run_gpu([t], 1, FP64)
+    pmx, _, _, _ = run_gpu([t], 1, MIXED)
+    moved = abs(p64[0][d] - t.x[d])
+    assert moved > 1e-5  # the inside pair pulls the DER
+    # FP32 cannot separate these pairs; the mixed path must agree with FP64
+    for k in range(3):
+        assert abs(pmx[k][d] - p64[k][d]) < 1e-9, (k, pmx[k][d], p64[k][d])
+        assert abs(pmx[k][d + 2] - p64[k][d + 2]) < 1e-9
