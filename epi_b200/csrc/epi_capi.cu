@@ -63,6 +63,7 @@ struct TissueHost {
 struct epi_ctx {
   epi_config cfg{};
   cudaStream_t stream = nullptr;
+  cudaStream_t side = nullptr;  // captures the bodies of conditional graph nodes
   LaunchCfg lc{148, 256, 0, 0, 0};
   bool loaded = false;
   bool lists_fresh = false;  // nbr / nn / dermis match the current positions
@@ -236,6 +237,60 @@ void enqueue_step(epi_ctx* c, int& cur, Timer* tm) {
   cur ^= 1;
 }
 
+// Appends to the graph being captured on c->stream a conditional (IF) node
+// whose body, captured on c->side, is the candidate rebuild; a one-thread
+// kernel before it sets the condition from the "some tissue is flagged"
+// word, so steps that need no rebuild launch none of its kernels.
+cudaError_t capture_conditional_rebuild(epi_ctx* c, int cur) {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  cudaError_t e = cudaStreamGetCaptureInfo(c->stream, &st, nullptr, &g, &deps, &nd);
+  if (e != cudaSuccess) return e;
+  cudaGraphConditionalHandle h;
+  if ((e = cudaGraphConditionalHandleCreate(&h, g, 0, 0)) != cudaSuccess) return e;
+  launch_rebuild_condition(make_state(c, cur), h, c->stream);
+  if ((e = cudaStreamGetCaptureInfo(c->stream, &st, nullptr, &g, &deps, &nd)) != cudaSuccess)
+    return e;
+  cudaGraphNodeParams p{};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = cudaGraphCondTypeIf;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  if ((e = cudaGraphAddNode(&node, g, deps, nd, &p)) != cudaSuccess) return e;
+  cudaGraph_t body = p.conditional.phGraph_out[0];
+  if ((e = cudaStreamBeginCaptureToGraph(c->side, body, nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+    return e;
+  launch_rebuild(make_state(c, cur), whole(c), c->scan, c->lc, c->side, nullptr);
+  if ((e = cudaStreamEndCapture(c->side, &body)) != cudaSuccess) return e;
+  return cudaStreamUpdateCaptureDependencies(c->stream, &node, 1,
+                                             cudaStreamSetCaptureDependencies);
+}
+
+// Captures the two-step graph of parity c->cur: per step, the conditional
+// rebuild, the prepass and the fused step.
+cudaError_t capture_step_graph(epi_ctx* c, cudaGraphExec_t* out) {
+  cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return e;
+  int cur = c->cur;
+  for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+    e = capture_conditional_rebuild(c, cur);
+    if (e != cudaSuccess) break;
+    prepass_all(c, cur, nullptr);
+    launch_step(make_state(c, cur), whole(c), c->cfg.precision, c->lc, c->stream, nullptr);
+    cur ^= 1;
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t e_end = cudaStreamEndCapture(c->stream, &g);
+  if (e == cudaSuccess) e = e_end;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(out, g, 0);
+  if (g) cudaGraphDestroy(g);
+  return e;
+}
+
 // connect_cell's results for the current positions: lists and dermis.
 void enqueue_materialize(epi_ctx* c) {
   const DevState S = make_state(c, c->cur);
@@ -266,17 +321,7 @@ int enqueue_graph_steps(epi_ctx* c, int32_t nsteps) {
   const int32_t pairs = nsteps / 2;
   if (pairs > 0) {
     cudaGraphExec_t& ge = c->graph[c->cur];
-    if (!ge) {
-      cudaGraph_t g;
-      EPI_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-      int cur = c->cur;
-      enqueue_step(c, cur, nullptr);
-      enqueue_step(c, cur, nullptr);
-      EPI_CUDA(cudaStreamEndCapture(c->stream, &g));
-      const cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
-      cudaGraphDestroy(g);
-      EPI_CUDA(e);
-    }
+    if (!ge) EPI_CUDA(capture_step_graph(c, &ge));
     for (int32_t k = 0; k < pairs; ++k) EPI_CUDA(cudaGraphLaunch(ge, c->stream));
   }
   if (nsteps % 2) enqueue_step(c, c->cur, nullptr);
@@ -500,6 +545,7 @@ int epi_create(epi_ctx** out, const epi_config* cfg) {
       sms > 0)
     ctx->lc.num_sms = sms;
   int rc = cuda_status(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  if (rc == EPI_OK) rc = cuda_status(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
   if (rc == EPI_OK) rc = dev_alloc(&ctx->status, 1);
   if (rc == EPI_OK) rc = cuda_status(cudaMallocHost((void**)&ctx->status_h, sizeof(DevStatus)));
   if (rc == EPI_OK) rc = cuda_status(cudaMemset(ctx->status, 0, sizeof(DevStatus)));
@@ -522,6 +568,7 @@ void epi_destroy(epi_ctx* ctx) {
   if (ctx->status) cudaFree(ctx->status);
   if (ctx->rebuilds) cudaFree(ctx->rebuilds);
   if (ctx->status_h) cudaFreeHost(ctx->status_h);
+  if (ctx->side) cudaStreamDestroy(ctx->side);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }

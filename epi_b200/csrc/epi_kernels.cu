@@ -448,6 +448,12 @@ __global__ void k_gate_clear(DevState S, int32_t clear_any) {
   }
 }
 
+// Condition of the rebuild node in the captured step graph: run the rebuild
+// kernels only when some tissue is flagged.
+__global__ void k_rebuild_condition(cudaGraphConditionalHandle h, const int32_t* gate) {
+  cudaGraphSetConditional(h, gate[0] != 0 ? 1u : 0u);
+}
+
 __global__ void k_gate_set_all(DevState S, int32_t ntissues) {
   GRID_STRIDE(t, 0, ntissues) S.gate[1 + t] = 1;
   if (blockIdx.x == 0 && threadIdx.x == 0) S.gate[0] = 1;
@@ -1058,6 +1064,10 @@ void launch_exact_lists(const DevState& S, const Range& r, const LaunchCfg& lc,
                         cudaStream_t s) {
   const int32_t np = r.p1 - r.p0;
   if (np > 0) k_exact_lists<<<stride_blocks(np, lc.block, lc), lc.block, 0, s>>>(S, r);
+}
+
+void launch_rebuild_condition(const DevState& S, cudaGraphConditionalHandle h, cudaStream_t s) {
+  k_rebuild_condition<<<1, 1, 0, s>>>(h, S.gate);
 }
 
 void launch_set_gates(const DevState& S, int32_t ntissues, cudaStream_t s) {

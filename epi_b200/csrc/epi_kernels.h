@@ -61,6 +61,8 @@ void launch_step(const DevState& S, const Range& r, int precision, const LaunchC
 void launch_exact_lists(const DevState& S, const Range& r, const LaunchCfg& lc,
                         cudaStream_t s);
 void launch_set_gates(const DevState& S, int32_t ntissues, cudaStream_t s);
+// Sets conditional handle h to (some tissue is flagged for a rebuild).
+void launch_rebuild_condition(const DevState& S, cudaGraphConditionalHandle h, cudaStream_t s);
 
 // CSR export of the connection lists (tissue-local indices, rows sorted).
 void launch_rowlen(const DevState& S, int32_t* rowlen, int32_t n, cudaStream_t s);
