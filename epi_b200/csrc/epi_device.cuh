@@ -12,6 +12,33 @@ inline int stride_blocks(int64_t n, int b, const LaunchCfg& lc) {
   return need < cap ? (need > 0 ? need : 1) : cap;
 }
 
+// Programmatic dependent launch. Kernels of the step sequence are launched
+// with programmatic stream serialisation, so each may be scheduled while its
+// predecessor's last blocks still run. pdl_entry() is the first statement of
+// such a kernel: it lets the next kernel be scheduled, then waits until the
+// predecessor has completed and its writes are visible (griddepcontrol.wait
+// returns at once for a kernel launched without the attribute). Every kernel
+// therefore starts its real work only after all earlier work on the stream.
+__device__ __forceinline__ void pdl_entry() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+template <typename... Params, typename... Args>
+void launch_pdl(void (*kernel)(Params...), int grid, int block, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, static_cast<Params>(args)...);
+}
+
 #define GRID_STRIDE(i, lo, hi) \
   for (int64_t i = (lo) + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (hi); \
        i += (int64_t)gridDim.x * blockDim.x)

@@ -153,6 +153,7 @@ __device__ __forceinline__ int32_t ref_bin(const TissueDev& T, double x, double 
 // With nothing gated the list is empty and each kernel exits at once.
 // ---------------------------------------------------------------------------
 __global__ void k_gate_compact(DevState S, int32_t t0, int32_t t1) {
+  pdl_entry();
   if (S.gate[0] == 0) {
     if (threadIdx.x == 0) {
       S.rl_count[0] = 0;
@@ -220,6 +221,7 @@ __device__ __forceinline__ int32_t gated_particle(const DevState& S, int32_t cnt
 
 // Binning on the reference's 2.0 grid (grid_init, cell_connection.cpp:38-62).
 __global__ void k_bin(DevState S) {
+  pdl_entry();
   GATED_PARTICLES(g, cnt) {
     int32_t t;
     const int32_t i = gated_particle(S, cnt, g, &t);
@@ -249,6 +251,7 @@ __global__ void k_bin(DevState S) {
 // particles occupy its own slots [pbase, pbase + n). Each tissue's bins end
 // with a sentinel entry that receives the end offset.
 __global__ void k_scan_tissue(DevState S) {
+  pdl_entry();
   const int32_t cnt = S.rl_count[0];
   for (int32_t k = blockIdx.x; k < cnt; k += gridDim.x) {
     const TissueDev& T = S.tissues[S.rl_list[k]];
@@ -280,6 +283,7 @@ __global__ void k_scan_tissue(DevState S) {
 }
 
 __global__ void k_scatter(DevState S) {
+  pdl_entry();
   GATED_PARTICLES(g, cnt) {
     int32_t t;
     const int32_t i = gated_particle(S, cnt, g, &t);
@@ -292,6 +296,7 @@ __global__ void k_scatter(DevState S) {
 // Per-bin insertion sort by particle index (bins hold a few to a few dozen
 // particles), then the sorted position copy the search streams through.
 __global__ void k_binsort(DevState S) {
+  pdl_entry();
   const int32_t cnt = S.rl_count[0];
   if (cnt == 0) return;
   const int32_t nbg = S.rl_bpre[cnt];
@@ -361,6 +366,7 @@ __device__ __forceinline__ int window_ranges(double x, double R, double L, int32
 // is a superset for every pair it can connect (reach <= 1.2 * 3.2 < 2 * 2.0).
 // Candidates come out in bin order, deterministic after k_binsort.
 __global__ void k_cand_search(DevState S) {
+  pdl_entry();
   // One warp per gated particle: the lanes stride the contiguous slots of
   // each bin column, and ballots keep the candidates in slot order.
   constexpr double kInvAG = 1.0 / kAreaGrid;
@@ -439,6 +445,7 @@ __global__ void k_cand_search(DevState S) {
 }
 
 __global__ void k_gate_clear(DevState S, int32_t clear_any) {
+  pdl_entry();
   const int32_t cnt = S.rl_count[0];
   for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x)
     S.gate[1 + S.rl_list[k]] = 0;
@@ -451,6 +458,7 @@ __global__ void k_gate_clear(DevState S, int32_t clear_any) {
 // Condition of the rebuild node in the captured step graph: run the rebuild
 // kernels only when some tissue is flagged.
 __global__ void k_rebuild_condition(cudaGraphConditionalHandle h, const int32_t* gate) {
+  pdl_entry();
   cudaGraphSetConditional(h, gate[0] != 0 ? 1u : 0u);
 }
 
@@ -465,6 +473,7 @@ __global__ void k_gate_set_all(DevState S, int32_t ntissues) {
 // particle, strict <, starting from LX*LX.
 // ---------------------------------------------------------------------------
 __global__ void k_dermis(DevState S, int32_t f0, int32_t f1) {
+  pdl_entry();
   GRID_STRIDE(e, f0, f1) {
     const int32_t i = S.prep[e];
     const TissueDev& T = S.tissues[attr_tissue(S.attr[i])];
@@ -540,6 +549,7 @@ struct SiteOffsets<float> {
 // the wall (:287-294). The sum goes to S.fmemb; k_step adds it.
 template <typename R>
 __global__ void __launch_bounds__(256) k_memb_force(DevState S, int32_t m0, int32_t m1) {
+  pdl_entry();
   GRID_STRIDE(e, m0, m1) {
     const int32_t i = S.prep[e];
     const TissueDev& T = S.tissues[attr_tissue(S.attr[i])];
@@ -842,6 +852,7 @@ __device__ __forceinline__ const float4* gather_source<float4>(const DevState& S
 
 template <typename R, bool kSimple, bool kOld, int kMinBlocks>
 __global__ void __launch_bounds__(256, kMinBlocks) k_step(DevState S, Range r) {
+  pdl_entry();
   const int64_t i = r.p0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= r.p1) return;
   const int64_t N = S.n_total;
@@ -992,23 +1003,24 @@ void launch_rebuild(const DevState& S, const Range& r, const ScanScratch&,
   const int B = lc.block;
   const int grid = lc.num_sms * 8;
   timer_begin(tm, KC_REBUILD_BIN, s);
-  k_gate_compact<<<1, kScanThreads, 0, s>>>(S, r.t0, r.t1);
-  k_bin<<<grid, B, 0, s>>>(S);
+  launch_pdl(k_gate_compact, 1, kScanThreads, s, S, r.t0, r.t1);
+  launch_pdl(k_bin, grid, B, s, S);
   timer_end(tm, KC_REBUILD_BIN, s);
   timer_begin(tm, KC_REBUILD_SCAN, s);
   const int nt = r.t1 - r.t0;
-  k_scan_tissue<<<nt < lc.num_sms * 4 ? (nt > 0 ? nt : 1) : lc.num_sms * 4, kScanThreads, 0, s>>>(S);
+  launch_pdl(k_scan_tissue, nt < lc.num_sms * 4 ? (nt > 0 ? nt : 1) : lc.num_sms * 4, kScanThreads, s,
+             S);
   timer_end(tm, KC_REBUILD_SCAN, s);
   timer_begin(tm, KC_REBUILD_SORT, s);
-  k_scatter<<<grid, B, 0, s>>>(S);
-  k_binsort<<<grid, B, 0, s>>>(S);
+  launch_pdl(k_scatter, grid, B, s, S);
+  launch_pdl(k_binsort, grid, B, s, S);
   timer_end(tm, KC_REBUILD_SORT, s);
   timer_begin(tm, KC_REBUILD_SEARCH, s);
-  k_cand_search<<<grid, B, 0, s>>>(S);
+  launch_pdl(k_cand_search, grid, B, s, S);
   timer_end(tm, KC_REBUILD_SEARCH, s);
   timer_begin(tm, KC_GATE, s);
   const bool whole = r.t0 == 0 && r.t1 == S.ntissues;
-  k_gate_clear<<<1, B, 0, s>>>(S, whole ? 1 : 0);
+  launch_pdl(k_gate_clear, 1, B, s, S, (int32_t)(whole ? 1 : 0));
   timer_end(tm, KC_GATE, s);
 }
 
@@ -1019,11 +1031,11 @@ void launch_prepass(const DevState& S, int32_t m0, int32_t m1, int32_t f0, int32
   if (m1 > m0) {
     const int gm = stride_blocks(m1 - m0, lc.block, lc);
     if (precision == 1)
-      k_memb_force<float><<<gm, lc.block, 0, s>>>(S, m0, m1);
+      launch_pdl(k_memb_force<float>, gm, lc.block, s, S, m0, m1);
     else
-      k_memb_force<double><<<gm, lc.block, 0, s>>>(S, m0, m1);
+      launch_pdl(k_memb_force<double>, gm, lc.block, s, S, m0, m1);
   }
-  if (f1 > f0) k_dermis<<<stride_blocks(f1 - f0, lc.block, lc), lc.block, 0, s>>>(S, f0, f1);
+  if (f1 > f0) launch_pdl(k_dermis, stride_blocks(f1 - f0, lc.block, lc), lc.block, s, S, f0, f1);
   timer_end(tm, KC_PREPASS, s);
 }
 
@@ -1031,10 +1043,10 @@ template <typename R, bool kSimple, bool kOld>
 void launch_step_v(const DevState& S, const Range& r, const LaunchCfg& lc, cudaStream_t s) {
   const int grid = blocks_for(r.p1 - r.p0, 256);
   switch (lc.variant) {
-    case 2: k_step<R, kSimple, kOld, 5><<<grid, 256, 0, s>>>(S, r); break;
-    case 3: k_step<R, kSimple, kOld, 6><<<grid, 256, 0, s>>>(S, r); break;
-    case 4: k_step<R, kSimple, kOld, 3><<<grid, 256, 0, s>>>(S, r); break;
-    default: k_step<R, kSimple, kOld, 4><<<grid, 256, 0, s>>>(S, r); break;
+    case 2: launch_pdl(k_step<R, kSimple, kOld, 5>, grid, 256, s, S, r); break;
+    case 3: launch_pdl(k_step<R, kSimple, kOld, 6>, grid, 256, s, S, r); break;
+    case 4: launch_pdl(k_step<R, kSimple, kOld, 3>, grid, 256, s, S, r); break;
+    default: launch_pdl(k_step<R, kSimple, kOld, 4>, grid, 256, s, S, r); break;
   }
 }
 
@@ -1067,7 +1079,7 @@ void launch_exact_lists(const DevState& S, const Range& r, const LaunchCfg& lc,
 }
 
 void launch_rebuild_condition(const DevState& S, cudaGraphConditionalHandle h, cudaStream_t s) {
-  k_rebuild_condition<<<1, 1, 0, s>>>(h, S.gate);
+  launch_pdl(k_rebuild_condition, 1, 1, s, h, (const int32_t*)S.gate);
 }
 
 void launch_set_gates(const DevState& S, int32_t ntissues, cudaStream_t s) {
