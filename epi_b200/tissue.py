@@ -110,6 +110,9 @@ class Tissue:
     nder: int = 0
     params: Params = field(default_factory=Params)
     name: str = ""
+    # ageb (division age) of each cell: used only by the reference's state
+    # renewal (cell_state_renew.cpp), never by the mechanics; None = all 0
+    ageb: Optional[np.ndarray] = None
 
     @property
     def n(self) -> int:
@@ -120,7 +123,8 @@ class Tissue:
                    self.x.copy(), self.y.copy(), self.z.copy(), self.radius.copy(),
                    self.state.copy(), self.agek.copy(), self.spr_nat_len.copy(),
                    self.pair.copy(), self.rest_div_times.copy(), self.nmemb, self.nder,
-                   Params(**self.params.__dict__), self.name)
+                   Params(**self.params.__dict__), self.name,
+                   None if self.ageb is None else self.ageb.copy())
         return t
 
     def validate(self) -> None:
@@ -140,7 +144,8 @@ class Tissue:
         for i in range(self.n):
             lines.append(
                 "%d %d %r %r %r %r %r %r %r %r %d %r %r %d %r %d %d" % (
-                    i, int(self.state[i]), float(self.radius[i]), 0.0, float(self.agek[i]),
+                    i, int(self.state[i]), float(self.radius[i]),
+                    0.0 if self.ageb is None else float(self.ageb[i]), float(self.agek[i]),
                     0.0, float(self.x[i]), float(self.y[i]), float(self.z[i]), 0.0,
                     int(self.rest_div_times[i]), 0.0, 0.0, 0, float(self.spr_nat_len[i]),
                     int(self.pair[i]), -1))
@@ -314,6 +319,31 @@ def mixed_state_tissue(seed: int = 7) -> Tissue:
                radius=cat(rs, np.float64), state=cat(st, np.uint8), agek=cat(ag, np.float64),
                spr_nat_len=cat(sp, np.float64), pair=cat(pr, np.int32),
                rest_div_times=cat(rd, np.int32), nmemb=nm, nder=nder, name="mixed")
+    t.validate()
+    return t
+
+
+def renewal_tissue(seed: int = 7) -> Tissue:
+    """mixed_state_tissue with ages set so that the reference's state renewal
+    (cell_state_renew.cpp:400-433) acts within the first steps: the two
+    unpaired FIX cells and the unpaired MUSUME with divisions left are past
+    their division age (cell_divide, :227-279; with a division draw that
+    passes they divide and the batch grows), the old DEAD cells are past
+    ADHE_CONST with few connections (removed, :330-345, which reorders the
+    cell array), and one ALIVE cell is at THRESH_DEAD (cornified, :347-361)."""
+    t = mixed_state_tissue(seed)
+    ageb = np.zeros(t.n)
+    cells = np.arange(t.nmemb + t.nder, t.n)
+    fix = cells[t.state[cells] == FIX]
+    ageb[fix[t.pair[fix] < 0]] = 100.0
+    mus = cells[(t.state[cells] == MUSUME) & (t.pair[cells] < 0) & (t.rest_div_times[cells] > 0)]
+    ageb[mus] = 5.0
+    dead = cells[t.state[cells] == DEAD]
+    t.agek[dead[::2]] = 40.0
+    alive = cells[(t.state[cells] == ALIVE) & (t.pair[cells] < 0)]
+    t.agek[alive[0]] = 22.0
+    t.ageb = ageb
+    t.name = "renewal"
     t.validate()
     return t
 

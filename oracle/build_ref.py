@@ -43,12 +43,15 @@ ROOT = HERE.parent
 REF_DIR = Path(os.environ.get("EPI_REFERENCE_DIR", "/root/reference")) / "epi5_MT"
 OUT = HERE / "_ref"
 
-# The mechanics path's translation units (cell_state_renew, chemistry and I/O
-# drivers are not needed by the harness).
+# The mechanics path's translation units plus cell_state_renew (the harness's
+# dyn mode runs the complete cell_dynamics); chemistry and I/O drivers are not
+# needed.
 SOURCES = [
     "cellmanager.cpp", "cell.cpp", "cell_connection.cpp", "cell_interaction.cpp",
-    "cell_init.cpp", "utils.cpp", "vec3.cpp", "DualValue.cpp", "Random_gen.cpp",
+    "cell_init.cpp", "cell_state_renew.cpp", "utils.cpp", "vec3.cpp", "DualValue.cpp",
 ]
+# Random_gen.cpp is replaced by the harness's fixed-seed genrand_real (the
+# reference seeds from std::random_device; see oracle/ref_harness.cpp).
 
 # name -> (NMX, NMY, LX, LY, LZ, MAX_CELL_NUM)
 GEOMETRIES = {

@@ -173,10 +173,12 @@ def reference_binary(t, variant: str = "serial") -> Optional[Path]:
 
 
 def run_reference(t, nsteps: int, every: int, variant: str = "serial",
-                  env: Optional[dict] = None):
+                  env: Optional[dict] = None, mode: str = "run"):
     """Run the compiled reference on `t` (default parameters only: the reference
     fixes its constants at compile time). Returns the parsed frames. `env`
-    adds environment variables (the dropin variant reads EPI_MECH_*)."""
+    adds environment variables (the dropin variant reads EPI_MECH_*, the
+    harness EPI_HARNESS_RNG / EPI_HARNESS_SEED); mode "dyn" runs the complete
+    cell_dynamics including state renewal."""
     from epi_b200.tissue import read_reference_frames
     exe = reference_binary(t, variant)
     if exe is None:
@@ -187,7 +189,7 @@ def run_reference(t, nsteps: int, every: int, variant: str = "serial",
         cells = os.path.join(d, "cells.dat")
         out = os.path.join(d, "frames.bin")
         t.write_reference_file(cells)
-        r = subprocess.run([str(exe), "run", cells, str(nsteps), out, str(every)],
+        r = subprocess.run([str(exe), mode, cells, str(nsteps), out, str(every)],
                            capture_output=True, text=True, env=full_env)
         if r.returncode != 0:
             raise RuntimeError(f"reference harness failed ({r.returncode}): {r.stderr[-2000:]}")

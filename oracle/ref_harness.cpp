@@ -15,13 +15,28 @@
 //   ref_harness run  <cells.dat> <nsteps> <out.bin> <dump_every>
 //       writes frames (positions, per-cell sorted connection lists, dermis)
 //       at step 0, every dump_every steps and at the last step.
+//   ref_harness dyn  <cells.dat> <nsteps> <out.bin> <dump_every>
+//       the same with the reference's complete cell_dynamics
+//       (epi5_MT/proc.cpp:22-32): cell_interaction -> pos_copy ->
+//       cell_state_renew -> cell_pos_periodic_fix -> connect_cell, so cells
+//       divide, cornify and are removed (frames then differ in size).
 //   ref_harness time <cells.dat> <warmup> <steps>
 //       times each step with steady_clock and prints one JSON line.
+//
+// genrand_real (epi5_MT/Random_gen.cpp) seeds itself from std::random_device,
+// so no two runs of the reference agree once a division test draws from it.
+// The harness builds leave Random_gen.cpp out and define genrand_real here:
+// a std::mt19937_64 with a fixed seed (EPI_HARNESS_SEED, default 1) and the
+// same uniform [0, 1) distribution, or, with EPI_HARNESS_RNG=zero, always 0
+// (every division test that is reached passes), so that two builds see the
+// same draws.
 #include "cellmanager.h"
 #include "cell.h"
 #include "cell_connection.h"
 #include "cell_interaction.h"
 #include "cell_init.h"
+#include "cell_state_renew.h"
+#include "Random_gen.h"
 
 #include <tbb/tbb_shim_config.h>
 
@@ -32,9 +47,23 @@
 #include <cstring>
 #include <fcntl.h>
 #include <memory>
+#include <random>
 #include <string>
 #include <unistd.h>
 #include <vector>
+
+double genrand_real() {
+  static thread_local bool zero = [] {
+    const char* m = std::getenv("EPI_HARNESS_RNG");
+    return m && std::strcmp(m, "zero") == 0;
+  }();
+  static thread_local std::mt19937_64 mt([] {
+    const char* v = std::getenv("EPI_HARNESS_SEED");
+    return (std::mt19937_64::result_type)(v ? std::strtoull(v, nullptr, 10) : 1ull);
+  }());
+  static thread_local std::uniform_real_distribution<double> dist(0.0, 1.0);
+  return zero ? 0.0 : dist(mt);
+}
 
 namespace {
 
@@ -72,6 +101,15 @@ void check_capacity(CellManager& cman) {
 void one_step(CellManager& cman) {
   cell_interaction(cman);
   pos_copy(cman);
+  cell_pos_periodic_fix(cman);
+  connect_cell(cman);
+}
+
+// cell_dynamics, epi5_MT/proc.cpp:22-32
+void dynamics_step(CellManager& cman) {
+  cell_interaction(cman);
+  pos_copy(cman);
+  cell_state_renew(cman);
   cell_pos_periodic_fix(cman);
   connect_cell(cman);
 }
@@ -117,6 +155,7 @@ void write_frame(std::FILE* f, CellManager& cman, int step) {
 int usage() {
   std::fprintf(stderr,
                "usage: ref_harness run <cells.dat> <nsteps> <out.bin> <dump_every>\n"
+               "       ref_harness dyn <cells.dat> <nsteps> <out.bin> <dump_every>\n"
                "       ref_harness time <cells.dat> <warmup> <steps>\n");
   return 2;
 }
@@ -127,7 +166,8 @@ int main(int argc, char** argv) {
   if (argc < 2) return usage();
   const std::string mode = argv[1];
   auto cman = std::unique_ptr<CellManager>(new CellManager());
-  if (mode == "run" && argc == 6) {
+  if ((mode == "run" || mode == "dyn") && argc == 6) {
+    const bool dyn = mode == "dyn";
     const int nsteps = std::atoi(argv[3]);
     const int every = std::max(1, std::atoi(argv[5]));
     {
@@ -139,7 +179,12 @@ int main(int argc, char** argv) {
     check_capacity(*cman);
     write_frame(f, *cman, 0);
     for (int s = 1; s <= nsteps; ++s) {
-      one_step(*cman);
+      if (dyn) {
+        SilenceStdout quiet;  // state renewal reports every division / cornification
+        dynamics_step(*cman);
+      } else {
+        one_step(*cman);
+      }
       check_capacity(*cman);
       if (s % every == 0 || s == nsteps) write_frame(f, *cman, s);
     }

@@ -7,7 +7,13 @@ connection lists and the dermis of FIX / MUSUME cells. Needs the reference
 checkout, so it runs in the build container only; the fixtures it writes are
 committed and the tests read them anywhere.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]
+
+Cases "c1" and "mixed" run the mechanics step (interaction, commit, wrap,
+connect). Case "renewal" runs the complete cell_dynamics including the
+reference's state renewal, with the harness's division draw fixed at 0 (every
+division test that is reached passes), so cells divide, cornify and are
+removed and the frames differ in size.
 """
 from __future__ import annotations
 
@@ -24,30 +30,32 @@ from oracle import oracle as O  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
 
-# name -> (tissue factory, steps, frame steps kept)
+# name -> (tissue factory, steps, frame steps kept, harness mode, harness environment)
 CASES = {
-    "c1": (T.config1, 1000, (0, 100, 1000)),
-    "mixed": (T.mixed_state_tissue, 300, (0, 50, 300)),
+    "c1": (T.config1, 1000, (0, 100, 1000), "run", {}),
+    "mixed": (T.mixed_state_tissue, 300, (0, 50, 300), "run", {}),
+    "renewal": (T.renewal_tissue, 200, (0, 1, 20, 100, 200), "dyn", {"EPI_HARNESS_RNG": "zero"}),
 }
 
 
 def make(name: str) -> Path:
-    factory, steps, keep = CASES[name]
+    factory, steps, keep, mode, env = CASES[name]
     t = factory()
     every = int(np.gcd.reduce([k for k in keep if k > 0] + [steps]))
-    frames = [f for f in O.run_reference(t, steps, every) if f["step"] in keep]
+    frames = [f for f in O.run_reference(t, steps, every, mode=mode, env=env)
+              if f["step"] in keep]
     assert [f["step"] for f in frames] == list(keep)
     out = OUT / f"{name}.npz"
+    cat = lambda key: np.concatenate([f[key] for f in frames])
     np.savez_compressed(
         out,
         steps=np.array(keep, np.int32),
-        x=np.stack([f["x"] for f in frames]),
-        y=np.stack([f["y"] for f in frames]),
-        z=np.stack([f["z"] for f in frames]),
-        conn_off=np.stack([f["conn_off"] for f in frames]),
-        conn_idx=np.concatenate([f["conn_idx"] for f in frames]),
+        n=np.array([len(f["x"]) for f in frames], np.int64),
+        x=cat("x"), y=cat("y"), z=cat("z"),
+        conn_off=cat("conn_off"),
+        conn_idx=cat("conn_idx"),
         conn_len=np.array([len(f["conn_idx"]) for f in frames], np.int64),
-        dermis=np.stack([f["dermis"] for f in frames]),
+        dermis=cat("dermis"),
     )
     return out
 
@@ -55,14 +63,19 @@ def make(name: str) -> Path:
 def load(name: str):
     d = np.load(OUT / f"{name}.npz")
     frames = []
-    cut = np.concatenate([[0], np.cumsum(d["conn_len"])])
+    n = d["n"]
+    pcut = np.concatenate([[0], np.cumsum(n)])
+    ocut = np.concatenate([[0], np.cumsum(n + 1)])
+    ccut = np.concatenate([[0], np.cumsum(d["conn_len"])])
     for k, s in enumerate(d["steps"]):
-        frames.append(dict(step=int(s), x=d["x"][k], y=d["y"][k], z=d["z"][k],
-                           conn_off=d["conn_off"][k], conn_idx=d["conn_idx"][cut[k]:cut[k + 1]],
-                           dermis=d["dermis"][k]))
+        a, b = pcut[k], pcut[k + 1]
+        frames.append(dict(step=int(s), x=d["x"][a:b], y=d["y"][a:b], z=d["z"][a:b],
+                           conn_off=d["conn_off"][ocut[k]:ocut[k + 1]],
+                           conn_idx=d["conn_idx"][ccut[k]:ccut[k + 1]],
+                           dermis=d["dermis"][a:b]))
     return frames
 
 
 if __name__ == "__main__":
-    for n in CASES:
+    for n in (sys.argv[1:] or CASES):
         print(make(n))

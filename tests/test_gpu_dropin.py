@@ -59,3 +59,27 @@ def test_dropin_mixed_precision_within_bar(built):
         f = frames[s]
         err = rel_pos_err((f["x"], f["y"], f["z"]), (g["x"], g["y"], g["z"]), t.lx, t.ly)
         assert err <= TOL_MIXED, (s, err)
+
+
+def test_dropin_runs_the_reference_state_renewal_loop(built):
+    """epi5_MT's complete cell_dynamics (cell_state_renew between pos_copy and
+    the periodic fix, proc.cpp:22-32) with the drop-in: cells divide (the batch
+    grows and is re-uploaded), are removed (the reference swaps the last cell
+    into the gap) and cornify, and every frame still matches the serial
+    reference's (division draw fixed at 0 in both)."""
+    t = T.renewal_tissue()
+    if O.reference_binary(t, "dropin") is None:
+        pytest.skip("drop-in harness not built (python oracle/build_ref.py --dropin)")
+    frames = {f["step"]: f for f in O.run_reference(
+        t, 200, 1, variant="dropin", mode="dyn",
+        env={"EPI_MECH_PRECISION": "fp64", "EPI_HARNESS_RNG": "zero"})}
+    golden = load("renewal")
+    assert len(golden[0]["x"]) != len(golden[-1]["x"])
+    for g in golden:
+        f = frames[g["step"]]
+        assert len(f["x"]) == len(g["x"]), g["step"]
+        err = rel_pos_err((f["x"], f["y"], f["z"]), (g["x"], g["y"], g["z"]), t.lx, t.ly)
+        assert err <= TOL_FP64, (g["step"], err)
+        assert lists_equal(f["conn_off"], f["conn_idx"], g["conn_off"], g["conn_idx"]), \
+            list_diff_summary(f["conn_off"], f["conn_idx"], g["conn_off"], g["conn_idx"])
+        assert np.array_equal(f["dermis"], g["dermis"]), g["step"]

@@ -77,3 +77,21 @@ def test_oracle_flags_out_of_grid(built):
     t.z[t.nmemb + 3] = 40.0  # above LZ = 32: grid_init's range assert
     ora = O.OracleTissue(t)
     assert ora.error()[0] == 5
+
+
+def test_renewal_fixture_reproduces_with_the_compiled_reference(built):
+    """tests/golden/renewal.npz: the reference's complete cell_dynamics (state
+    renewal included, division draw fixed at 0) is deterministic and the
+    committed frames are what it writes."""
+    t = T.renewal_tissue()
+    if not _ref_available(t):
+        pytest.skip("compiled reference not built here (no reference checkout)")
+    golden = load("renewal")
+    frames = {f["step"]: f for f in O.run_reference(t, 200, 1, mode="dyn",
+                                                     env={"EPI_HARNESS_RNG": "zero"})}
+    for g in golden:
+        f = frames[g["step"]]
+        for k in ("x", "y", "z", "conn_off", "conn_idx", "dermis"):
+            assert np.array_equal(f[k], g[k]), (g["step"], k)
+    # the run divides, cornifies and removes cells: the batch size changes
+    assert len(golden[0]["x"]) != len(golden[-1]["x"])
