@@ -21,6 +21,7 @@ import numpy as np
 
 # Cell states, epi5_MT/define.h:36-47.
 ALIVE, DEAD, DISA, UNUSED, FIX, BLANK, DER, MUSUME, AIR, MEMB = range(10)
+SQUARE, TRIANGULAR = 0, 1  # membrane lattices
 
 R_MAX = 1.4     # define.h:116
 R_DER = 1.4     # define.h:119
@@ -113,6 +114,9 @@ class Tissue:
     # ageb (division age) of each cell: used only by the reference's state
     # renewal (cell_state_renew.cpp), never by the mechanics; None = all 0
     ageb: Optional[np.ndarray] = None
+    # membrane lattice: SQUARE (4 links, TRI_MEMB undefined) or TRIANGULAR
+    # (6 links, the reference's default TRI_MEMB build); nmy counts rows
+    lattice: int = 0
 
     @property
     def n(self) -> int:
@@ -124,7 +128,7 @@ class Tissue:
                    self.state.copy(), self.agek.copy(), self.spr_nat_len.copy(),
                    self.pair.copy(), self.rest_div_times.copy(), self.nmemb, self.nder,
                    Params(**self.params.__dict__), self.name,
-                   None if self.ageb is None else self.ageb.copy())
+                   None if self.ageb is None else self.ageb.copy(), self.lattice)
         return t
 
     def validate(self) -> None:
@@ -191,6 +195,44 @@ def layered_tissue(side: int, layers: int, seed: int, *, spacing: float = 1.0,
         agek=np.zeros(n), spr_nat_len=np.zeros(n), pair=np.full(n, -1, np.int32),
         rest_div_times=np.zeros(n, np.int32), nmemb=nm, nder=0,
         params=params or Params(), name=name)
+    t.validate()
+    return t
+
+
+def tri_layered_tissue(nmx: int, rows: int, layers: int, seed: int, *, spacing: float = 1.0,
+                       cell_radius: float = 0.5, memb_z: float = 1.0, first_layer_z: float = 2.0,
+                       jitter: float = 0.1, lz: float = 32.0, params: Optional[Params] = None,
+                       name: str = "") -> Tissue:
+    """Triangular membrane (the reference's default TRI_MEMB lattice,
+    cellmanager.cpp:70-111) of nmx x rows particles under `layers` jittered
+    layers of ALIVE cells on the same lattice. Site (j, k) sits at
+    ((j + 0.5 (k mod 2)) s, k s sqrt(3)/2): even rows' diagonal neighbours are
+    j-1 and j, odd rows' j and j+1, as the reference wires them; the box is
+    nmx s by rows s sqrt(3)/2 (rows even, so the lattice is periodic)."""
+    assert rows % 2 == 0
+    dy = spacing * math.sqrt(3.0) / 2.0
+    lx, ly = nmx * spacing, rows * dy
+    nm = nmx * rows
+    jj, kk = np.meshgrid(np.arange(nmx), np.arange(rows), indexing="xy")
+    sx = ((jj.ravel() + 0.5 * (kk.ravel() % 2)) * spacing).astype(np.float64)
+    sy = (kk.ravel() * dy + 0.25 * dy).astype(np.float64)
+    nc = layers * nm
+    u = splitmix64_uniform(seed, 3 * nc).reshape(nc, 3) if nc else np.zeros((0, 3))
+    jit = (2.0 * u - 1.0) * jitter
+    lay = np.repeat(np.arange(layers), nm)
+    cx = _wrap(np.tile(sx, layers) + jit[:, 0], lx)
+    cy = _wrap(np.tile(sy, layers) + jit[:, 1], ly)
+    cz = first_layer_z + lay * spacing + jit[:, 2]
+    n = nm + nc
+    t = Tissue(
+        nmx=nmx, nmy=rows, lx=lx, ly=ly, lz=lz,
+        x=np.concatenate([sx, cx]), y=np.concatenate([sy, cy]),
+        z=np.concatenate([np.full(nm, memb_z), cz]),
+        radius=np.concatenate([np.full(nm, R_MEMB), np.full(nc, cell_radius)]),
+        state=np.concatenate([np.full(nm, MEMB, np.uint8), np.full(nc, ALIVE, np.uint8)]),
+        agek=np.zeros(n), spr_nat_len=np.zeros(n), pair=np.full(n, -1, np.int32),
+        rest_div_times=np.zeros(n, np.int32), nmemb=nm, nder=0,
+        params=params or Params(), name=name, lattice=TRIANGULAR)
     t.validate()
     return t
 

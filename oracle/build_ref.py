@@ -31,6 +31,7 @@ Usage: python oracle/build_ref.py [--dropin] [geometry ...]   (default: all know
 """
 from __future__ import annotations
 
+import math
 import os
 import re
 import subprocess
@@ -53,7 +54,7 @@ SOURCES = [
 # Random_gen.cpp is replaced by the harness's fixed-seed genrand_real (the
 # reference seeds from std::random_device; see oracle/ref_harness.cpp).
 
-# name -> (NMX, NMY, LX, LY, LZ, MAX_CELL_NUM)
+# name -> (NMX, NMY, LX, LY, LZ, MAX_CELL_NUM[, triangular])
 GEOMETRIES = {
     "sq16_L16": (16, 16, 16.0, 16.0, 32.0, 20000),
     "sq24_L24": (24, 24, 24.0, 24.0, 32.0, 40000),
@@ -63,7 +64,16 @@ GEOMETRIES = {
     "sq256_L256": (256, 256, 256.0, 256.0, 32.0, 1300000),
     # membrane at the reference's natural spacing (0.5) for the mixed-state case
     "sq32_L16": (32, 32, 16.0, 16.0, 32.0, 20000),
+    # triangular membrane (the reference's default build): NMX x rows sites at
+    # unit spacing, rows sqrt(3)/2 apart; the wiring uses only NMX and the
+    # number of membrane particles (cellmanager.cpp:70-111)
+    "tri16x18": (16, 18, 16.0, 18 * math.sqrt(3.0) / 2.0, 32.0, 20000, True),
+    "tri32x36": (32, 36, 32.0, 36 * math.sqrt(3.0) / 2.0, 32.0, 60000, True),
 }
+
+
+def is_tri(name: str) -> bool:
+    return len(GEOMETRIES[name]) > 6 and GEOMETRIES[name][6]
 
 COMMON_FLAGS = [
     "-std=c++14", "-w",
@@ -82,9 +92,9 @@ COMMON_FLAGS = [
 ]
 
 
-def geometry_for(nmx: int, nmy: int, lx: float, ly: float, lz: float) -> str:
+def geometry_for(nmx: int, nmy: int, lx: float, ly: float, lz: float, lattice: int = 0) -> str:
     for name, g in GEOMETRIES.items():
-        if g[:5] == (nmx, nmy, float(lx), float(ly), float(lz)):
+        if g[:5] == (nmx, nmy, float(lx), float(ly), float(lz)) and is_tri(name) == bool(lattice):
             return name
     raise KeyError(f"no oracle geometry for NMX={nmx} NMY={nmy} L=({lx},{ly},{lz})")
 
@@ -94,10 +104,12 @@ def _fmt(v: float) -> str:
 
 
 def write_overlay(name: str) -> Path:
-    nmx, nmy, lx, ly, lz, maxc = GEOMETRIES[name]
+    nmx, nmy, lx, ly, lz, maxc = GEOMETRIES[name][:6]
+    tri = is_tri(name)
     text = (REF_DIR / "define.h").read_text(encoding="latin-1")
-    subs = [
-        (r"#define\s+TRI_MEMB\s+1", "/* TRI_MEMB undefined: square membrane */"),
+    subs = [] if tri else [
+        (r"#define\s+TRI_MEMB\s+1", "/* TRI_MEMB undefined: square membrane */")]
+    subs += [
         (r"(unsigned int NMX\s*=\s*)\d+", rf"\g<1>{nmx}"),
         (r"(unsigned int NMY\s*=\s*)\d+", rf"\g<1>{nmy}"),
         (r"(cdefs MAX_CELL_NUM\s*=\s*)[^;]+", rf"\g<1>{maxc}"),
@@ -119,14 +131,17 @@ def write_overlay(name: str) -> Path:
     # cell_interaction.cpp:502) therefore takes its square branch.
     text = text.rstrip()
     assert text.endswith("#endif // DEFINE_H"), "unexpected define.h tail"
-    text = text[: -len("#endif // DEFINE_H")] + (
-        "#endif // DEFINE_H\n"
-        "#ifdef __cplusplus\n"
-        "#define TRI_MEMB 1\n"
-        "#include \"cell.h\"\n"
-        "#undef TRI_MEMB\n"
-        "#endif\n"
-    )
+    if not tri:
+        text = text[: -len("#endif // DEFINE_H")] + (
+            "#endif // DEFINE_H\n"
+            "#ifdef __cplusplus\n"
+            "#define TRI_MEMB 1\n"
+            "#include \"cell.h\"\n"
+            "#undef TRI_MEMB\n"
+            "#endif\n"
+        )
+    else:
+        text += "\n"
     d = OUT / name
     d.mkdir(parents=True, exist_ok=True)
     p = d / "define.h"

@@ -18,10 +18,13 @@ enum { S_ALIVE = 0, S_DEAD = 1, S_FIX = 4, S_DER = 6, S_MUSUME = 7, S_AIR = 8, S
 #define AREA_GRID (AREA_GRID_ORIGINAL + 1e-7) /* cell_connection.cpp:19 */
 #define BIN_CAP 200                     /* N3, cell_connection.cpp:28 */
 #define CONN_CAP 400                    /* N2 / MAX_CONNECT_CELL_NUM, define.h:80 */
-#define MEMB_ADJ 4                      /* MEMB_ADJ_CONN_NUM, square, define.h:147-153 */
+#define MEMB_ADJ_SQUARE 4               /* MEMB_ADJ_CONN_NUM, define.h:147-153 */
+#define MEMB_ADJ_TRI 6
 
 struct ora_tissue {
   int32_t n, nmemb, nder, nmx, nmy;
+  int32_t tri;   /* triangular membrane (TRI_MEMB, define.h:66) */
+  int32_t nadj;  /* MEMB_ADJ_CONN_NUM: 4 square, 6 triangular */
   double lx, ly, lz;
   int32_t anx, any, anz;
   ora_params P;
@@ -33,6 +36,7 @@ struct ora_tissue {
   int32_t* conn;        /* n x CONN_CAP, push order (Lockfree_push_stack) */
   int32_t* nconn;
   int32_t *lat_l, *lat_ll, *lat_r, *lat_b, *lat_bb, *lat_u;
+  int32_t* tri_nb; /* Memb_data::memb[6] per membrane particle (cell.h:57-59) */
   double *nv, *mv, *dn, *dm, *ipn, *ipm; /* Memb_data scratch, cell.h:60-62 */
   int32_t* bin_cnt;
   int32_t* bin_list;
@@ -106,7 +110,7 @@ static int grid_init(ora_tissue* t) {
       return t->err;
     }
     t->bin_list[(int64_t)b * BIN_CAP + t->bin_cnt[b]++] = c;
-    t->nconn[c] = t->state[c] == S_MEMB ? MEMB_ADJ : 0; /* force_set_count, :60 */
+    t->nconn[c] = t->state[c] == S_MEMB ? t->nadj : 0; /* force_set_count, :60 */
   }
   return ORA_OK;
 }
@@ -357,18 +361,88 @@ static void bend_calc3(ora_tissue* t, int32_t m) {
   t->nz[m] += s * f[2];
 }
 
+/* Triangular-membrane bending, tri_memb_bend and tri_bend_1 / tri_bend_2,
+ * :451-499, with vec3 (vec3.h:5-54) restated operation by operation.
+ * normalize() works in place (vec3.h:40-44), so the reference's divisions
+ * by norm1_pre.norm() / norm2_pre.norm() divide by the norm of an already
+ * normalised vector; kept as is. */
+typedef struct { double x, y, z; } v3;
+static inline v3 v3_pos(const ora_tissue* t, int32_t c) { v3 r = {t->x[c], t->y[c], t->z[c]}; return r; }
+static inline v3 v3_psub(const ora_tissue* t, v3 a, v3 b) { /* vpsub */
+  v3 r = {pdx(t, a.x, b.x), pdy(t, a.y, b.y), a.z - b.z};
+  return r;
+}
+static inline v3 v3_cross(v3 a, v3 b) {
+  v3 r = {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+  return r;
+}
+static inline double v3_dot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline double v3_norm(v3 a) { return sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+static inline v3 v3_normalize(v3* a) {
+  const double nm = v3_norm(*a);
+  a->x /= nm; a->y /= nm; a->z /= nm;
+  return *a;
+}
+static inline v3 v3_scale(double c, v3 a) { v3 r = {c * a.x, c * a.y, c * a.z}; return r; }
+static inline v3 v3_div(v3 a, double c) { v3 r = {a.x / c, a.y / c, a.z / c}; return r; }
+static inline v3 v3_add(v3 a, v3 b) { v3 r = {a.x + b.x, a.y + b.y, a.z + b.z}; return r; }
+static inline v3 v3_sub(v3 a, v3 b) { v3 r = {a.x - b.x, a.y - b.y, a.z - b.z}; return r; }
+/* tri_rho, :470-472 */
+static inline v3 tri_rho(v3 n1, v3 b1) { return v3_sub(b1, v3_scale(v3_dot(n1, b1), n1)); }
+/* tri_bend_1, :475-481 */
+static v3 tri_bend_1(const ora_tissue* t, int32_t r1, int32_t a1, int32_t b1, int32_t c1) {
+  const v3 r1v = v3_pos(t, r1), a1v = v3_pos(t, a1), b1v = v3_pos(t, b1), c1v = v3_pos(t, c1);
+  v3 norm1_pre = v3_cross(v3_psub(t, r1v, b1v), v3_psub(t, a1v, b1v));
+  const v3 norm1 = v3_normalize(&norm1_pre);
+  v3 n2 = v3_cross(v3_psub(t, a1v, b1v), v3_psub(t, c1v, b1v));
+  const v3 norm2 = v3_normalize(&n2);
+  const double dot1 = v3_dot(norm1, norm2);
+  return v3_scale(bend_factor(dot1),
+                  v3_div(v3_cross(v3_psub(t, a1v, b1v), tri_rho(norm1, norm2)), v3_norm(norm1_pre)));
+}
+/* tri_bend_2, :483-495 */
+static v3 tri_bend_2(const ora_tissue* t, int32_t r1, int32_t a1, int32_t b1, int32_t c1) {
+  const v3 r1v = v3_pos(t, r1), a1v = v3_pos(t, a1), b1v = v3_pos(t, b1), c1v = v3_pos(t, c1);
+  v3 norm1_pre = v3_cross(v3_psub(t, r1v, c1v), v3_psub(t, b1v, c1v));
+  v3 norm2_pre = v3_cross(v3_psub(t, r1v, b1v), v3_psub(t, a1v, b1v));
+  const v3 norm1 = v3_normalize(&norm1_pre), norm2 = v3_normalize(&norm2_pre);
+  const double dot1 = v3_dot(norm1, norm2);
+  return v3_scale(bend_factor(dot1),
+                  v3_add(v3_div(v3_cross(v3_psub(t, b1v, c1v), tri_rho(norm1, norm2)),
+                                v3_norm(norm1_pre)),
+                         v3_div(v3_cross(v3_psub(t, a1v, b1v), tri_rho(norm2, norm1)),
+                                v3_norm(norm2_pre))));
+}
+/* tri_memb_bend, :497-508 */
+static void tri_memb_bend(ora_tissue* t, int32_t m) {
+  const int32_t* nb = &t->tri_nb[6 * m];
+  v3 dr = {0, 0, 0};
+  for (int i = 0; i < 6; ++i) {
+    const int32_t b = nb[(i + 1) % 6];
+    dr = v3_add(dr, tri_bend_1(t, m, nb[i], b, t->tri_nb[6 * b + i]));
+  }
+  for (int i = 0; i < 6; ++i) dr = v3_add(dr, tri_bend_2(t, m, nb[i], nb[(i + 1) % 6], nb[(i + 2) % 6]));
+  t->nx[m] += t->P.dt * t->P.kbend * dr.x;
+  t->ny[m] += t->P.dt * t->P.kbend * dr.y;
+  t->nz[m] += t->P.dt * t->P.kbend * dr.z;
+}
+
 static inline int is_aad(uint8_t s) { return s == S_ALIVE || s == S_AIR || s == S_DEAD; }
 
 /* cell_interaction, :648-685, with the per-state bodies :529-641 */
 int ora_interact(ora_tissue* t) {
   const int64_t C = CONN_CAP;
-  for (int32_t m = 0; m < t->nmemb; ++m) bend_calc1(t, m);
-  for (int32_t m = 0; m < t->nmemb; ++m) bend_calc2(t, m);
-  for (int32_t m = 0; m < t->nmemb; ++m) bend_calc3(t, m);
+  if (t->tri) { /* memb_bend, TRI_MEMB branch, :501-506 */
+    for (int32_t m = 0; m < t->nmemb; ++m) tri_memb_bend(t, m);
+  } else {
+    for (int32_t m = 0; m < t->nmemb; ++m) bend_calc1(t, m);
+    for (int32_t m = 0; m < t->nmemb; ++m) bend_calc2(t, m);
+    for (int32_t m = 0; m < t->nmemb; ++m) bend_calc3(t, m);
+  }
   /* _MEMB_interaction, :529-547 */
   for (int32_t m = 0; m < t->nmemb; ++m) {
     if (t->z[m] < t->radius[m]) wall(t, m);
-    for (int32_t i = 0; i < MEMB_ADJ; ++i) {
+    for (int32_t i = 0; i < t->nadj; ++i) {
       const int32_t o = t->conn[m * C + i];
       if (t->state[o] == S_MEMB && m > o) apply(t, m, o, ci_memb_memb(t, m, o));
     }
@@ -478,6 +552,36 @@ int ora_step(ora_tissue* t, int32_t nsteps) {
 }
 
 /* Square lattice wiring, _memb_init, cellmanager.cpp:114-166. */
+/* Triangular lattice wiring, _memb_init TRI_MEMB branch, cellmanager.cpp:70-111:
+ * memb[0] right, [3] left; rows alternate their offset, so the upper / lower
+ * neighbours depend on the row's parity. */
+static void wire_membrane_tri(ora_tissue* t) {
+  const int32_t NMX = t->nmx, nm = t->nmemb;
+  for (int32_t j = 0; j < nm; ++j) {
+    const int32_t jj = j % NMX;
+    t->tri_nb[6 * j + 3] = jj == 0 ? j + NMX - 1 : j - 1;
+    t->tri_nb[6 * j + 0] = jj == NMX - 1 ? j - (NMX - 1) : j + 1;
+  }
+  for (int32_t j = 0; j < nm; ++j) {
+    const int32_t kk = j / NMX;
+    const int32_t top = (j - NMX + nm) % nm, bot = (j + NMX) % nm;
+    int32_t* nb = &t->tri_nb[6 * j];
+    if (kk % 2 == 0) {
+      nb[1] = top;
+      nb[2] = t->tri_nb[6 * top + 3];
+      nb[4] = t->tri_nb[6 * bot + 3];
+      nb[5] = bot;
+    } else {
+      nb[1] = t->tri_nb[6 * top + 0];
+      nb[2] = top;
+      nb[4] = bot;
+      nb[5] = t->tri_nb[6 * bot + 0];
+    }
+    t->nconn[j] = 0;
+    for (int i = 0; i < 6; ++i) push_conn(t, j, nb[i]);
+  }
+}
+
 static void wire_membrane(ora_tissue* t) {
   const int32_t NMX = t->nmx, NMY = t->nmy;
   for (int32_t j = 0; j < t->nmemb; ++j) {
@@ -504,12 +608,24 @@ ora_tissue* ora_new(int32_t n, int32_t nmemb, int32_t nder, int32_t nmx, int32_t
                     const double* x, const double* y, const double* z,
                     const double* radius, const double* agek, const double* spr_nat_len,
                     const uint8_t* state, const int32_t* pair, const int32_t* rest_div_times) {
+  return ora_new_lattice(n, nmemb, nder, nmx, nmy, lx, ly, lz, params14, x, y, z, radius, agek,
+                         spr_nat_len, state, pair, rest_div_times, 0);
+}
+
+ora_tissue* ora_new_lattice(int32_t n, int32_t nmemb, int32_t nder, int32_t nmx, int32_t nmy,
+                            double lx, double ly, double lz, const double* params14,
+                            const double* x, const double* y, const double* z,
+                            const double* radius, const double* agek, const double* spr_nat_len,
+                            const uint8_t* state, const int32_t* pair,
+                            const int32_t* rest_div_times, int32_t lattice) {
   if (n < 0 || nmemb < 0 || nder < 0 || nmemb + nder > n || nmx < 3 || nmy < 3 ||
-      nmemb != nmx * nmy)
+      nmemb != nmx * nmy || lattice < 0 || lattice > 1 || (lattice == 1 && nmy % 2 != 0))
     return NULL;
   ora_tissue* t = calloc(1, sizeof(ora_tissue));
   if (!t) return NULL;
   t->n = n; t->nmemb = nmemb; t->nder = nder; t->nmx = nmx; t->nmy = nmy;
+  t->tri = lattice;
+  t->nadj = lattice ? MEMB_ADJ_TRI : MEMB_ADJ_SQUARE;
   t->lx = lx; t->ly = ly; t->lz = lz;
   /* ANX, ANY, ANZ, cell_connection.cpp:22-26 */
   t->anx = (int32_t)(lx / AREA_GRID_ORIGINAL + 0.5);
@@ -523,6 +639,7 @@ ora_tissue* ora_new(int32_t n, int32_t nmemb, int32_t nder, int32_t nmx, int32_t
   ALLOC(t->conn, (int64_t)n * CONN_CAP); ALLOC(t->nconn, n);
   ALLOC(t->lat_l, nmemb); ALLOC(t->lat_ll, nmemb); ALLOC(t->lat_r, nmemb);
   ALLOC(t->lat_b, nmemb); ALLOC(t->lat_bb, nmemb); ALLOC(t->lat_u, nmemb);
+  ALLOC(t->tri_nb, 6 * (int64_t)nmemb);
   ALLOC(t->nv, 3 * (int64_t)nmemb); ALLOC(t->mv, 3 * (int64_t)nmemb);
   ALLOC(t->dn, nmemb); ALLOC(t->dm, nmemb); ALLOC(t->ipn, nmemb); ALLOC(t->ipm, nmemb);
   ALLOC(t->bin_cnt, (int64_t)t->anx * t->any * t->anz);
@@ -539,7 +656,10 @@ ora_tissue* ora_new(int32_t n, int32_t nmemb, int32_t nder, int32_t nmx, int32_t
     t->rest_div[i] = rest_div_times[i];
     t->dermis[i] = -1;
   }
-  wire_membrane(t);
+  if (t->tri)
+    wire_membrane_tri(t);
+  else
+    wire_membrane(t);
   ora_connect(t);
   return t;
 fail:
@@ -554,7 +674,7 @@ void ora_free(ora_tissue* t) {
   free(t->pair); free(t->rest_div); free(t->dermis); free(t->conn); free(t->nconn);
   free(t->lat_l); free(t->lat_ll); free(t->lat_r); free(t->lat_b); free(t->lat_bb);
   free(t->lat_u); free(t->nv); free(t->mv); free(t->dn); free(t->dm); free(t->ipn);
-  free(t->ipm); free(t->bin_cnt); free(t->bin_list);
+  free(t->ipm); free(t->bin_cnt); free(t->bin_list); free(t->tri_nb);
   free(t);
 }
 

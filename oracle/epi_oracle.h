@@ -49,6 +49,14 @@ ora_tissue* ora_new(int32_t n, int32_t nmemb, int32_t nder, int32_t nmx, int32_t
                     const double* x, const double* y, const double* z,
                     const double* radius, const double* agek, const double* spr_nat_len,
                     const uint8_t* state, const int32_t* pair, const int32_t* rest_div_times);
+/* Same, with the membrane lattice: 0 square (TRI_MEMB undefined), 1
+ * triangular (TRI_MEMB, the reference's default; nmy = number of rows, even). */
+ora_tissue* ora_new_lattice(int32_t n, int32_t nmemb, int32_t nder, int32_t nmx, int32_t nmy,
+                            double lx, double ly, double lz, const double* params14,
+                            const double* x, const double* y, const double* z,
+                            const double* radius, const double* agek, const double* spr_nat_len,
+                            const uint8_t* state, const int32_t* pair,
+                            const int32_t* rest_div_times, int32_t lattice);
 void ora_free(ora_tissue* t);
 
 int ora_connect(ora_tissue* t);         /* connect_cell without gj_refresh */

@@ -67,6 +67,8 @@ def lib():
         u8 = ctypes.POINTER(ctypes.c_uint8)
         L.ora_new.restype = P
         L.ora_new.argtypes = [ctypes.c_int32] * 5 + [ctypes.c_double] * 3 + [d] * 7 + [u8, i32, i32]
+        L.ora_new_lattice.restype = P
+        L.ora_new_lattice.argtypes = L.ora_new.argtypes + [ctypes.c_int32]
         L.ora_free.argtypes = [P]
         for f in ("ora_connect", "ora_interact"):
             getattr(L, f).argtypes = [P]
@@ -107,11 +109,11 @@ class OracleTissue:
         pr = np.ascontiguousarray(t.pair, dtype=np.int32)
         rd = np.ascontiguousarray(t.rest_div_times, dtype=np.int32)
         self.n = t.n
-        self._h = L.ora_new(t.n, t.nmemb, t.nder, t.nmx, t.nmy, t.lx, t.ly, t.lz,
-                            _p(p, ctypes.c_double),
-                            *[_p(a, ctypes.c_double) for a in self._keep],
-                            _p(st, ctypes.c_uint8), _p(pr, ctypes.c_int32),
-                            _p(rd, ctypes.c_int32))
+        self._h = L.ora_new_lattice(t.n, t.nmemb, t.nder, t.nmx, t.nmy, t.lx, t.ly, t.lz,
+                                    _p(p, ctypes.c_double),
+                                    *[_p(a, ctypes.c_double) for a in self._keep],
+                                    _p(st, ctypes.c_uint8), _p(pr, ctypes.c_int32),
+                                    _p(rd, ctypes.c_int32), int(getattr(t, "lattice", 0)))
         if not self._h:
             raise ValueError("oracle rejected the tissue")
 
@@ -165,7 +167,7 @@ def reference_binary(t, variant: str = "serial") -> Optional[Path]:
     br = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(br)
     try:
-        name = br.geometry_for(t.nmx, t.nmy, t.lx, t.ly, t.lz)
+        name = br.geometry_for(t.nmx, t.nmy, t.lx, t.ly, t.lz, getattr(t, "lattice", 0))
     except KeyError:
         return None
     p = br.binary_path(name, variant)

@@ -9,8 +9,8 @@ committed and the tests read them anywhere.
 
     python tests/golden/make_golden.py [case ...]
 
-Cases "c1" and "mixed" run the mechanics step (interaction, commit, wrap,
-connect). Case "renewal" runs the complete cell_dynamics including the
+Cases "c1", "mixed" and "tri" (triangular membrane, the reference's default
+TRI_MEMB build) run the mechanics step (interaction, commit, wrap, connect). Case "renewal" runs the complete cell_dynamics including the
 reference's state renewal, with the harness's division draw fixed at 0 (every
 division test that is reached passes), so cells divide, cornify and are
 removed and the frames differ in size.
@@ -35,6 +35,8 @@ CASES = {
     "c1": (T.config1, 1000, (0, 100, 1000), "run", {}),
     "mixed": (T.mixed_state_tissue, 300, (0, 50, 300), "run", {}),
     "renewal": (T.renewal_tissue, 200, (0, 1, 20, 100, 200), "dyn", {"EPI_HARNESS_RNG": "zero"}),
+    # triangular membrane: the reference's default TRI_MEMB build
+    "tri": (lambda: T.tri_layered_tissue(16, 18, 2, 0), 300, (0, 50, 300), "run", {}),
 }
 
 

@@ -14,7 +14,12 @@ from tests.golden.make_golden import load
 from tests.helpers import lists_equal
 
 
-@pytest.mark.parametrize("name,factory", [("c1", T.config1), ("mixed", T.mixed_state_tissue)])
+def tri_c1():
+    return T.tri_layered_tissue(16, 18, 2, 0)
+
+
+@pytest.mark.parametrize("name,factory", [("c1", T.config1), ("mixed", T.mixed_state_tissue),
+                                          ("tri", tri_c1)])
 def test_oracle_reproduces_reference_golden_frames(built, name, factory):
     frames = load(name)
     t = factory()
@@ -39,6 +44,7 @@ def _ref_available(t):
     (lambda: T.layered_tissue(24, 3, 11), 40),
     (lambda: T.layered_tissue(64, 8, 1), 3),
     (lambda: T.config1(5), 200),
+    (lambda: T.tri_layered_tissue(32, 36, 4, 3), 50),
 ])
 def test_oracle_matches_compiled_reference_live(built, factory, steps):
     t = factory()
