@@ -10,10 +10,11 @@ committed and the tests read them anywhere.
     python tests/golden/make_golden.py [case ...]
 
 Cases "c1", "mixed" and "tri" (triangular membrane, the reference's default
-TRI_MEMB build) run the mechanics step (interaction, commit, wrap, connect). Case "renewal" runs the complete cell_dynamics including the
-reference's state renewal, with the harness's division draw fixed at 0 (every
-division test that is reached passes), so cells divide, cornify and are
-removed and the frames differ in size.
+TRI_MEMB build) run the mechanics step (interaction, commit, wrap, connect).
+Case "renewal" runs the complete cell_dynamics including the reference's
+state renewal, with the harness's division draw fixed at 0 (every division
+test that is reached passes), so cells divide, cornify and are removed and
+the frames differ in size.
 """
 from __future__ import annotations
 
