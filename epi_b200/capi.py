@@ -73,7 +73,8 @@ class TissueViewC(ctypes.Structure):
                 ("lx", ctypes.c_double), ("ly", ctypes.c_double), ("lz", ctypes.c_double),
                 ("x", _dp), ("y", _dp), ("z", _dp), ("radius", _dp), ("agek", _dp),
                 ("spr_nat_len", _dp), ("state", _up), ("pair", _ip),
-                ("rest_div_times", _ip)]
+                ("rest_div_times", _ip), ("lattice", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
 
 class LossC(ctypes.Structure):
@@ -230,6 +231,8 @@ class Context:
             v.state = _ptr(arrs["state"], ctypes.c_uint8)
             v.pair = _ptr(arrs["pair"], ctypes.c_int32)
             v.rest_div_times = _ptr(arrs["rest"], ctypes.c_int32)
+            v.lattice = int(getattr(t, "lattice", 0))
+            v.reserved = 0
             p = (params[k] if params is not None else t.params)
             pars[k] = ParamsC.from_params(p)
         rc = lib().epi_upload(self._h, len(tissues), views, pars)

@@ -425,6 +425,12 @@ int validate_tissue(const epi_tissue_view& v, const epi_params& P) {
   if (v.n > 0 && (!v.x || !v.y || !v.z || !v.radius || !v.state)) return EPI_ERR_INVALID_ARG;
   if (!(v.lx > 0) || !(v.ly > 0) || !(v.lz > 0)) return EPI_ERR_INVALID_ARG;
   if (v.nmemb != v.nmx * v.nmy || v.nmx < 3 || v.nmy < 3) return EPI_ERR_UNSUPPORTED;
+  if (v.lattice != EPI_LATTICE_SQUARE && v.lattice != EPI_LATTICE_TRIANGULAR)
+    return EPI_ERR_INVALID_ARG;
+  if (v.reserved != 0) return EPI_ERR_INVALID_ARG;
+  // the triangular wiring alternates row offsets: an odd row count breaks
+  // the periodic wrap (cellmanager.cpp:95-108)
+  if (v.lattice == EPI_LATTICE_TRIANGULAR && v.nmy % 2 != 0) return EPI_ERR_UNSUPPORTED;
   // The 5-bin search window of connect_proc must not wrap onto itself
   // (cell_connection.cpp:101-109), else the reference pushes pairs twice.
   const int anx = (int)(v.lx / 2.0 + 0.5), any = (int)(v.ly / 2.0 + 0.5), anz = (int)(v.lz / 2.0);
@@ -627,6 +633,8 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
     T.any = (int32_t)(v.ly / 2.0 + 0.5);
     T.anz = (int32_t)(v.lz / 2.0);
     T.binbase = binbase;
+    T.lattice = v.lattice;
+    T.nadj = v.lattice == EPI_LATTICE_TRIANGULAR ? kMembAdjTri : kMembAdj;
     T.mbase = (int32_t)prep_m.size();
     T.lx = v.lx;
     T.ly = v.ly;
@@ -745,6 +753,8 @@ int epi_adjoint(epi_ctx* c, int32_t nsteps, int32_t K, const epi_loss* loss, dou
     return EPI_ERR_INVALID_ARG;
   if (!c->loaded) return EPI_ERR_STATE;
   if (!c->lc.simple) return EPI_ERR_UNSUPPORTED;
+  for (const TissueDev& T : c->tissues_h)
+    if (T.lattice != EPI_LATTICE_SQUARE) return EPI_ERR_UNSUPPORTED;
   EPI_GUARD_BEGIN
   int rc = set_device(c);
   if (rc) return rc;

@@ -37,6 +37,8 @@ enum ErrCode : int32_t {
 constexpr double kAreaGrid = 2.0 + 1e-7;  // AREA_GRID, cell_connection.cpp:16-19
 constexpr int kBinCap = 200;              // N3, cell_connection.cpp:28
 constexpr int kMembAdj = 4;               // MEMB_ADJ_CONN_NUM (square), define.h:147-153
+constexpr int kMembAdjTri = 6;            // MEMB_ADJ_CONN_NUM (TRI_MEMB)
+constexpr int kLatticeSquare = 0, kLatticeTriangular = 1;
 
 struct Params {
   double dt, eps_m, p_memb, der_der_const, k_total, k_desmosome, kspring, kspring_d, kbend,
@@ -302,6 +304,8 @@ struct TissueDev {
   int32_t pbase, n, nmemb, nder, nmx, nmy;
   int32_t anx, any, anz;  // reference grid (cell_connection.cpp:22-26)
   int32_t binbase;        // first bin; a tissue owns anx*any*anz bins + 1 sentinel
+  int32_t lattice;        // kLatticeSquare / kLatticeTriangular
+  int32_t nadj;           // lattice links per membrane particle (4 / 6)
   int32_t mbase;          // index in prep of the tissue's first membrane particle
   double lx, ly, lz, hlx, hly;     // box and half box
   double rmax;     // largest radius in the tissue
@@ -360,6 +364,33 @@ __device__ __forceinline__ Lattice lattice_of(int32_t j, int32_t NMX, int32_t NM
   L.bb = kk <= 1 ? j + NMX * NMY - 2 * NMX : j - 2 * NMX;
   L.u = kk == NMY - 1 ? j - (NMX * NMY - NMX) : j + NMX;
   return L;
+}
+
+// Triangular lattice: Memb_data::memb[k] of membrane particle j (tissue-local)
+// as _memb_init's TRI_MEMB branch wires it (epi5_MT/cellmanager.cpp:70-111):
+// 0 right, 3 left; 1, 2 in the row above (j - NMX) and 4, 5 in the row
+// below (j + NMX), which of the two columns depending on the row's parity.
+__host__ __device__ __forceinline__ int32_t tri_link(int32_t j, int k, int32_t NMX, int32_t nm) {
+  auto left = [NMX](int32_t v) { return v % NMX == 0 ? v + NMX - 1 : v - 1; };
+  auto right = [NMX](int32_t v) { return v % NMX == NMX - 1 ? v - (NMX - 1) : v + 1; };
+  const bool even = (j / NMX) % 2 == 0;
+  const int32_t top = (j - NMX + nm) % nm, bot = (j + NMX) % nm;
+  switch (k) {
+    case 0: return right(j);
+    case 1: return even ? top : right(top);
+    case 2: return even ? left(top) : top;
+    case 3: return left(j);
+    case 4: return even ? left(bot) : bot;
+    default: return even ? bot : right(bot);
+  }
+}
+
+// The k-th lattice link of membrane particle j in connected_cell's push
+// order: square l, r, b, u (cellmanager.cpp:160-163), triangular memb[0..5].
+__device__ __forceinline__ int32_t lattice_link(const TissueDev& T, int32_t j, int k) {
+  if (T.lattice == kLatticeTriangular) return tri_link(j, k, T.nmx, T.nmemb);
+  const Lattice L = lattice_of(j, T.nmx, T.nmy);
+  return k == 0 ? L.l : (k == 1 ? L.r : (k == 2 ? L.b : L.u));
 }
 
 }  // namespace epi

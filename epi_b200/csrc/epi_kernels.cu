@@ -542,11 +542,86 @@ struct SiteOffsets<float> {
   }
 };
 
-// Membrane particles: bending (_memb_bend_calc1..3, :296-449; the unit
-// vectors of calc1 are recomputed from the eleven lattice positions the
-// stencil reaches instead of being stored), the four lattice springs of
-// _MEMB_interaction (:529-547, each applied once by the higher index) and
-// the wall (:287-294). The sum goes to S.fmemb; k_step adds it.
+template <typename R>
+__device__ __forceinline__ Vec3<R> v3_cross(const Vec3<R>& a, const Vec3<R>& b) {
+  return Vec3<R>{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+template <typename R>
+__device__ __forceinline__ Vec3<R> v3_sub(const Vec3<R>& a, const Vec3<R>& b) {
+  return Vec3<R>{a.x - b.x, a.y - b.y, a.z - b.z};
+}
+template <typename R>
+__device__ __forceinline__ Vec3<R> v3_axpy(R s, const Vec3<R>& a, const Vec3<R>& b) {
+  return Vec3<R>{s * a.x + b.x, s * a.y + b.y, s * a.z + b.z};
+}
+template <typename R>
+__device__ __forceinline__ R v3_dot(const Vec3<R>& a, const Vec3<R>& b) {
+  return a.x * b.x + a.y * b.y + a.z * b.z;
+}
+template <typename R>
+__device__ __forceinline__ Vec3<R> v3_unit(const Vec3<R>& a) {
+  const R inv = frsqrt(v3_dot(a, a));
+  return Vec3<R>{a.x * inv, a.y * inv, a.z * inv};
+}
+
+// Triangular-membrane bending of particle j (tri_memb_bend, tri_bend_1 and
+// tri_bend_2, cell_interaction.cpp:451-508) from the offsets of its six
+// lattice neighbours n[i] = memb[i] and of the six second-ring sites
+// c[i] = memb[(i+1)%6]->memb[i]; the particle itself is the origin. Returns
+// the sum dr before the DT * KBEND factor. The reference divides each term
+// by the norm of a normal it has already normalised in place
+// (vec3::normalize, vec3.h:40-44), i.e. by 1 up to rounding; that division
+// is left out.
+template <typename R, typename Off>
+__device__ __forceinline__ Vec3<R> tri_bending(const Off& off, int32_t j, int32_t NMX,
+                                               int32_t nm, int32_t pb) {
+  Vec3<R> n[6], c[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) n[i] = off(pb + tri_link(j, i, NMX, nm));
+#pragma unroll
+  for (int i = 0; i < 6; ++i)
+    c[i] = off(pb + tri_link(tri_link(j, (i + 1) % 6, NMX, nm), i, NMX, nm));
+  Vec3<R> dr{R(0), R(0), R(0)};
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    // tri_bend_1(r1 = self, a1 = n[i], b1 = n[i+1], c1 = c[i])
+    const Vec3<R>& a = n[i];
+    const Vec3<R>& b = n[(i + 1) % 6];
+    const Vec3<R> rb{-b.x, -b.y, -b.z};
+    const Vec3<R> ab = v3_sub(a, b);
+    const Vec3<R> n1 = v3_unit(v3_cross(rb, ab));
+    const Vec3<R> n2 = v3_unit(v3_cross(ab, v3_sub(c[i], b)));
+    const R d = v3_dot(n1, n2);
+    const Vec3<R> t = v3_cross(ab, v3_axpy(-d, n1, n2));  // ab x tri_rho(n1, n2)
+    dr = v3_axpy(bend_factor(d), t, dr);
+  }
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    // tri_bend_2(r1 = self, a1 = n[i], b1 = n[i+1], c1 = n[i+2])
+    const Vec3<R>& a = n[i];
+    const Vec3<R>& b = n[(i + 1) % 6];
+    const Vec3<R>& cc = n[(i + 2) % 6];
+    const Vec3<R> rc{-cc.x, -cc.y, -cc.z};
+    const Vec3<R> rb{-b.x, -b.y, -b.z};
+    const Vec3<R> bc = v3_sub(b, cc);
+    const Vec3<R> ab = v3_sub(a, b);
+    const Vec3<R> n1 = v3_unit(v3_cross(rc, bc));
+    const Vec3<R> n2 = v3_unit(v3_cross(rb, ab));
+    const R d = v3_dot(n1, n2);
+    const Vec3<R> t1 = v3_cross(bc, v3_axpy(-d, n1, n2));  // bc x tri_rho(n1, n2)
+    const Vec3<R> t2 = v3_cross(ab, v3_axpy(-d, n2, n1));  // ab x tri_rho(n2, n1)
+    const R g = bend_factor(d);
+    dr = v3_axpy(g, Vec3<R>{t1.x + t2.x, t1.y + t2.y, t1.z + t2.z}, dr);
+  }
+  return dr;
+}
+
+// Membrane particles: bending (square: _memb_bend_calc1..3, :296-449, the
+// unit vectors of calc1 recomputed from the eleven lattice positions the
+// stencil reaches instead of being stored; triangular: tri_memb_bend,
+// :451-508), the lattice springs of _MEMB_interaction (:529-547, each
+// applied once by the higher index) and the wall (:287-294). The sum goes to
+// S.fmemb; k_step adds it.
 template <typename R>
 __global__ void __launch_bounds__(256) k_memb_force(DevState S, int32_t m0, int32_t m1) {
   pdl_entry();
@@ -570,7 +645,13 @@ __global__ void __launch_bounds__(256) k_memb_force(DevState S, int32_t m0, int3
     const double4 p = S.pos_cur[i];
     const SiteOffsets<R> off(S, i, p, T);
     double ax = 0.0, ay = 0.0, az = 0.0;
-    {
+    if (T.lattice == kLatticeTriangular) {
+      const Vec3<R> b = tri_bending<R>(off, j, NMX, T.nmemb, pb);
+      const R s = R(dt * T.P.kbend);
+      ax += double(s * b.x);
+      ay += double(s * b.y);
+      az += double(s * b.z);
+    } else {
       const Vec3<R> o_r = off(site(1, 0));
       const Vec3<R> o_rr = off(site(2, 0));
       const Vec3<R> o_l = off(site(-1, 0));
@@ -610,10 +691,8 @@ __global__ void __launch_bounds__(256) k_memb_force(DevState S, int32_t m0, int3
         else az += d;
       }
     }
-    const int32_t links[4] = {site(-1, 0), site(1, 0), site(0, -1), site(0, 1)};
-#pragma unroll
-    for (int k = 0; k < kMembAdj; ++k) {
-      const int32_t q = links[k];
+    for (int k = 0; k < T.nadj; ++k) {
+      const int32_t q = pb + lattice_link(T, j, k);
       const double4 pq = S.pos_cur[q];
       const bool hi = i > q;
       double dx, dy, dz;
@@ -911,7 +990,8 @@ __global__ void k_exact_lists(DevState S, Range r) {
 __global__ void k_rowlen(DevState S, int32_t* rowlen, int32_t n) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  rowlen[i] = S.nn[i] + (attr_state(S.attr[i]) == ST_MEMB ? kMembAdj : 0);
+  const uint32_t a = S.attr[i];
+  rowlen[i] = S.nn[i] + (attr_state(a) == ST_MEMB ? S.tissues[attr_tissue(a)].nadj : 0);
 }
 
 __global__ void k_fill_csr(DevState S, const int32_t* rowoff, int32_t* idx, int32_t n) {
@@ -921,13 +1001,8 @@ __global__ void k_fill_csr(DevState S, const int32_t* rowoff, int32_t* idx, int3
   const TissueDev& T = S.tissues[attr_tissue(a)];
   int32_t o = rowoff[i];
   const int32_t o0 = o;
-  if (attr_state(a) == ST_MEMB) {
-    const Lattice Lt = lattice_of(i - T.pbase, T.nmx, T.nmy);
-    idx[o++] = Lt.l;  // push order of _memb_init, cellmanager.cpp:160-163
-    idx[o++] = Lt.r;
-    idx[o++] = Lt.b;
-    idx[o++] = Lt.u;
-  }
+  if (attr_state(a) == ST_MEMB)  // push order of _memb_init, cellmanager.cpp:70-166
+    for (int k = 0; k < T.nadj; ++k) idx[o++] = lattice_link(T, i - T.pbase, k);
   const int32_t nn = S.nn[i];
   for (int32_t k = 0; k < nn; ++k) idx[o++] = S.nbr[(int64_t)k * S.n_total + i] - T.pbase;
   for (int32_t s = o0 + 1; s < o; ++s) {

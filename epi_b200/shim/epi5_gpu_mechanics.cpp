@@ -54,7 +54,7 @@ class GpuMechanics {
     for (int32_t i = 0; i < n; ++i) {
       Cell* c = cells_[i];
       if (c->state == MEMB) {
-        // the lattice links _memb_init pushed stay first (cellmanager.cpp:160-163)
+        // the lattice links _memb_init pushed stay first (cellmanager.cpp:70-166)
         c->connected_cell.force_set_count(cont::MEMB_ADJ_CONN_NUM);
         for (int32_t k = off_[i]; k < off_[i + 1]; ++k) {
           Cell* o = cells_[idx_[k]];
@@ -171,7 +171,9 @@ class GpuMechanics {
     view_.nmemb = nmemb;
     view_.nder = nder;
     view_.nmx = (int32_t)cont::NMX;
-    view_.nmy = (int32_t)cont::NMY;
+    // rows of the lattice: NMY for the square build; the triangular build
+    // wires by NMX and the membrane count only (cellmanager.cpp:70-111)
+    view_.nmy = nmemb / (int32_t)cont::NMX;
     view_.lx = cont::LX;
     view_.ly = cont::LY;
     view_.lz = cont::LZ;
@@ -184,6 +186,12 @@ class GpuMechanics {
     view_.state = state_.data();
     view_.pair = pair_.data();
     view_.rest_div_times = rest_.data();
+#ifdef TRI_MEMB
+    view_.lattice = EPI_LATTICE_TRIANGULAR;  // define.h:66
+#else
+    view_.lattice = EPI_LATTICE_SQUARE;
+#endif
+    view_.reserved = 0;
   }
 
   void check(int rc, const char* where) {

@@ -71,10 +71,17 @@ typedef struct epi_params {
   double thresh_sp;
 } epi_params;
 
+/* Membrane lattices of epi5_MT (define.h:66, TRI_MEMB). */
+typedef enum epi_lattice {
+  EPI_LATTICE_SQUARE = 0,     /* TRI_MEMB undefined: 4 links, cellmanager.cpp:114-166 */
+  EPI_LATTICE_TRIANGULAR = 1  /* TRI_MEMB (the reference's default): 6 links,
+                                 cellmanager.cpp:70-111; nmy = rows, even */
+} epi_lattice;
+
 /* One tissue in structure-of-arrays form: what epi5_MT's Cell objects hold for
  * the mechanics (epi5_MT/cell.h:101-247). Indices (pair) are tissue-local,
- * -1 for none; pairs must be mutual. nmemb must equal nmx * nmy (square
- * membrane wired as epi5_MT/cellmanager.cpp:114-166). */
+ * -1 for none; pairs must be mutual. nmemb must equal nmx * nmy; the
+ * membrane particles come first, row by row, wired as `lattice` says. */
 typedef struct epi_tissue_view {
   int32_t n, nmemb, nder;
   int32_t nmx, nmy;
@@ -88,6 +95,8 @@ typedef struct epi_tissue_view {
   const uint8_t* state;          /* CELL_STATE, epi5_MT/define.h:36-47 */
   const int32_t* pair;
   const int32_t* rest_div_times;
+  int32_t lattice;               /* epi_lattice (0 = square) */
+  int32_t reserved;              /* must be 0 */
 } epi_tissue_view;
 
 typedef enum epi_precision {

@@ -127,3 +127,12 @@ def test_adjoint_rejects_unsupported_tissues_and_arguments(built):
         with pytest.raises(capi.EpiError) as e:
             ctx.adjoint(5, (t.x, t.y, t.z), checkpoint_every=0)
         assert e.value.code == capi.EPI_ERR_INVALID_ARG
+
+
+def test_adjoint_rejects_triangular_membranes(built):
+    t = T.tri_layered_tissue(16, 18, 2, 0)
+    with capi.Context(precision=FP64) as ctx:
+        ctx.upload([t])
+        with pytest.raises(capi.EpiError) as e:
+            ctx.adjoint(5, (t.x, t.y, t.z))
+        assert e.value.code == capi.EPI_ERR_UNSUPPORTED

@@ -83,3 +83,15 @@ def test_dropin_runs_the_reference_state_renewal_loop(built):
         assert lists_equal(f["conn_off"], f["conn_idx"], g["conn_off"], g["conn_idx"]), \
             list_diff_summary(f["conn_off"], f["conn_idx"], g["conn_off"], g["conn_idx"])
         assert np.array_equal(f["dermis"], g["dermis"]), g["step"]
+
+
+def test_dropin_triangular_build_matches_reference_frames(built):
+    """The drop-in compiled into the reference's default TRI_MEMB build."""
+    t = T.tri_layered_tissue(16, 18, 2, 0)
+    golden = {f["step"]: f for f in load("tri")}
+    frames = {f["step"]: f for f in _dropin_frames(t, 300, 50, "fp64")}
+    for s, g in golden.items():
+        f = frames[s]
+        err = rel_pos_err((f["x"], f["y"], f["z"]), (g["x"], g["y"], g["z"]), t.lx, t.ly)
+        assert err <= TOL_FP64, (s, err)
+        assert lists_equal(f["conn_off"], f["conn_idx"], g["conn_off"], g["conn_idx"])

@@ -350,3 +350,48 @@ def test_mixed_path_decides_threshold_pairs_with_the_fp64_predicate(built):
     for k in range(3):
         assert abs(pmx[k][d] - p64[k][d]) < 1e-9, (k, pmx[k][d], p64[k][d])
         assert abs(pmx[k][d + 2] - p64[k][d + 2]) < 1e-9
+
+
+def tri_c1():
+    return T.tri_layered_tissue(16, 18, 2, 0)
+
+
+def test_triangular_membrane_fp64_vs_reference_frames(built):
+    """The reference's default build (TRI_MEMB): six lattice links and the
+    dihedral bending of tri_memb_bend (cell_interaction.cpp:451-508)."""
+    frames = load("tri")
+    t = tri_c1()
+    _, off, idx, _ = run_gpu([t], 0, FP64)
+    assert lists_equal(off, idx, frames[0]["conn_off"], frames[0]["conn_idx"])
+    with capi.Context(precision=FP64) as ctx:
+        ctx.upload([t])
+        done = 0
+        for f in frames[1:]:
+            ctx.step(f["step"] - done)
+            done = f["step"]
+            pos = ctx.positions()
+            err = rel_pos_err(pos, (f["x"], f["y"], f["z"]), t.lx, t.ly)
+            assert err <= TOL_FP64, (f["step"], err)
+            off, idx = ctx.connections()
+            assert lists_equal(off, idx, f["conn_off"], f["conn_idx"]), \
+                list_diff_summary(off, idx, f["conn_off"], f["conn_idx"])
+
+
+def test_triangular_membrane_mixed_precision(built):
+    frames = load("tri")
+    t = tri_c1()
+    pos, _, _, _ = run_gpu([t], frames[-1]["step"], MIXED)
+    f = frames[-1]
+    assert rel_pos_err(pos, (f["x"], f["y"], f["z"]), t.lx, t.ly) <= TOL_MIXED
+
+
+def test_square_and_triangular_tissues_in_one_batch(built):
+    ts = [T.config1(3), tri_c1(), T.tri_layered_tissue(32, 36, 3, 5), T.mixed_state_tissue()]
+    steps = 40
+    pos_b, off_b, idx_b, _ = run_gpu(ts, steps, FP64, max_conn=96)
+    o = 0
+    for t in ts:
+        pos_1, off_1, idx_1, _ = run_gpu([t], steps, FP64, max_conn=96)
+        for k in range(3):
+            assert np.array_equal(pos_b[k][o:o + t.n], pos_1[k])
+        o += t.n
