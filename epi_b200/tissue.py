@@ -282,22 +282,38 @@ def config5(seed: int = 4) -> Tissue:
     return layered_tissue(64, 8, seed, name="C5")
 
 
-def mixed_state_tissue(seed: int = 7) -> Tissue:
+def mixed_state_tissue(seed: int = 7, lattice: int = SQUARE) -> Tissue:
     """Small tissue exercising every force law of the path: dermis (DER) under a
-    32x32 membrane at the reference's natural 0.5 spacing, stem (FIX) cells
+    32-wide membrane at the reference's natural 0.5 spacing, stem (FIX) cells
     paired with daughters (MUSUME), unpaired MUSUME with divisions left, and
     ALIVE / DEAD / AIR cells above, some older than THRESH_SP. The layout
     follows the reference's own initial-state generator
     (epi_intg/calc/init_gen.cpp:46-104): DER lattice at pitch 2 R_der, membrane
-    at Z_LEVEL + R_memb, FIX at R_max + R_memb + Z_LEVEL + R_memb."""
+    at Z_LEVEL + R_memb, FIX at R_max + R_memb + Z_LEVEL + R_memb. The
+    membrane is a 32 x 32 square lattice in a 16 x 16 box, or (TRIANGULAR)
+    32 x 36 rows of the reference's default triangular lattice, rows
+    0.5 sqrt(3)/2 apart, in a 16 x 15.59 box."""
     L = 16.0
     side = 32
     pitch = 0.5
     z_level = 2.0 * R_DER
-    nm = side * side
-    jj, kk = np.meshgrid(np.arange(side), np.arange(side), indexing="xy")
-    xs = [list((jj.ravel() + 0.5) * pitch)]
-    ys = [list((kk.ravel() + 0.5) * pitch)]
+    if lattice == TRIANGULAR:
+        rows = 36
+        dy = pitch * math.sqrt(3.0) / 2.0
+        LY = rows * dy
+        nm = side * rows
+        jj, kk = np.meshgrid(np.arange(side), np.arange(rows), indexing="xy")
+        mx = (jj.ravel() + 0.5 * (kk.ravel() % 2)) * pitch
+        my = kk.ravel() * dy + 0.25 * dy
+    else:
+        rows = side
+        LY = L
+        nm = side * side
+        jj, kk = np.meshgrid(np.arange(side), np.arange(side), indexing="xy")
+        mx = (jj.ravel() + 0.5) * pitch
+        my = (kk.ravel() + 0.5) * pitch
+    xs = [list(mx)]
+    ys = [list(my)]
     zs = [[z_level + R_MEMB] * nm]
     rs = [[R_MEMB] * nm]
     st = [[MEMB] * nm]
@@ -352,15 +368,16 @@ def mixed_state_tissue(seed: int = 7) -> Tissue:
                 k += 1
     base = nm + nder
     for o in others:
-        xs.append([o[1] % L]); ys.append([o[2] % L]); zs.append([o[3]]); rs.append([o[4]])
+        xs.append([o[1] % L]); ys.append([o[2] % LY]); zs.append([o[3]]); rs.append([o[4]])
         st.append([o[0]]); ag.append([o[5]]); rd.append([o[6]])
         pr.append([-1 if o[7] is None else base + o[7]]); sp.append([o[8]])
     cat = lambda a, dt: np.array([v for part in a for v in part], dtype=dt)
-    t = Tissue(nmx=side, nmy=side, lx=L, ly=L, lz=32.0,
+    t = Tissue(nmx=side, nmy=rows, lx=L, ly=LY, lz=32.0,
                x=cat(xs, np.float64), y=cat(ys, np.float64), z=cat(zs, np.float64),
                radius=cat(rs, np.float64), state=cat(st, np.uint8), agek=cat(ag, np.float64),
                spr_nat_len=cat(sp, np.float64), pair=cat(pr, np.int32),
-               rest_div_times=cat(rd, np.int32), nmemb=nm, nder=nder, name="mixed")
+               rest_div_times=cat(rd, np.int32), nmemb=nm, nder=nder,
+               name="mixed" if lattice == SQUARE else "mixed_tri", lattice=lattice)
     t.validate()
     return t
 
@@ -387,6 +404,37 @@ def renewal_tissue(seed: int = 7) -> Tissue:
     t.ageb = ageb
     t.name = "renewal"
     t.validate()
+    return t
+
+
+def read_reference_file(path: str, nmx: int, lx: float, ly: float, lz: float,
+                        lattice: int = TRIANGULAR, name: str = "") -> Tissue:
+    """Loads an epi5_MT initial-state file (the format of its cman_init
+    loader, cellmanager.cpp:198-330: id, state, radius, ageb, agek, ca2p, x,
+    y, z, ca2p_avg, rest_div_times, ex_fat, in_fat, touch, spr_nat_len,
+    pair id, stem id; reading stops at the first BLANK cell). nmx is the
+    membrane's row length (define.h NMX); the membrane rows are
+    nmemb / nmx."""
+    rows = []
+    with open(path) as f:
+        for line in f:
+            v = line.split()
+            if not v:
+                continue
+            if int(v[1]) == BLANK:
+                break
+            rows.append(v)
+    n = len(rows)
+    st = np.array([int(r[1]) for r in rows], np.uint8)
+    col = lambda k: np.array([float(r[k]) for r in rows], np.float64)
+    nmemb = int((st == MEMB).sum())
+    nder = int((st == DER).sum())
+    pair = np.array([int(r[15]) for r in rows], np.int32)
+    pair[pair < 0] = -1
+    t = Tissue(nmx=nmx, nmy=nmemb // nmx, lx=lx, ly=ly, lz=lz, x=col(6), y=col(7), z=col(8),
+               radius=col(2), state=st, agek=col(4), spr_nat_len=col(14), pair=pair,
+               rest_div_times=np.array([int(r[10]) for r in rows], np.int32), nmemb=nmemb,
+               nder=nder, name=name or path, ageb=col(3), lattice=lattice)
     return t
 
 

@@ -54,7 +54,7 @@ SOURCES = [
 # Random_gen.cpp is replaced by the harness's fixed-seed genrand_real (the
 # reference seeds from std::random_device; see oracle/ref_harness.cpp).
 
-# name -> (NMX, NMY, LX, LY, LZ, MAX_CELL_NUM[, triangular])
+# name -> (NMX, NMY or rows, LX, LY, LZ, MAX_CELL_NUM[, triangular[, define.h NMY]])
 GEOMETRIES = {
     "sq16_L16": (16, 16, 16.0, 16.0, 32.0, 20000),
     "sq24_L24": (24, 24, 24.0, 24.0, 32.0, 40000),
@@ -69,6 +69,12 @@ GEOMETRIES = {
     # number of membrane particles (cellmanager.cpp:70-111)
     "tri16x18": (16, 18, 16.0, 18 * math.sqrt(3.0) / 2.0, 32.0, 20000, True),
     "tri32x36": (32, 36, 32.0, 36 * math.sqrt(3.0) / 2.0, 32.0, 60000, True),
+    # the all-laws tissue on the triangular lattice at the natural 0.5 spacing
+    "tri32x36_L16": (32, 36, 16.0, 36 * 0.5 * math.sqrt(3.0) / 2.0, 32.0, 20000, True),
+    # the reference's own default geometry (define.h as shipped: TRI_MEMB,
+    # NMX = NMY = 100, 50 x 50 x 100 box), for its shipped input files; the
+    # triangular wiring has 114 rows there (NMY / (sqrt(3)/2), even)
+    "default": (100, 114, 50.0, 50.0, 100.0, 100 * 100 + 50000 * 10, True, 100),
 }
 
 
@@ -106,6 +112,9 @@ def _fmt(v: float) -> str:
 def write_overlay(name: str) -> Path:
     nmx, nmy, lx, ly, lz, maxc = GEOMETRIES[name][:6]
     tri = is_tri(name)
+    # NMY as written into define.h (a triangular entry may differ from its rows)
+    if len(GEOMETRIES[name]) > 7:
+        nmy = GEOMETRIES[name][7]
     text = (REF_DIR / "define.h").read_text(encoding="latin-1")
     subs = [] if tri else [
         (r"#define\s+TRI_MEMB\s+1", "/* TRI_MEMB undefined: square membrane */")]

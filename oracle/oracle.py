@@ -29,6 +29,8 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "liboracle.so"
 REF_OUT = HERE / "_ref"
+# the reference checkout (present where the oracle is built, not on GPU hosts)
+REF_DIR = Path(os.environ.get("EPI_REFERENCE_DIR", "/root/reference"))
 
 _lib = None
 

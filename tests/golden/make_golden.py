@@ -38,6 +38,8 @@ CASES = {
     "renewal": (T.renewal_tissue, 200, (0, 1, 20, 100, 200), "dyn", {"EPI_HARNESS_RNG": "zero"}),
     # triangular membrane: the reference's default TRI_MEMB build
     "tri": (lambda: T.tri_layered_tissue(16, 18, 2, 0), 300, (0, 50, 300), "run", {}),
+    "mixed_tri": (lambda: T.mixed_state_tissue(lattice=T.TRIANGULAR), 300, (0, 50, 300), "run",
+                  {}),
 }
 
 

@@ -75,9 +75,10 @@ def test_fp64_c1_1000_steps_vs_reference_frames(built):
             assert lists_equal(off, idx, ooff, oidx)
 
 
-def test_fp64_mixed_states_all_laws_vs_reference_frames(built):
-    frames = load("mixed")
-    t = T.mixed_state_tissue()
+@pytest.mark.parametrize("name,lattice", [("mixed", T.SQUARE), ("mixed_tri", T.TRIANGULAR)])
+def test_fp64_mixed_states_all_laws_vs_reference_frames(built, name, lattice):
+    frames = load(name)
+    t = T.mixed_state_tissue(lattice=lattice)
     fm = (t.state == T.FIX) | (t.state == T.MUSUME)
     with capi.Context(precision=FP64, max_conn=96, max_cand=192) as ctx:
         ctx.upload([t])
@@ -89,9 +90,11 @@ def test_fp64_mixed_states_all_laws_vs_reference_frames(built):
             err = rel_pos_err(pos, (f["x"], f["y"], f["z"]), t.lx, t.ly)
             assert err <= TOL_FP64, (f["step"], err)
             off, idx = ctx.connections()
+            assert lists_equal(off, idx, f["conn_off"], f["conn_idx"])
             (ooff, oidx), oder = oracle_lists_at(t, pos)
             assert lists_equal(off, idx, ooff, oidx)
             assert np.array_equal(ctx.dermis()[fm], oder[fm])
+            assert np.array_equal(ctx.dermis()[fm], f["dermis"][fm])
 
 
 def test_mixed_precision_c1_1000_steps_within_1e5(built):

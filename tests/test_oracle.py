@@ -18,8 +18,10 @@ def tri_c1():
     return T.tri_layered_tissue(16, 18, 2, 0)
 
 
-@pytest.mark.parametrize("name,factory", [("c1", T.config1), ("mixed", T.mixed_state_tissue),
-                                          ("tri", tri_c1)])
+@pytest.mark.parametrize("name,factory", [
+    ("c1", T.config1), ("mixed", T.mixed_state_tissue), ("tri", tri_c1),
+    ("mixed_tri", lambda: T.mixed_state_tissue(lattice=T.TRIANGULAR)),
+])
 def test_oracle_reproduces_reference_golden_frames(built, name, factory):
     frames = load(name)
     t = factory()
@@ -101,3 +103,29 @@ def test_renewal_fixture_reproduces_with_the_compiled_reference(built):
             assert np.array_equal(f[k], g[k]), (g["step"], k)
     # the run divides, cornifies and removes cells: the batch size changes
     assert len(golden[0]["x"]) != len(golden[-1]["x"])
+
+
+SHIPPED_INPUT = O.REF_DIR / "epi5_MT" / "input_2layer_nfix16.dat"
+
+
+def test_oracle_matches_reference_default_build_on_its_shipped_input(built):
+    """The reference's own default build (define.h as shipped: TRI_MEMB,
+    NMX = 100, 50 x 50 x 100 box) on its own initial state
+    (epi5_MT/input_2layer_nfix16.dat: 11,400 membrane, 2,312 dermis and 16
+    stem cells): the oracle reproduces it bit for bit. Runs where the
+    reference checkout is present."""
+    if not SHIPPED_INPUT.exists():
+        pytest.skip("reference checkout not present")
+    t = T.read_reference_file(str(SHIPPED_INPUT), 100, 50.0, 50.0, 100.0)
+    assert (t.nmemb, t.nder, t.nmy) == (11400, 2312, 114)
+    if not _ref_available(t):
+        pytest.skip("compiled reference default build not present")
+    f = O.run_reference(t, 20, 20)[-1]
+    ora = O.OracleTissue(t)
+    assert ora.step(20) == 0, ora.error()
+    x, y, z = ora.positions()
+    assert np.array_equal(x, f["x"]) and np.array_equal(y, f["y"]) and np.array_equal(z, f["z"])
+    off, idx = ora.connections()
+    assert lists_equal(off, idx, f["conn_off"], f["conn_idx"])
+    fix = t.state == T.FIX
+    assert np.array_equal(ora.dermis()[fix], f["dermis"][fix])
