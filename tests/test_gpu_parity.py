@@ -398,3 +398,25 @@ def test_square_and_triangular_tissues_in_one_batch(built):
         for k in range(3):
             assert np.array_equal(pos_b[k][o:o + t.n], pos_1[k])
         o += t.n
+
+
+def test_mixed_precision_error_curve_c2_vs_fp64_oracle(built):
+    """The 64x64-membrane, 32,768-cell tissue: the mixed path (FP32 forces,
+    FP64 sums and positions) against the FP64 CPU oracle at every one of
+    1000 steps, max over particles of |dr|_min-image / L_x. Bar 1e-5 at every
+    step. The curve is printed (pytest -s) for the record."""
+    t = T.config2()
+    ora = O.OracleTissue(t)
+    curve = []
+    with capi.Context(precision=MIXED) as ctx:
+        ctx.upload([t])
+        for s in range(1, 1001):
+            ctx.step(1)
+            assert ora.step(1) == 0
+            e = rel_pos_err(ctx.positions(), ora.positions(), t.lx, t.ly)
+            curve.append(e)
+            assert e <= TOL_MIXED, (s, e)
+    picks = [1, 2, 5, 10, 20, 50, 100, 200, 500, 1000]
+    print("mixed-vs-FP64-oracle error curve (step: max |dr|/L_x): " +
+          ", ".join(f"{s}: {curve[s - 1]:.3e}" for s in picks))
+    print(f"max over 1000 steps: {max(curve):.3e}")
