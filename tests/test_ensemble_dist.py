@@ -55,3 +55,45 @@ def test_two_rank_shards_partition_the_batch(world):
     loads = [sum(sizes[i] for i in shard) for shard in g0]
     assert tmax0 == tmax1 == max(loads)
     assert imbalance(sizes, shard_tissues(sizes, world)) < 1.01
+
+
+def _failing_rank_main(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    import torch
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=5))
+    if rank == 1:
+        # the failing rank: leaves between steps, before the timing reduction
+        out[rank] = "left"
+        os._exit(0)
+    t = torch.tensor([1.0], dtype=torch.float64)
+    try:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        out[rank] = "completed"
+    except Exception as e:  # the bounded wait ends with an error, not a hang
+        out[rank] = f"error: {type(e).__name__}"
+
+
+def test_rank_that_leaves_is_detected_by_the_bounded_wait():
+    """A rank that exits between steps: the surviving rank's next collective
+    (the max-over-ranks timing reduction bench.py performs) ends with an
+    error within the process group's timeout instead of waiting forever."""
+    port = 29700 + (os.getpid() % 200)
+    with mp.Manager() as m:
+        out = m.dict()
+        ctx = mp.get_context("spawn")
+        procs = [ctx.Process(target=_failing_rank_main, args=(r, 2, port, out)) for r in range(2)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(timeout=60)
+        alive = [p.is_alive() for p in procs]
+        for p in procs:
+            if p.is_alive():
+                p.kill()
+        res = dict(out)
+    assert not any(alive), "a rank hung"
+    assert res.get(1) == "left"
+    assert str(res.get(0, "")).startswith("error"), res
