@@ -407,6 +407,22 @@ def renewal_tissue(seed: int = 7) -> Tissue:
     return t
 
 
+def field_tissue(seed: int = 7, lattice: int = SQUARE) -> Tissue:
+    """mixed_state_tissue with cell ages inside the window where the
+    external-stimulus source is on (ext_stim.cpp:8-16: an ALIVE or DEAD cell
+    with THRESH_DEAD - 0.5 < agek <= THRESH_DEAD + 2): every other DEAD cell
+    at 22.5 and two ALIVE cells at 21.8, so the diffusion has sources."""
+    t = mixed_state_tissue(seed, lattice)
+    cells = np.arange(t.nmemb + t.nder, t.n)
+    dead = cells[t.state[cells] == DEAD]
+    t.agek[dead[::2]] = 22.5
+    alive = cells[(t.state[cells] == ALIVE) & (t.pair[cells] < 0)]
+    t.agek[alive[:2]] = 21.8
+    t.name = "field"
+    t.validate()
+    return t
+
+
 def read_reference_file(path: str, nmx: int, lx: float, ly: float, lz: float,
                         lattice: int = TRIANGULAR, name: str = "") -> Tissue:
     """Loads an epi5_MT initial-state file (the format of its cman_init

@@ -50,6 +50,7 @@ OUT = HERE / "_ref"
 SOURCES = [
     "cellmanager.cpp", "cell.cpp", "cell_connection.cpp", "cell_interaction.cpp",
     "cell_init.cpp", "cell_state_renew.cpp", "utils.cpp", "vec3.cpp", "DualValue.cpp",
+    "map.cpp", "ext_stim.cpp",
 ]
 # Random_gen.cpp is replaced by the harness's fixed-seed genrand_real (the
 # reference seeds from std::random_device; see oracle/ref_harness.cpp).
@@ -75,6 +76,16 @@ GEOMETRIES = {
     # NMX = NMY = 100, 50 x 50 x 100 box), for its shipped input files; the
     # triangular wiring has 114 rows there (NMY / (sqrt(3)/2), even)
     "default": (100, 114, 50.0, 50.0, 100.0, 100 * 100 + 50000 * 10, True, 100),
+}
+
+
+# Field grid (define.h NX, NY, NZ) per geometry, for the harness's field
+# mode; the mechanics never read it. Geometries not listed keep the shipped
+# 100 x 100 x 200. These give the reference's default resolution, 0.5.
+GRIDS = {
+    "sq16_L16": (32, 32, 64),
+    "sq32_L16": (32, 32, 64),
+    "tri16x18": (32, 32, 64),
 }
 
 
@@ -126,6 +137,11 @@ def write_overlay(name: str) -> Path:
         (r"(cdefd LY\s*=\s*)[^;]+", rf"\g<1>{_fmt(ly)}"),
         (r"(cdefd LZ\s*=\s*)[^;]+", rf"\g<1>{_fmt(lz)}"),
     ]
+    if name in GRIDS:
+        gx, gy, gz = GRIDS[name]
+        subs += [(r"(cdefs NX\s*=\s*)\d+", rf"\g<1>{gx}"),
+                 (r"(cdefs NY\s*=\s*)\d+", rf"\g<1>{gy}"),
+                 (r"(cdefs NZ\s*=\s*)\d+", rf"\g<1>{gz}")]
     for pat, rep in subs:
         text, k = re.subn(pat, rep, text, count=1)
         if k != 1:

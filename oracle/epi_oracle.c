@@ -732,3 +732,199 @@ int ora_error_info(const ora_tissue* t, int32_t* a, int32_t* b, double* value) {
   if (value) *value = t->err_v;
   return t->err;
 }
+
+/* ---------------------------------------------------------------------------
+ * Cell maps and external-stimulus diffusion: the rest of the reference's
+ * per-step loop before its chemistry (epi5_MT/proc.cpp:152-157). Grids are
+ * (nx+1) x (ny+1) x (nz+1), z fastest, like FArr3D (define.h:243).
+ * ------------------------------------------------------------------------- */
+struct ora_field {
+  int32_t nx, ny, nz;
+  double dx, dy, dz, inv_dx, inv_dy, inv_dz;
+  int32_t* cmap1;  /* cell index, -1 for none (FArr3D<const Cell*>) */
+  uint8_t* cmap2;  /* FArr3D<cmask_ty> */
+  double* ext[2];  /* SwapData<FArr3D<double>>: ext[cur] is first() */
+  int cur;
+};
+
+#define FIELD_RAD 1.4         /* Rad, map.cpp:26 */
+#define FIELD_FAC_MAP 2.0     /* FAC_MAP, define.h:184 */
+#define FIELD_R_MAX 1.4       /* R_max, define.h:116 */
+#define FIELD_DT_CA 0.01      /* DT_Ca, define.h:89 */
+#define FIELD_DB 0.0009       /* DB, ext_stim.cpp:20 */
+#define FIELD_KB 0.025        /* kb, ext_stim.cpp:10 */
+#define FIELD_DUR_ALIVE 0.5   /* ext_stim.cpp:11 */
+#define FIELD_DUR_DEAD 2.0    /* ext_stim.cpp:12 */
+#define FIELD_THRESH_DEAD 22.0 /* define.h:156 */
+
+static inline size_t fidx(const ora_field* f, int32_t a, int32_t b, int32_t c) {
+  return ((size_t)a * (size_t)(f->ny + 1) + (size_t)b) * (size_t)(f->nz + 1) + (size_t)c;
+}
+
+ora_field* ora_field_new(const ora_tissue* t, int32_t nx, int32_t ny, int32_t nz) {
+  if (!t || nx < 3 || ny < 3 || nz < 3) return NULL;
+  ora_field* f = calloc(1, sizeof(ora_field));
+  if (!f) return NULL;
+  f->nx = nx; f->ny = ny; f->nz = nz;
+  /* cdefd dx = LX / NX; inv_dx = NX / LX (define.h:111-113) */
+  f->dx = t->lx / (double)nx; f->inv_dx = (double)nx / t->lx;
+  f->dy = t->ly / (double)ny; f->inv_dy = (double)ny / t->ly;
+  f->dz = t->lz / (double)nz; f->inv_dz = (double)nz / t->lz;
+  const size_t nv = (size_t)(nx + 1) * (size_t)(ny + 1) * (size_t)(nz + 1);
+  f->cmap1 = malloc(sizeof(int32_t) * nv);
+  f->cmap2 = calloc(nv, 1);
+  f->ext[0] = calloc(nv, sizeof(double));
+  f->ext[1] = calloc(nv, sizeof(double));
+  if (!f->cmap1 || !f->cmap2 || !f->ext[0] || !f->ext[1]) {
+    ora_field_free(f);
+    return NULL;
+  }
+  for (size_t v = 0; v < nv; ++v) f->cmap1[v] = -1;
+  return f;
+}
+
+void ora_field_free(ora_field* f) {
+  if (!f) return;
+  free(f->cmap1); free(f->cmap2); free(f->ext[0]); free(f->ext[1]);
+  free(f);
+}
+
+static inline int fafm(uint8_t s) { return s == S_ALIVE || s == S_FIX || s == S_MUSUME; }
+
+/* setup_map_lat, map.cpp:24-167 (cells visited in index order, so where
+ * spheres overlap the last, highest-index cell is the one cmap1 keeps) */
+static void field_map(const ora_tissue* t, ora_field* f) {
+  const int32_t NX = f->nx, NY = f->ny, NZ = f->nz;
+  const size_t nv = (size_t)(NX + 1) * (size_t)(NY + 1) * (size_t)(NZ + 1);
+  for (size_t v = 0; v < nv; ++v) { f->cmap1[v] = -1; f->cmap2[v] = 0; }
+  const int irx = (int)(FIELD_RAD * (double)NX / t->lx);
+  const int iry = (int)(FIELD_RAD * (double)NY / t->ly);
+  const int irz = (int)(FIELD_RAD * (double)NZ / t->lz);
+  for (int32_t c = 0; c < t->n; ++c) {
+    /* set_lattice, map.cpp:18-22 */
+    const int lat0 = (int)(((size_t)((int)(t->x[c] * f->inv_dx)) + (size_t)NX) % (size_t)NX);
+    const int lat1 = (int)(((size_t)((int)(t->y[c] * f->inv_dy)) + (size_t)NY) % (size_t)NY);
+    const int lat2 = (int)(((size_t)((int)(t->z[c] * f->inv_dz)) + (size_t)NZ) % (size_t)NZ);
+    const int afm = fafm(t->state[c]);
+    const int rx = afm ? 2 * irx : irx, ry = afm ? 2 * iry : iry, rz = afm ? 2 * irz : irz;
+    const double normal_radSq = t->radius[c] * t->radius[c];
+    const double crad = FIELD_FAC_MAP * t->radius[c];
+    const double cradSq = crad * crad;
+    const int ymin = lat1 - ry, ymax = lat1 + ry;
+    const int z_b = lat2 - rz, z_u = lat2 + rz;
+    const int zmin = z_b >= 1 ? z_b : 1;
+    const int zmax = z_u < NZ ? z_u : NZ - 1;
+    for (int k = lat0 - rx; k <= lat0 + rx; ++k) {
+      const double mx = k * f->dx;
+      const int ipx = (k + NX) % NX;
+      const double diffx = pdx(t, mx, t->x[c]);
+      const double diffxSq = diffx * diffx;
+      for (int l = ymin; l <= ymax; ++l) {
+        const double my = l * f->dy;
+        const int ipy = (l + NY) % NY;
+        const double diffy = pdy(t, my, t->y[c]);
+        const double tmps = diffxSq + diffy * diffy;
+        for (int m = zmin; m <= zmax; ++m) {
+          const double mz = m * f->dz;
+          const double diffz = mz - t->z[c];
+          const double distSq = tmps + diffz * diffz;
+          const size_t v = fidx(f, ipx, ipy, m);
+          if (afm) {
+            if (distSq < cradSq) {
+              f->cmap2[v] = 1;
+              if (distSq < normal_radSq) f->cmap1[v] = c;
+            }
+          } else if (distSq < normal_radSq) {
+            f->cmap1[v] = c;
+          }
+        }
+      }
+    }
+  }
+  for (int32_t l = 0; l < NZ; ++l) { /* periodic copies, map.cpp:156-166 */
+    for (int32_t j = 0; j <= NX; ++j) {
+      f->cmap2[fidx(f, j, NY, l)] = f->cmap2[fidx(f, j, 0, l)];
+      f->cmap1[fidx(f, j, NY, l)] = f->cmap1[fidx(f, j, 0, l)];
+    }
+    for (int32_t k = 0; k <= NY; ++k) {
+      f->cmap2[fidx(f, NX, k, l)] = f->cmap2[fidx(f, 0, k, l)];
+      f->cmap1[fidx(f, NX, k, l)] = f->cmap1[fidx(f, 0, k, l)];
+    }
+  }
+}
+
+/* fB, ext_stim.cpp:8-16 */
+static inline double field_fB(double age, double B, int cornif) {
+  return (cornif && age > FIELD_THRESH_DEAD - FIELD_DUR_ALIVE &&
+                  age <= FIELD_THRESH_DEAD + FIELD_DUR_DEAD
+              ? 1
+              : 0) -
+         FIELD_KB * B;
+}
+
+/* calc_ext_stim, ext_stim.cpp:18-69 */
+static int field_ext_stim(const ora_tissue* t, ora_field* f, double zzmax) {
+  const int32_t NX = f->nx, NY = f->ny, NZ = f->nz;
+  const int iz_bound = (int)((zzmax + FIELD_FAC_MAP * FIELD_R_MAX) * f->inv_dz);
+  if (iz_bound > NZ) return ORA_ERR_INVALID_ARG; /* the reference would read past the grid */
+  const double* carr = f->ext[f->cur];
+  double* narr = f->ext[f->cur ^ 1];
+  for (int32_t j = 0; j < NX; ++j) {
+    const int32_t px = j == 0 ? NX - 1 : j - 1, nxi = j + 1 == NX ? 0 : j + 1;
+    for (int32_t k = 0; k < NY; ++k) {
+      const int32_t py = k == 0 ? NY - 1 : k - 1, nyi = k + 1 == NY ? 0 : k + 1;
+      for (int32_t l = 0; l < iz_bound; ++l) {
+        const int32_t pz = l == 0 ? 1 : l - 1, nzi = l + 1 == NZ ? NZ - 1 : l + 1;
+        double dum_age = 0;
+        int cornif = 0;
+        const int32_t cm = f->cmap1[fidx(f, j, k, l)];
+        if (cm >= 0 && (t->state[cm] == S_DEAD || t->state[cm] == S_ALIVE)) {
+          dum_age = t->agek[cm];
+          cornif = 1;
+        }
+        const double cext = carr[fidx(f, j, k, l)];
+        narr[fidx(f, j, k, l)] =
+            cext + FIELD_DT_CA *
+                       (FIELD_DB *
+                            (f->cmap2[fidx(f, px, k, l)] * (carr[fidx(f, px, k, l)] - cext) +
+                             f->cmap2[fidx(f, j, py, l)] * (carr[fidx(f, j, py, l)] - cext) +
+                             f->cmap2[fidx(f, j, k, pz)] * (carr[fidx(f, j, k, pz)] - cext) +
+                             f->cmap2[fidx(f, j, k, nzi)] * (carr[fidx(f, j, k, nzi)] - cext) +
+                             f->cmap2[fidx(f, j, nyi, l)] * (carr[fidx(f, j, nyi, l)] - cext) +
+                             f->cmap2[fidx(f, nxi, k, l)] * (carr[fidx(f, nxi, k, l)] - cext)) *
+                            f->inv_dz * f->inv_dz +
+                        field_fB(dum_age, cext, cornif));
+      }
+    }
+  }
+  for (int32_t l = 0; l < iz_bound; ++l) { /* periodic copies, ext_stim.cpp:63-66 */
+    for (int32_t j = 0; j < NX; ++j) narr[fidx(f, j, NY, l)] = narr[fidx(f, j, 0, l)];
+    for (int32_t k = 0; k <= NY; ++k) narr[fidx(f, NX, k, l)] = narr[fidx(f, 0, k, l)];
+  }
+  f->cur ^= 1; /* ext_stim.swap() */
+  return ORA_OK;
+}
+
+/* calc_zzmax, proc.cpp:34-43 */
+static double field_zzmax(const ora_tissue* t) {
+  double zmax = 0;
+  for (int32_t c = t->nmemb + t->nder; c < t->n; ++c) {
+    const uint8_t s = t->state[c];
+    if ((s == S_DEAD || s == S_ALIVE || s == S_MUSUME || s == S_FIX) && zmax < t->z[c]) zmax = t->z[c];
+  }
+  return zmax;
+}
+
+int ora_field_step(const ora_tissue* t, ora_field* f, double* zzmax_out) {
+  const double zzmax = field_zzmax(t);
+  if (zzmax_out) *zzmax_out = zzmax;
+  field_map(t, f);
+  return field_ext_stim(t, f, zzmax);
+}
+
+void ora_field_get(const ora_field* f, int32_t* cmap1, uint8_t* cmap2, double* ext) {
+  const size_t nv = (size_t)(f->nx + 1) * (size_t)(f->ny + 1) * (size_t)(f->nz + 1);
+  if (cmap1) memcpy(cmap1, f->cmap1, sizeof(int32_t) * nv);
+  if (cmap2) memcpy(cmap2, f->cmap2, nv);
+  if (ext) memcpy(ext, f->ext[f->cur], sizeof(double) * nv);
+}

@@ -75,6 +75,17 @@ int64_t ora_get_connections_raw(const ora_tissue* t, int32_t* offsets, int32_t* 
 void ora_get_dermis(const ora_tissue* t, int32_t* dermis);
 int ora_error_info(const ora_tissue* t, int32_t* a, int32_t* b, double* value);
 
+/* Cell maps and external-stimulus diffusion on an (nx+1) x (ny+1) x (nz+1)
+ * grid (define.h NX, NY, NZ), z fastest: the reference's per-step
+ * calc_zzmax, setup_map_lat and calc_ext_stim (epi5_MT/proc.cpp:152-157,
+ * map.cpp:24-167, ext_stim.cpp:18-69) on the tissue's current positions. */
+typedef struct ora_field ora_field;
+ora_field* ora_field_new(const ora_tissue* t, int32_t nx, int32_t ny, int32_t nz);
+void ora_field_free(ora_field* f);
+int ora_field_step(const ora_tissue* t, ora_field* f, double* zzmax);
+/* cmap1: cell index or -1; ext: the current external stimulus */
+void ora_field_get(const ora_field* f, int32_t* cmap1, uint8_t* cmap2, double* ext);
+
 #ifdef __cplusplus
 }
 #endif

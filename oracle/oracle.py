@@ -87,6 +87,12 @@ def lib():
         L.ora_get_dermis.argtypes = [P, i32]
         L.ora_error_info.argtypes = [P, i32, i32, d]
         L.ora_error_info.restype = ctypes.c_int
+        L.ora_field_new.restype = P
+        L.ora_field_new.argtypes = [P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
+        L.ora_field_free.argtypes = [P]
+        L.ora_field_step.argtypes = [P, P, d]
+        L.ora_field_step.restype = ctypes.c_int
+        L.ora_field_get.argtypes = [P, i32, u8, d]
         L.ora_tangent_gradient.argtypes = (
             [ctypes.c_int32] * 5 + [ctypes.c_double] * 3 + [d] * 7 + [u8, i32, i32] +
             [ctypes.c_int32, d, d, d, ctypes.c_int32, ctypes.c_int32, d, d, d, d, d])
@@ -252,3 +258,75 @@ def tangent_gradient(t, nsteps: int, target=None, cells_only: bool = True, dual:
     if rc != 0:
         raise RuntimeError(f"oracle tangent failed with code {rc}")
     return loss.value, (grad if dual else None), tuple(out)
+
+
+class OracleField:
+    """Cell maps and external stimulus of an OracleTissue (ora_field_*)."""
+
+    def __init__(self, ora: "OracleTissue", nx: int, ny: int, nz: int):
+        self.ora = ora
+        self.dims = (nx + 1, ny + 1, nz + 1)
+        self._h = lib().ora_field_new(ora._h, nx, ny, nz)
+        if not self._h:
+            raise ValueError("oracle rejected the field")
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().ora_field_free(self._h)
+            self._h = None
+
+    def step(self):
+        z = ctypes.c_double()
+        rc = lib().ora_field_step(self.ora._h, self._h, ctypes.byref(z))
+        return rc, z.value
+
+    def get(self):
+        nv = int(np.prod(self.dims))
+        m1 = np.empty(nv, np.int32)
+        m2 = np.empty(nv, np.uint8)
+        ex = np.empty(nv, np.float64)
+        lib().ora_field_get(self._h, _p(m1, ctypes.c_int32), _p(m2, ctypes.c_uint8),
+                            _p(ex, ctypes.c_double))
+        return m1.reshape(self.dims), m2.reshape(self.dims), ex.reshape(self.dims)
+
+
+def read_field_frames(path: str):
+    """Field frames written by the reference harness's field mode."""
+    data = open(path, "rb").read()
+    off = 0
+    frames = []
+    while off < len(data):
+        tag, step, n, X, Y, Z = np.frombuffer(data, np.int32, 6, off)
+        assert tag == 0x46444C46, "bad field frame tag"
+        off += 24
+        zzmax = float(np.frombuffer(data, np.float64, 1, off)[0])
+        off += 8
+        pos = np.frombuffer(data, np.float64, 3 * n, off).reshape(3, n)
+        off += 24 * n
+        nv = int(X) * int(Y) * int(Z)
+        m1 = np.frombuffer(data, np.int32, nv, off).reshape(X, Y, Z)
+        off += 4 * nv
+        m2 = np.frombuffer(data, np.uint8, nv, off).reshape(X, Y, Z)
+        off += nv
+        ex = np.frombuffer(data, np.float64, nv, off).reshape(X, Y, Z)
+        off += 8 * nv
+        frames.append(dict(step=int(step), zzmax=zzmax, x=pos[0].copy(), y=pos[1].copy(),
+                           z=pos[2].copy(), cmap1=m1.copy(), cmap2=m2.copy(), ext=ex.copy()))
+    return frames
+
+
+def run_reference_field(t, nsteps: int, every: int):
+    """The compiled reference's field mode (mechanics step, zzmax, cell maps,
+    external-stimulus diffusion per step) on `t`."""
+    exe = reference_binary(t, "serial")
+    if exe is None:
+        raise FileNotFoundError("compiled reference harness not built for this geometry")
+    with tempfile.TemporaryDirectory() as d:
+        cells = os.path.join(d, "cells.dat")
+        out = os.path.join(d, "field.bin")
+        t.write_reference_file(cells)
+        r = subprocess.run([str(exe), "field", cells, str(nsteps), out, str(every)],
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"reference harness failed ({r.returncode}): {r.stderr[-2000:]}")
+        return read_field_frames(out)

@@ -20,6 +20,12 @@
 //       (epi5_MT/proc.cpp:22-32): cell_interaction -> pos_copy ->
 //       cell_state_renew -> cell_pos_periodic_fix -> connect_cell, so cells
 //       divide, cornify and are removed (frames then differ in size).
+//   ref_harness field <cells.dat> <nsteps> <out.bin> <dump_every>
+//       after each mechanics step, the rest of the reference's per-step loop
+//       up to the chemistry (epi5_MT/proc.cpp:152-157): zzmax, the cell maps
+//       (setup_map_lat, map.cpp:24-167) and the external-stimulus diffusion
+//       (calc_ext_stim, ext_stim.cpp:18-69); writes field frames (positions,
+//       zzmax, cell map as cell indices, mask map, external stimulus).
 //   ref_harness time <cells.dat> <warmup> <steps>
 //       times each step with steady_clock and prints one JSON line.
 //
@@ -37,6 +43,10 @@
 #include "cell_init.h"
 #include "cell_state_renew.h"
 #include "Random_gen.h"
+#include "ext_stim.h"
+#include "map.h"
+#include "swapdata.h"
+#include "utils.h"
 
 #include <tbb/tbb_shim_config.h>
 
@@ -152,10 +162,63 @@ void write_frame(std::FILE* f, CellManager& cman, int step) {
   std::fwrite(dermis.data(), 4, n, f);
 }
 
+// Highest z of a DEAD / ALIVE / MUSUME / FIX cell, 0 if none: the zzmax the
+// reference's loop computes before its maps (calc_zzmax, proc.cpp:34-43).
+double highest_cell_z(CellManager& cman) {
+  double zmax = 0;
+  cman.other_foreach([&](Cell* c) {
+    const CELL_STATE st = c->state;
+    if ((st == DEAD || st == ALIVE || st == MUSUME || st == FIX) && c->z() > zmax) zmax = c->z();
+  });
+  return zmax;
+}
+
+struct FieldState {
+  std::unique_ptr<FArr3D<const Cell*>> map1{new FArr3D<const Cell*>()};
+  std::unique_ptr<FArr3D<cmask_ty>> map2{new FArr3D<cmask_ty>()};
+  std::unique_ptr<SwapData<FArr3D<double>>> ext{new SwapData<FArr3D<double>>()};
+};
+
+void write_field_frame(std::FILE* f, CellManager& cman, int step, double zzmax, FieldState& F) {
+  const std::vector<Cell*> cells = cells_of(cman);
+  const int32_t n = static_cast<int32_t>(cells.size());
+  const int32_t dims[3] = {(int32_t)cont::NX + 1, (int32_t)cont::NY + 1, (int32_t)cont::NZ + 1};
+  const int32_t tag = 0x46444C46;  // "FLDF"
+  std::fwrite(&tag, 4, 1, f);
+  std::fwrite(&step, 4, 1, f);
+  std::fwrite(&n, 4, 1, f);
+  std::fwrite(dims, 4, 3, f);
+  std::fwrite(&zzmax, 8, 1, f);
+  std::vector<double> buf(n);
+  for (int32_t i = 0; i < n; ++i) buf[i] = cells[i]->x();
+  std::fwrite(buf.data(), 8, n, f);
+  for (int32_t i = 0; i < n; ++i) buf[i] = cells[i]->y();
+  std::fwrite(buf.data(), 8, n, f);
+  for (int32_t i = 0; i < n; ++i) buf[i] = cells[i]->z();
+  std::fwrite(buf.data(), 8, n, f);
+  const size_t nv = (size_t)dims[0] * dims[1] * dims[2];
+  std::vector<int32_t> m1(nv);
+  std::vector<uint8_t> m2(nv);
+  std::vector<double> ex(nv);
+  size_t v = 0;
+  for (int32_t a = 0; a < dims[0]; ++a)
+    for (int32_t b = 0; b < dims[1]; ++b)
+      for (int32_t c = 0; c < dims[2]; ++c, ++v) {
+        const Cell* p = (*F.map1)()[a][b][c];
+        m1[v] = p ? static_cast<int32_t>(p->get_index()) : -1;
+        m2[v] = static_cast<uint8_t>((*F.map2)()[a][b][c]);
+        ex[v] = F.ext->first()()[a][b][c];
+      }
+  std::fwrite(m1.data(), 4, nv, f);
+  std::fwrite(m2.data(), 1, nv, f);
+  std::fwrite(ex.data(), 8, nv, f);
+}
+
 int usage() {
   std::fprintf(stderr,
                "usage: ref_harness run <cells.dat> <nsteps> <out.bin> <dump_every>\n"
                "       ref_harness dyn <cells.dat> <nsteps> <out.bin> <dump_every>\n"
+               "       ref_harness field <cells.dat> <nsteps> <out.bin> <dump_every>\n"
                "       ref_harness time <cells.dat> <warmup> <steps>\n");
   return 2;
 }
@@ -187,6 +250,29 @@ int main(int argc, char** argv) {
       }
       check_capacity(*cman);
       if (s % every == 0 || s == nsteps) write_frame(f, *cman, s);
+    }
+    std::fclose(f);
+    return 0;
+  }
+  if (mode == "field" && argc == 6) {
+    const int nsteps = std::atoi(argv[3]);
+    const int every = std::max(1, std::atoi(argv[5]));
+    {
+      SilenceStdout quiet;
+      cman_init(*cman, argv[2]);
+    }
+    init_precalc_lat();
+    init_precalc_per();
+    FieldState F;
+    std::FILE* f = std::fopen(argv[4], "wb");
+    if (!f) return 3;
+    for (int s = 1; s <= nsteps; ++s) {
+      one_step(*cman);
+      check_capacity(*cman);
+      const double zzmax = highest_cell_z(*cman);
+      setup_map_lat(*cman, *F.map1, *F.map2);
+      calc_ext_stim(*F.ext, *F.map1, *F.map2, zzmax);
+      if (s % every == 0 || s == nsteps) write_field_frame(f, *cman, s, zzmax, F);
     }
     std::fclose(f);
     return 0;

@@ -129,3 +129,28 @@ def test_oracle_matches_reference_default_build_on_its_shipped_input(built):
     assert lists_equal(off, idx, f["conn_off"], f["conn_idx"])
     fix = t.state == T.FIX
     assert np.array_equal(ora.dermis()[fix], f["dermis"][fix])
+
+
+@pytest.mark.parametrize("factory", [T.field_tissue, T.config1])
+def test_oracle_field_matches_compiled_reference(built, factory):
+    """Cell maps and external stimulus (setup_map_lat, calc_ext_stim) after
+    each mechanics step, bit for bit against the compiled reference's own
+    map.cpp and ext_stim.cpp (32 x 32 x 64 grid)."""
+    t = factory()
+    if not _ref_available(t):
+        pytest.skip("compiled reference not built here (no reference checkout)")
+    frames = {f["step"]: f for f in O.run_reference_field(t, 20, 5)}
+    ora = O.OracleTissue(t)
+    fld = O.OracleField(ora, 32, 32, 64)
+    for s in range(1, 21):
+        assert ora.step(1) == 0
+        rc, zz = fld.step()
+        assert rc == 0
+        if s in frames:
+            f = frames[s]
+            m1, m2, ex = fld.get()
+            assert zz == f["zzmax"]
+            assert np.array_equal(m1, f["cmap1"]) and np.array_equal(m2, f["cmap2"])
+            assert np.array_equal(ex, f["ext"])
+    if factory is T.field_tissue:
+        assert f["ext"].max() > 0.1  # sources were on
