@@ -16,7 +16,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libepi_mech.so"
 
-SOURCES = ["epi_kernels.cu", "epi_adjoint.cu", "epi_capi.cu", "epi_noalloc.cu"]
+SOURCES = ["epi_kernels.cu", "epi_adjoint.cu", "epi_field.cu", "epi_capi.cu", "epi_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

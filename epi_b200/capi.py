@@ -40,8 +40,8 @@ EXPORTED = [
     "epi_upload", "epi_connect", "epi_interact_commit", "epi_step", "epi_step_graph",
     "epi_step_per_tissue", "epi_sync", "epi_num_particles", "epi_download_positions",
     "epi_upload_positions", "epi_get_connections", "epi_get_dermis", "epi_error_info",
-    "epi_stream", "epi_rebuild_count", "epi_time_kernels", "epi_autotune", "epi_adjoint",
-    "epi_connect_noalloc",
+    "epi_stream", "epi_rebuild_count", "epi_time_kernels", "epi_autotune", "epi_field_init",
+    "epi_field_step", "epi_field_get", "epi_field_set_ext", "epi_adjoint", "epi_connect_noalloc",
 ]
 
 
@@ -130,6 +130,10 @@ def lib():
         L.epi_time_kernels.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, _dp, _ip,
                                        ctypes.POINTER(ctypes.c_char_p), _ip]
         L.epi_autotune.argtypes = [vp, ctypes.c_int32, _dp, _ip, _dp]
+        L.epi_field_init.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
+        L.epi_field_step.argtypes = [vp, ctypes.c_int32]
+        L.epi_field_get.argtypes = [vp, ctypes.c_int32, _ip, _up, _dp, _dp]
+        L.epi_field_set_ext.argtypes = [vp, ctypes.c_int32, _dp]
         L.epi_adjoint.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(LossC),
                                   _dp, _dp]
         for f in EXPORTED:
@@ -350,3 +354,29 @@ class Context:
         _check(lib().epi_autotune(self._h, trial_steps, ctypes.byref(skin), ctypes.byref(variant),
                                   ctypes.byref(ms)), "epi_autotune")
         return float(skin.value), int(variant.value), float(ms.value)
+
+    # --- cell maps and external stimulus ------------------------------------
+    def field_init(self, nx: int, ny: int, nz: int):
+        _check(lib().epi_field_init(self._h, nx, ny, nz), "epi_field_init")
+        self.field_dims = (nx + 1, ny + 1, nz + 1)
+
+    def field_step(self, nsteps: int = 1):
+        _check(lib().epi_field_step(self._h, nsteps), "epi_field_step")
+
+    def field(self, tissue: int = 0):
+        """(cmap1, cmap2, ext, zzmax) of one tissue, grids shaped (nx+1, ny+1, nz+1)."""
+        nv = int(np.prod(self.field_dims))
+        m1 = np.empty(nv, np.int32)
+        m2 = np.empty(nv, np.uint8)
+        ex = np.empty(nv, np.float64)
+        zz = ctypes.c_double()
+        _check(lib().epi_field_get(self._h, tissue, _ptr(m1, ctypes.c_int32),
+                                   _ptr(m2, ctypes.c_uint8), _ptr(ex, ctypes.c_double),
+                                   ctypes.byref(zz)), "epi_field_get")
+        d = self.field_dims
+        return m1.reshape(d), m2.reshape(d), ex.reshape(d), float(zz.value)
+
+    def field_set_ext(self, tissue: int, ext):
+        e = np.ascontiguousarray(ext, np.float64).ravel()
+        _check(lib().epi_field_set_ext(self._h, tissue, _ptr(e, ctypes.c_double)),
+               "epi_field_set_ext")

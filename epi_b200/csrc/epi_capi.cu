@@ -105,6 +105,19 @@ struct epi_ctx {
   ScanScratch scan{};
   // graphs: one per buffer parity, each replaying two steps
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  // cell maps and external stimulus (epi_field_*)
+  double* agek = nullptr;  // per particle, for the stimulus source
+  bool field_on = false;
+  int32_t fnx = 0, fny = 0, fnz = 0;
+  int64_t nvox = 0;
+  std::vector<FieldDev> fd_h;
+  FieldDev* fd = nullptr;
+  int32_t* cmap1 = nullptr;
+  uint8_t* cmap2 = nullptr;
+  double* ext[2] = {nullptr, nullptr};
+  int ext_cur = 0;
+  double* zzmax = nullptr;
+  int32_t* izb = nullptr;
   // last error details
   DevStatus last{};
 };
@@ -138,8 +151,22 @@ void destroy_graphs(epi_ctx* c) {
   }
 }
 
+void free_field(epi_ctx* c) {
+  void* ptrs[] = {c->fd, c->cmap1, c->cmap2, c->ext[0], c->ext[1], c->zzmax, c->izb};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  c->fd = nullptr; c->cmap1 = nullptr; c->cmap2 = nullptr;
+  c->ext[0] = c->ext[1] = nullptr; c->zzmax = nullptr; c->izb = nullptr;
+  c->field_on = false;
+  c->nvox = 0;
+  c->fd_h.clear();
+}
+
 void free_buffers(epi_ctx* c) {
   destroy_graphs(c);
+  free_field(c);
+  if (c->agek) cudaFree(c->agek);
+  c->agek = nullptr;
   void* ptrs[] = {c->tissues, c->pos[0], c->pos[1], c->posf[0], c->posf[1], c->attr, c->pair, c->spr, c->dermis,
                   c->cand, c->ncand, c->bpos, c->nbr, c->nn, c->fmemb, c->bin,
                   c->rank, c->counts, c->starts, c->skey, c->spos, c->gate, c->rl, c->prep,
@@ -602,7 +629,31 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
   const bool reuse = c->loaded && c->ntissues == ntissues && c->n == n && c->nbins == nbins;
   const int32_t old_nprep = c->nprep;
   destroy_graphs(c);
+  // The field grids depend on the tissue count and the grid size only: they
+  // survive an upload that keeps the tissue count (divisions, removals).
+  epi_ctx kept;
+  const bool keep_field = c->field_on && c->ntissues == ntissues;
+  if (keep_field && !reuse) {
+    kept.fd = c->fd; kept.cmap1 = c->cmap1; kept.cmap2 = c->cmap2;
+    kept.ext[0] = c->ext[0]; kept.ext[1] = c->ext[1]; kept.zzmax = c->zzmax; kept.izb = c->izb;
+    c->fd = nullptr; c->cmap1 = nullptr; c->cmap2 = nullptr;
+    c->ext[0] = c->ext[1] = nullptr; c->zzmax = nullptr; c->izb = nullptr;
+  } else if (!keep_field) {
+    free_field(c);
+  }
+  const int32_t fnx = c->fnx, fny = c->fny, fnz = c->fnz, fcur = c->ext_cur;
+  const int64_t fnvox = c->nvox;
+  const std::vector<FieldDev> ffd = c->fd_h;
   if (!reuse) free_buffers(c);
+  if (keep_field && !reuse) {
+    c->fd = kept.fd; c->cmap1 = kept.cmap1; c->cmap2 = kept.cmap2;
+    c->ext[0] = kept.ext[0]; c->ext[1] = kept.ext[1]; c->zzmax = kept.zzmax; c->izb = kept.izb;
+    kept.fd = nullptr; kept.cmap1 = nullptr; kept.cmap2 = nullptr;
+    kept.ext[0] = kept.ext[1] = nullptr; kept.zzmax = nullptr; kept.izb = nullptr;
+    c->field_on = true;
+    c->fnx = fnx; c->fny = fny; c->fnz = fnz; c->ext_cur = fcur; c->nvox = fnvox;
+    c->fd_h = ffd;
+  }
   c->loaded = false;
   c->ntissues = ntissues;
   c->n = n;
@@ -613,6 +664,7 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
   std::vector<uint32_t> attr(n);
   std::vector<int32_t> pair(n, -1);
   std::vector<double> spr(n, 0.0);
+  std::vector<double> agek(n, 0.0);
   std::vector<int32_t> prep_m, prep_f;
   int32_t pbase = 0, binbase = 0;
   bool simple = true, any_old = false;
@@ -672,6 +724,7 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
       pair[g] = q >= 0 ? pbase + q : -1;
       if (q >= 0) simple = false;
       spr[g] = v.spr_nat_len ? v.spr_nat_len[i] : 0.0;
+      agek[g] = v.agek ? v.agek[i] : 0.0;
       if (st == ST_MEMB) prep_m.push_back((int32_t)g);
       if (st == ST_FIX || st == ST_MUSUME) prep_f.push_back((int32_t)g);
     }
@@ -710,7 +763,8 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
       (rc = dev_alloc(&c->skey, n)) || (rc = dev_alloc(&c->spos, n)) ||
       (rc = dev_alloc(&c->gate, (size_t)ntissues + 1)) ||
       (rc = dev_alloc(&c->rl, 3 + 3 * (size_t)ntissues)) ||
-      (rc = dev_alloc(&c->prep, prep.size())) || (rc = dev_alloc(&c->stage, 3 * (size_t)n)))) {
+      (rc = dev_alloc(&c->prep, prep.size())) || (rc = dev_alloc(&c->stage, 3 * (size_t)n)) ||
+      (rc = dev_alloc(&c->agek, n)))) {
     free_buffers(c);
     return rc;
   }
@@ -730,6 +784,15 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
   EPI_CUDA(cudaMemcpyAsync(c->attr, attr.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s));
   EPI_CUDA(cudaMemcpyAsync(c->pair, pair.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
   EPI_CUDA(cudaMemcpyAsync(c->spr, spr.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  EPI_CUDA(cudaMemcpyAsync(c->agek, agek.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  if (c->field_on) {
+    // boxes may have changed: refresh the grids' spacing
+    for (int32_t t = 0; t < ntissues; ++t)
+      field_params(c->fd_h[t], c->tissues_h[t].lx, c->tissues_h[t].ly, c->tissues_h[t].lz,
+                   c->fnx, c->fny, c->fnz);
+    EPI_CUDA(cudaMemcpyAsync(c->fd, c->fd_h.data(), sizeof(FieldDev) * ntissues,
+                             cudaMemcpyHostToDevice, s));
+  }
   if (!prep.empty())
     EPI_CUDA(cudaMemcpyAsync(c->prep, prep.data(), sizeof(int32_t) * prep.size(),
                              cudaMemcpyHostToDevice, s));
@@ -837,6 +900,119 @@ int epi_adjoint(epi_ctx* c, int32_t nsteps, int32_t K, const epi_loss* loss, dou
       for (int k = 0; k < 3; ++k) grad[3 * t + k] = h[4 * t + k];
   }
   return EPI_OK;
+  EPI_GUARD_END
+}
+
+int epi_field_init(epi_ctx* c, int32_t nx, int32_t ny, int32_t nz) {
+  if (!c || nx < 3 || ny < 3 || nz < 3) return EPI_ERR_INVALID_ARG;
+  if (!c->loaded) return EPI_ERR_STATE;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  free_field(c);
+  const int32_t nt = c->ntissues;
+  if (nt > 65535) return EPI_ERR_UNSUPPORTED;  // one grid row of blocks per tissue
+  const int64_t per = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
+  c->fd_h.assign(nt, FieldDev{});
+  for (int32_t t = 0; t < nt; ++t) {
+    FieldDev& F = c->fd_h[t];
+    F.base = per * t;
+    field_params(F, c->tissues_h[t].lx, c->tissues_h[t].ly, c->tissues_h[t].lz, nx, ny, nz);
+    // a stamp window must not wrap onto itself (it spans 2 x 2 ir + 1 points)
+    if (2 * F.irx >= nx || 2 * F.iry >= ny || 2 * F.irz >= nz) {
+      c->fd_h.clear();
+      return EPI_ERR_UNSUPPORTED;
+    }
+  }
+  c->nvox = per * nt;
+  if ((rc = dev_alloc(&c->fd, nt)) || (rc = dev_alloc(&c->cmap1, c->nvox)) ||
+      (rc = dev_alloc(&c->cmap2, c->nvox)) || (rc = dev_alloc(&c->ext[0], c->nvox)) ||
+      (rc = dev_alloc(&c->ext[1], c->nvox)) || (rc = dev_alloc(&c->zzmax, nt)) ||
+      (rc = dev_alloc(&c->izb, nt))) {
+    free_field(c);
+    return rc;
+  }
+  c->field_on = true;
+  c->fnx = nx; c->fny = ny; c->fnz = nz;
+  c->ext_cur = 0;
+  cudaStream_t s = c->stream;
+  EPI_CUDA(cudaMemcpyAsync(c->fd, c->fd_h.data(), sizeof(FieldDev) * nt, cudaMemcpyHostToDevice, s));
+  // ext_stim_init = 0 (define.h:180); Field zero-initialises (Field.h:16)
+  EPI_CUDA(cudaMemsetAsync(c->ext[0], 0, sizeof(double) * c->nvox, s));
+  EPI_CUDA(cudaMemsetAsync(c->ext[1], 0, sizeof(double) * c->nvox, s));
+  EPI_CUDA(cudaMemsetAsync(c->cmap1, 0, sizeof(int32_t) * c->nvox, s));
+  EPI_CUDA(cudaMemsetAsync(c->cmap2, 0, c->nvox, s));
+  EPI_CUDA(cudaMemsetAsync(c->zzmax, 0, sizeof(double) * nt, s));
+  EPI_CUDA(cudaMemsetAsync(c->izb, 0, sizeof(int32_t) * nt, s));
+  return check_status(c);
+  EPI_GUARD_END
+}
+
+int epi_field_step(epi_ctx* c, int32_t nsteps) {
+  if (!c || nsteps < 0) return EPI_ERR_INVALID_ARG;
+  if (!c->loaded || !c->field_on) return EPI_ERR_STATE;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  for (int32_t k = 0; k < nsteps; ++k) {
+    FieldState FS;
+    FS.fd = c->fd;
+    FS.cmap1 = c->cmap1;
+    FS.cmap2 = c->cmap2;
+    FS.cur = c->ext[c->ext_cur];
+    FS.nxt = c->ext[c->ext_cur ^ 1];
+    FS.zzmax = c->zzmax;
+    FS.izb = c->izb;
+    FS.nvox = c->nvox;
+    FS.agek = c->agek;
+    launch_field_step(make_state(c, c->cur), FS, c->lc, c->stream);
+    c->ext_cur ^= 1;  // ext_stim.swap()
+  }
+  return check_status(c);
+  EPI_GUARD_END
+}
+
+int epi_field_get(epi_ctx* c, int32_t tissue, int32_t* cmap1, uint8_t* cmap2, double* ext,
+                  double* zzmax) {
+  if (!c || tissue < 0) return EPI_ERR_INVALID_ARG;
+  if (!c->loaded || !c->field_on) return EPI_ERR_STATE;
+  if (tissue >= c->ntissues) return EPI_ERR_INVALID_ARG;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  const FieldDev& F = c->fd_h[tissue];
+  const size_t per = (size_t)(F.nx + 1) * (F.ny + 1) * (F.nz + 1);
+  cudaStream_t s = c->stream;
+  if (cmap1)
+    EPI_CUDA(cudaMemcpyAsync(cmap1, c->cmap1 + F.base, sizeof(int32_t) * per,
+                             cudaMemcpyDeviceToHost, s));
+  if (cmap2) EPI_CUDA(cudaMemcpyAsync(cmap2, c->cmap2 + F.base, per, cudaMemcpyDeviceToHost, s));
+  if (ext)
+    EPI_CUDA(cudaMemcpyAsync(ext, c->ext[c->ext_cur] + F.base, sizeof(double) * per,
+                             cudaMemcpyDeviceToHost, s));
+  if (zzmax)
+    EPI_CUDA(cudaMemcpyAsync(zzmax, c->zzmax + tissue, sizeof(double), cudaMemcpyDeviceToHost, s));
+  if ((rc = check_status(c))) return rc;
+  // stored as index + 1 (0: none)
+  if (cmap1)
+    for (size_t v = 0; v < per; ++v) cmap1[v] -= 1;
+  return EPI_OK;
+  EPI_GUARD_END
+}
+
+int epi_field_set_ext(epi_ctx* c, int32_t tissue, const double* ext) {
+  if (!c || tissue < 0 || !ext) return EPI_ERR_INVALID_ARG;
+  if (!c->loaded || !c->field_on) return EPI_ERR_STATE;
+  if (tissue >= c->ntissues) return EPI_ERR_INVALID_ARG;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  const FieldDev& F = c->fd_h[tissue];
+  const size_t per = (size_t)(F.nx + 1) * (F.ny + 1) * (F.nz + 1);
+  for (int b = 0; b < 2; ++b)  // both buffers, as read_binary into first() and second()
+    EPI_CUDA(cudaMemcpyAsync(c->ext[b] + F.base, ext, sizeof(double) * per,
+                             cudaMemcpyHostToDevice, c->stream));
+  return check_status(c);
   EPI_GUARD_END
 }
 

@@ -31,7 +31,7 @@ enum State : uint32_t {
 
 enum ErrCode : int32_t {
   E_OK = 0, E_BIN_RANGE = 5, E_BIN_OVERFLOW = 6, E_LIST_OVERFLOW = 7, E_COEF_RANGE = 8,
-  E_MEMB_COEF_RANGE = 9, E_NONFINITE = 10, E_TIMEOUT = 11
+  E_MEMB_COEF_RANGE = 9, E_NONFINITE = 10, E_TIMEOUT = 11, E_UNSUPPORTED = 13
 };
 
 constexpr double kAreaGrid = 2.0 + 1e-7;  // AREA_GRID, cell_connection.cpp:16-19

@@ -76,6 +76,30 @@ void launch_pack_positions(const DevState& S, const double* x, const double* y,
 // FP32 copies of the current positions (S.posf_cur from S.pos_cur).
 void launch_posf(const DevState& S, const LaunchCfg& lc, cudaStream_t s);
 
+// ---- cell maps and external-stimulus diffusion (FP64) ----
+struct FieldDev {   // one tissue's grid
+  int64_t base;     // first grid point of the tissue in the field arrays
+  int32_t nx, ny, nz, irx, iry, irz;
+  double dx, dy, dz, inv_dx, inv_dy, inv_dz;
+};
+struct FieldState {
+  const FieldDev* fd;  // per tissue
+  int32_t* cmap1;      // tissue-local cell index + 1 (0: none)
+  uint8_t* cmap2;      // the ALIVE / FIX / MUSUME mask
+  const double* cur;   // external stimulus, current
+  double* nxt;         // external stimulus, next
+  double* zzmax;       // per tissue
+  int32_t* izb;        // per tissue: grid planes below the diffusion's z bound
+  int64_t nvox;        // grid points over all tissues
+  const double* agek;  // per particle
+};
+// Grid spacing and stamp radii of a tissue's (nx+1) x (ny+1) x (nz+1) grid.
+void field_params(FieldDev& F, double lx, double ly, double lz, int32_t nx, int32_t ny,
+                  int32_t nz);
+// zzmax, cell maps, external-stimulus update into FS.nxt (the caller swaps).
+void launch_field_step(const DevState& S, const FieldState& FS, const LaunchCfg& lc,
+                       cudaStream_t s);
+
 // ---- reverse-mode adjoint (FP64), membrane + ALIVE / DEAD / AIR tissues ----
 struct AdjointBuffers {
   const double4* lam_in;  // dL/dX_{t+1}

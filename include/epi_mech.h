@@ -200,6 +200,28 @@ int epi_time_kernels(epi_ctx* ctx, int32_t nsteps, int32_t max_classes, double* 
 int epi_autotune(epi_ctx* ctx, int32_t trial_steps, double* skin, int32_t* variant,
                  double* ms_per_step);
 
+/* ---- cell maps and external-stimulus diffusion -----------------------------
+ * The rest of the reference's per-step loop before its chemistry
+ * (epi5_MT/proc.cpp:152-157): calc_zzmax, setup_map_lat (map.cpp:24-167) and
+ * calc_ext_stim (ext_stim.cpp:18-69), per tissue on an (nx+1) x (ny+1) x
+ * (nz+1) grid over its box (define.h NX, NY, NZ; z fastest, the layout of
+ * FArr3D). Results equal the reference's bit for bit on the same positions.
+ *
+ * epi_field_init allocates the grids of every tissue of the batch and zeroes
+ * the stimulus (ext_stim_init, define.h:180); the grids survive uploads that
+ * keep the tissue count. */
+int epi_field_init(epi_ctx* ctx, int32_t nx, int32_t ny, int32_t nz);
+/* nsteps of: zzmax, cell maps, one stimulus update, from the current positions. */
+int epi_field_step(epi_ctx* ctx, int32_t nsteps);
+/* Tissue `tissue`'s grids: cmap1 (tissue-local cell index, -1 none; the
+ * reference's cell pointers), cmap2 (the ALIVE / FIX / MUSUME mask), ext
+ * (the current stimulus) and the last zzmax; each output may be NULL. */
+int epi_field_get(epi_ctx* ctx, int32_t tissue, int32_t* cmap1, uint8_t* cmap2, double* ext,
+                  double* zzmax);
+/* Sets tissue `tissue`'s stimulus (both buffers, as the reference's
+ * read_binary of saved field data does, proc.cpp:106-109). */
+int epi_field_set_ext(epi_ctx* ctx, int32_t tissue, const double* ext);
+
 /* ---- gradients: reverse-mode adjoint of the step --------------------------
  * No counterpart in the reference, which has no gradients. The loss of
  * tissue t is L_t = mean over its loss set of |x_i(T) - x*_i|^2, x_i(T) the
