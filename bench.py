@@ -266,6 +266,41 @@ def adjoint_check(capi, device: int, steps: int, every: int = 20, h: float = 1e-
             "grad_order": ["s_spring", "s_eps", "s_bend"]}
 
 
+def field_check(capi, device: int, steps: int, with_cpu: bool):
+    """The field part of the reference's step (zzmax, cell maps, external-
+    stimulus update; epi_field_step) on the 64x64, 32,768-cell tissue with a
+    129 x 129 x 65 grid (the reference's 0.5 spacing), timed with CUDA events;
+    beside it the reference's own OpenMP build on the same tissue."""
+    import torch
+    t = T.config2()
+    grid = (128, 128, 64)
+    with capi.Context(precision=capi.EPI_PREC_MIXED, device=device) as c:
+        c.upload([t])
+        c.field_init(*grid)
+        c.field_step(3)
+        s = torch.cuda.ExternalStream(c.stream_handle())
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        c.field_step(steps)
+        e1.record(s)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+    out = {"workload": "64x64 membrane + 32,768 cells, grid 129 x 129 x 65",
+           "gpu_ms_per_step": ms, "steps": steps}
+    if with_cpu:
+        try:
+            from oracle import oracle as O
+            d = O.time_reference_field(t, 2, 5, threads=os.cpu_count())
+            out["cpu_reference_ms_per_step"] = d["median_s"] * 1e3
+            out["cpu_cores"] = d["threads"]
+            out["speedup_vs_cpu_reference"] = d["median_s"] * 1e3 / ms
+        except Exception as e:  # reference build missing on this host
+            out["cpu_reference"] = f"unavailable: {e}"
+    return out
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -297,6 +332,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="timed region only (profiling)")
     ap.add_argument("--adjoint-steps", type=int, default=200,
                     help="steps of the adjoint workload (0: skip)")
+    ap.add_argument("--field-steps", type=int, default=50,
+                    help="timed steps of the cell-map / stimulus part (0: skip)")
     ap.add_argument("--accuracy-steps", type=int, default=1000,
                     help="steps of the mixed-vs-FP64 position error check (0: skip)")
     args = ap.parse_args()
@@ -466,6 +503,9 @@ def main():
             extras["accuracy"] = accuracy_check(capi, local, args.accuracy_steps)
         if args.adjoint_steps > 0:
             extras["adjoint"] = adjoint_check(capi, local, args.adjoint_steps)
+        if args.field_steps > 0:
+            extras["field"] = field_check(capi, local, args.field_steps,
+                                          not args.no_cpu_baseline)
 
     if rank == 0:
         cfg = {"workload": desc, "tissues": len(tissues), "particles": n_all,

@@ -86,6 +86,7 @@ GRIDS = {
     "sq16_L16": (32, 32, 64),
     "sq32_L16": (32, 32, 64),
     "tri16x18": (32, 32, 64),
+    "sq64_L64": (128, 128, 64),
 }
 
 

@@ -330,3 +330,23 @@ def run_reference_field(t, nsteps: int, every: int):
         if r.returncode != 0:
             raise RuntimeError(f"reference harness failed ({r.returncode}): {r.stderr[-2000:]}")
         return read_field_frames(out)
+
+
+def time_reference_field(t, warmup: int, steps: int, threads: Optional[int] = None):
+    """Time the OpenMP build's field part of the step (zzmax, cell maps,
+    external-stimulus update) on `t`; returns its JSON summary."""
+    import json
+    exe = reference_binary(t, "omp")
+    if exe is None:
+        raise FileNotFoundError("compiled reference harness (omp) not built for this geometry")
+    env = dict(os.environ)
+    if threads:
+        env["OMP_NUM_THREADS"] = str(threads)
+    with tempfile.TemporaryDirectory() as d:
+        cells = os.path.join(d, "cells.dat")
+        t.write_reference_file(cells)
+        r = subprocess.run([str(exe), "time_field", cells, str(warmup), str(steps)],
+                           capture_output=True, text=True, env=env)
+        if r.returncode != 0:
+            raise RuntimeError(f"reference harness failed ({r.returncode}): {r.stderr[-2000:]}")
+        return json.loads(r.stdout.strip().splitlines()[-1])

@@ -28,6 +28,9 @@
 //       zzmax, cell map as cell indices, mask map, external stimulus).
 //   ref_harness time <cells.dat> <warmup> <steps>
 //       times each step with steady_clock and prints one JSON line.
+//   ref_harness time_field <cells.dat> <warmup> <steps>
+//       the same for the field part of the step only (zzmax, cell maps,
+//       external-stimulus update), each after a mechanics step.
 //
 // genrand_real (epi5_MT/Random_gen.cpp) seeds itself from std::random_device,
 // so no two runs of the reference agree once a division test draws from it.
@@ -275,6 +278,34 @@ int main(int argc, char** argv) {
       if (s % every == 0 || s == nsteps) write_field_frame(f, *cman, s, zzmax, F);
     }
     std::fclose(f);
+    return 0;
+  }
+  if (mode == "time_field" && argc == 5) {
+    const int warmup = std::atoi(argv[3]);
+    const int steps = std::atoi(argv[4]);
+    {
+      SilenceStdout quiet;
+      cman_init(*cman, argv[2]);
+    }
+    init_precalc_lat();
+    init_precalc_per();
+    FieldState F;
+    std::vector<double> t(steps);
+    for (int s = 0; s < warmup + steps; ++s) {
+      one_step(*cman);
+      auto a = std::chrono::steady_clock::now();
+      const double zzmax = highest_cell_z(*cman);
+      setup_map_lat(*cman, *F.map1, *F.map2);
+      calc_ext_stim(*F.ext, *F.map1, *F.map2, zzmax);
+      auto b = std::chrono::steady_clock::now();
+      if (s >= warmup) t[s - warmup] = std::chrono::duration<double>(b - a).count();
+    }
+    std::vector<double> sorted = t;
+    std::sort(sorted.begin(), sorted.end());
+    std::printf("{\"cells\": %zu, \"steps\": %d, \"threads\": %d, \"median_s\": %.9g, "
+                "\"grid\": [%zu, %zu, %zu]}\n",
+                cman->size(), steps, tbb::shim_threads(), steps > 0 ? sorted[steps / 2] : 0.0,
+                (size_t)cont::NX, (size_t)cont::NY, (size_t)cont::NZ);
     return 0;
   }
   if (mode == "time" && argc == 5) {
