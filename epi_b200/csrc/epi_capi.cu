@@ -72,6 +72,10 @@ struct epi_ctx {
   int32_t nbins = 0;
   int32_t nprep = 0, nprep_memb = 0;
   std::vector<TissueDev> tissues_h;
+  // what the candidate lists depend on besides positions, as last uploaded
+  // (radius and attribute word per particle), to re-gate only changed tissues
+  std::vector<double> h_radius;
+  std::vector<uint32_t> h_attr;
   std::vector<TissueHost> thost;
   // device buffers
   TissueDev* tissues = nullptr;
@@ -645,6 +649,7 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
   const int64_t fnvox = c->nvox;
   const std::vector<FieldDev> ffd = c->fd_h;
   if (!reuse) free_buffers(c);
+  c->lists_fresh = false;
   if (keep_field && !reuse) {
     c->fd = kept.fd; c->cmap1 = kept.cmap1; c->cmap2 = kept.cmap2;
     c->ext[0] = kept.ext[0]; c->ext[1] = kept.ext[1]; c->zzmax = kept.zzmax; c->izb = kept.izb;
@@ -658,6 +663,7 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
   c->ntissues = ntissues;
   c->n = n;
   c->nbins = (int32_t)nbins;
+  const std::vector<TissueDev> old_tissues = reuse ? c->tissues_h : std::vector<TissueDev>();
   c->tissues_h.assign(ntissues, TissueDev{});
   c->thost.assign(ntissues, TissueHost{});
   std::vector<double4> pos(n);
@@ -797,13 +803,42 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
     EPI_CUDA(cudaMemcpyAsync(c->prep, prep.data(), sizeof(int32_t) * prep.size(),
                              cudaMemcpyHostToDevice, s));
   EPI_CUDA(cudaMemsetAsync(c->counts, 0, sizeof(int32_t) * (size_t)std::max<int64_t>(nbins, 1), s));
-  EPI_CUDA(cudaMemsetAsync(c->nn, 0, sizeof(int32_t) * n, s));
-  EPI_CUDA(cudaMemsetAsync(c->ncand, 0, sizeof(int32_t) * n, s));
-  EPI_CUDA(cudaMemsetAsync(c->dermis, 0xff, sizeof(int32_t) * n, s));
+  // Candidate lists stay valid for a same-shape upload wherever the radii,
+  // states and box are unchanged and no particle moved skin/2 from the
+  // positions of its tissue's last candidate build: gate only the others.
+  std::vector<int32_t> gates;
+  if (reuse && c->h_radius.size() == (size_t)n && c->h_attr.size() == (size_t)n) {
+    gates.assign(1 + (size_t)ntissues, 0);
+    for (int32_t t = 0; t < ntissues; ++t) {
+      const TissueDev& A = old_tissues[t];
+      const TissueDev& B = c->tissues_h[t];
+      bool changed = A.n != B.n || A.lx != B.lx || A.ly != B.ly || A.lz != B.lz ||
+                     A.lattice != B.lattice || A.nmx != B.nmx || A.nmy != B.nmy ||
+                     std::memcmp(&A.P, &B.P, sizeof(Params)) != 0;
+      for (int32_t i = B.pbase; !changed && i < B.pbase + B.n; ++i)
+        changed = c->h_radius[i] != pos[i].w || c->h_attr[i] != attr[i];
+      gates[1 + t] = changed ? 1 : 0;
+      gates[0] |= gates[1 + t];
+    }
+  }
+  c->h_radius.resize(n);
+  c->h_attr.assign(attr.begin(), attr.end());
+  for (int64_t i = 0; i < n; ++i) c->h_radius[i] = pos[i].w;
+  if (gates.empty()) {
+    EPI_CUDA(cudaMemsetAsync(c->nn, 0, sizeof(int32_t) * n, s));
+    EPI_CUDA(cudaMemsetAsync(c->ncand, 0, sizeof(int32_t) * n, s));
+    EPI_CUDA(cudaMemsetAsync(c->dermis, 0xff, sizeof(int32_t) * n, s));
+  }
   EPI_CUDA(cudaMemsetAsync(c->status, 0, sizeof(DevStatus), s));
   c->cur = 0;
   c->loaded = true;
-  launch_set_gates(make_state(c, c->cur), ntissues, s);
+  if (gates.empty()) {
+    launch_set_gates(make_state(c, c->cur), ntissues, s);
+  } else {
+    EPI_CUDA(cudaMemcpyAsync(c->gate, gates.data(), sizeof(int32_t) * gates.size(),
+                             cudaMemcpyHostToDevice, s));
+    launch_gate_check(make_state(c, c->cur), c->lc, s);
+  }
   // all pending host copies read std::vector storage: finish before return
   return materialize(c);
   EPI_GUARD_END
@@ -1200,8 +1235,9 @@ int epi_upload_positions(epi_ctx* c, const double* x, const double* y, const dou
   EPI_CUDA(cudaMemcpyAsync(d + 2 * n, z, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
   const DevState S = make_state(c, c->cur);
   launch_pack_positions(S, d, d + n, d + 2 * n, (int32_t)n, c->stream);
-  // positions may have jumped anywhere: every tissue re-derives its candidates
-  launch_set_gates(S, c->ntissues, c->stream);
+  // a tissue re-derives its candidates once one of its particles is skin/2
+  // from its last candidate build (the test the step itself applies)
+  launch_gate_check(S, c->lc, c->stream);
   c->lists_fresh = false;
   launch_rebuild(S, whole(c), c->scan, c->lc, c->stream, nullptr);
   return check_status(c);

@@ -420,3 +420,48 @@ def test_mixed_precision_error_curve_c2_vs_fp64_oracle(built):
     print("mixed-vs-FP64-oracle error curve (step: max |dr|/L_x): " +
           ", ".join(f"{s}: {curve[s - 1]:.3e}" for s in picks))
     print(f"max over 1000 steps: {max(curve):.3e}")
+
+
+def test_reupload_and_position_upload_regate_only_what_changed(built):
+    """A same-shape re-upload (the drop-in's per-step connect) and a position
+    upload keep the candidate lists of tissues nothing moved in; results stay
+    those of a fresh context."""
+    ts = T.config4(n_tissues=12)
+    with capi.Context(precision=FP64) as ctx:
+        ctx.upload(ts)
+        ctx.step(20)
+        pos = ctx.positions()
+        r0 = ctx.rebuild_count()
+        ctx.set_positions(*pos)  # unchanged positions: nothing to rebuild
+        assert ctx.rebuild_count() == r0
+        off_a, idx_a = ctx.connections()
+        moved = [a.copy() for a in pos]
+        moved[2][ts[0].n + 5] += 0.3  # one particle of tissue 1 jumps
+        ctx.set_positions(*moved)
+        assert ctx.rebuild_count() == r0 + 1
+        off_b, idx_b = ctx.connections()
+        # re-upload of the same tissues with new positions and one changed radius
+        ts2 = [t.copy() for t in ts]
+        o = 0
+        for t in ts2:
+            t.x[:], t.y[:], t.z[:] = moved[0][o:o + t.n], moved[1][o:o + t.n], moved[2][o:o + t.n]
+            o += t.n
+        ts2[3].radius[ts2[3].nmemb + 1] *= 1.01
+        r1 = ctx.rebuild_count()
+        ctx.upload(ts2)
+        assert ctx.rebuild_count() == r1 + 1
+        off_c, idx_c = ctx.connections()
+        ctx.step(10)
+        end = ctx.positions()
+    for tissues, positions, (off, idx) in ((ts, pos, (off_a, idx_a)), (ts, moved, (off_b, idx_b))):
+        fresh = [t.copy() for t in tissues]
+        o = 0
+        for t in fresh:
+            t.x[:], t.y[:], t.z[:] = (positions[k][o:o + t.n] for k in range(3))
+            o += t.n
+        _, foff, fidx, _ = run_gpu(fresh, 0, FP64)
+        assert lists_equal(off, idx, foff, fidx)
+    fpos, foff, fidx, _ = run_gpu(ts2, 0, FP64)
+    assert lists_equal(off_c, idx_c, foff, fidx)
+    fpos, _, _, _ = run_gpu(ts2, 10, FP64)
+    assert max(abs(a - b).max() for a, b in zip(end, fpos)) <= 1e-12
