@@ -1000,7 +1000,9 @@ int epi_field_step(epi_ctx* c, int32_t nsteps) {
     FS.izb = c->izb;
     FS.nvox = c->nvox;
     FS.agek = c->agek;
-    launch_field_step(make_state(c, c->cur), FS, c->lc, c->stream);
+    int32_t wmax = 1;
+    for (const FieldDev& F : c->fd_h) wmax = std::max(wmax, 4 * std::max(F.irx, F.iry) + 1);
+    launch_field_step(make_state(c, c->cur), FS, wmax, c->lc, c->stream);
     c->ext_cur ^= 1;  // ext_stim.swap()
   }
   return check_status(c);

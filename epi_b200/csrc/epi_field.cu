@@ -48,44 +48,43 @@ __global__ void k_field_clear(FieldState FS) {
   }
 }
 
-// One block per tissue (grid-stride over tissues).
+// zzmax of every tissue: the z of its qualifying cells folded in with
+// atomicMax on the bit patterns (non-negative doubles order like their
+// bits; zzmax starts at 0), so the result does not depend on the order.
 __global__ void __launch_bounds__(256) k_field_zzmax(DevState S, FieldState FS) {
-  __shared__ double sh[256];
-  for (int32_t t = blockIdx.x; t < S.ntissues; t += gridDim.x) {
-    const TissueDev& T = S.tissues[t];
-    double z = 0.0;
-    for (int32_t k = T.nmemb + T.nder + threadIdx.x; k < T.n; k += blockDim.x) {
-      const int32_t i = T.pbase + k;
-      const uint32_t st = attr_state(S.attr[i]);
-      if (st == ST_DEAD || st == ST_ALIVE || st == ST_MUSUME || st == ST_FIX) {
-        const double zi = S.pos_cur[i].z;
-        if (z < zi) z = zi;
-      }
+  GRID_STRIDE(i, 0, S.n_total) {
+    const uint32_t a = S.attr[i];
+    const uint32_t st = attr_state(a);
+    if (st == ST_DEAD || st == ST_ALIVE || st == ST_MUSUME || st == ST_FIX) {
+      const double z = S.pos_cur[i].z;
+      if (z > 0.0)
+        atomicMax(reinterpret_cast<unsigned long long*>(&FS.zzmax[attr_tissue(a)]),
+                  (unsigned long long)__double_as_longlong(z));
     }
-    sh[threadIdx.x] = z;
-    __syncthreads();
-    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
-      if ((int)threadIdx.x < h && sh[threadIdx.x] < sh[threadIdx.x + h])
-        sh[threadIdx.x] = sh[threadIdx.x + h];
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-      const FieldDev& F = FS.fd[t];
-      const double zz = sh[0];
-      FS.zzmax[t] = zz;
-      const int32_t izb = (int32_t)(__dmul_rn(__dadd_rn(zz, kFacMap * kRMax), F.inv_dz));
-      // beyond the grid the reference would read outside its arrays
-      if (izb > F.nz) raise_error(S.status, E_UNSUPPORTED, T.pbase, -1, zz);
-      FS.izb[t] = izb > F.nz ? F.nz : izb;
-    }
-    __syncthreads();
   }
 }
 
-// One thread per particle: its window of grid points (set_lattice and the
-// two branches of setup_map_lat).
-__global__ void __launch_bounds__(256) k_field_stamp(DevState S, FieldState FS) {
-  GRID_STRIDE(i, 0, S.n_total) {
+// The diffusion's z bound per tissue, (int)((zzmax + FAC_MAP R_max) inv_dz)
+// (ext_stim.cpp:22).
+__global__ void k_field_bound(DevState S, FieldState FS) {
+  GRID_STRIDE(t, 0, S.ntissues) {
+    const FieldDev& F = FS.fd[t];
+    const double zz = FS.zzmax[t];
+    const int32_t izb = (int32_t)(__dmul_rn(__dadd_rn(zz, kFacMap * kRMax), F.inv_dz));
+    // beyond the grid the reference would read outside its arrays
+    if (izb > F.nz) raise_error(S.status, E_UNSUPPORTED, S.tissues[t].pbase, -1, zz);
+    FS.izb[t] = izb > F.nz ? F.nz : izb;
+  }
+}
+
+// One thread per (particle, x offset, y offset) of the widest window (wmax
+// x wmax columns per particle), each walking its z column: set_lattice and
+// the two branches of setup_map_lat.
+__global__ void __launch_bounds__(256) k_field_stamp(DevState S, FieldState FS, int32_t wmax) {
+  const int64_t cols = (int64_t)wmax * wmax;
+  GRID_STRIDE(g, 0, S.n_total * cols) {
+    const int64_t i = g / cols;
+    const int32_t col = (int32_t)(g % cols);
     const uint32_t a = S.attr[i];
     const int32_t t = attr_tissue(a);
     const TissueDev& T = S.tissues[t];
@@ -104,11 +103,15 @@ __global__ void __launch_bounds__(256) k_field_stamp(DevState S, FieldState FS) 
     const int32_t zmin = z_b >= 1 ? z_b : 1;
     const int32_t zmax = z_u < F.nz ? z_u : F.nz - 1;
     const int32_t mark = (int32_t)i - T.pbase + 1;
-    for (int32_t kx = lat0 - rx; kx <= lat0 + rx; ++kx) {
+    const int32_t ox = col / wmax, oy = col % wmax;
+    if (ox > 2 * rx || oy > 2 * ry) continue;  // outside this particle's window
+    {
+      const int32_t kx = lat0 - rx + ox;
       const double diffx = pdiff(__dmul_rn((double)kx, F.dx), p.x, T.lx);
       const double diffxSq = __dmul_rn(diffx, diffx);
       const int32_t ipx = (kx + F.nx) % F.nx;
-      for (int32_t ly = lat1 - ry; ly <= lat1 + ry; ++ly) {
+      {
+        const int32_t ly = lat1 - ry + oy;
         const double diffy = pdiff(__dmul_rn((double)ly, F.dy), p.y, T.ly);
         const double tmps = __dadd_rn(diffxSq, __dmul_rn(diffy, diffy));
         const int32_t ipy = (ly + F.ny) % F.ny;
@@ -241,13 +244,16 @@ void field_params(FieldDev& F, double lx, double ly, double lz, int32_t nx, int3
   F.irz = (int32_t)(kRad * (double)nz / lz);
 }
 
-void launch_field_step(const DevState& S, const FieldState& FS, const LaunchCfg& lc,
-                       cudaStream_t s) {
+void launch_field_step(const DevState& S, const FieldState& FS, int32_t wmax,
+                       const LaunchCfg& lc, cudaStream_t s) {
   const int nt = S.ntissues;
   const int grid = lc.num_sms * 8;
-  k_field_zzmax<<<nt < grid ? nt : grid, 256, 0, s>>>(S, FS);
+  cudaMemsetAsync(FS.zzmax, 0, sizeof(double) * nt, s);
+  if (S.n_total > 0) k_field_zzmax<<<stride_blocks(S.n_total, 256, lc), 256, 0, s>>>(S, FS);
+  k_field_bound<<<(nt + 255) / 256, 256, 0, s>>>(S, FS);
   k_field_clear<<<grid, 256, 0, s>>>(FS);
-  if (S.n_total > 0) k_field_stamp<<<blocks_for(S.n_total, 256), 256, 0, s>>>(S, FS);
+  if (S.n_total > 0)
+    k_field_stamp<<<stride_blocks(S.n_total * wmax * wmax, 256, lc), 256, 0, s>>>(S, FS, wmax);
   const dim3 g2(64, nt);
   k_field_copy_map_y<<<g2, 256, 0, s>>>(FS);
   k_field_copy_map_x<<<g2, 256, 0, s>>>(FS);

@@ -97,8 +97,9 @@ struct FieldState {
 void field_params(FieldDev& F, double lx, double ly, double lz, int32_t nx, int32_t ny,
                   int32_t nz);
 // zzmax, cell maps, external-stimulus update into FS.nxt (the caller swaps).
-void launch_field_step(const DevState& S, const FieldState& FS, const LaunchCfg& lc,
-                       cudaStream_t s);
+// wmax: the widest stamp window over the batch's tissues, 2 (2 irx) + 1.
+void launch_field_step(const DevState& S, const FieldState& FS, int32_t wmax,
+                       const LaunchCfg& lc, cudaStream_t s);
 
 // ---- reverse-mode adjoint (FP64), membrane + ALIVE / DEAD / AIR tissues ----
 struct AdjointBuffers {
