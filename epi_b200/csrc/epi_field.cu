@@ -51,16 +51,35 @@ __global__ void k_field_clear(FieldState FS) {
 // zzmax of every tissue: the z of its qualifying cells folded in with
 // atomicMax on the bit patterns (non-negative doubles order like their
 // bits; zzmax starts at 0), so the result does not depend on the order.
+// Lanes of a warp holding the same tissue first fold their values with
+// shuffles, so one atomic per (warp, tissue) run reaches memory.
 __global__ void __launch_bounds__(256) k_field_zzmax(DevState S, FieldState FS) {
-  GRID_STRIDE(i, 0, S.n_total) {
-    const uint32_t a = S.attr[i];
-    const uint32_t st = attr_state(a);
-    if (st == ST_DEAD || st == ST_ALIVE || st == ST_MUSUME || st == ST_FIX) {
-      const double z = S.pos_cur[i].z;
-      if (z > 0.0)
-        atomicMax(reinterpret_cast<unsigned long long*>(&FS.zzmax[attr_tissue(a)]),
-                  (unsigned long long)__double_as_longlong(z));
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t base0 = (int64_t)blockIdx.x * blockDim.x;
+  for (int64_t base = base0; base < S.n_total; base += stride) {
+    const int64_t i = base + threadIdx.x;
+    int32_t t = -1;
+    unsigned long long z = 0;
+    if (i < S.n_total) {
+      const uint32_t a = S.attr[i];
+      const uint32_t st = attr_state(a);
+      t = attr_tissue(a);
+      if (st == ST_DEAD || st == ST_ALIVE || st == ST_MUSUME || st == ST_FIX) {
+        const double zd = S.pos_cur[i].z;
+        if (zd > 0.0) z = (unsigned long long)__double_as_longlong(zd);
+      }
     }
+    const int lane = threadIdx.x & 31;
+    // same-tissue lanes form contiguous runs (particles are grouped by tissue)
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long zo = __shfl_down_sync(0xffffffffu, z, o);
+      const int32_t to = __shfl_down_sync(0xffffffffu, t, o);
+      if (lane + o < 32 && to == t && zo > z) z = zo;
+    }
+    const int32_t tprev = __shfl_up_sync(0xffffffffu, t, 1);
+    if (t >= 0 && z > 0 && (lane == 0 || tprev != t))
+      atomicMax(reinterpret_cast<unsigned long long*>(&FS.zzmax[t]), z);
   }
 }
 
@@ -80,11 +99,14 @@ __global__ void k_field_bound(DevState S, FieldState FS) {
 // One thread per (particle, x offset, y offset) of the widest window (wmax
 // x wmax columns per particle), each walking its z column: set_lattice and
 // the two branches of setup_map_lat.
+template <typename Index>
 __global__ void __launch_bounds__(256) k_field_stamp(DevState S, FieldState FS, int32_t wmax) {
-  const int64_t cols = (int64_t)wmax * wmax;
-  GRID_STRIDE(g, 0, S.n_total * cols) {
-    const int64_t i = g / cols;
-    const int32_t col = (int32_t)(g % cols);
+  const Index cols = (Index)wmax * (Index)wmax;
+  const Index total = (Index)S.n_total * cols;
+  for (Index g = (Index)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (Index)gridDim.x * blockDim.x) {
+    const Index i = g / cols;
+    const int32_t col = (int32_t)(g - i * cols);
     const uint32_t a = S.attr[i];
     const int32_t t = attr_tissue(a);
     const TissueDev& T = S.tissues[t];
@@ -252,8 +274,14 @@ void launch_field_step(const DevState& S, const FieldState& FS, int32_t wmax,
   if (S.n_total > 0) k_field_zzmax<<<stride_blocks(S.n_total, 256, lc), 256, 0, s>>>(S, FS);
   k_field_bound<<<(nt + 255) / 256, 256, 0, s>>>(S, FS);
   k_field_clear<<<grid, 256, 0, s>>>(FS);
-  if (S.n_total > 0)
-    k_field_stamp<<<stride_blocks(S.n_total * wmax * wmax, 256, lc), 256, 0, s>>>(S, FS, wmax);
+  const int64_t columns = S.n_total * (int64_t)wmax * wmax;
+  if (columns > 0) {
+    // 32-bit index arithmetic whenever the columns fit
+    if (columns + (int64_t)lc.num_sms * 8 * 256 < (int64_t)UINT32_MAX)
+      k_field_stamp<uint32_t><<<stride_blocks(columns, 256, lc), 256, 0, s>>>(S, FS, wmax);
+    else
+      k_field_stamp<uint64_t><<<stride_blocks(columns, 256, lc), 256, 0, s>>>(S, FS, wmax);
+  }
   const dim3 g2(64, nt);
   k_field_copy_map_y<<<g2, 256, 0, s>>>(FS);
   k_field_copy_map_x<<<g2, 256, 0, s>>>(FS);
