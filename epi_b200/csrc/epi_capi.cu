@@ -106,6 +106,7 @@ struct epi_ctx {
   DevStatus* status = nullptr;
   DevStatus* status_h = nullptr;  // pinned
   unsigned long long* rebuilds = nullptr;
+  int32_t* loop_left = nullptr;  // passes left in the step graph's device loop
   ScanScratch scan{};
   // graphs: one per buffer parity, each replaying two steps
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -301,24 +302,46 @@ cudaError_t capture_conditional_rebuild(epi_ctx* c, int cur) {
                                              cudaStreamSetCaptureDependencies);
 }
 
-// Captures the two-step graph of parity c->cur: per step, the conditional
-// rebuild, the prepass and the fused step.
+// The step graph of parity c->cur: one launch runs a whole sequence of steps.
+// A WHILE node repeats its body -- two steps (per step: the conditional
+// rebuild, the prepass and the fused step), then a one-thread kernel that
+// counts down the passes left (set before each launch) and sets the loop
+// condition -- so the device drives the loop and the host launches once.
 cudaError_t capture_step_graph(epi_ctx* c, cudaGraphExec_t* out) {
-  cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
-  if (e != cudaSuccess) return e;
-  int cur = c->cur;
-  for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
-    e = capture_conditional_rebuild(c, cur);
-    if (e != cudaSuccess) break;
-    prepass_all(c, cur, nullptr);
-    launch_step(make_state(c, cur), whole(c), c->cfg.precision, c->lc, c->stream, nullptr);
-    cur ^= 1;
-  }
   cudaGraph_t g = nullptr;
-  const cudaError_t e_end = cudaStreamEndCapture(c->stream, &g);
-  if (e == cudaSuccess) e = e_end;
+  cudaError_t e = cudaGraphCreate(&g, 0);
+  if (e != cudaSuccess) return e;
+  cudaGraphConditionalHandle hw;
+  e = cudaGraphConditionalHandleCreate(&hw, g, 1, cudaGraphCondAssignDefault);
+  cudaGraphNodeParams p{};
+  cudaGraphNode_t loop;
+  if (e == cudaSuccess) {
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = hw;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    e = cudaGraphAddNode(&loop, g, nullptr, 0, &p);
+  }
+  if (e == cudaSuccess) {
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      int cur = c->cur;
+      for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+        e = capture_conditional_rebuild(c, cur);
+        if (e != cudaSuccess) break;
+        prepass_all(c, cur, nullptr);
+        launch_step(make_state(c, cur), whole(c), c->cfg.precision, c->lc, c->stream, nullptr);
+        cur ^= 1;
+      }
+      if (e == cudaSuccess) launch_loop_tick(c->loop_left, hw, c->stream);
+      const cudaError_t e_end = cudaStreamEndCapture(c->stream, &body);
+      if (e == cudaSuccess) e = e_end;
+    }
+  }
   if (e == cudaSuccess) e = cudaGraphInstantiate(out, g, 0);
-  if (g) cudaGraphDestroy(g);
+  cudaGraphDestroy(g);
   return e;
 }
 
@@ -353,7 +376,8 @@ int enqueue_graph_steps(epi_ctx* c, int32_t nsteps) {
   if (pairs > 0) {
     cudaGraphExec_t& ge = c->graph[c->cur];
     if (!ge) EPI_CUDA(capture_step_graph(c, &ge));
-    for (int32_t k = 0; k < pairs; ++k) EPI_CUDA(cudaGraphLaunch(ge, c->stream));
+    launch_set_counter(c->loop_left, pairs, c->stream);
+    EPI_CUDA(cudaGraphLaunch(ge, c->stream));
   }
   if (nsteps % 2) enqueue_step(c, c->cur, nullptr);
   if (nsteps > 0) c->lists_fresh = false;
@@ -587,6 +611,7 @@ int epi_create(epi_ctx** out, const epi_config* cfg) {
   if (rc == EPI_OK) rc = cuda_status(cudaMallocHost((void**)&ctx->status_h, sizeof(DevStatus)));
   if (rc == EPI_OK) rc = cuda_status(cudaMemset(ctx->status, 0, sizeof(DevStatus)));
   if (rc == EPI_OK) rc = dev_alloc(&ctx->rebuilds, 1);
+  if (rc == EPI_OK) rc = dev_alloc(&ctx->loop_left, 1);
   if (rc == EPI_OK) rc = cuda_status(cudaMemset(ctx->rebuilds, 0, sizeof(unsigned long long)));
   if (rc != EPI_OK) {
     epi_destroy(ctx);
@@ -604,6 +629,7 @@ void epi_destroy(epi_ctx* ctx) {
   free_buffers(ctx);
   if (ctx->status) cudaFree(ctx->status);
   if (ctx->rebuilds) cudaFree(ctx->rebuilds);
+  if (ctx->loop_left) cudaFree(ctx->loop_left);
   if (ctx->status_h) cudaFreeHost(ctx->status_h);
   if (ctx->side) cudaStreamDestroy(ctx->side);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);

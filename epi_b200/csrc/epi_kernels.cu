@@ -1153,6 +1153,23 @@ void launch_exact_lists(const DevState& S, const Range& r, const LaunchCfg& lc,
   if (np > 0) k_exact_lists<<<stride_blocks(np, lc.block, lc), lc.block, 0, s>>>(S, r);
 }
 
+// Loop counter of the step graph's WHILE node: one pass of the body (two
+// steps) done; run another while pairs remain.
+__global__ void k_loop_tick(int32_t* remaining, cudaGraphConditionalHandle h) {
+  pdl_entry();
+  const int32_t left = *remaining - 1;
+  *remaining = left;
+  cudaGraphSetConditional(h, left > 0 ? 1u : 0u);
+}
+
+void launch_loop_tick(int32_t* remaining, cudaGraphConditionalHandle h, cudaStream_t s) {
+  launch_pdl(k_loop_tick, 1, 1, s, remaining, h);
+}
+
+void launch_set_counter(int32_t* remaining, int32_t value, cudaStream_t s) {
+  k_set1<<<1, 1, 0, s>>>(remaining, value, nullptr);
+}
+
 void launch_rebuild_condition(const DevState& S, cudaGraphConditionalHandle h, cudaStream_t s) {
   launch_pdl(k_rebuild_condition, 1, 1, s, h, (const int32_t*)S.gate);
 }

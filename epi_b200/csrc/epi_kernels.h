@@ -63,6 +63,10 @@ void launch_exact_lists(const DevState& S, const Range& r, const LaunchCfg& lc,
 void launch_set_gates(const DevState& S, int32_t ntissues, cudaStream_t s);
 // Sets conditional handle h to (some tissue is flagged for a rebuild).
 void launch_rebuild_condition(const DevState& S, cudaGraphConditionalHandle h, cudaStream_t s);
+// WHILE-node bookkeeping of the step graph: set the number of passes left,
+// and decrement it at the end of a pass (setting h to "more passes").
+void launch_set_counter(int32_t* remaining, int32_t value, cudaStream_t s);
+void launch_loop_tick(int32_t* remaining, cudaGraphConditionalHandle h, cudaStream_t s);
 
 // CSR export of the connection lists (tissue-local indices, rows sorted).
 void launch_rowlen(const DevState& S, int32_t* rowlen, int32_t n, cudaStream_t s);
