@@ -515,7 +515,7 @@ def main():
                "variant": tuned["variant"] if tuned else (args.variant or 1),
                "autotune": tuned,
                "tissue_rebuilds_per_step": rebuilds_timed / max(args.steps, 1) / len(mine),
-               "launch": "one CUDA graph per 2 steps over the whole batch",
+               "launch": "one graph launch per run (device WHILE loop over a 2-step body)",
                "l2": "inputs larger than L2 (working set >> 126 MB)"
                if n_all * 200 > 126e6 else "working set fits in L2 (no flush)",
                "parallelism": f"tissue sharding x{world}" if world > 1 else "1 GPU"}
