@@ -41,11 +41,6 @@ from epi_b200.ensemble import shard_tissues  # noqa: E402
 
 METRIC = "cell-updates/s: FP32/batched vs plain FP64 GPU @≤1e-5 rel pos err; grad err"
 UNIT = "cell-updates/s"
-# per step: rebuild (gate compaction, bin, per-tissue scan, scatter, binsort,
-# candidate search, gate clear; each exits at once unless a tissue needs a
-# rebuild), membrane prepass, step; plus the dermis kernel when a tissue holds
-# FIX / MUSUME cells
-KERNEL_LAUNCHES_PER_STEP = 9
 
 
 def workload(name: str, tissues: int = 512):
@@ -389,6 +384,7 @@ def main():
     if args.warmup:
         ctx.step(args.warmup, args.mode)
     rebuilds0 = ctx.rebuild_count()
+    launches0 = ctx.launch_count()
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
@@ -403,6 +399,7 @@ def main():
     barrier()
     ms = e0.elapsed_time(e1)
     rebuilds_timed = ctx.rebuild_count() - rebuilds0
+    launches_timed = ctx.launch_count() - launches0
     if dist is not None:
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -524,9 +521,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32-force/f64-sum" if args.precision == "mixed" else "f64",
                 "data": "synthetic (seeded splitmix64 jittered lattices)", "config": cfg,
-                "gpu_launches": (KERNEL_LAUNCHES_PER_STEP + int(any(
-                    ((t.state == T.FIX) | (t.state == T.MUSUME)).any() for t in mine)))
-                * args.steps,
+                "gpu_launches": launches_timed,
                 "clocks": clk.summary()}
         line.update(extras)
         if world == 1 and not args.no_cpu_baseline and not args.no_extras:

@@ -40,7 +40,8 @@ EXPORTED = [
     "epi_upload", "epi_connect", "epi_interact_commit", "epi_step", "epi_step_graph",
     "epi_step_per_tissue", "epi_sync", "epi_num_particles", "epi_download_positions",
     "epi_upload_positions", "epi_get_connections", "epi_get_dermis", "epi_error_info",
-    "epi_stream", "epi_rebuild_count", "epi_time_kernels", "epi_autotune", "epi_field_init",
+    "epi_stream", "epi_rebuild_count", "epi_launch_count", "epi_time_kernels", "epi_autotune",
+    "epi_field_init",
     "epi_field_step", "epi_field_get", "epi_field_set_ext", "epi_adjoint", "epi_connect_noalloc",
 ]
 
@@ -125,6 +126,7 @@ def lib():
         L.epi_get_dermis.argtypes = [vp, _ip]
         L.epi_error_info.argtypes = [vp, _ip, _ip, _ip, _dp]
         L.epi_rebuild_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.epi_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         L.epi_stream.argtypes = [vp]
         L.epi_stream.restype = vp
         L.epi_time_kernels.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, _dp, _ip,
@@ -313,6 +315,11 @@ class Context:
     def rebuild_count(self) -> int:
         v = ctypes.c_int64()
         _check(lib().epi_rebuild_count(self._h, ctypes.byref(v)), "epi_rebuild_count")
+        return int(v.value)
+
+    def launch_count(self) -> int:
+        v = ctypes.c_int64()
+        _check(lib().epi_launch_count(self._h, ctypes.byref(v)), "epi_launch_count")
         return int(v.value)
 
     def stream_handle(self) -> int:

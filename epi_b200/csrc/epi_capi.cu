@@ -107,6 +107,7 @@ struct epi_ctx {
   DevStatus* status_h = nullptr;  // pinned
   unsigned long long* rebuilds = nullptr;
   int32_t* loop_left = nullptr;  // passes left in the step graph's device loop
+  unsigned long long* launches = nullptr;  // step-sequence kernels executed
   ScanScratch scan{};
   // graphs: one per buffer parity, each replaying two steps
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -225,6 +226,7 @@ DevState make_state(epi_ctx* c, int cur) {
   S.nprep_memb = c->nprep_memb;
   S.status = c->status;
   S.rebuilds = c->rebuilds;
+  S.launches = c->launches;
   S.n_total = c->n;
   S.max_conn = c->cfg.max_conn;
   S.max_cand = c->cfg.max_cand;
@@ -335,7 +337,7 @@ cudaError_t capture_step_graph(epi_ctx* c, cudaGraphExec_t* out) {
         launch_step(make_state(c, cur), whole(c), c->cfg.precision, c->lc, c->stream, nullptr);
         cur ^= 1;
       }
-      if (e == cudaSuccess) launch_loop_tick(c->loop_left, hw, c->stream);
+      if (e == cudaSuccess) launch_loop_tick(c->loop_left, hw, c->launches, c->stream);
       const cudaError_t e_end = cudaStreamEndCapture(c->stream, &body);
       if (e == cudaSuccess) e = e_end;
     }
@@ -612,6 +614,8 @@ int epi_create(epi_ctx** out, const epi_config* cfg) {
   if (rc == EPI_OK) rc = cuda_status(cudaMemset(ctx->status, 0, sizeof(DevStatus)));
   if (rc == EPI_OK) rc = dev_alloc(&ctx->rebuilds, 1);
   if (rc == EPI_OK) rc = dev_alloc(&ctx->loop_left, 1);
+  if (rc == EPI_OK) rc = dev_alloc(&ctx->launches, 1);
+  if (rc == EPI_OK) rc = cuda_status(cudaMemset(ctx->launches, 0, sizeof(unsigned long long)));
   if (rc == EPI_OK) rc = cuda_status(cudaMemset(ctx->rebuilds, 0, sizeof(unsigned long long)));
   if (rc != EPI_OK) {
     epi_destroy(ctx);
@@ -630,6 +634,7 @@ void epi_destroy(epi_ctx* ctx) {
   if (ctx->status) cudaFree(ctx->status);
   if (ctx->rebuilds) cudaFree(ctx->rebuilds);
   if (ctx->loop_left) cudaFree(ctx->loop_left);
+  if (ctx->launches) cudaFree(ctx->launches);
   if (ctx->status_h) cudaFreeHost(ctx->status_h);
   if (ctx->side) cudaStreamDestroy(ctx->side);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1371,6 +1376,19 @@ int epi_rebuild_count(epi_ctx* c, int64_t* count) {
   if (rc) return rc;
   unsigned long long v = 0;
   EPI_CUDA(cudaMemcpyAsync(&v, c->rebuilds, sizeof(v), cudaMemcpyDeviceToHost, c->stream));
+  EPI_CUDA(cudaStreamSynchronize(c->stream));
+  *count = (int64_t)v;
+  return EPI_OK;
+  EPI_GUARD_END
+}
+
+int epi_launch_count(epi_ctx* c, int64_t* count) {
+  if (!c || !count) return EPI_ERR_INVALID_ARG;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  unsigned long long v = 0;
+  EPI_CUDA(cudaMemcpyAsync(&v, c->launches, sizeof(v), cudaMemcpyDeviceToHost, c->stream));
   EPI_CUDA(cudaStreamSynchronize(c->stream));
   *count = (int64_t)v;
   return EPI_OK;

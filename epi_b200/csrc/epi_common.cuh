@@ -90,6 +90,7 @@ struct DevState {
   int32_t nprep, nprep_memb;
   DevStatus* status;
   unsigned long long* rebuilds;  // tissue candidate rebuilds so far
+  unsigned long long* launches;  // kernels of the step sequence executed so far
   int64_t n_total;  // column stride of cand / nbr
   int32_t max_conn, max_cand;
   double skin;

@@ -24,6 +24,11 @@ __device__ __forceinline__ void pdl_entry() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
+// One count per kernel launch (the first thread of the first block).
+__device__ __forceinline__ void count_launch(unsigned long long* launches) {
+  if (launches && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) atomicAdd(launches, 1ull);
+}
+
 template <typename... Params, typename... Args>
 void launch_pdl(void (*kernel)(Params...), int grid, int block, cudaStream_t s, Args... args) {
   cudaLaunchConfig_t cfg{};

@@ -154,6 +154,7 @@ __device__ __forceinline__ int32_t ref_bin(const TissueDev& T, double x, double 
 // ---------------------------------------------------------------------------
 __global__ void k_gate_compact(DevState S, int32_t t0, int32_t t1) {
   pdl_entry();
+  count_launch(S.launches);
   if (S.gate[0] == 0) {
     if (threadIdx.x == 0) {
       S.rl_count[0] = 0;
@@ -222,6 +223,7 @@ __device__ __forceinline__ int32_t gated_particle(const DevState& S, int32_t cnt
 // Binning on the reference's 2.0 grid (grid_init, cell_connection.cpp:38-62).
 __global__ void k_bin(DevState S) {
   pdl_entry();
+  count_launch(S.launches);
   GATED_PARTICLES(g, cnt) {
     int32_t t;
     const int32_t i = gated_particle(S, cnt, g, &t);
@@ -252,6 +254,7 @@ __global__ void k_bin(DevState S) {
 // with a sentinel entry that receives the end offset.
 __global__ void k_scan_tissue(DevState S) {
   pdl_entry();
+  count_launch(S.launches);
   const int32_t cnt = S.rl_count[0];
   for (int32_t k = blockIdx.x; k < cnt; k += gridDim.x) {
     const TissueDev& T = S.tissues[S.rl_list[k]];
@@ -284,6 +287,7 @@ __global__ void k_scan_tissue(DevState S) {
 
 __global__ void k_scatter(DevState S) {
   pdl_entry();
+  count_launch(S.launches);
   GATED_PARTICLES(g, cnt) {
     int32_t t;
     const int32_t i = gated_particle(S, cnt, g, &t);
@@ -297,6 +301,7 @@ __global__ void k_scatter(DevState S) {
 // particles), then the sorted position copy the search streams through.
 __global__ void k_binsort(DevState S) {
   pdl_entry();
+  count_launch(S.launches);
   const int32_t cnt = S.rl_count[0];
   if (cnt == 0) return;
   const int32_t nbg = S.rl_bpre[cnt];
@@ -367,6 +372,7 @@ __device__ __forceinline__ int window_ranges(double x, double R, double L, int32
 // Candidates come out in bin order, deterministic after k_binsort.
 __global__ void k_cand_search(DevState S) {
   pdl_entry();
+  count_launch(S.launches);
   // One warp per gated particle: the lanes stride the contiguous slots of
   // each bin column, and ballots keep the candidates in slot order.
   constexpr double kInvAG = 1.0 / kAreaGrid;
@@ -446,6 +452,7 @@ __global__ void k_cand_search(DevState S) {
 
 __global__ void k_gate_clear(DevState S, int32_t clear_any) {
   pdl_entry();
+  count_launch(S.launches);
   const int32_t cnt = S.rl_count[0];
   for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x)
     S.gate[1 + S.rl_list[k]] = 0;
@@ -457,8 +464,10 @@ __global__ void k_gate_clear(DevState S, int32_t clear_any) {
 
 // Condition of the rebuild node in the captured step graph: run the rebuild
 // kernels only when some tissue is flagged.
-__global__ void k_rebuild_condition(cudaGraphConditionalHandle h, const int32_t* gate) {
+__global__ void k_rebuild_condition(cudaGraphConditionalHandle h, const int32_t* gate,
+                                    unsigned long long* launches) {
   pdl_entry();
+  count_launch(launches);
   cudaGraphSetConditional(h, gate[0] != 0 ? 1u : 0u);
 }
 
@@ -474,6 +483,7 @@ __global__ void k_gate_set_all(DevState S, int32_t ntissues) {
 // ---------------------------------------------------------------------------
 __global__ void k_dermis(DevState S, int32_t f0, int32_t f1) {
   pdl_entry();
+  count_launch(S.launches);
   GRID_STRIDE(e, f0, f1) {
     const int32_t i = S.prep[e];
     const TissueDev& T = S.tissues[attr_tissue(S.attr[i])];
@@ -625,6 +635,7 @@ __device__ __forceinline__ Vec3<R> tri_bending(const Off& off, int32_t j, int32_
 template <typename R>
 __global__ void __launch_bounds__(256) k_memb_force(DevState S, int32_t m0, int32_t m1) {
   pdl_entry();
+  count_launch(S.launches);
   GRID_STRIDE(e, m0, m1) {
     const int32_t i = S.prep[e];
     const TissueDev& T = S.tissues[attr_tissue(S.attr[i])];
@@ -932,6 +943,7 @@ __device__ __forceinline__ const float4* gather_source<float4>(const DevState& S
 template <typename R, bool kSimple, bool kOld, int kMinBlocks>
 __global__ void __launch_bounds__(256, kMinBlocks) k_step(DevState S, Range r) {
   pdl_entry();
+  count_launch(S.launches);
   const int64_t i = r.p0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= r.p1) return;
   const int64_t N = S.n_total;
@@ -1155,15 +1167,18 @@ void launch_exact_lists(const DevState& S, const Range& r, const LaunchCfg& lc,
 
 // Loop counter of the step graph's WHILE node: one pass of the body (two
 // steps) done; run another while pairs remain.
-__global__ void k_loop_tick(int32_t* remaining, cudaGraphConditionalHandle h) {
+__global__ void k_loop_tick(int32_t* remaining, cudaGraphConditionalHandle h,
+                            unsigned long long* launches) {
   pdl_entry();
+  count_launch(launches);
   const int32_t left = *remaining - 1;
   *remaining = left;
   cudaGraphSetConditional(h, left > 0 ? 1u : 0u);
 }
 
-void launch_loop_tick(int32_t* remaining, cudaGraphConditionalHandle h, cudaStream_t s) {
-  launch_pdl(k_loop_tick, 1, 1, s, remaining, h);
+void launch_loop_tick(int32_t* remaining, cudaGraphConditionalHandle h,
+                      unsigned long long* launches, cudaStream_t s) {
+  launch_pdl(k_loop_tick, 1, 1, s, remaining, h, launches);
 }
 
 void launch_set_counter(int32_t* remaining, int32_t value, cudaStream_t s) {
@@ -1171,7 +1186,7 @@ void launch_set_counter(int32_t* remaining, int32_t value, cudaStream_t s) {
 }
 
 void launch_rebuild_condition(const DevState& S, cudaGraphConditionalHandle h, cudaStream_t s) {
-  launch_pdl(k_rebuild_condition, 1, 1, s, h, (const int32_t*)S.gate);
+  launch_pdl(k_rebuild_condition, 1, 1, s, h, (const int32_t*)S.gate, S.launches);
 }
 
 void launch_set_gates(const DevState& S, int32_t ntissues, cudaStream_t s) {

@@ -66,7 +66,8 @@ void launch_rebuild_condition(const DevState& S, cudaGraphConditionalHandle h, c
 // WHILE-node bookkeeping of the step graph: set the number of passes left,
 // and decrement it at the end of a pass (setting h to "more passes").
 void launch_set_counter(int32_t* remaining, int32_t value, cudaStream_t s);
-void launch_loop_tick(int32_t* remaining, cudaGraphConditionalHandle h, cudaStream_t s);
+void launch_loop_tick(int32_t* remaining, cudaGraphConditionalHandle h,
+                      unsigned long long* launches, cudaStream_t s);
 
 // CSR export of the connection lists (tissue-local indices, rows sorted).
 void launch_rowlen(const DevState& S, int32_t* rowlen, int32_t n, cudaStream_t s);

@@ -181,6 +181,11 @@ void* epi_stream(epi_ctx* ctx);
 /* Tissue candidate-list rebuilds since the context was created (the count
  * the skin trades against candidate-list length). */
 int epi_rebuild_count(epi_ctx* ctx, int64_t* count);
+/* Kernels of the step sequence (rebuild, membrane prepass, dermis, step, and
+ * the graph's condition and loop kernels) executed on the device since the
+ * context was created, counted by the kernels themselves; kernels a graph's
+ * conditional node skipped are not counted. */
+int epi_launch_count(epi_ctx* ctx, int64_t* count);
 /* Per-kernel timing: runs nsteps (not graph-captured) recording CUDA events
  * around each kernel class on the context stream. ms receives the summed
  * milliseconds per class, launches the launch count per class, names the

@@ -465,3 +465,21 @@ def test_reupload_and_position_upload_regate_only_what_changed(built):
     assert lists_equal(off_c, idx_c, foff, fidx)
     fpos, _, _, _ = run_gpu(ts2, 10, FP64)
     assert max(abs(a - b).max() for a, b in zip(end, fpos)) <= 1e-12
+
+
+def test_launch_count_counts_the_step_sequence(built):
+    """epi_launch_count: eager steps run 9 kernels each (7 rebuild kernels,
+    the membrane prepass, the step); a graph run adds one condition kernel
+    per step and one loop kernel per pass of two steps, and runs the rebuild
+    kernels only in steps where some tissue was flagged."""
+    with capi.Context(precision=MIXED) as ctx:
+        ctx.upload([T.config1()])
+        c0 = ctx.launch_count()
+        ctx.step(10, "eager")
+        assert ctx.launch_count() - c0 == 90
+        c1 = ctx.launch_count()
+        r1 = ctx.rebuild_count()
+        ctx.step(10, "graph")
+        n = ctx.launch_count() - c1
+        rebuilt_steps = ctx.rebuild_count() - r1  # one tissue: one rebuild per rebuilding step
+        assert n == 10 * 3 + 5 + 7 * rebuilt_steps
