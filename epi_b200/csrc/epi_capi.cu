@@ -499,7 +499,9 @@ int validate_tissue(const epi_tissue_view& v, const epi_params& P) {
     if ((i < v.nmemb) != (s == ST_MEMB)) return EPI_ERR_INVALID_ARG;
     if (i >= v.nmemb && i < v.nmemb + v.nder && s != ST_DER) return EPI_ERR_INVALID_ARG;
     if (i >= v.nmemb + v.nder && s == ST_DER) return EPI_ERR_INVALID_ARG;
-    if (!(v.radius[i] > 0)) return EPI_ERR_INVALID_ARG;
+    if (!(v.radius[i] > 0) || !std::isfinite(v.radius[i])) return EPI_ERR_INVALID_ARG;
+    if (!std::isfinite(v.x[i]) || !std::isfinite(v.y[i]) || !std::isfinite(v.z[i]))
+      return EPI_ERR_NONFINITE;
     rmax = std::max(rmax, v.radius[i]);
     if (v.pair) {
       const int32_t q = v.pair[i];
@@ -508,9 +510,15 @@ int validate_tissue(const epi_tissue_view& v, const epi_params& P) {
         return EPI_ERR_INVALID_ARG;
     }
   }
+  // Constants: finite; DT > 0; LJ_THRESH > 1 (adhesion divides by
+  // (LJ_THRESH - 1)^2, cell_interaction.cpp:113-124).
+  const double* pv = reinterpret_cast<const double*>(&P);
+  for (size_t k = 0; k < sizeof(epi_params) / sizeof(double); ++k)
+    if (!std::isfinite(pv[k])) return EPI_ERR_INVALID_ARG;
+  if (!(P.dt > 0) || !(P.lj_thresh > 1.0)) return EPI_ERR_INVALID_ARG;
   // Every pair the reference can connect must lie inside its +-2 bin window:
   // LJ_THRESH * (r_i + r_j) < 2 * AREA_GRID (cell_connection.cpp:92-109).
-  if (!(P.lj_thresh > 0) || P.lj_thresh * 2.0 * rmax >= 4.0 - 1e-6) return EPI_ERR_UNSUPPORTED;
+  if (P.lj_thresh * 2.0 * rmax >= 4.0 - 1e-6) return EPI_ERR_UNSUPPORTED;
   return EPI_OK;
 }
 
@@ -595,6 +603,7 @@ int epi_create(epi_ctx** out, const epi_config* cfg) {
   if (!(c.skin > 0) || c.skin > 2.0) return EPI_ERR_INVALID_ARG;
   if (c.variant < 0 || c.variant > 4) return EPI_ERR_INVALID_ARG;
   if (c.precision != EPI_PREC_FP64 && c.precision != EPI_PREC_MIXED) return EPI_ERR_INVALID_ARG;
+  if (c.reserved != 0) return EPI_ERR_INVALID_ARG;
   int ndev = 0;
   const cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev <= 0) return EPI_ERR_NO_DEVICE;

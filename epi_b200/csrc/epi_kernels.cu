@@ -1052,6 +1052,8 @@ __global__ void k_pack(DevState S, const double* x, const double* y, const doubl
   if (i >= n) return;
   const double r = S.pos_cur[i].w;
   const double4 p = make_double4(x[i], y[i], z[i], r);
+  if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z))
+    raise_error(S.status, E_NONFINITE, (int32_t)i, -1, p.z);
   S.pos_cur[i] = p;
   S.pos_nxt[i] = p;
   const float4 f = make_float4((float)p.x, (float)p.y, (float)p.z, (float)r);

@@ -258,6 +258,33 @@ def test_nan_input_reports_nonfinite(built):
         assert e.value.code == capi.EPI_ERR_NONFINITE
 
 
+def test_upload_rejects_invalid_constants_and_views(built):
+    t = T.config1()
+    with capi.Context(precision=FP64) as ctx:
+        for bad in (t.params.scaled(1, 1, 1), ):
+            bad.lj_thresh = 1.0  # adhesion divides by (LJ_THRESH - 1)^2
+            with pytest.raises(capi.EpiError) as e:
+                ctx.upload([t], [bad])
+            assert e.value.code == capi.EPI_ERR_INVALID_ARG
+        bad = t.params.scaled(1, 1, 1)
+        bad.dt = 0.0
+        with pytest.raises(capi.EpiError) as e:
+            ctx.upload([t], [bad])
+        assert e.value.code == capi.EPI_ERR_INVALID_ARG
+        r = t.copy()
+        r.radius[r.nmemb + 2] = np.inf
+        with pytest.raises(capi.EpiError) as e:
+            ctx.upload([r])
+        assert e.value.code == capi.EPI_ERR_INVALID_ARG
+        ctx.upload([t])  # usable afterwards
+        ctx.step(2)
+        x, y, z = ctx.positions()
+        x[3] = np.nan
+        with pytest.raises(capi.EpiError) as e:
+            ctx.set_positions(x, y, z)
+        assert e.value.code == capi.EPI_ERR_NONFINITE
+
+
 def test_list_capacity_overflow_reported(built):
     t = T.config1()
     with capi.Context(precision=FP64, max_conn=3, max_cand=64) as ctx:
