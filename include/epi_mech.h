@@ -9,8 +9,11 @@
  *                                       epi5_MT/cellmanager.cpp:19-26
  *   cell_pos_periodic_fix(CellManager&) epi5_MT/cellmanager.h:111,
  *                                       epi5_MT/cellmanager.cpp:395-414
- * for the square-membrane build, on one GPU, for one tissue or a batch of
- * independent tissues. A tissue is what one epi5_MT CellManager holds:
+ * for the square- and the triangular-membrane (TRI_MEMB) builds, on one
+ * GPU, for one tissue or a batch of independent tissues, and the cell maps
+ * and external-stimulus diffusion that follow them in the reference's loop
+ * (setup_map_lat, calc_ext_stim); it adds gradients (epi_adjoint) and an
+ * autotuner. A tissue is what one epi5_MT CellManager holds:
  * particles in the reference's index layout (membrane [0,nmemb), dermis
  * [nmemb,nmemb+nder), every other cell after), a periodic box LX x LY and an
  * open height LZ.
