@@ -72,6 +72,26 @@ __device__ __forceinline__ int32_t block_excl_scan(int32_t v, int32_t* total) {
   return before + incl - v;
 }
 
+// Same for NT threads (a multiple of 32, at most 1024).
+template <int NT>
+__device__ __forceinline__ int32_t block_excl_scan_n(int32_t v, int32_t* total) {
+  __shared__ int32_t wsum[NT / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int32_t incl = warp_incl_scan(v);
+  if (lane == 31) wsum[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    int32_t w = lane < NT / 32 ? wsum[lane] : 0;
+    w = warp_incl_scan(w);
+    if (lane < NT / 32) wsum[lane] = w;
+  }
+  __syncthreads();
+  const int32_t before = wid == 0 ? 0 : wsum[wid - 1];
+  *total = wsum[NT / 32 - 1];
+  __syncthreads();
+  return before + incl - v;
+}
+
 __device__ __forceinline__ bool closed(const int32_t* gate) { return gate && *gate == 0; }
 
 __global__ void k_scan_partial(const int32_t* __restrict__ in, int32_t n,
@@ -251,8 +271,10 @@ __global__ void k_bin(DevState S) {
 // Per gated tissue, one block: exclusive scan of its bin counts into
 // starts, offset by the tissue's first particle, so each tissue's sorted
 // particles occupy its own slots [pbase, pbase + n). Each tissue's bins end
-// with a sentinel entry that receives the end offset.
-__global__ void k_scan_tissue(DevState S) {
+// with a sentinel entry that receives the end offset. 1024 threads scan
+// 8192 bins per tile.
+constexpr int kTissueScanThreads = 1024;
+__global__ void __launch_bounds__(kTissueScanThreads) k_scan_tissue(DevState S) {
   pdl_entry();
   count_launch(S.launches);
   const int32_t cnt = S.rl_count[0];
@@ -262,7 +284,8 @@ __global__ void k_scan_tissue(DevState S) {
     const int32_t* in = S.counts + T.binbase;
     int32_t* out = S.starts + T.binbase;
     int32_t carry = T.pbase;
-    for (int32_t base = 0; base < nb; base += kScanTile) {
+    constexpr int32_t kTile = kTissueScanThreads * kScanItems;
+    for (int32_t base = 0; base < nb; base += kTile) {
       const int32_t b0 = base + threadIdx.x * kScanItems;
       int32_t v[kScanItems];
       int32_t sum = 0;
@@ -272,7 +295,7 @@ __global__ void k_scan_tissue(DevState S) {
         sum += v[q];
       }
       int32_t tot;
-      int32_t run = carry + block_excl_scan(sum, &tot);
+      int32_t run = carry + block_excl_scan_n<kTissueScanThreads>(sum, &tot);
 #pragma unroll
       for (int q = 0; q < kScanItems; ++q) {
         if (b0 + q < nb) out[b0 + q] = run;
@@ -311,14 +334,30 @@ __global__ void k_binsort(DevState S) {
     const int32_t s0 = S.starts[b], s1 = S.starts[b + 1];
     if (s1 <= s0) continue;
     S.counts[b] = 0;  // ready for the next binning
-    for (int32_t s = s0 + 1; s < s1; ++s) {
-      const uint32_t v = S.skey[s];
-      int32_t q = s - 1;
-      while (q >= s0 && S.skey[q] > v) {
-        S.skey[q + 1] = S.skey[q];
-        --q;
+    constexpr int kLocal = 24;  // a bin holds about 8 particles at unit density
+    if (s1 - s0 <= kLocal) {
+      uint32_t key[kLocal];
+      const int m = s1 - s0;
+      for (int k = 0; k < m; ++k) {
+        const uint32_t v = S.skey[s0 + k];
+        int q = k - 1;
+        while (q >= 0 && key[q] > v) {
+          key[q + 1] = key[q];
+          --q;
+        }
+        key[q + 1] = v;
       }
-      S.skey[q + 1] = v;
+      for (int k = 0; k < m; ++k) S.skey[s0 + k] = key[k];
+    } else {
+      for (int32_t s = s0 + 1; s < s1; ++s) {
+        const uint32_t v = S.skey[s];
+        int32_t q = s - 1;
+        while (q >= s0 && S.skey[q] > v) {
+          S.skey[q + 1] = S.skey[q];
+          --q;
+        }
+        S.skey[q + 1] = v;
+      }
     }
     for (int32_t s = s0; s < s1; ++s) {
       const uint32_t gi = S.skey[s];
@@ -1097,8 +1136,8 @@ void launch_rebuild(const DevState& S, const Range& r, const ScanScratch&,
   timer_end(tm, KC_REBUILD_BIN, s);
   timer_begin(tm, KC_REBUILD_SCAN, s);
   const int nt = r.t1 - r.t0;
-  launch_pdl(k_scan_tissue, nt < lc.num_sms * 4 ? (nt > 0 ? nt : 1) : lc.num_sms * 4, kScanThreads, s,
-             S);
+  launch_pdl(k_scan_tissue, nt < lc.num_sms * 4 ? (nt > 0 ? nt : 1) : lc.num_sms * 4,
+             kTissueScanThreads, s, S);
   timer_end(tm, KC_REBUILD_SCAN, s);
   timer_begin(tm, KC_REBUILD_SORT, s);
   launch_pdl(k_scatter, grid, B, s, S);
