@@ -671,8 +671,10 @@ __device__ __forceinline__ Vec3<R> tri_bending(const Off& off, int32_t j, int32_
 // :451-508), the lattice springs of _MEMB_interaction (:529-547, each
 // applied once by the higher index) and the wall (:287-294). The sum goes to
 // S.fmemb; k_step adds it.
+// The mixed path is held to 64 registers (four blocks per SM; a few bytes
+// spill) and runs about a quarter faster than at its natural 80.
 template <typename R>
-__global__ void __launch_bounds__(256) k_memb_force(DevState S, int32_t m0, int32_t m1) {
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 1) k_memb_force(DevState S, int32_t m0, int32_t m1) {
   pdl_entry();
   count_launch(S.launches);
   GRID_STRIDE(e, m0, m1) {
@@ -743,18 +745,31 @@ __global__ void __launch_bounds__(256) k_memb_force(DevState S, int32_t m0, int3
     }
     for (int k = 0; k < T.nadj; ++k) {
       const int32_t q = pb + lattice_link(T, j, k);
-      const double4 pq = S.pos_cur[q];
       const bool hi = i > q;
-      double dx, dy, dz;
-      pair_sep(p, pq, hi, T, dx, dy, dz);
-      const R d2 = R(dist_sq_exact(dx, dy, dz));
+      R dx, dy, dz, rs, d2;
+      if constexpr (sizeof(R) == 4) {
+        // mixed path: the FP32 copies, as for the bending stencil; the
+        // minimum-image FP32 difference is antisymmetric, so both ends of a
+        // link see opposite forces
+        const Vec3<float> o = off(q);
+        dx = -o.x;
+        dy = -o.y;
+        dz = -o.z;
+        rs = off.pf.w + S.posf_cur[q].w;
+        d2 = dx * dx + dy * dy + dz * dz;
+      } else {
+        const double4 pq = S.pos_cur[q];
+        pair_sep(p, pq, hi, T, dx, dy, dz);
+        rs = p.w + pq.w;
+        d2 = dist_sq_exact(dx, dy, dz);
+      }
       bool bad;
-      const R c = L.memb_memb(d2, R(p.w + pq.w), &bad);
+      const R c = L.memb_memb(d2, rs, &bad);
       if (bad) raise_error(S.status, E_MEMB_COEF_RANGE, hi ? i : q, hi ? q : i, double(c));
       const R sdt = R(dt) * c;
-      ax += double(sdt * R(dx));
-      ay += double(sdt * R(dy));
-      az += double(sdt * R(dz));
+      ax += double(sdt * dx);
+      ay += double(sdt * dy);
+      az += double(sdt * dz);
     }
     if (p.z < p.w) {
       const R z = R(p.z), rad = R(p.w);
