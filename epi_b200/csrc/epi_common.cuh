@@ -184,6 +184,22 @@ struct Laws {
     if (near(d2, rs)) return ljmain(d2, rs);
     return adhesion(d2, rs, both_old ? k_total : k_desmosome);
   }
+  // The same law in FP32 without a branch: both sides from one reciprocal
+  // square root, then a select, so lanes of a warp on either side of
+  // is_near do not run both paths one after the other.
+  __device__ __forceinline__ float aad_fused(float d2, float rs, bool both_old) const {
+    const float inv_d = rsqrtf(d2);
+    const float inv_d2 = inv_d * inv_d;
+    const float r2 = rs * rs;
+    const float s = r2 * inv_d2;
+    const float lj6 = s * s * s;
+    const float c_lj = eps4 * lj6 * (lj6 - 1.f) * inv_d2;
+    const float m1 = __fdividef(d2 * inv_d, rs) - 1.f;
+    const float k = both_old ? k_total : k_desmosome;
+    const float c_ad =
+        (m1 + 1.f > lj_thresh) ? 0.f : -k * inv_d * m1 * (1.f - __fdividef(m1 * m1, ljt1sq));
+    return d2 < r2 ? c_lj : c_ad;
+  }
   // CI_fix_mu_to_fix_mu, :154-162
   __device__ __forceinline__ R fixmu(R d2, R rs) const {
     if (near(d2, rs)) return ljmain(d2, rs);

@@ -879,7 +879,8 @@ struct Particle {
     R coef;
     if (kSimple) {
       const bool both_old = kOld && attr_old(a) && attr_old(__ldg(&S.attr[q]));
-      coef = L.aad(d2, rs, both_old);
+      if constexpr (sizeof(R) == 4) coef = L.aad_fused(d2, rs, both_old);
+      else coef = L.aad(d2, rs, both_old);
       if (fabs(coef) > R(1000)) raise_error(S.status, E_COEF_RANGE, i, q, double(coef));
     } else {
       const uint32_t aq = __ldg(&S.attr[q]);
