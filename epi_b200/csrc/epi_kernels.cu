@@ -408,25 +408,18 @@ __device__ __forceinline__ int window_ranges(double x, double R, double L, int32
 // iterates non-membrane cells, cell_connection.cpp:93). The window covers
 // every bin that can hold such a partner; the reference's fixed 5x5x5 window
 // is a superset for every pair it can connect (reach <= 1.2 * 3.2 < 2 * 2.0).
-// Candidates come out in bin order, deterministic after k_binsort.
-__global__ void k_cand_search(DevState S) {
-  pdl_entry();
-  count_launch(S.launches);
-  // One warp per gated particle: the lanes stride the contiguous slots of
-  // each bin column, and ballots keep the candidates in slot order.
-  constexpr double kInvAG = 1.0 / kAreaGrid;
-  const int32_t cnt = S.rl_count[0];
-  if (cnt == 0) return;
-  const int32_t ngated = S.rl_ppre[cnt];
-  const int lane = threadIdx.x & 31;
-  const unsigned lt_mask = (1u << lane) - 1u;
-  const int32_t warps = (gridDim.x * blockDim.x) >> 5;
-  for (int32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ngated; g += warps) {
-    int32_t t;
-    const int32_t i = gated_particle(S, cnt, g, &t);
-    const uint32_t a = S.attr[i];
-    const TissueDev& T = S.tissues[t];
-    const bool memb_i = attr_state(a) == ST_MEMB;
+// Candidates come out in column order (x ranges outer, y ranges inner), slot
+// order within a column: deterministic after k_binsort.
+struct SearchWindow {
+  int32_t xlo[2], xhi[2], ylo[2], yhi[2];
+  int nxr, nyr;
+  int32_t z0, z1;
+  float px, py, pz, pw, flx, fly, fhx, fhy, flt, fskin;
+  bool memb_i;
+
+  __device__ __forceinline__ SearchWindow(const DevState& S, const TissueDev& T, int32_t i) {
+    constexpr double kInvAG = 1.0 / kAreaGrid;
+    memb_i = attr_state(S.attr[i]) == ST_MEMB;
     const double4 p = S.pos_cur[i];
     const double lt = T.P.lj_thresh;
     const double skin = S.skin;
@@ -434,59 +427,166 @@ __global__ void k_cand_search(DevState S) {
     // float coordinates up to the box size (and the window widens with it).
     const double margin = 1e-4 + 5e-7 * (T.lx > T.ly ? T.lx : T.ly) + 5e-7 * T.lz;
     const double R = lt * (p.w + (memb_i ? T.rmax_nm : T.rmax)) + skin + margin + 1e-6;
-    int32_t xlo[2], xhi[2], ylo[2], yhi[2];
-    const int nxr = window_ranges(p.x, R, T.lx, T.anx, xlo, xhi);
-    const int nyr = window_ranges(p.y, R, T.ly, T.any, ylo, yhi);
-    int32_t z0 = (int32_t)floor((p.z - R) * kInvAG) - 1;
-    int32_t z1 = (int32_t)floor((p.z + R) * kInvAG) + 1;
+    nxr = window_ranges(p.x, R, T.lx, T.anx, xlo, xhi);
+    nyr = window_ranges(p.y, R, T.ly, T.any, ylo, yhi);
+    // z bins are floor(max(z, 0) / AG) (ref_bin); the margin in R covers the
+    // multiply-for-divide rounding, so [z - R, z + R] needs no extra bins
+    z0 = (int32_t)floor((p.z - R) * kInvAG);
+    z1 = (int32_t)floor((p.z + R) * kInvAG);
     z0 = z0 < 0 ? 0 : (z0 > T.anz - 1 ? T.anz - 1 : z0);
     z1 = z1 < 0 ? 0 : (z1 > T.anz - 1 ? T.anz - 1 : z1);
-    const float px = (float)p.x, py = (float)p.y, pz = (float)p.z, pw = (float)p.w;
-    const float flx = (float)T.lx, fly = (float)T.ly, fhx = 0.5f * flx, fhy = 0.5f * fly;
-    const float flt = (float)lt, fskin = (float)(skin + margin);
-    const int32_t cap = S.max_cand;
-    const int64_t N = S.n_total;
+    px = (float)p.x;
+    py = (float)p.y;
+    pz = (float)p.z;
+    pw = (float)p.w;
+    flx = (float)T.lx;
+    fly = (float)T.ly;
+    fhx = 0.5f * flx;
+    fhy = 0.5f * fly;
+    flt = (float)lt;
+    fskin = (float)(skin + margin);
+  }
+  // Is the particle in slot s (key, FP32 copy q) a candidate of i?
+  __device__ __forceinline__ bool hit(int32_t i, uint32_t key, const float4& q) const {
+    const int32_t j = (int32_t)(key & 0x7fffffffu);
+    if (j == i || (memb_i && (key >> 31))) return false;
+    float dx = px - q.x, dy = py - q.y;
+    dx = dx > fhx ? dx - flx : (dx <= -fhx ? dx + flx : dx);
+    dy = dy > fhy ? dy - fly : (dy <= -fhy ? dy + fly : dy);
+    const float dz = pz - q.z;
+    const float reach = flt * (pw + q.w) + fskin;
+    return dx * dx + dy * dy + dz * dz <= reach * reach;
+  }
+};
+
+__device__ __forceinline__ void finish_search(const DevState& S, int32_t i, int32_t count) {
+  const int32_t cap = S.max_cand;
+  if (count > cap) raise_error(S.status, E_LIST_OVERFLOW, i, -1, (double)count);
+  S.ncand[i] = count < cap ? count : cap;
+  const double4 p = S.pos_cur[i];
+  S.bpos[i] = make_float4((float)p.x, (float)p.y, (float)p.z, 0.f);
+}
+
+// Few gated particles (a tissue or two): one warp per particle, so the GPU
+// has work for all its warps. Each lane fetches the slot range of one bin
+// column; a warp scan lays the ranges end to end, the warp sweeps the
+// concatenation 32 slots at a time, and ballots keep the slot order.
+__device__ __forceinline__ void cand_search_warps(const DevState& S, int32_t cnt,
+                                                  int32_t ngated) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  const int32_t warps = (gridDim.x * blockDim.x) >> 5;
+  const int32_t cap = S.max_cand;
+  const int64_t N = S.n_total;
+  for (int32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ngated; g += warps) {
+    int32_t t;
+    const int32_t i = gated_particle(S, cnt, g, &t);
+    const TissueDev& T = S.tissues[t];
+    const SearchWindow W(S, T, i);
+    const int32_t nx0 = W.xhi[0] - W.xlo[0] + 1, ny0 = W.yhi[0] - W.ylo[0] + 1;
+    const int32_t ncx = nx0 + (W.nxr > 1 ? W.xhi[1] - W.xlo[1] + 1 : 0);
+    const int32_t ncy = ny0 + (W.nyr > 1 ? W.yhi[1] - W.ylo[1] + 1 : 0);
+    const int32_t ncol = ncx * ncy;  // column c = cx * ncy + cy
     int32_t count = 0;
-    for (int xr = 0; xr < nxr; ++xr) {
-      for (int32_t bx = xlo[xr]; bx <= xhi[xr]; ++bx) {
-        for (int yr = 0; yr < nyr; ++yr) {
-          for (int32_t by = ylo[yr]; by <= yhi[yr]; ++by) {
-            const int32_t col = T.binbase + (bx * T.any + by) * T.anz;
-            const int32_t s_lo = S.starts[col + z0], s_hi = S.starts[col + z1 + 1];
-            for (int32_t base = s_lo; base < s_hi; base += 32) {
-              const int32_t s = base + lane;
-              bool hit = false;
-              int32_t j = 0;
-              if (s < s_hi) {
-                const uint32_t key = S.skey[s];
-                j = (int32_t)(key & 0x7fffffffu);
-                if (j != i && !(memb_i && (key >> 31))) {
-                  const float4 q = S.spos[s];
-                  float dx = px - q.x, dy = py - q.y;
-                  dx = dx > fhx ? dx - flx : (dx <= -fhx ? dx + flx : dx);
-                  dy = dy > fhy ? dy - fly : (dy <= -fhy ? dy + fly : dy);
-                  const float dz = pz - q.z;
-                  const float reach = flt * (pw + q.w) + fskin;
-                  hit = dx * dx + dy * dy + dz * dz <= reach * reach;
+    for (int32_t c0 = 0; c0 < ncol; c0 += 32) {
+      const int32_t c = c0 + lane;
+      int32_t lo = 0, len = 0;
+      if (c < ncol) {
+        const int32_t cx = c / ncy, cy = c - cx * ncy;
+        const int32_t bx = cx < nx0 ? W.xlo[0] + cx : W.xlo[1] + (cx - nx0);
+        const int32_t by = cy < ny0 ? W.ylo[0] + cy : W.ylo[1] + (cy - ny0);
+        const int32_t col = T.binbase + (bx * T.any + by) * T.anz;
+        lo = S.starts[col + W.z0];
+        len = S.starts[col + W.z1 + 1] - lo;
+      }
+      const int32_t incl = warp_incl_scan(len);
+      const int32_t excl = incl - len;
+      const int32_t total = __shfl_sync(0xffffffffu, incl, 31);
+      for (int32_t base = 0; base < total; base += 32) {
+        const int32_t f = base + lane;
+        // the last column whose range starts at or before f (k + step <= 31)
+        int32_t k = 0;
+#pragma unroll
+        for (int32_t step = 16; step > 0; step >>= 1) {
+          const int32_t e = __shfl_sync(0xffffffffu, excl, k + step);
+          if (e <= f) k += step;
+        }
+        const int32_t s = __shfl_sync(0xffffffffu, lo, k) + (f - __shfl_sync(0xffffffffu, excl, k));
+        bool hit = false;
+        uint32_t key = 0;
+        if (f < total) {
+          key = S.skey[s];
+          hit = W.hit(i, key, S.spos[s]);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+          const int32_t kk = count + __popc(m & lt_mask);
+          if (kk < cap) S.cand[(int64_t)kk * N + i] = (int32_t)(key & 0x7fffffffu);
+        }
+        count += __popc(m);
+      }
+    }
+    if (lane == 0) finish_search(S, i, count);
+  }
+}
+
+// Many gated particles: one thread per particle. A particle sweeps about a
+// hundred slots (bins of 2.0 hold about six particles), four at a time so
+// their loads overlap; a warp keeps 32 particles in flight and writes the
+// column-major candidate rows coalesced.
+__device__ __forceinline__ void cand_search_threads(const DevState& S, int32_t cnt,
+                                                    int32_t ngated) {
+  const int64_t N = S.n_total;
+  const int32_t cap = S.max_cand;
+  for (int32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ngated;
+       g += gridDim.x * blockDim.x) {
+    int32_t t;
+    const int32_t i = gated_particle(S, cnt, g, &t);
+    const TissueDev& T = S.tissues[t];
+    const SearchWindow W(S, T, i);
+    const int32_t any = T.any, anz = T.anz, binbase = T.binbase;
+    int32_t count = 0;
+    for (int xr = 0; xr < W.nxr; ++xr) {
+      for (int32_t bx = W.xlo[xr]; bx <= W.xhi[xr]; ++bx) {
+        for (int yr = 0; yr < W.nyr; ++yr) {
+          for (int32_t by = W.ylo[yr]; by <= W.yhi[yr]; ++by) {
+            const int32_t col = binbase + (bx * any + by) * anz;
+            const int32_t s_hi = S.starts[col + W.z1 + 1];
+            for (int32_t s = S.starts[col + W.z0]; s < s_hi; s += 4) {
+              uint32_t key[4];
+              float4 q[4];
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                key[u] = s + u < s_hi ? S.skey[s + u] : 0u;
+                q[u] = s + u < s_hi ? S.spos[s + u] : make_float4(0.f, 0.f, 0.f, 0.f);
+              }
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                if (s + u < s_hi && W.hit(i, key[u], q[u])) {
+                  if (count < cap) S.cand[(int64_t)count * N + i] = (int32_t)(key[u] & 0x7fffffffu);
+                  ++count;
                 }
               }
-              const unsigned m = __ballot_sync(0xffffffffu, hit);
-              if (hit) {
-                const int32_t k = count + __popc(m & lt_mask);
-                if (k < cap) S.cand[(int64_t)k * N + i] = j;
-              }
-              count += __popc(m);
             }
           }
         }
       }
     }
-    if (lane == 0) {
-      if (count > cap) raise_error(S.status, E_LIST_OVERFLOW, i, -1, (double)count);
-      S.ncand[i] = count < cap ? count : cap;
-      S.bpos[i] = make_float4((float)p.x, (float)p.y, (float)p.z, 0.f);
-    }
+    finish_search(S, i, count);
   }
+}
+
+// Below this many gated particles the warp-per-particle search is faster.
+constexpr int32_t kWarpSearchMax = 48 * 1024;
+
+__global__ void k_cand_search(DevState S) {
+  pdl_entry();
+  count_launch(S.launches);
+  const int32_t cnt = S.rl_count[0];
+  if (cnt == 0) return;
+  const int32_t ngated = S.rl_ppre[cnt];
+  if (ngated < kWarpSearchMax) cand_search_warps(S, cnt, ngated);
+  else cand_search_threads(S, cnt, ngated);
 }
 
 __global__ void k_gate_clear(DevState S, int32_t clear_any) {
