@@ -511,7 +511,8 @@ def main():
                         (args.skin if args.skin is not None else 0.1)),
                "variant": tuned["variant"] if tuned else (args.variant or 1),
                "autotune": tuned,
-               "tissue_rebuilds_per_step": rebuilds_timed / max(args.steps, 1) / len(mine),
+               "tissues_rebuilt_per_step": rebuilds_timed / max(args.steps, 1),
+               "rebuilt_fraction_per_step": rebuilds_timed / max(args.steps, 1) / len(mine),
                "launch": "one graph launch per run (device WHILE loop over a 2-step body)",
                "l2": "inputs larger than L2 (working set >> 126 MB)"
                if n_all * 200 > 126e6 else "working set fits in L2 (no flush)",
