@@ -39,7 +39,7 @@ EXPORTED = [
     "epi_params_default", "epi_config_default", "epi_strerror", "epi_create", "epi_destroy",
     "epi_upload", "epi_connect", "epi_interact_commit", "epi_step", "epi_step_graph",
     "epi_step_per_tissue", "epi_sync", "epi_num_particles", "epi_download_positions",
-    "epi_upload_positions", "epi_get_connections", "epi_get_dermis", "epi_error_info",
+    "epi_upload_positions", "epi_step_host", "epi_get_connections", "epi_get_dermis", "epi_error_info",
     "epi_stream", "epi_rebuild_count", "epi_launch_count", "epi_time_kernels", "epi_autotune",
     "epi_field_init",
     "epi_field_step", "epi_field_get", "epi_field_set_ext", "epi_adjoint", "epi_connect_noalloc",
@@ -121,6 +121,7 @@ def lib():
         L.epi_num_particles.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         L.epi_download_positions.argtypes = [vp, _dp, _dp, _dp]
         L.epi_upload_positions.argtypes = [vp, _dp, _dp, _dp]
+        L.epi_step_host.argtypes = [vp, _dp, _dp, _dp, _dp, _dp, _dp]
         L.epi_get_connections.argtypes = [vp, _ip, _ip, ctypes.c_int64,
                                           ctypes.POINTER(ctypes.c_int64)]
         L.epi_get_dermis.argtypes = [vp, _ip]
@@ -287,6 +288,21 @@ class Context:
         _check(lib().epi_upload_positions(self._h, _ptr(x, ctypes.c_double),
                                           _ptr(y, ctypes.c_double), _ptr(z, ctypes.c_double)),
                "epi_upload_positions")
+
+    def step_host(self, pos_in, pos_out=None):
+        """epi_step_host: one step of a batch whose positions are in host
+        memory (x, y, z arrays in, new positions out; the same arrays may be
+        given for both). Pinned host arrays let the copies overlap."""
+        x, y, z = pos_in
+        for a in (x, y, z):
+            if a.dtype != np.float64 or not a.flags.c_contiguous or a.shape != (self.n,):
+                raise ValueError("positions must be contiguous float64 arrays of n entries")
+        if pos_out is None:
+            pos_out = (np.empty(self.n), np.empty(self.n), np.empty(self.n))
+        ox, oy, oz = pos_out
+        _check(lib().epi_step_host(self._h, *(_ptr(a, ctypes.c_double) for a in (x, y, z, ox, oy, oz))),
+               "epi_step_host")
+        return pos_out
 
     def connections(self):
         n = self.n

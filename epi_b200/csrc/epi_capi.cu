@@ -51,6 +51,9 @@ void timer_end(Timer* tm, int cls, cudaStream_t s) {
 
 namespace {
 
+// epi_step_host splits the batch into at most this many groups of tissues.
+constexpr int kHostStepGroups = 8;
+
 // Host-side bookkeeping of one tissue in the batch.
 struct TissueHost {
   int32_t prep_m;  // offset of its membrane particles in the prep list
@@ -103,6 +106,10 @@ struct epi_ctx {
   int32_t* rl = nullptr;    // rebuild work list: [count | list (T) | ppre (T+1) | bpre (T+1)]
   int32_t* prep = nullptr;
   double* stage = nullptr;        // 3n doubles: x | y | z for host transfers
+  // epi_step_host: copy streams, per-chunk events, the outbound staging (3n)
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  std::vector<cudaEvent_t> ev_in, ev_done;
+  double* stage_out = nullptr;
   DevStatus* status = nullptr;
   DevStatus* status_h = nullptr;  // pinned
   unsigned long long* rebuilds = nullptr;
@@ -176,7 +183,7 @@ void free_buffers(epi_ctx* c) {
   void* ptrs[] = {c->tissues, c->pos[0], c->pos[1], c->posf[0], c->posf[1], c->attr, c->pair, c->spr, c->dermis,
                   c->cand, c->ncand, c->bpos, c->nbr, c->nn, c->fmemb, c->bin,
                   c->rank, c->counts, c->starts, c->skey, c->spos, c->gate, c->rl, c->prep,
-                  c->scan.partial, c->stage};
+                  c->scan.partial, c->stage, c->stage_out};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   c->tissues = nullptr;
@@ -187,7 +194,7 @@ void free_buffers(epi_ctx* c) {
   c->nbr = nullptr; c->nn = nullptr; c->fmemb = nullptr;
   c->bin = nullptr; c->rank = nullptr; c->counts = nullptr; c->starts = nullptr;
   c->skey = nullptr; c->spos = nullptr; c->gate = nullptr; c->rl = nullptr; c->prep = nullptr;
-  c->scan.partial = nullptr; c->stage = nullptr;
+  c->scan.partial = nullptr; c->stage = nullptr; c->stage_out = nullptr;
   c->loaded = false;
   c->lists_fresh = false;
 }
@@ -645,6 +652,10 @@ void epi_destroy(epi_ctx* ctx) {
   if (ctx->loop_left) cudaFree(ctx->loop_left);
   if (ctx->launches) cudaFree(ctx->launches);
   if (ctx->status_h) cudaFreeHost(ctx->status_h);
+  for (cudaEvent_t e : ctx->ev_in) cudaEventDestroy(e);
+  for (cudaEvent_t e : ctx->ev_done) cudaEventDestroy(e);
+  if (ctx->copy_in) cudaStreamDestroy(ctx->copy_in);
+  if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
   if (ctx->side) cudaStreamDestroy(ctx->side);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -1282,6 +1293,94 @@ int epi_upload_positions(epi_ctx* c, const double* x, const double* y, const dou
   launch_gate_check(S, c->lc, c->stream);
   c->lists_fresh = false;
   launch_rebuild(S, whole(c), c->scan, c->lc, c->stream, nullptr);
+  return check_status(c);
+  EPI_GUARD_END
+}
+
+// One step of a batch whose positions live in host memory: what
+// epi_upload_positions + epi_interact_commit + epi_download_positions do,
+// split into groups of whole tissues of about equal particle count. A
+// group's inbound copies, its kernels and its outbound copies run on three
+// streams, so one group's copies overlap the next group's copies in the
+// other direction and the compute between them. Tissues never interact, so
+// the result equals the three calls'. Returns once the new positions are in
+// x_out, y_out, z_out (which may be the input arrays).
+int epi_step_host(epi_ctx* c, const double* x_in, const double* y_in, const double* z_in,
+                  double* x_out, double* y_out, double* z_out) {
+  if (!c || !x_in || !y_in || !z_in || !x_out || !y_out || !z_out) return EPI_ERR_INVALID_ARG;
+  if (!c->loaded) return EPI_ERR_STATE;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  const int64_t n = c->n;
+  if (!c->copy_in)
+    EPI_CUDA(cudaStreamCreateWithFlags(&c->copy_in, cudaStreamNonBlocking));
+  if (!c->copy_out)
+    EPI_CUDA(cudaStreamCreateWithFlags(&c->copy_out, cudaStreamNonBlocking));
+  if (!c->stage_out && (rc = dev_alloc(&c->stage_out, 3 * (size_t)n))) return rc;
+  // groups: whole tissues, split at multiples of n / K particles
+  const int K = std::min(kHostStepGroups, c->ntissues);
+  while ((int)c->ev_in.size() < K) {
+    cudaEvent_t a, b;
+    EPI_CUDA(cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
+    EPI_CUDA(cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
+    c->ev_in.push_back(a);
+    c->ev_done.push_back(b);
+  }
+  std::vector<int> split{0};
+  for (int t = 0, k = 1; t < c->ntissues && k < K; ++t) {
+    const TissueDev& T = c->tissues_h[t];
+    if ((int64_t)(T.pbase + T.n) * K >= (int64_t)k * n && t + 1 < c->ntissues) {
+      split.push_back(t + 1);
+      ++k;
+    }
+  }
+  split.push_back(c->ntissues);
+  double* in = c->stage;
+  double* out = c->stage_out;
+  // the compute stream's earlier work (a previous step) precedes the copies
+  EPI_CUDA(cudaEventRecord(c->ev_done[0], c->stream));
+  EPI_CUDA(cudaStreamWaitEvent(c->copy_in, c->ev_done[0], 0));
+  EPI_CUDA(cudaStreamWaitEvent(c->copy_out, c->ev_done[0], 0));
+  const int cur = c->cur;
+  const DevState S = make_state(c, cur);
+  const DevState Snew = make_state(c, cur ^ 1);
+  for (size_t g = 0; g + 1 < split.size(); ++g) {
+    const int t0 = split[g], t1 = split[g + 1];
+    const TissueDev& A = c->tissues_h[t0];
+    const TissueDev& B = c->tissues_h[t1 - 1];
+    const int32_t p0 = A.pbase, p1 = B.pbase + B.n;
+    const size_t off = (size_t)p0, bytes = sizeof(double) * (size_t)(p1 - p0);
+    const double* src[3] = {x_in, y_in, z_in};
+    for (int k = 0; k < 3; ++k)
+      EPI_CUDA(cudaMemcpyAsync(in + k * n + off, src[k] + off, bytes, cudaMemcpyHostToDevice,
+                               c->copy_in));
+    EPI_CUDA(cudaEventRecord(c->ev_in[g], c->copy_in));
+    EPI_CUDA(cudaStreamWaitEvent(c->stream, c->ev_in[g], 0));
+    launch_pack_gate(S, in, in + n, in + 2 * n, p0, p1, c->lc, c->stream);
+    const Range r{p0, p1, A.binbase, B.binbase + B.anx * B.any * B.anz + 1, t0, t1};
+    launch_rebuild(S, r, c->scan, c->lc, c->stream, nullptr);
+    const TissueHost& HA = c->thost[t0];
+    const TissueHost& HB = c->thost[t1 - 1];
+    launch_prepass(S, HA.prep_m, HB.prep_m + B.nmemb, c->nprep_memb + HA.prep_f,
+                   c->nprep_memb + HB.prep_f + HB.nfm, c->cfg.precision, c->lc, c->stream,
+                   nullptr);
+    launch_step(S, r, c->cfg.precision, c->lc, c->stream, nullptr);
+    launch_unpack_range(Snew, out, out + n, out + 2 * n, p0, p1, c->lc, c->stream);
+    EPI_CUDA(cudaEventRecord(c->ev_done[g], c->stream));
+    EPI_CUDA(cudaStreamWaitEvent(c->copy_out, c->ev_done[g], 0));
+    double* dst[3] = {x_out, y_out, z_out};
+    for (int k = 0; k < 3; ++k)
+      EPI_CUDA(cudaMemcpyAsync(dst[k] + off, out + k * n + off, bytes, cudaMemcpyDeviceToHost,
+                               c->copy_out));
+  }
+  c->cur ^= 1;
+  c->posf_stale = false;
+  c->lists_fresh = false;
+  // later work on the compute stream waits for the outbound copies
+  EPI_CUDA(cudaEventRecord(c->ev_in[0], c->copy_out));
+  EPI_CUDA(cudaStreamWaitEvent(c->stream, c->ev_in[0], 0));
+  EPI_CUDA(cudaStreamSynchronize(c->copy_out));
   return check_status(c);
   EPI_GUARD_END
 }

@@ -1216,6 +1216,48 @@ __global__ void k_pack(DevState S, const double* x, const double* y, const doubl
   S.posf_nxt[i] = f;
 }
 
+// Particles [p0, p1) of a host step: positions from the staged host arrays
+// into both buffers and both FP32 copies (as k_pack), and the displacement
+// test of the candidate rows (as k_gate_check).
+__global__ void k_pack_gate(DevState S, const double* x, const double* y, const double* z,
+                            int32_t p0, int32_t p1) {
+  GRID_STRIDE(i, p0, p1) {
+    const double r = S.pos_cur[i].w;
+    const double4 p = make_double4(x[i], y[i], z[i], r);
+    if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z))
+      raise_error(S.status, E_NONFINITE, (int32_t)i, -1, p.z);
+    S.pos_cur[i] = p;
+    S.pos_nxt[i] = p;
+    const float4 f = make_float4((float)p.x, (float)p.y, (float)p.z, (float)r);
+    S.posf_cur[i] = f;
+    S.posf_nxt[i] = f;
+    const uint32_t t = attr_tissue(S.attr[i]);
+    const TissueDev& T = S.tissues[t];
+    const float4 b = S.bpos[i];
+    double ex = p.x - (double)b.x, ey = p.y - (double)b.y;
+    if (ex > T.hlx) ex -= T.lx;
+    else if (ex < -T.hlx) ex += T.lx;
+    if (ey > T.hly) ey -= T.ly;
+    else if (ey < -T.hly) ey += T.ly;
+    const double ez = p.z - (double)b.z;
+    const double lim = 0.5 * S.skin - 1e-3;
+    if (!(ex * ex + ey * ey + ez * ez <= lim * lim)) {
+      S.gate[1 + t] = 1;
+      S.gate[0] = 1;
+    }
+  }
+}
+
+__global__ void k_unpack_range(DevState S, double* x, double* y, double* z, int32_t p0,
+                               int32_t p1) {
+  GRID_STRIDE(i, p0, p1) {
+    const double4 p = S.pos_cur[i];
+    x[i] = p.x;
+    y[i] = p.y;
+    z[i] = p.z;
+  }
+}
+
 __global__ void k_posf(DevState S) {
   GRID_STRIDE(i, 0, S.n_total) {
     const double4 p = S.pos_cur[i];
@@ -1363,6 +1405,15 @@ void launch_dermis_local(const DevState& S, int32_t* out, int32_t n, cudaStream_
 void launch_unpack_positions(const DevState& S, double* x, double* y, double* z, int32_t n,
                              cudaStream_t s) {
   if (n > 0) k_unpack<<<blocks_for(n, 256), 256, 0, s>>>(S, x, y, z, n);
+}
+void launch_pack_gate(const DevState& S, const double* x, const double* y, const double* z,
+                      int32_t p0, int32_t p1, const LaunchCfg& lc, cudaStream_t s) {
+  if (p1 > p0) k_pack_gate<<<stride_blocks(p1 - p0, lc.block, lc), lc.block, 0, s>>>(S, x, y, z, p0, p1);
+}
+void launch_unpack_range(const DevState& S, double* x, double* y, double* z, int32_t p0,
+                         int32_t p1, const LaunchCfg& lc, cudaStream_t s) {
+  if (p1 > p0)
+    k_unpack_range<<<stride_blocks(p1 - p0, lc.block, lc), lc.block, 0, s>>>(S, x, y, z, p0, p1);
 }
 void launch_pack_positions(const DevState& S, const double* x, const double* y,
                            const double* z, int32_t n, cudaStream_t s) {

@@ -78,6 +78,12 @@ void launch_unpack_positions(const DevState& S, double* x, double* y, double* z,
                              cudaStream_t s);
 void launch_pack_positions(const DevState& S, const double* x, const double* y,
                            const double* z, int32_t n, cudaStream_t s);
+// Host step, particles [p0, p1): staged positions into both buffers with the
+// displacement test (pack_gate); positions of S.pos_cur out to staging.
+void launch_pack_gate(const DevState& S, const double* x, const double* y, const double* z,
+                      int32_t p0, int32_t p1, const LaunchCfg& lc, cudaStream_t s);
+void launch_unpack_range(const DevState& S, double* x, double* y, double* z, int32_t p0,
+                         int32_t p1, const LaunchCfg& lc, cudaStream_t s);
 // FP32 copies of the current positions (S.posf_cur from S.pos_cur).
 void launch_posf(const DevState& S, const LaunchCfg& lc, cudaStream_t s);
 

@@ -164,6 +164,16 @@ int epi_num_particles(const epi_ctx* ctx, int64_t* n);
 int epi_download_positions(epi_ctx* ctx, double* x, double* y, double* z);
 /* Overwrites positions (both buffers, like dual_double::_set) and re-connects. */
 int epi_upload_positions(epi_ctx* ctx, const double* x, const double* y, const double* z);
+/* One mechanics step of a batch whose positions live in host memory: the
+ * loop body the drop-in runs per step (connect_cell, then cell_interaction,
+ * pos_copy and cell_pos_periodic_fix; epi5_MT/proc.cpp:22-32), equal to
+ * epi_upload_positions(in) + epi_interact_commit + epi_download_positions(out).
+ * The batch is split into groups of whole tissues whose host copies in both
+ * directions overlap the other groups' kernels. Blocks until the new
+ * positions are in the out arrays; in and out may be the same arrays. Host
+ * memory should be pinned (page-locked) for the copies to overlap. */
+int epi_step_host(epi_ctx* ctx, const double* x_in, const double* y_in, const double* z_in,
+                  double* x_out, double* y_out, double* z_out);
 /* Connection lists as CSR over all particles (offsets has n+1 entries). Each
  * row holds tissue-local indices sorted ascending; membrane rows include their
  * four lattice links, as connected_cell does (epi5_MT/cell.h:132). Writes at
