@@ -769,16 +769,11 @@ __device__ __forceinline__ Vec3<R> tri_bending(const Off& off, int32_t j, int32_
 // unit vectors of calc1 recomputed from the eleven lattice positions the
 // stencil reaches instead of being stored; triangular: tri_memb_bend,
 // :451-508), the lattice springs of _MEMB_interaction (:529-547, each
-// applied once by the higher index) and the wall (:287-294). The sum goes to
-// S.fmemb; k_step adds it.
-// The mixed path is held to 64 registers (four blocks per SM; a few bytes
-// spill) and runs about a quarter faster than at its natural 80.
+// applied once by the higher index) and the wall (:287-294), summed for
+// membrane particle i.
 template <typename R>
-__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 1) k_memb_force(DevState S, int32_t m0, int32_t m1) {
-  pdl_entry();
-  count_launch(S.launches);
-  GRID_STRIDE(e, m0, m1) {
-    const int32_t i = S.prep[e];
+__device__ __forceinline__ double3 memb_force(const DevState& S, int32_t i) {
+  {
     const TissueDev& T = S.tissues[attr_tissue(S.attr[i])];
     const Laws<R>& L = T.laws<R>();
     const double dt = T.P.dt;
@@ -878,7 +873,23 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 1) k_memb_force(DevS
       const R ljm = L.eps4 * lj6 * (lj6 - R(1)) / (distlj * distlj);
       az += double(R(dt) * ljm * R(2) * z);
     }
-    S.fmemb[i] = make_double4(ax, ay, az, 0.0);
+    return make_double3(ax, ay, az);
+  }
+}
+
+// The membrane sum of memb_force for the prep list's membrane particles
+// [m0, m1), into S.fmemb for k_step. Computing it inside k_step instead
+// spills the step kernel's registers and costs more than this launch. The
+// mixed path is held to 64 registers (four blocks per SM; a few bytes spill)
+// and runs about a quarter faster than at its natural 80.
+template <typename R>
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 1) k_memb_force(DevState S, int32_t m0, int32_t m1) {
+  pdl_entry();
+  count_launch(S.launches);
+  GRID_STRIDE(e, m0, m1) {
+    const int32_t i = S.prep[e];
+    const double3 f = memb_force<R>(S, i);
+    S.fmemb[i] = make_double4(f.x, f.y, f.z, 0.0);
   }
 }
 
