@@ -12,9 +12,12 @@ all ranks) x steps / device time.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload ensemble|c2|c3|c1] [--precision mixed|fp64]
 
-Under torchrun (N > 1) the tissues are sharded across ranks (no collective on
-the data path); the timed region is bracketed by barriers and the max over
-ranks is reported.
+Under torchrun (N > 1) the ensemble scales weakly: the job is N x 512
+tissues of the same generator (the first 512 are the 1-GPU batch), balanced
+over the ranks so each holds about 512, with no collective on the data path;
+the timed region is bracketed by barriers and the max over ranks is
+reported. A single-tissue workload (c1-c3) runs as N replicas, one per
+rank (one tissue is not split).
 
 --impl reference times the reference's own CPU implementation (epi5_MT built
 by oracle/build_ref.py, OpenMP TBB stand-in, all host threads) on a bounded
@@ -56,6 +59,30 @@ def workload(name: str, tissues: int = 512):
     if name == "c1":
         return [T.config1()], "single tissue 16x16 membrane + 512 cells (config 1)"
     raise SystemExit(f"unknown workload {name}")
+
+
+def rank_workload(name: str, tissues: int, world: int, rank: int):
+    """This rank's tissues of the job: (mine, particles of the whole job,
+    tissues of the whole job, description, the whole tissue list or None).
+
+    Ensemble, N > 1: weak scaling. The job is N x `tissues` tissues of the
+    same generator (the first `tissues` are the 1-GPU batch), balanced over
+    the ranks by shard_tissues; each rank generates only its own. Single
+    tissue, N > 1: one replica per rank. N = 1: the workload itself."""
+    if name == "ensemble" and world > 1:
+        nt = tissues * world
+        specs = T.config4_specs(n_tissues=nt)
+        sizes = [side * side * (1 + layers) for side, layers, _ in specs]
+        shards = shard_tissues(sizes, world)
+        mine = T.config4(n_tissues=nt, indices=shards[rank])
+        desc = (f"batched ensemble, {tissues} tissues per GPU: {nt} tissues, "
+                f"side {{16..64}}, 2-8 layers (config 4)")
+        return mine, sum(sizes), nt, desc, None
+    every, desc = workload(name, tissues)
+    if world > 1:
+        return (every, world * sum(t.n for t in every), world * len(every),
+                f"{desc}, one replica per GPU", every)
+    return every, sum(t.n for t in every), len(every), desc, every
 
 
 # --------------------------------------------------------------------------
@@ -350,11 +377,9 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    tissues, desc = workload(args.workload, args.tissues)
-    shards = shard_tissues([t.n for t in tissues], world)
-    mine = [tissues[i] for i in shards[rank]]
+    mine, n_all, n_tissues_all, desc, tissues = rank_workload(args.workload, args.tissues,
+                                                               world, rank)
     n_mine = sum(t.n for t in mine)
-    n_all = sum(t.n for t in tissues)
     prec = capi.EPI_PREC_MIXED if args.precision == "mixed" else capi.EPI_PREC_FP64
 
     ctx = capi.Context(precision=prec, max_conn=64, device=local, skin=args.skin,
@@ -523,7 +548,7 @@ def main():
                                           not args.no_cpu_baseline)
 
     if rank == 0:
-        cfg = {"workload": desc, "tissues": len(tissues), "particles": n_all,
+        cfg = {"workload": desc, "tissues": n_tissues_all, "particles": n_all,
                "mean_connections": kbar, "precision": args.precision,
                "skin": (tuned["skin"] if tuned else
                         (args.skin if args.skin is not None else 0.1)),
@@ -534,7 +559,10 @@ def main():
                "launch": "one graph launch per run (device WHILE loop over a 2-step body)",
                "l2": "inputs larger than L2 (working set >> 126 MB)"
                if n_all * 200 > 126e6 else "working set fits in L2 (no flush)",
-               "parallelism": f"tissue sharding x{world}" if world > 1 else "1 GPU"}
+               "parallelism": ("1 GPU" if world == 1 else
+                               f"{world} GPUs, tissue shards of the {world}x ensemble (weak)"
+                               if args.workload == "ensemble" else
+                               f"{world} GPUs, one replica each (weak)")}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

@@ -15,7 +15,7 @@ from __future__ import annotations
 
 import math
 from dataclasses import dataclass, field
-from typing import List, Optional
+from typing import List, Optional, Sequence
 
 import numpy as np
 
@@ -255,10 +255,12 @@ def config3(seed: int = 2) -> Tissue:
 C4_SIDES = (16, 24, 32, 48, 64)
 
 
-def config4(seed: int = 3, n_tissues: int = 512) -> List[Tissue]:
-    """Ensemble of independent tissues: side uniform in {16,24,32,48,64}, layers
-    uniform in 2..8, accepted when layers*side^2 is in [2048, 40000]; spring, LJ
-    epsilon and bending scale each log-uniform in [0.5, 2]."""
+def config4_specs(seed: int = 3, n_tissues: int = 512) -> List[tuple]:
+    """Per tissue of the ensemble: (side, layers, params), without positions.
+    Side uniform in {16,24,32,48,64}, layers uniform in 2..8, accepted when
+    layers*side^2 is in [2048, 40000]; spring, LJ epsilon and bending scale
+    each log-uniform in [0.5, 2]. A tissue has side^2 membrane particles and
+    layers*side^2 cells."""
     out = []
     for t in range(n_tissues):
         s = mix_seed(seed, t)
@@ -273,8 +275,20 @@ def config4(seed: int = 3, n_tissues: int = 512) -> List[Tissue]:
         sc = splitmix64_uniform(s, 3, start=draw)
         scale = np.exp(np.log(0.5) + sc * (np.log(2.0) - np.log(0.5)))
         p = Params().scaled(spring=float(scale[0]), eps=float(scale[1]), bend=float(scale[2]))
-        out.append(layered_tissue(side, layers, mix_seed(seed, t, 1), params=p, name=f"C4[{t}]"))
+        out.append((side, layers, p))
     return out
+
+
+def config4(seed: int = 3, n_tissues: int = 512,
+            indices: Optional[Sequence[int]] = None) -> List[Tissue]:
+    """Ensemble of independent tissues (config4_specs); `indices` selects
+    which of the n_tissues to generate (default: all), so a rank can build
+    only its own shard. Tissue t is the same whatever n_tissues is."""
+    specs = config4_specs(seed, n_tissues)
+    if indices is None:
+        indices = range(n_tissues)
+    return [layered_tissue(specs[t][0], specs[t][1], mix_seed(seed, t, 1), params=specs[t][2],
+                           name=f"C4[{t}]") for t in indices]
 
 
 def config5(seed: int = 4) -> Tissue:

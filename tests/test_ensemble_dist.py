@@ -97,3 +97,28 @@ def test_rank_that_leaves_is_detected_by_the_bounded_wait():
     assert not any(alive), "a rank hung"
     assert res.get(1) == "left"
     assert str(res.get(0, "")).startswith("error"), res
+
+
+def test_weak_scaling_job_per_rank():
+    """bench.py's N-GPU ensemble job: N x 512 tissues of the same generator,
+    balanced over the ranks, each rank generating only its own. The ranks'
+    tissues partition the job, the first 512 tissues are the 1-GPU batch,
+    and every rank holds about one GPU's worth (weak scaling)."""
+    import bench
+    world, per = 2, 64
+    one, n_one, nt_one, _, _ = bench.rank_workload("ensemble", per, 1, 0)
+    assert nt_one == per and n_one == sum(t.n for t in one)
+    parts = [bench.rank_workload("ensemble", per, world, r) for r in range(world)]
+    n_job = parts[0][1]
+    assert all(p[1] == n_job and p[2] == world * per for p in parts)
+    names = sorted(int(t.name[3:-1]) for p in parts for t in p[0])
+    assert names == list(range(world * per))
+    assert sum(t.n for p in parts for t in p[0]) == n_job
+    loads = [sum(t.n for t in p[0]) for p in parts]
+    assert max(loads) / (n_job / world) < 1.05
+    by_name = {t.name: t for p in parts for t in p[0]}
+    for t in one:
+        assert np.array_equal(by_name[t.name].x, t.x)
+    # a single tissue runs as one replica per rank
+    mine, n_job1, nt1, _, _ = bench.rank_workload("c1", per, world, 1)
+    assert len(mine) == 1 and nt1 == world and n_job1 == world * mine[0].n
