@@ -67,6 +67,9 @@ struct epi_ctx {
   epi_config cfg{};
   cudaStream_t stream = nullptr;
   cudaStream_t side = nullptr;  // captures the bodies of conditional graph nodes
+  // the membrane sums run on `aux` beside the candidate rebuild (fork / join)
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   LaunchCfg lc{148, 256, 0, 0, 0};
   bool loaded = false;
   bool lists_fresh = false;  // nbr / nn / dermis match the current positions
@@ -269,11 +272,39 @@ void ensure_posf(epi_ctx* c) {
   c->posf_stale = false;
 }
 
-// One reference step over the batch: [rebuild] -> prepass -> fused step.
+// The membrane sums read only positions, so they run on c->aux beside the
+// candidate rebuild (whose kernels are short and occupy few SMs): fork_memb
+// starts them after the work queued so far, join_memb makes the step kernel
+// wait for them. Recorded the same way inside a stream capture, the fork and
+// join become edges of the captured graph.
+cudaError_t fork_memb(epi_ctx* c, int cur, Timer* tm) {
+  if (c->nprep_memb == 0) return cudaSuccess;
+  cudaError_t e = cudaEventRecord(c->ev_fork, c->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(c->aux, c->ev_fork, 0);
+  if (e != cudaSuccess) return e;
+  launch_memb_force(make_state(c, cur), 0, c->nprep_memb, c->cfg.precision, c->lc, c->aux, tm);
+  return cudaEventRecord(c->ev_join, c->aux);
+}
+
+cudaError_t join_memb(epi_ctx* c) {
+  if (c->nprep_memb == 0) return cudaSuccess;
+  return cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+}
+
+// The dermis of FIX / MUSUME cells reads the candidate lists: after the rebuild.
+void dermis_all(epi_ctx* c, int cur, Timer* tm) {
+  launch_dermis(make_state(c, cur), c->nprep_memb, c->nprep, c->lc, c->stream, tm);
+}
+
+// One reference step over the batch: [rebuild] and the membrane sums side by
+// side, the dermis, then the fused step. Errors of the stream calls surface
+// at the next synchronising call.
 void enqueue_step(epi_ctx* c, int& cur, Timer* tm) {
   ensure_posf(c);
+  (void)fork_memb(c, cur, tm);
   launch_rebuild(make_state(c, cur), whole(c), c->scan, c->lc, c->stream, tm);
-  prepass_all(c, cur, tm);
+  dermis_all(c, cur, tm);
+  (void)join_memb(c);
   launch_step(make_state(c, cur), whole(c), c->cfg.precision, c->lc, c->stream, tm);
   cur ^= 1;
 }
@@ -338,9 +369,11 @@ cudaError_t capture_step_graph(epi_ctx* c, cudaGraphExec_t* out) {
     if (e == cudaSuccess) {
       int cur = c->cur;
       for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
-        e = capture_conditional_rebuild(c, cur);
+        e = fork_memb(c, cur, nullptr);
+        if (e == cudaSuccess) e = capture_conditional_rebuild(c, cur);
         if (e != cudaSuccess) break;
-        prepass_all(c, cur, nullptr);
+        dermis_all(c, cur, nullptr);
+        if ((e = join_memb(c)) != cudaSuccess) break;
         launch_step(make_state(c, cur), whole(c), c->cfg.precision, c->lc, c->stream, nullptr);
         cur ^= 1;
       }
@@ -349,7 +382,8 @@ cudaError_t capture_step_graph(epi_ctx* c, cudaGraphExec_t* out) {
       if (e == cudaSuccess) e = e_end;
     }
   }
-  if (e == cudaSuccess) e = cudaGraphInstantiate(out, g, 0);
+  // each captured kernel keeps its stream's priority
+  if (e == cudaSuccess) e = cudaGraphInstantiate(out, g, cudaGraphInstantiateFlagUseNodePriority);
   cudaGraphDestroy(g);
   return e;
 }
@@ -623,8 +657,20 @@ int epi_create(epi_ctx** out, const epi_config* cfg) {
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device) == cudaSuccess &&
       sms > 0)
     ctx->lc.num_sms = sms;
-  int rc = cuda_status(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  // The step sequence's stream gets the highest priority and the membrane
+  // sums' side stream the lowest, so the rebuild chain (the critical path
+  // of a step) takes SM slots first and the membrane blocks fill the rest.
+  int prio_least = 0, prio_greatest = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest);
+  int rc = cuda_status(
+      cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, prio_greatest));
   if (rc == EPI_OK) rc = cuda_status(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+  if (rc == EPI_OK)
+    rc = cuda_status(cudaStreamCreateWithPriority(&ctx->aux, cudaStreamNonBlocking, prio_least));
+  if (rc == EPI_OK)
+    rc = cuda_status(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+  if (rc == EPI_OK)
+    rc = cuda_status(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
   if (rc == EPI_OK) rc = dev_alloc(&ctx->status, 1);
   if (rc == EPI_OK) rc = cuda_status(cudaMallocHost((void**)&ctx->status_h, sizeof(DevStatus)));
   if (rc == EPI_OK) rc = cuda_status(cudaMemset(ctx->status, 0, sizeof(DevStatus)));
@@ -656,6 +702,10 @@ void epi_destroy(epi_ctx* ctx) {
   for (cudaEvent_t e : ctx->ev_done) cudaEventDestroy(e);
   if (ctx->copy_in) cudaStreamDestroy(ctx->copy_in);
   if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
+  if (ctx->aux) cudaStreamSynchronize(ctx->aux);
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+  if (ctx->aux) cudaStreamDestroy(ctx->aux);
   if (ctx->side) cudaStreamDestroy(ctx->side);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;

@@ -1321,19 +1321,30 @@ void launch_rebuild(const DevState& S, const Range& r, const ScanScratch&,
   timer_end(tm, KC_GATE, s);
 }
 
+void launch_memb_force(const DevState& S, int32_t m0, int32_t m1, int precision,
+                       const LaunchCfg& lc, cudaStream_t s, Timer* tm) {
+  if (m1 <= m0) return;
+  timer_begin(tm, KC_PREPASS, s);
+  const int gm = stride_blocks(m1 - m0, lc.block, lc);
+  if (precision == 1)
+    launch_pdl(k_memb_force<float>, gm, lc.block, s, S, m0, m1);
+  else
+    launch_pdl(k_memb_force<double>, gm, lc.block, s, S, m0, m1);
+  timer_end(tm, KC_PREPASS, s);
+}
+
+void launch_dermis(const DevState& S, int32_t f0, int32_t f1, const LaunchCfg& lc,
+                   cudaStream_t s, Timer* tm) {
+  if (f1 <= f0) return;
+  timer_begin(tm, KC_PREPASS, s);
+  launch_pdl(k_dermis, stride_blocks(f1 - f0, lc.block, lc), lc.block, s, S, f0, f1);
+  timer_end(tm, KC_PREPASS, s);
+}
+
 void launch_prepass(const DevState& S, int32_t m0, int32_t m1, int32_t f0, int32_t f1,
                     int precision, const LaunchCfg& lc, cudaStream_t s, Timer* tm) {
-  if (m1 <= m0 && f1 <= f0) return;
-  timer_begin(tm, KC_PREPASS, s);
-  if (m1 > m0) {
-    const int gm = stride_blocks(m1 - m0, lc.block, lc);
-    if (precision == 1)
-      launch_pdl(k_memb_force<float>, gm, lc.block, s, S, m0, m1);
-    else
-      launch_pdl(k_memb_force<double>, gm, lc.block, s, S, m0, m1);
-  }
-  if (f1 > f0) launch_pdl(k_dermis, stride_blocks(f1 - f0, lc.block, lc), lc.block, s, S, f0, f1);
-  timer_end(tm, KC_PREPASS, s);
+  launch_memb_force(S, m0, m1, precision, lc, s, tm);
+  launch_dermis(S, f0, f1, lc, s, tm);
 }
 
 template <typename R, bool kSimple, bool kOld>

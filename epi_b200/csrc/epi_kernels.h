@@ -52,6 +52,13 @@ void launch_rebuild(const DevState& S, const Range& r, const ScanScratch& sc,
 // prep entries [m0, m1) (membrane role) and [f0, f1) (FIX / MUSUME role).
 void launch_prepass(const DevState& S, int32_t m0, int32_t m1, int32_t f0, int32_t f1,
                     int precision, const LaunchCfg& lc, cudaStream_t s, Timer* tm);
+// The two halves of launch_prepass: the membrane sums of prep[m0, m1) (reads
+// positions only, so it may run beside a candidate rebuild) and the dermis of
+// the FIX / MUSUME cells prep[f0, f1) (reads the candidate lists).
+void launch_memb_force(const DevState& S, int32_t m0, int32_t m1, int precision,
+                       const LaunchCfg& lc, cudaStream_t s, Timer* tm);
+void launch_dermis(const DevState& S, int32_t f0, int32_t f1, const LaunchCfg& lc,
+                   cudaStream_t s, Timer* tm);
 // cell_interaction + pos_copy + cell_pos_periodic_fix from the current
 // positions into S.pos_nxt; flags tissues whose particles moved more than
 // skin/2 since their last rebuild.
