@@ -310,9 +310,10 @@ void enqueue_step(epi_ctx* c, int& cur, Timer* tm) {
 }
 
 // Appends to the graph being captured on c->stream a conditional (IF) node
-// whose body, captured on c->side, is the candidate rebuild; a one-thread
-// kernel before it sets the condition from the "some tissue is flagged"
-// word, so steps that need no rebuild launch none of its kernels.
+// whose body, captured on c->side, is the candidate rebuild; a one-block
+// kernel before it builds the rebuild work list and sets the condition to
+// "the list is not empty", so steps that need no rebuild launch none of the
+// rebuild's kernels.
 cudaError_t capture_conditional_rebuild(epi_ctx* c, int cur) {
   cudaStreamCaptureStatus st;
   cudaGraph_t g;
@@ -322,7 +323,7 @@ cudaError_t capture_conditional_rebuild(epi_ctx* c, int cur) {
   if (e != cudaSuccess) return e;
   cudaGraphConditionalHandle h;
   if ((e = cudaGraphConditionalHandleCreate(&h, g, 0, 0)) != cudaSuccess) return e;
-  launch_rebuild_condition(make_state(c, cur), h, c->stream);
+  launch_rebuild_condition(make_state(c, cur), whole(c), h, c->stream);
   if ((e = cudaStreamGetCaptureInfo(c->stream, &st, nullptr, &g, &deps, &nd)) != cudaSuccess)
     return e;
   cudaGraphNodeParams p{};
@@ -336,7 +337,7 @@ cudaError_t capture_conditional_rebuild(epi_ctx* c, int cur) {
   if ((e = cudaStreamBeginCaptureToGraph(c->side, body, nullptr, nullptr, 0,
                                          cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
     return e;
-  launch_rebuild(make_state(c, cur), whole(c), c->scan, c->lc, c->side, nullptr);
+  launch_rebuild(make_state(c, cur), whole(c), c->scan, c->lc, c->side, nullptr, true);
   if ((e = cudaStreamEndCapture(c->side, &body)) != cudaSuccess) return e;
   return cudaStreamUpdateCaptureDependencies(c->stream, &node, 1,
                                              cudaStreamSetCaptureDependencies);

@@ -172,9 +172,7 @@ __device__ __forceinline__ int32_t ref_bin(const TissueDev& T, double x, double 
 // index back to (tissue, local index) by binary search in the prefix sums.
 // With nothing gated the list is empty and each kernel exits at once.
 // ---------------------------------------------------------------------------
-__global__ void k_gate_compact(DevState S, int32_t t0, int32_t t1) {
-  pdl_entry();
-  count_launch(S.launches);
+__device__ __forceinline__ void gate_compact(const DevState& S, int32_t t0, int32_t t1) {
   if (S.gate[0] == 0) {
     if (threadIdx.x == 0) {
       S.rl_count[0] = 0;
@@ -211,6 +209,23 @@ __global__ void k_gate_compact(DevState S, int32_t t0, int32_t t1) {
     S.rl_ppre[cc] = cp;
     S.rl_bpre[cc] = cb;
   }
+}
+
+// Once the work list is built nothing of the rebuild reads the flags: clear
+// the listed tissues' flags (and the "some tissue" word for a whole-batch
+// rebuild) and count the rebuilds. Run by one block of the candidate search.
+__device__ __forceinline__ void gate_clear(const DevState& S, int32_t cnt, int32_t clear_any) {
+  for (int32_t k = threadIdx.x; k < cnt; k += blockDim.x) S.gate[1 + S.rl_list[k]] = 0;
+  if (threadIdx.x == 0) {
+    if (cnt) atomicAdd(S.rebuilds, (unsigned long long)cnt);
+    if (clear_any) S.gate[0] = 0;
+  }
+}
+
+__global__ void k_gate_compact(DevState S, int32_t t0, int32_t t1) {
+  pdl_entry();
+  count_launch(S.launches);
+  gate_compact(S, t0, t1);
 }
 
 // index k of the last prefix entry <= g (pre[0] = 0, non-decreasing, n+1 entries)
@@ -579,35 +594,27 @@ __device__ __forceinline__ void cand_search_threads(const DevState& S, int32_t c
 // Below this many gated particles the warp-per-particle search is faster.
 constexpr int32_t kWarpSearchMax = 48 * 1024;
 
-__global__ void k_cand_search(DevState S) {
+__global__ void k_cand_search(DevState S, int32_t clear_any) {
   pdl_entry();
   count_launch(S.launches);
   const int32_t cnt = S.rl_count[0];
+  if (blockIdx.x == 0) gate_clear(S, cnt, clear_any);
   if (cnt == 0) return;
   const int32_t ngated = S.rl_ppre[cnt];
   if (ngated < kWarpSearchMax) cand_search_warps(S, cnt, ngated);
   else cand_search_threads(S, cnt, ngated);
 }
 
-__global__ void k_gate_clear(DevState S, int32_t clear_any) {
+// Condition of the rebuild node in the captured step graph: builds the work
+// list of [t0, t1) (as k_gate_compact) and runs the rebuild kernels only
+// when it is not empty.
+__global__ void k_rebuild_condition(DevState S, int32_t t0, int32_t t1,
+                                    cudaGraphConditionalHandle h) {
   pdl_entry();
   count_launch(S.launches);
-  const int32_t cnt = S.rl_count[0];
-  for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x)
-    S.gate[1 + S.rl_list[k]] = 0;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    if (cnt) atomicAdd(S.rebuilds, (unsigned long long)cnt);
-    if (clear_any) S.gate[0] = 0;
-  }
-}
-
-// Condition of the rebuild node in the captured step graph: run the rebuild
-// kernels only when some tissue is flagged.
-__global__ void k_rebuild_condition(cudaGraphConditionalHandle h, const int32_t* gate,
-                                    unsigned long long* launches) {
-  pdl_entry();
-  count_launch(launches);
-  cudaGraphSetConditional(h, gate[0] != 0 ? 1u : 0u);
+  gate_compact(S, t0, t1);
+  __syncthreads();
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, S.rl_count[0] > 0 ? 1u : 0u);
 }
 
 __global__ void k_gate_set_all(DevState S, int32_t ntissues) {
@@ -1296,11 +1303,15 @@ void launch_scan(const int32_t* in, int32_t* out, int32_t n, int32_t init,
 }
 
 void launch_rebuild(const DevState& S, const Range& r, const ScanScratch&,
-                    const LaunchCfg& lc, cudaStream_t s, Timer* tm) {
+                    const LaunchCfg& lc, cudaStream_t s, Timer* tm, bool listed) {
   const int B = lc.block;
   const int grid = lc.num_sms * 8;
+  if (!listed) {
+    timer_begin(tm, KC_GATE, s);
+    launch_pdl(k_gate_compact, 1, kScanThreads, s, S, r.t0, r.t1);
+    timer_end(tm, KC_GATE, s);
+  }
   timer_begin(tm, KC_REBUILD_BIN, s);
-  launch_pdl(k_gate_compact, 1, kScanThreads, s, S, r.t0, r.t1);
   launch_pdl(k_bin, grid, B, s, S);
   timer_end(tm, KC_REBUILD_BIN, s);
   timer_begin(tm, KC_REBUILD_SCAN, s);
@@ -1312,13 +1323,10 @@ void launch_rebuild(const DevState& S, const Range& r, const ScanScratch&,
   launch_pdl(k_scatter, grid, B, s, S);
   launch_pdl(k_binsort, grid, B, s, S);
   timer_end(tm, KC_REBUILD_SORT, s);
-  timer_begin(tm, KC_REBUILD_SEARCH, s);
-  launch_pdl(k_cand_search, grid, B, s, S);
-  timer_end(tm, KC_REBUILD_SEARCH, s);
-  timer_begin(tm, KC_GATE, s);
   const bool whole = r.t0 == 0 && r.t1 == S.ntissues;
-  launch_pdl(k_gate_clear, 1, B, s, S, (int32_t)(whole ? 1 : 0));
-  timer_end(tm, KC_GATE, s);
+  timer_begin(tm, KC_REBUILD_SEARCH, s);
+  launch_pdl(k_cand_search, grid, B, s, S, (int32_t)(whole ? 1 : 0));
+  timer_end(tm, KC_REBUILD_SEARCH, s);
 }
 
 void launch_memb_force(const DevState& S, int32_t m0, int32_t m1, int precision,
@@ -1406,8 +1414,9 @@ void launch_set_counter(int32_t* remaining, int32_t value, cudaStream_t s) {
   k_set1<<<1, 1, 0, s>>>(remaining, value, nullptr);
 }
 
-void launch_rebuild_condition(const DevState& S, cudaGraphConditionalHandle h, cudaStream_t s) {
-  launch_pdl(k_rebuild_condition, 1, 1, s, h, (const int32_t*)S.gate, S.launches);
+void launch_rebuild_condition(const DevState& S, const Range& r, cudaGraphConditionalHandle h,
+                              cudaStream_t s) {
+  launch_pdl(k_rebuild_condition, 1, kScanThreads, s, S, r.t0, r.t1, h);
 }
 
 void launch_set_gates(const DevState& S, int32_t ntissues, cudaStream_t s) {

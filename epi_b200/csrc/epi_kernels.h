@@ -43,11 +43,12 @@ void launch_scan(const int32_t* in, int32_t* out, int32_t n, int32_t init,
                  const ScanScratch& sc, const int32_t* gate, const LaunchCfg& lc,
                  cudaStream_t s);
 
-// Verlet candidate rebuild of every tissue whose gate is set (all kernels
-// exit at once when no gate is set): bin -> scan -> scatter -> per-bin sort
-// -> candidate search -> gate reset.
+// Verlet candidate rebuild of every tissue of r whose gate is set (all
+// kernels exit at once when none is): work list -> bin -> scan -> scatter ->
+// per-bin sort -> candidate search (which also resets the listed gates).
+// listed: the work list was already built (launch_rebuild_condition).
 void launch_rebuild(const DevState& S, const Range& r, const ScanScratch& sc,
-                    const LaunchCfg& lc, cudaStream_t s, Timer* tm);
+                    const LaunchCfg& lc, cudaStream_t s, Timer* tm, bool listed = false);
 // Membrane bending scratch (_memb_bend_calc1) and dermis (find_dermis) for
 // prep entries [m0, m1) (membrane role) and [f0, f1) (FIX / MUSUME role).
 void launch_prepass(const DevState& S, int32_t m0, int32_t m1, int32_t f0, int32_t f1,
@@ -68,8 +69,10 @@ void launch_step(const DevState& S, const Range& r, int precision, const LaunchC
 void launch_exact_lists(const DevState& S, const Range& r, const LaunchCfg& lc,
                         cudaStream_t s);
 void launch_set_gates(const DevState& S, int32_t ntissues, cudaStream_t s);
-// Sets conditional handle h to (some tissue is flagged for a rebuild).
-void launch_rebuild_condition(const DevState& S, cudaGraphConditionalHandle h, cudaStream_t s);
+// Builds the rebuild work list of r's flagged tissues and sets conditional
+// handle h to (the list is not empty).
+void launch_rebuild_condition(const DevState& S, const Range& r, cudaGraphConditionalHandle h,
+                              cudaStream_t s);
 // WHILE-node bookkeeping of the step graph: set the number of passes left,
 // and decrement it at the end of a pass (setting h to "more passes").
 void launch_set_counter(int32_t* remaining, int32_t value, cudaStream_t s);

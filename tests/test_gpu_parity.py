@@ -495,18 +495,19 @@ def test_reupload_and_position_upload_regate_only_what_changed(built):
 
 
 def test_launch_count_counts_the_step_sequence(built):
-    """epi_launch_count: eager steps run 9 kernels each (7 rebuild kernels,
-    the membrane prepass, the step); a graph run adds one condition kernel
-    per step and one loop kernel per pass of two steps, and runs the rebuild
-    kernels only in steps where some tissue was flagged."""
+    """epi_launch_count: eager steps run 8 kernels each (6 rebuild kernels,
+    the membrane sums, the step); a graph step runs the work-list kernel
+    that sets the rebuild condition, the membrane sums and the step, one loop
+    kernel per pass of two steps, and the 5 remaining rebuild kernels only in
+    steps where some tissue was flagged."""
     with capi.Context(precision=MIXED) as ctx:
         ctx.upload([T.config1()])
         c0 = ctx.launch_count()
         ctx.step(10, "eager")
-        assert ctx.launch_count() - c0 == 90
+        assert ctx.launch_count() - c0 == 80
         c1 = ctx.launch_count()
         r1 = ctx.rebuild_count()
         ctx.step(10, "graph")
         n = ctx.launch_count() - c1
         rebuilt_steps = ctx.rebuild_count() - r1  # one tissue: one rebuild per rebuilding step
-        assert n == 10 * 3 + 5 + 7 * rebuilt_steps
+        assert n == 10 * 3 + 5 + 5 * rebuilt_steps
