@@ -20,12 +20,14 @@
 //   lattice   the four lattice springs of _MEMB_interaction (CI_memb_to_memb,
 //             :185-234), the same gather over fixed partners.
 //   wall      z += DT W(z) for z < r (:287-294).
-//   bending   D_k += DT KBEND B_k(eleven lattice sites) (:296-449). Its
-//             vector-Jacobian product is derived by hand below; each
-//             membrane particle writes the products for the eleven sites of
-//             its stencil and every site gathers the eleven entries that
-//             name it, so no atomics are needed and results are
-//             deterministic.
+//   bending   D_k += DT KBEND B_k(stencil sites): square, eleven lattice
+//             sites (_memb_bend_calc1..3, :296-449); triangular, the six
+//             neighbours and six second-ring sites of the twelve dihedral
+//             terms of tri_memb_bend (:451-508). Their vector-Jacobian
+//             products are derived by hand below; each membrane particle
+//             writes the products for the sites of its stencil and every
+//             site gathers the entries that name it, so no atomics are
+//             needed and results are deterministic.
 #include "epi_kernels.h"
 #include "epi_device.cuh"
 
@@ -43,6 +45,9 @@ __device__ __forceinline__ D3& operator+=(D3& a, D3 b) { return a = a + b; }
 __device__ __forceinline__ D3& operator-=(D3& a, D3 b) { return a = a - b; }
 __device__ __forceinline__ double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 __device__ __forceinline__ D3 xyz(double4 v) { return D3{v.x, v.y, v.z}; }
+__device__ __forceinline__ D3 cross(D3 a, D3 b) {
+  return D3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
 
 // A pair coefficient with its derivatives: c, dc/d(r2), and the parts of c
 // that scale with s_spring and with s_eps (each law is linear in them).
@@ -133,6 +138,11 @@ __device__ __forceinline__ void unit3_back(const U3& u, D3 ub, double lb, D3& ab
 // Stencil slots of the bending term of particle k, as lattice offsets:
 // k, r, rr, l, ll, u, uu, b, bb, r of bb, rr of bb.
 constexpr int kSlots = 11;
+// Triangular lattice: k, its neighbour in direction i (slot 1 + i), and the
+// second-ring site c_i = memb[(i+1)%6]->memb[i] (slot 7 + i).
+constexpr int kTriSlots = 13;
+// Entries per membrane particle in the bending-product buffer.
+constexpr int kBendStride = 13;
 __constant__ int kSlotDj[kSlots] = {0, 1, 2, -1, -2, 0, 0, 0, 0, 1, 2};
 __constant__ int kSlotDk[kSlots] = {0, 0, 0, 0, 0, 1, 2, -1, -2, -2, -2};
 
@@ -167,9 +177,87 @@ __device__ __forceinline__ double half_back(D3 yb, D3 n, D3 a, D3 l, D3 m, doubl
   return val;
 }
 
+// tri_bend_1 (:475-481) of particle k with offsets a = n_i, b = n_{i+1},
+// c = c_i (k at the origin): term = g(d) ab x (n2 - d n1), n1 = unit(rb x
+// ab), n2 = unit(ab x cb), d = n1 . n2, rb = -b, ab = a - b, cb = c - b (the
+// reference's division by the norm of an already normalised normal is 1 up
+// to rounding and is left out, as in the forward step). Returns y . term and
+// accumulates the adjoints of a, b, c. For p x q the adjoints are q x ybar
+// and ybar x p; for n = N / |N|, Nbar = (nbar - (nbar . n) n) / |N|.
+__device__ __forceinline__ double tri1_back(D3 y, D3 a, D3 b, D3 c, D3& abar, D3& bbar,
+                                            D3& cbar) {
+  const D3 rb = d3(-b.x, -b.y, -b.z), ab = a - b, cb = c - b;
+  const D3 N1 = cross(rb, ab), N2 = cross(ab, cb);
+  const double l1 = sqrt(dot(N1, N1)), l2 = sqrt(dot(N2, N2));
+  const D3 n1 = (1.0 / l1) * N1, n2 = (1.0 / l2) * N2;
+  const double d = dot(n1, n2);
+  const D3 v = n2 - d * n1;
+  const D3 t = cross(ab, v);
+  const double g = bf(d), yt = dot(y, t);
+  double dbar = bf_d(d) * yt;
+  const D3 tbar = g * y;
+  D3 abbar = cross(v, tbar);
+  const D3 vbar = cross(tbar, ab);
+  D3 n2bar = vbar, n1bar = (-d) * vbar;
+  dbar -= dot(vbar, n1);
+  n1bar += dbar * n2;
+  n2bar += dbar * n1;
+  const D3 N1bar = (1.0 / l1) * (n1bar - dot(n1bar, n1) * n1);
+  const D3 N2bar = (1.0 / l2) * (n2bar - dot(n2bar, n2) * n2);
+  const D3 rbbar = cross(ab, N1bar);
+  abbar += cross(N1bar, rb);
+  abbar += cross(cb, N2bar);
+  const D3 cbbar = cross(N2bar, ab);
+  abar += abbar;
+  bbar -= abbar;
+  bbar -= rbbar;
+  bbar -= cbbar;
+  cbar += cbbar;
+  return g * yt;
+}
+
+// tri_bend_2 (:483-495) with a = n_i, b = n_{i+1}, cc = n_{i+2}: term =
+// g(d) [bc x (n2 - d n1) + ab x (n1 - d n2)], n1 = unit(rc x bc), n2 =
+// unit(rb x ab), rc = -cc, rb = -b, bc = b - cc, ab = a - b.
+__device__ __forceinline__ double tri2_back(D3 y, D3 a, D3 b, D3 cc, D3& abar, D3& bbar,
+                                            D3& ccbar) {
+  const D3 rc = d3(-cc.x, -cc.y, -cc.z), rb = d3(-b.x, -b.y, -b.z);
+  const D3 bc = b - cc, ab = a - b;
+  const D3 N1 = cross(rc, bc), N2 = cross(rb, ab);
+  const double l1 = sqrt(dot(N1, N1)), l2 = sqrt(dot(N2, N2));
+  const D3 n1 = (1.0 / l1) * N1, n2 = (1.0 / l2) * N2;
+  const double d = dot(n1, n2);
+  const D3 v1 = n2 - d * n1, v2 = n1 - d * n2;
+  const D3 t = cross(bc, v1) + cross(ab, v2);
+  const double g = bf(d), yt = dot(y, t);
+  double dbar = bf_d(d) * yt;
+  const D3 tbar = g * y;
+  D3 bcbar = cross(v1, tbar);
+  const D3 v1bar = cross(tbar, bc);
+  D3 abbar = cross(v2, tbar);
+  const D3 v2bar = cross(tbar, ab);
+  D3 n2bar = v1bar - d * v2bar, n1bar = v2bar - d * v1bar;
+  dbar -= dot(v1bar, n1) + dot(v2bar, n2);
+  n1bar += dbar * n2;
+  n2bar += dbar * n1;
+  const D3 N1bar = (1.0 / l1) * (n1bar - dot(n1bar, n1) * n1);
+  const D3 N2bar = (1.0 / l2) * (n2bar - dot(n2bar, n2) * n2);
+  const D3 rcbar = cross(bc, N1bar);
+  bcbar += cross(N1bar, rc);
+  const D3 rbbar = cross(ab, N2bar);
+  abbar += cross(N2bar, rb);
+  ccbar -= rcbar;
+  ccbar -= bcbar;
+  bbar -= rbbar;
+  bbar += bcbar;
+  bbar -= abbar;
+  abar += abbar;
+  return g * yt;
+}
+
 // Membrane particles: bending, lattice-spring and wall adjoints. Writes the
-// bending products for the eleven stencil sites to bend[e * 11 + slot], the
-// lattice + wall product at the particle itself to madj[e], and the
+// bending products for the stencil sites to bend[e * kBendStride + slot],
+// the lattice + wall product at the particle itself to madj[e], and the
 // parameter partials to gmemb[e].
 __global__ void __launch_bounds__(256) k_adj_memb(DevState S, const double4* __restrict__ lam,
                                                   double4* __restrict__ bend,
@@ -194,58 +282,87 @@ __global__ void __launch_bounds__(256) k_adj_memb(DevState S, const double4* __r
     const D3 li = xyz(lam[i]);
     double g_spring = 0.0, g_eps = 0.0, g_bend = 0.0;
     // --- bending: forward recompute of the stencil, then its adjoint
-    D3 o[kSlots];
-    o[0] = d3(0.0, 0.0, 0.0);
-#pragma unroll
-    for (int s = 1; s < kSlots; ++s) {
-      const Vec3<double> v = offset_of<double>(S.pos_cur[site(kSlotDj[s], kSlotDk[s])], p, T);
-      o[s] = d3(v.x, v.y, v.z);
-    }
-    const U3 nv = unit3(o[0], o[1]), nvr = unit3(o[1], o[2]);
-    const U3 nvl = unit3(o[3], o[0]), nvll = unit3(o[4], o[3]);
-    const U3 mv = unit3(o[0], o[5]), mvu = unit3(o[5], o[6]);
-    const U3 mvb = unit3(o[7], o[0]), mvbb = unit3(o[8], o[7]);
-    const U3 nvbb = unit3(o[8], o[9]), nvbbr = unit3(o[9], o[10]);
     const double sb = dt * T.P.kbend;
     const D3 yb = sb * li;
-    HalfBar hn, hm;
-    const double ipnll = dot(nvll.v, nvl.v);
-    const double ipmbb = dot(nvbb.v, nvbbr.v);  // memb_bb's ipn (:380)
-    const double fn = half_back(yb, nv.v, nvr.v, nvl.v, nvll.v, nv.len, nvl.len, ipnll, hn);
-    const double fm = half_back(yb, mv.v, mvu.v, mvb.v, mvbb.v, mv.len, mvb.len, ipmbb, hm);
-    g_bend = fn + fm;  // lambda . (dt kbend BCALC): d/ds_bend of the bending term
-    D3 ob[kSlots];
+    if (T.lattice == kLatticeTriangular) {
+      const int32_t nm = T.nmemb;
+      D3 o[kTriSlots], ob[kTriSlots];
+      o[0] = d3(0.0, 0.0, 0.0);
 #pragma unroll
-    for (int s = 0; s < kSlots; ++s) ob[s] = d3(0.0, 0.0, 0.0);
-    // ipnll = nvll . nvl
-    hn.m += hn.w * nvl.v;
-    hn.l += hn.w * nvll.v;
-    unit3_back(nv, hn.n, hn.D, ob[0], ob[1]);
-    unit3_back(nvr, hn.a, 0.0, ob[1], ob[2]);
-    unit3_back(nvl, hn.l, hn.E, ob[3], ob[0]);
-    unit3_back(nvll, hn.m, 0.0, ob[4], ob[3]);
-    unit3_back(mv, hm.n, hm.D, ob[0], ob[5]);
-    unit3_back(mvu, hm.a, 0.0, ob[5], ob[6]);
-    unit3_back(mvb, hm.l, hm.E, ob[7], ob[0]);
-    unit3_back(mvbb, hm.m, 0.0, ob[8], ob[7]);
-    // ipmbb = nvbb . nvbbr
-    unit3_back(nvbb, hm.w * nvbbr.v, 0.0, ob[8], ob[9]);
-    unit3_back(nvbbr, hm.w * nvbb.v, 0.0, ob[9], ob[10]);
-    // o[s] = x_site - x_k: the particle itself receives minus every offset's
-    // adjoint (o[0] is the constant zero)
-    D3 self = d3(0.0, 0.0, 0.0);
+      for (int k = 0; k < 6; ++k) {
+        const Vec3<double> v = offset_of<double>(S.pos_cur[pb + tri_link(j, k, NMX, nm)], p, T);
+        o[1 + k] = d3(v.x, v.y, v.z);
+        const int32_t c2 = tri_link(tri_link(j, (k + 1) % 6, NMX, nm), k, NMX, nm);
+        const Vec3<double> w = offset_of<double>(S.pos_cur[pb + c2], p, T);
+        o[7 + k] = d3(w.x, w.y, w.z);
+      }
 #pragma unroll
-    for (int s = 1; s < kSlots; ++s) {
-      self -= ob[s];
-      bend[e * kSlots + s] = make_double4(ob[s].x, ob[s].y, ob[s].z, 0.0);
+      for (int s = 0; s < kTriSlots; ++s) ob[s] = d3(0.0, 0.0, 0.0);
+      for (int k = 0; k < 6; ++k) {
+        const int b = 1 + (k + 1) % 6;
+        g_bend += tri1_back(yb, o[1 + k], o[b], o[7 + k], ob[1 + k], ob[b], ob[7 + k]);
+      }
+      for (int k = 0; k < 6; ++k) {
+        const int b = 1 + (k + 1) % 6, c = 1 + (k + 2) % 6;
+        g_bend += tri2_back(yb, o[1 + k], o[b], o[c], ob[1 + k], ob[b], ob[c]);
+      }
+      D3 self = d3(0.0, 0.0, 0.0);
+#pragma unroll
+      for (int s = 1; s < kTriSlots; ++s) {
+        self -= ob[s];
+        bend[(int64_t)e * kBendStride + s] = make_double4(ob[s].x, ob[s].y, ob[s].z, 0.0);
+      }
+      bend[(int64_t)e * kBendStride] = make_double4(self.x, self.y, self.z, 0.0);
+    } else {
+      D3 o[kSlots];
+      o[0] = d3(0.0, 0.0, 0.0);
+#pragma unroll
+      for (int s = 1; s < kSlots; ++s) {
+        const Vec3<double> v = offset_of<double>(S.pos_cur[site(kSlotDj[s], kSlotDk[s])], p, T);
+        o[s] = d3(v.x, v.y, v.z);
+      }
+      const U3 nv = unit3(o[0], o[1]), nvr = unit3(o[1], o[2]);
+      const U3 nvl = unit3(o[3], o[0]), nvll = unit3(o[4], o[3]);
+      const U3 mv = unit3(o[0], o[5]), mvu = unit3(o[5], o[6]);
+      const U3 mvb = unit3(o[7], o[0]), mvbb = unit3(o[8], o[7]);
+      const U3 nvbb = unit3(o[8], o[9]), nvbbr = unit3(o[9], o[10]);
+      HalfBar hn, hm;
+      const double ipnll = dot(nvll.v, nvl.v);
+      const double ipmbb = dot(nvbb.v, nvbbr.v);  // memb_bb's ipn (:380)
+      const double fn = half_back(yb, nv.v, nvr.v, nvl.v, nvll.v, nv.len, nvl.len, ipnll, hn);
+      const double fm = half_back(yb, mv.v, mvu.v, mvb.v, mvbb.v, mv.len, mvb.len, ipmbb, hm);
+      g_bend = fn + fm;  // lambda . (dt kbend BCALC): d/ds_bend of the bending term
+      D3 ob[kSlots];
+#pragma unroll
+      for (int s = 0; s < kSlots; ++s) ob[s] = d3(0.0, 0.0, 0.0);
+      // ipnll = nvll . nvl
+      hn.m += hn.w * nvl.v;
+      hn.l += hn.w * nvll.v;
+      unit3_back(nv, hn.n, hn.D, ob[0], ob[1]);
+      unit3_back(nvr, hn.a, 0.0, ob[1], ob[2]);
+      unit3_back(nvl, hn.l, hn.E, ob[3], ob[0]);
+      unit3_back(nvll, hn.m, 0.0, ob[4], ob[3]);
+      unit3_back(mv, hm.n, hm.D, ob[0], ob[5]);
+      unit3_back(mvu, hm.a, 0.0, ob[5], ob[6]);
+      unit3_back(mvb, hm.l, hm.E, ob[7], ob[0]);
+      unit3_back(mvbb, hm.m, 0.0, ob[8], ob[7]);
+      // ipmbb = nvbb . nvbbr
+      unit3_back(nvbb, hm.w * nvbbr.v, 0.0, ob[8], ob[9]);
+      unit3_back(nvbbr, hm.w * nvbb.v, 0.0, ob[9], ob[10]);
+      // o[s] = x_site - x_k: the particle itself receives minus every offset's
+      // adjoint (o[0] is the constant zero)
+      D3 self = d3(0.0, 0.0, 0.0);
+#pragma unroll
+      for (int s = 1; s < kSlots; ++s) {
+        self -= ob[s];
+        bend[(int64_t)e * kBendStride + s] = make_double4(ob[s].x, ob[s].y, ob[s].z, 0.0);
+      }
+      bend[(int64_t)e * kBendStride] = make_double4(self.x, self.y, self.z, 0.0);
     }
-    bend[e * kSlots] = make_double4(self.x, self.y, self.z, 0.0);
     // --- lattice springs (each pair from both sides: gather)
     D3 mu = d3(0.0, 0.0, 0.0);
-    const int32_t links[4] = {site(-1, 0), site(1, 0), site(0, -1), site(0, 1)};
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int32_t q = links[k];
+    for (int k = 0; k < T.nadj; ++k) {
+      const int32_t q = pb + lattice_link(T, j, k);
       const double4 pq = S.pos_cur[q];
       double dx, dy, dz;
       pair_sep(p, pq, i > q, T, dx, dy, dz);
@@ -319,16 +436,35 @@ __global__ void __launch_bounds__(256) k_adj_pairs(DevState S, const double4* __
       g_spring += gm.x;
       g_eps += gm.y;
       g_bend += gm.z;
-      // bending products naming this site: slot s of the particle at
-      // (jj - dj_s, kk - dk_s)
+      if (T.lattice == kLatticeTriangular) {
+        // slot 1 + d names this site for its neighbour in the opposite
+        // direction (d + 3) % 6; slot 7 + k (the site two links away, along
+        // (k + 1) % 6 then k) for the particle reached back along the
+        // opposite directions, (k + 3) % 6 then (k + 4) % 6
+        const int32_t nm = T.nmemb;
+        mu += xyz(bend[(int64_t)(T.mbase + j) * kBendStride]);
 #pragma unroll
-      for (int s = 0; s < kSlots; ++s) {
-        int32_t c = jj - kSlotDj[s], w = kk - kSlotDk[s];
-        c += c < 0 ? NMX : 0;
-        c -= c >= NMX ? NMX : 0;
-        w += w < 0 ? NMY : 0;
-        w -= w >= NMY ? NMY : 0;
-        mu += xyz(bend[(int64_t)(T.mbase + w * NMX + c) * kSlots + s]);
+        for (int d = 0; d < 6; ++d) {
+          const int32_t src = tri_link(j, (d + 3) % 6, NMX, nm);
+          mu += xyz(bend[(int64_t)(T.mbase + src) * kBendStride + 1 + d]);
+        }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          const int32_t src = tri_link(tri_link(j, (k + 3) % 6, NMX, nm), (k + 4) % 6, NMX, nm);
+          mu += xyz(bend[(int64_t)(T.mbase + src) * kBendStride + 7 + k]);
+        }
+      } else {
+        // bending products naming this site: slot s of the particle at
+        // (jj - dj_s, kk - dk_s)
+#pragma unroll
+        for (int s = 0; s < kSlots; ++s) {
+          int32_t c = jj - kSlotDj[s], w = kk - kSlotDk[s];
+          c += c < 0 ? NMX : 0;
+          c -= c >= NMX ? NMX : 0;
+          w += w < 0 ? NMY : 0;
+          w -= w >= NMY ? NMY : 0;
+          mu += xyz(bend[(int64_t)(T.mbase + w * NMX + c) * kBendStride + s]);
+        }
       }
     }
     lam_out[i] = make_double4(mu.x, mu.y, mu.z, 0.0);

@@ -953,8 +953,6 @@ int epi_adjoint(epi_ctx* c, int32_t nsteps, int32_t K, const epi_loss* loss, dou
     return EPI_ERR_INVALID_ARG;
   if (!c->loaded) return EPI_ERR_STATE;
   if (!c->lc.simple) return EPI_ERR_UNSUPPORTED;
-  for (const TissueDev& T : c->tissues_h)
-    if (T.lattice != EPI_LATTICE_SQUARE) return EPI_ERR_UNSUPPORTED;
   EPI_GUARD_BEGIN
   int rc = set_device(c);
   if (rc) return rc;
@@ -968,7 +966,7 @@ int epi_adjoint(epi_ctx* c, int32_t nsteps, int32_t K, const epi_loss* loss, dou
   double *acc, *target, *inv_cnt;
   const size_t nm = (size_t)std::max(c->nprep_memb, 1);
   if ((rc = mem.get(&lam0, n)) || (rc = mem.get(&lam1, n)) || (rc = mem.get(&gpart, n)) ||
-      (rc = mem.get(&bend, 11 * nm)) || (rc = mem.get(&madj, nm)) || (rc = mem.get(&gmemb, nm)) ||
+      (rc = mem.get(&bend, 13 * nm)) || (rc = mem.get(&madj, nm)) || (rc = mem.get(&gmemb, nm)) ||
       (rc = mem.get(&ckpt, n * (size_t)std::max(nseg, 1))) || (rc = mem.get(&hist, n * hist_len)) ||
       (rc = mem.get(&xT, n)) || (rc = mem.get(&acc, 4 * (size_t)nt)) ||
       (rc = mem.get(&target, 3 * n)) || (rc = mem.get(&inv_cnt, (size_t)nt)))

@@ -126,7 +126,7 @@ void launch_field_step(const DevState& S, const FieldState& FS, int32_t wmax,
 struct AdjointBuffers {
   const double4* lam_in;  // dL/dX_{t+1}
   double4* lam_out;       // dL/dX_t
-  double4* bend;          // 11 bending products per membrane particle
+  double4* bend;          // 13 bending-product slots per membrane particle
   double4* madj;          // lattice + wall product per membrane particle
   double4* gmemb;         // membrane parameter partials
   double4* gpart;         // per-particle parameter partials (spring, eps, bend, loss)

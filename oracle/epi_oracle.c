@@ -726,6 +726,12 @@ void ora_get_dermis(const ora_tissue* t, int32_t* dermis) {
   memcpy(dermis, t->dermis, sizeof(int32_t) * (size_t)t->n);
 }
 
+int ora_get_tri_neighbours(const ora_tissue* t, int32_t* nb) {
+  if (!t->tri) return -1;
+  memcpy(nb, t->tri_nb, sizeof(int32_t) * 6 * (size_t)t->nmemb);
+  return 0;
+}
+
 int ora_error_info(const ora_tissue* t, int32_t* a, int32_t* b, double* value) {
   if (a) *a = t->err_a;
   if (b) *b = t->err_b;

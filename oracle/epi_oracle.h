@@ -73,6 +73,10 @@ int64_t ora_get_connections(const ora_tissue* t, int32_t* offsets, int32_t* idx,
 /* Lists in the reference's own push order (unsorted). */
 int64_t ora_get_connections_raw(const ora_tissue* t, int32_t* offsets, int32_t* idx, int64_t cap);
 void ora_get_dermis(const ora_tissue* t, int32_t* dermis);
+/* Triangular lattice: the six neighbours of each membrane particle
+ * (Memb_data::memb[6], 6 * nmemb entries). Returns 0, or -1 (nothing
+ * written) for a square lattice. */
+int ora_get_tri_neighbours(const ora_tissue* t, int32_t* nb);
 int ora_error_info(const ora_tissue* t, int32_t* a, int32_t* b, double* value);
 
 /* Cell maps and external-stimulus diffusion on an (nx+1) x (ny+1) x (nz+1)

@@ -19,8 +19,10 @@
 // dual arithmetic differentiates the restated step itself, which makes this
 // an independent check of a hand-written reverse-mode adjoint.
 //
-// Scope: membrane particles plus ALIVE / DEAD / AIR cells without pairs (the
-// states of the synthetic tissues); other tissues are rejected.
+// Scope: square or triangular membranes (the triangular bending of
+// tri_memb_bend, :451-508, restated from epi_oracle.c) plus ALIVE / DEAD /
+// AIR cells without pairs (the states of the synthetic tissues); other
+// tissues are rejected.
 #include "epi_oracle.h"
 
 #include <cmath>
@@ -89,9 +91,45 @@ struct Consts {
   T eps_m, der_der_const, k_total, k_desmosome, kbend;
 };
 
+// vec3 (vec3.h:5-54) over T, operation by operation as epi_oracle.c's v3
+template <class T>
+struct V3 {
+  T x, y, z;
+};
+template <class T>
+inline V3<T> v3_cross(const V3<T>& a, const V3<T>& b) {
+  return V3<T>{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+template <class T>
+inline T v3_dot(const V3<T>& a, const V3<T>& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class T>
+inline T v3_norm(const V3<T>& a) { return sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+template <class T>
+inline V3<T> v3_normalize(V3<T>* a) {  // in place, like vec3::normalize
+  const T nm = v3_norm(*a);
+  a->x = a->x / nm;
+  a->y = a->y / nm;
+  a->z = a->z / nm;
+  return *a;
+}
+template <class T>
+inline V3<T> v3_scale(const T& c, const V3<T>& a) { return V3<T>{c * a.x, c * a.y, c * a.z}; }
+template <class T>
+inline V3<T> v3_div(const V3<T>& a, const T& c) { return V3<T>{a.x / c, a.y / c, a.z / c}; }
+template <class T>
+inline V3<T> v3_add(const V3<T>& a, const V3<T>& b) { return V3<T>{a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class T>
+inline V3<T> v3_sub(const V3<T>& a, const V3<T>& b) { return V3<T>{a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class T>
+inline V3<T> tri_rho(const V3<T>& n1, const V3<T>& b1) {  // :470-472
+  return v3_sub(b1, v3_scale(v3_dot(n1, b1), n1));
+}
+
 template <class T>
 struct Tissue {
-  int32_t n, nmemb, nmx, nmy;
+  int32_t n, nmemb, nmx, nmy, nadj = 4;
+  bool tri = false;
+  std::vector<int32_t> tri_nb;  // Memb_data::memb[6] per membrane particle
   double lx, ly;
   Consts<T> P;
   std::vector<T> x, y, z, nx, ny, nz;
@@ -240,14 +278,59 @@ struct Tissue {
     nz[m] += s * f[2];
   }
 
+  // tri_bend_1 / tri_bend_2 / tri_memb_bend, :475-508 (the division by the
+  // norm of the already normalised normal kept, as in the reference)
+  V3<T> vpos(int32_t c) const { return V3<T>{x[c], y[c], z[c]}; }
+  V3<T> vpsub(const V3<T>& a, const V3<T>& b) const {
+    return V3<T>{pdx(a.x, b.x), pdy(a.y, b.y), a.z - b.z};
+  }
+  V3<T> tri_bend_1(int32_t r1, int32_t a1, int32_t b1, int32_t c1) const {
+    const V3<T> r1v = vpos(r1), a1v = vpos(a1), b1v = vpos(b1), c1v = vpos(c1);
+    V3<T> norm1_pre = v3_cross(vpsub(r1v, b1v), vpsub(a1v, b1v));
+    const V3<T> norm1 = v3_normalize(&norm1_pre);
+    V3<T> n2 = v3_cross(vpsub(a1v, b1v), vpsub(c1v, b1v));
+    const V3<T> norm2 = v3_normalize(&n2);
+    const T dot1 = v3_dot(norm1, norm2);
+    return v3_scale(bend_factor(dot1),
+                    v3_div(v3_cross(vpsub(a1v, b1v), tri_rho(norm1, norm2)), v3_norm(norm1_pre)));
+  }
+  V3<T> tri_bend_2(int32_t r1, int32_t a1, int32_t b1, int32_t c1) const {
+    const V3<T> r1v = vpos(r1), a1v = vpos(a1), b1v = vpos(b1), c1v = vpos(c1);
+    V3<T> norm1_pre = v3_cross(vpsub(r1v, c1v), vpsub(b1v, c1v));
+    V3<T> norm2_pre = v3_cross(vpsub(r1v, b1v), vpsub(a1v, b1v));
+    const V3<T> norm1 = v3_normalize(&norm1_pre), norm2 = v3_normalize(&norm2_pre);
+    const T dot1 = v3_dot(norm1, norm2);
+    return v3_scale(bend_factor(dot1),
+                    v3_add(v3_div(v3_cross(vpsub(b1v, c1v), tri_rho(norm1, norm2)),
+                                  v3_norm(norm1_pre)),
+                           v3_div(v3_cross(vpsub(a1v, b1v), tri_rho(norm2, norm1)),
+                                  v3_norm(norm2_pre))));
+  }
+  void tri_memb_bend(int32_t m) {
+    const int32_t* nb = &tri_nb[6 * (size_t)m];
+    V3<T> dr{T(0.0), T(0.0), T(0.0)};
+    for (int i = 0; i < 6; ++i) {
+      const int32_t b = nb[(i + 1) % 6];
+      dr = v3_add(dr, tri_bend_1(m, nb[i], b, tri_nb[6 * (size_t)b + i]));
+    }
+    for (int i = 0; i < 6; ++i) dr = v3_add(dr, tri_bend_2(m, nb[i], nb[(i + 1) % 6], nb[(i + 2) % 6]));
+    nx[m] += P.dt * P.kbend * dr.x;
+    ny[m] += P.dt * P.kbend * dr.y;
+    nz[m] += P.dt * P.kbend * dr.z;
+  }
+
   // cell_interaction, :648-685, for membrane and ALIVE / DEAD / AIR cells
   void interact() {
-    for (int32_t m = 0; m < nmemb; ++m) bend_calc1(m);
-    for (int32_t m = 0; m < nmemb; ++m) bend_calc2(m);
-    for (int32_t m = 0; m < nmemb; ++m) bend_calc3(m);
+    if (tri) {
+      for (int32_t m = 0; m < nmemb; ++m) tri_memb_bend(m);
+    } else {
+      for (int32_t m = 0; m < nmemb; ++m) bend_calc1(m);
+      for (int32_t m = 0; m < nmemb; ++m) bend_calc2(m);
+      for (int32_t m = 0; m < nmemb; ++m) bend_calc3(m);
+    }
     for (int32_t m = 0; m < nmemb; ++m) {  // _MEMB_interaction, :529-547
       if (val(z[m]) < radius[m]) wall(m);
-      for (int32_t i = 0; i < 4; ++i) {
+      for (int32_t i = 0; i < nadj; ++i) {
         const int32_t o = idx[off[m] + i];
         if (state[o] == S_MEMB && m > o) apply(m, o, ci_memb_memb(m, o));
       }
@@ -316,6 +399,11 @@ int run(ora_tissue* o, int32_t n, int32_t nmemb, int32_t nmx, int32_t nmy, doubl
   t.dn.assign(nmemb, T(0.0)); t.dm = t.dn; t.ipn = t.dn; t.ipm = t.dn;
   t.lat_l.resize(nmemb); t.lat_ll.resize(nmemb); t.lat_r.resize(nmemb);
   t.lat_b.resize(nmemb); t.lat_bb.resize(nmemb); t.lat_u.resize(nmemb);
+  t.tri_nb.assign(6 * (size_t)nmemb, 0);
+  if (nmemb > 0 && ora_get_tri_neighbours(o, t.tri_nb.data()) == 0) {
+    t.tri = true;  // TRI_MEMB: six lattice links, tri_memb_bend
+    t.nadj = 6;
+  }
   for (int32_t j = 0; j < nmemb; ++j) {  // _memb_init square branch, cellmanager.cpp:114-158
     const int32_t jj = j % nmx, kk = j / nmx;
     t.lat_l[j] = jj == 0 ? j + nmx - 1 : j - 1;
@@ -375,17 +463,17 @@ extern "C" int ora_tangent_gradient(
     int32_t n, int32_t nmemb, int32_t nder, int32_t nmx, int32_t nmy, double lx, double ly,
     double lz, const double* params14, const double* x, const double* y, const double* z,
     const double* radius, const double* agek, const double* spr_nat_len, const uint8_t* state,
-    const int32_t* pair, const int32_t* rest_div_times, int32_t nsteps, const double* tx,
-    const double* ty, const double* tz, int32_t cells_only, int32_t use_dual, double* loss,
-    double* grad3, double* out_x, double* out_y, double* out_z) {
+    const int32_t* pair, const int32_t* rest_div_times, int32_t lattice, int32_t nsteps,
+    const double* tx, const double* ty, const double* tz, int32_t cells_only, int32_t use_dual,
+    double* loss, double* grad3, double* out_x, double* out_y, double* out_z) {
   if (n <= 0 || nsteps < 0 || !params14 || nder != 0) return ORA_ERR_INVALID_ARG;
   for (int32_t i = 0; i < n; ++i) {
     if (pair && pair[i] >= 0) return ORA_ERR_INVALID_ARG;
     if ((i < nmemb) != (state[i] == S_MEMB)) return ORA_ERR_INVALID_ARG;
     if (i >= nmemb && !is_aad(state[i])) return ORA_ERR_INVALID_ARG;
   }
-  ora_tissue* o = ora_new(n, nmemb, nder, nmx, nmy, lx, ly, lz, params14, x, y, z, radius, agek,
-                          spr_nat_len, state, pair, rest_div_times);
+  ora_tissue* o = ora_new_lattice(n, nmemb, nder, nmx, nmy, lx, ly, lz, params14, x, y, z,
+                                  radius, agek, spr_nat_len, state, pair, rest_div_times, lattice);
   if (!o) return ORA_ERR_INVALID_ARG;
   ora_params p;
   std::memcpy(&p, params14, sizeof(p));

@@ -95,7 +95,7 @@ def lib():
         L.ora_field_get.argtypes = [P, i32, u8, d]
         L.ora_tangent_gradient.argtypes = (
             [ctypes.c_int32] * 5 + [ctypes.c_double] * 3 + [d] * 7 + [u8, i32, i32] +
-            [ctypes.c_int32, d, d, d, ctypes.c_int32, ctypes.c_int32, d, d, d, d, d])
+            [ctypes.c_int32, ctypes.c_int32, d, d, d, ctypes.c_int32, ctypes.c_int32, d, d, d, d, d])
         L.ora_tangent_gradient.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -251,7 +251,7 @@ def tangent_gradient(t, nsteps: int, target=None, cells_only: bool = True, dual:
     rc = L.ora_tangent_gradient(
         t.n, t.nmemb, t.nder, t.nmx, t.nmy, t.lx, t.ly, t.lz, _p(p, ctypes.c_double),
         *[_p(a, ctypes.c_double) for a in keep], _p(st, ctypes.c_uint8),
-        _p(pr, ctypes.c_int32), _p(rd, ctypes.c_int32), nsteps,
+        _p(pr, ctypes.c_int32), _p(rd, ctypes.c_int32), int(getattr(t, "lattice", 0)), nsteps,
         *[(_p(a, ctypes.c_double) if a is not None else None) for a in tgt],
         1 if cells_only else 0, 1 if dual else 0, ctypes.byref(loss),
         _p(grad, ctypes.c_double), *[_p(a, ctypes.c_double) for a in out])

@@ -6,10 +6,13 @@ target made by a run with every force constant +10% (spring, LJ epsilon,
 bending), as the adjoint workload specifies. Gradient: d loss / d (s_spring,
 s_eps, s_bend), the multipliers of those constants at 1.
 
+Tissues: square membranes and a triangular one (TRI_MEMB, the reference's
+default lattice), under ALIVE / DEAD / AIR cells.
+
 Bars: FP64 adjoint vs the FP64 forward-mode reference gradient within 1e-6
 relative per component; vs central differences (h = 1e-4 relative) within
 1e-4 relative; independent of the checkpoint interval; per-tissue results
-of a batch equal single-tissue runs.
+of a batch (one lattice or both) equal single-tissue runs.
 """
 import numpy as np
 import pytest
@@ -17,7 +20,7 @@ import pytest
 from epi_b200 import capi
 from epi_b200 import tissue as T
 from oracle import oracle as O
-from tests.test_oracle_tangent import aged_tissue, min_image_loss
+from tests.test_oracle_tangent import aged_tissue, min_image_loss, tri_tissue
 
 pytestmark = pytest.mark.gpu
 
@@ -47,7 +50,7 @@ def target_of(t, steps):
 
 
 @pytest.mark.parametrize("factory,steps", [(T.config1, 200), (aged_tissue, 200),
-                                           (T.config5, 200)])
+                                           (T.config5, 200), (tri_tissue, 200)])
 def test_adjoint_matches_forward_mode_reference_gradient(built, factory, steps):
     t = factory()
     target = target_of(t, steps)
@@ -58,7 +61,7 @@ def test_adjoint_matches_forward_mode_reference_gradient(built, factory, steps):
         assert abs(grad[0, k] - rgrad[k]) <= 1e-6 * abs(rgrad[k]), (k, grad[0], rgrad)
 
 
-@pytest.mark.parametrize("factory", [T.config1, T.config5])
+@pytest.mark.parametrize("factory", [T.config1, T.config5, tri_tissue])
 def test_adjoint_matches_central_differences(built, factory):
     t = factory()
     steps = 200
@@ -129,10 +132,16 @@ def test_adjoint_rejects_unsupported_tissues_and_arguments(built):
         assert e.value.code == capi.EPI_ERR_INVALID_ARG
 
 
-def test_adjoint_rejects_triangular_membranes(built):
-    t = T.tri_layered_tissue(16, 18, 2, 0)
-    with capi.Context(precision=FP64) as ctx:
-        ctx.upload([t])
-        with pytest.raises(capi.EpiError) as e:
-            ctx.adjoint(5, (t.x, t.y, t.z))
-        assert e.value.code == capi.EPI_ERR_UNSUPPORTED
+def test_adjoint_square_and_triangular_tissues_in_one_batch(built):
+    """A batch mixing both lattices: each tissue's gradient equals its own
+    single-tissue run (the bending-product buffer and the gathers are per
+    tissue and per lattice)."""
+    ta, tb = T.config1(1), tri_tissue()
+    steps = 60
+    tga, tgb = target_of(ta, steps), target_of(tb, steps)
+    loss, grad, _ = gpu_adjoint([ta, tb], steps, [tga, tgb])
+    la, ga, _ = gpu_adjoint([ta], steps, [tga])
+    lb, gb, _ = gpu_adjoint([tb], steps, [tgb])
+    assert loss[0] == pytest.approx(la[0], rel=1e-12) and loss[1] == pytest.approx(lb[0], rel=1e-12)
+    assert np.allclose(grad[0], ga[0], rtol=1e-10, atol=0)
+    assert np.allclose(grad[1], gb[0], rtol=1e-10, atol=0)

@@ -29,6 +29,11 @@ def aged_tissue():
     return t
 
 
+def tri_tissue():
+    """Two cell layers over a 16 x 18 triangular membrane (TRI_MEMB)."""
+    return T.tri_layered_tissue(16, 18, 2, 0)
+
+
 def min_image_loss(t, pos, target):
     d = [pos[k] - target[k] for k in range(3)]
     for k, L in ((0, t.lx), (1, t.ly)):
@@ -43,7 +48,7 @@ def oracle_positions(t, steps, params=None):
     return ora.positions()
 
 
-@pytest.mark.parametrize("factory", [T.config1, aged_tissue])
+@pytest.mark.parametrize("factory", [T.config1, aged_tissue, tri_tissue])
 def test_tangent_value_path_is_the_oracle_bit_for_bit(built, factory):
     t = factory()
     ref = oracle_positions(t, STEPS)
@@ -54,7 +59,7 @@ def test_tangent_value_path_is_the_oracle_bit_for_bit(built, factory):
         assert np.array_equal(dual[k], ref[k])
 
 
-@pytest.mark.parametrize("factory", [T.config1, aged_tissue])
+@pytest.mark.parametrize("factory", [T.config1, aged_tissue, tri_tissue])
 def test_tangent_gradient_matches_central_differences(built, factory):
     t = factory()
     target = oracle_positions(t, STEPS, t.params.scaled(1.1, 1.1, 1.1))
