@@ -11,15 +11,17 @@
 // predicate of connect_proc at X_t (piecewise constant in X), evaluated on
 // the Verlet candidates like the forward step.
 //
-// Terms of D for membrane particles and ALIVE / DEAD / AIR cells (the state
-// set the adjoint supports):
-//   pairs     D_i += DT c(r2) d_ij, c the law of the pair (ljmain below the
-//             radius sum, adhesion above, :103-152); J = c I + 2 c'(r2) d d^T
-//             and D_j gets -DT c d_ij, so (dD/dX)^T lambda at i is
-//             DT sum_j J (lambda_i - lambda_j): a gather over the same lists.
+// Terms of D, for every cell state of the path:
+//   pairs     D_i += DT c(r2) d_ij, c the sum of the laws the reference
+//             applies to the pair from either side (law_of: ljmain, adhesion,
+//             CI_der_to_der, the FIX / MUSUME dermis springs, :103-183,
+//             549-634); J = c I + 2 c'(r2) d d^T and D_j gets -DT c d_ij, so
+//             (dD/dX)^T lambda at i is DT sum_j J (lambda_i - lambda_j): a
+//             gather over the same lists. The pair springs of dividing cells
+//             (CI_pair, :281-285, 637-641) add the same form for the partner.
 //   lattice   the four lattice springs of _MEMB_interaction (CI_memb_to_memb,
 //             :185-234), the same gather over fixed partners.
-//   wall      z += DT W(z) for z < r (:287-294).
+//   wall      z += DT W(z) for z < r, membrane and DER (:287-294, 549-561).
 //   bending   D_k += DT KBEND B_k(stencil sites): square, eleven lattice
 //             sites (_memb_bend_calc1..3, :296-449); triangular, the six
 //             neighbours and six second-ring sites of the twelve dihedral
@@ -54,6 +56,9 @@ __device__ __forceinline__ D3 cross(D3 a, D3 b) {
 struct LawD {
   double c, dc_dr2, c_spring, c_eps;
 };
+__device__ __forceinline__ LawD operator+(const LawD& a, const LawD& b) {
+  return LawD{a.c + b.c, a.dc_dr2 + b.dc_dr2, a.c_spring + b.c_spring, a.c_eps + b.c_eps};
+}
 
 // ljmain (:103-111): c = eps4 u (u - 1) / r2 with u = rs^6 / r2^3.
 __device__ __forceinline__ LawD ljmain_d(const Laws<double>& L, double r2, double rs) {
@@ -64,11 +69,9 @@ __device__ __forceinline__ LawD ljmain_d(const Laws<double>& L, double r2, doubl
   return LawD{c, dc, 0.0, c};
 }
 
-// CI_al_air_de_to_al_air_de_fix_mu (:141-152) with adhesion (:113-124).
-__device__ __forceinline__ LawD aad_d(const Laws<double>& L, double r2, double rs,
-                                      bool both_old) {
-  if (r2 < rs * rs) return ljmain_d(L, r2, rs);
-  const double k = both_old ? L.k_total : L.k_desmosome;
+// adhesion (:113-124) with spring constant k.
+__device__ __forceinline__ LawD adhesion_d(const Laws<double>& L, double r2, double rs,
+                                           double k) {
   const double r = sqrt(r2);
   const double y = r / rs - 1.0;
   if (y + 1.0 > L.lj_thresh) return LawD{0.0, 0.0, 0.0, 0.0};
@@ -77,6 +80,92 @@ __device__ __forceinline__ LawD aad_d(const Laws<double>& L, double r2, double r
   // dc/dr = k y h / r^2 - (k / r) (1 - 3 y^2 / a^2) / rs
   const double dcdr = k * y * h / r2 - (k / r) * (1.0 - 3.0 * y * y / L.ljt1sq) / rs;
   return LawD{c, dcdr / (2.0 * r), c, 0.0};
+}
+
+// CI_al_air_de_to_al_air_de_fix_mu (:141-152).
+__device__ __forceinline__ LawD aad_d(const Laws<double>& L, double r2, double rs,
+                                      bool both_old) {
+  if (r2 < rs * rs) return ljmain_d(L, r2, rs);
+  return adhesion_d(L, r2, rs, both_old ? L.k_total : L.k_desmosome);
+}
+
+// CI_fix_mu_to_fix_mu (:154-162).
+__device__ __forceinline__ LawD fixmu_d(const Laws<double>& L, double r2, double rs) {
+  if (r2 < rs * rs) return ljmain_d(L, r2, rs);
+  return adhesion_d(L, r2, rs, L.k_desmosome);
+}
+
+// CI_mu_to_memb (:164-172) with the MUSUME's spring_force_to_memb.
+__device__ __forceinline__ LawD mu_memb_d(const Laws<double>& L, double r2, double rs,
+                                          uint32_t sfm) {
+  if (r2 < rs * rs) return ljmain_d(L, r2, rs);
+  return adhesion_d(L, r2, rs, sfm_value(sfm, L));
+}
+
+// CI_fix_to_memb (:174-183): c = -(kspring / r) (r / rs - 1) = kspring (1/r - 1/rs).
+__device__ __forceinline__ LawD fix_memb_d(const Laws<double>& L, double r2, double rs) {
+  if (r2 < rs * rs) return ljmain_d(L, r2, rs);
+  const double r = sqrt(r2);
+  const double c = -(L.kspring / r) * (r / rs - 1.0);
+  return LawD{c, -L.kspring / (2.0 * r2 * r), c, 0.0};
+}
+
+// CI_der_to_der (:129-139), dd = r + delta_R, u = (rs / dd)^6, h = u (u - 1):
+// eps4 h / (r dd) + para_ljp2 while dd < rs, para_ljp2 inside the radius
+// sum, eps4 h / r^2 + para_ljp2 beyond; dh/dr = -6 u (2 u - 1) / dd.
+__device__ __forceinline__ LawD der_der_d(const Laws<double>& L, double r2, double rs) {
+  const double r = sqrt(r2);
+  const double dd = r + L.delta_r;
+  if (!(dd < rs) && r2 < rs * rs) return LawD{L.para_ljp2, 0.0, 0.0, 0.0};
+  const double rs2 = rs * rs, dd2 = dd * dd;
+  const double u = rs2 * rs2 * rs2 / (dd2 * dd2 * dd2);
+  const double h = u * (u - 1.0);
+  const double dh = -6.0 * u * (2.0 * u - 1.0) / dd;
+  double ce, dce;
+  if (dd < rs) {
+    const double q = r * dd;
+    ce = L.eps4 * h / q;
+    dce = L.eps4 * (dh / q - h * (dd + r) / (q * q));
+  } else {
+    ce = L.eps4 * h / r2;
+    dce = L.eps4 * (dh / r2 - 2.0 * h / (r2 * r));
+  }
+  return LawD{ce + L.para_ljp2, dce / (2.0 * r), 0.0, ce};
+}
+
+// CI_pair (:281-285): c = -Kdiv (r - rest) / r, rest the higher index's
+// spr_nat_len.
+__device__ __forceinline__ LawD pair_d(const Laws<double>& L, double r2, double rest) {
+  const double r = sqrt(r2);
+  const double c = -(L.kspring_division * (r - rest)) / r;
+  return LawD{c, -L.kspring_division * rest / (2.0 * r2 * r), c, 0.0};
+}
+
+// The law `law` (law_of) as a LawD.
+__device__ __forceinline__ LawD law_d(int law, const Laws<double>& L, double r2, double rs,
+                                      bool both_old, uint32_t sfm) {
+  switch (law) {
+    case L_OTHER: return ljmain_d(L, r2, rs);
+    case L_DER_DER: return der_der_d(L, r2, rs);
+    case L_AAD: return aad_d(L, r2, rs, both_old);
+    case L_FIXMU: return fixmu_d(L, r2, rs);
+    case L_FIX_MEMB: return fix_memb_d(L, r2, rs);
+    case L_MU_MEMB: return mu_memb_d(L, r2, rs, sfm);
+    default: return LawD{0.0, 0.0, 0.0, 0.0};
+  }
+}
+
+// wall_interaction (:287-294): dz = dt eps4 u (u - 1) / (2 z), u = (r / z)^6;
+// adds its adjoint to mu.z and its eps part to g_eps.
+__device__ __forceinline__ void wall_back(const Laws<double>& L, double dt, double z, double rad,
+                                          double lz, D3& mu, double& g_eps) {
+  const double rz = rad / z;
+  const double rz2 = rz * rz;
+  const double u = rz2 * rz2 * rz2;
+  const double W = dt * L.eps4 * u * (u - 1.0) / (2.0 * z);
+  const double dW = -dt * L.eps4 * u * (13.0 * u - 7.0) / (2.0 * z * z);
+  mu.z += dW * lz;
+  g_eps += W * lz;
 }
 
 // CI_memb_to_memb (:185-234), three branches.
@@ -374,17 +463,8 @@ __global__ void __launch_bounds__(256) k_adj_memb(DevState S, const double4* __r
       g_spring += dt * w.c_spring * ld;
       g_eps += dt * w.c_eps * ld;
     }
-    // --- wall: dz = dt eps4 u (u - 1) / (2 z), u = (r / z)^6
-    if (p.z < p.w) {
-      const double z = p.z;
-      const double rz = p.w / z;
-      const double rz2 = rz * rz;
-      const double u = rz2 * rz2 * rz2;
-      const double W = dt * L.eps4 * u * (u - 1.0) / (2.0 * z);
-      const double dW = -dt * L.eps4 * u * (13.0 * u - 7.0) / (2.0 * z * z);
-      mu.z += dW * li.z;
-      g_eps += W * li.z;
-    }
+    // --- wall
+    if (p.z < p.w) wall_back(L, dt, p.z, p.w, li.z, mu, g_eps);
     madj[e] = make_double4(mu.x, mu.y, mu.z, 0.0);
     gmemb[e] = make_double4(g_spring, g_eps, g_bend, 0.0);
   }
@@ -409,6 +489,12 @@ __global__ void __launch_bounds__(256) k_adj_pairs(DevState S, const double4* __
     const D3 li = xyz(lam[i]);
     D3 mu = li;
     double g_spring = 0.0, g_eps = 0.0, g_bend = 0.0;
+    const uint32_t st = attr_state(a);
+    int32_t pair_i = -1, dermis_i = -1;
+    if (st != ST_MEMB) {
+      pair_i = S.pair[i];
+      if (st == ST_FIX || st == ST_MUSUME) dermis_i = S.dermis[i];
+    }
     const int32_t nc = S.ncand[i];
     for (int32_t k = 0; k < nc; ++k) {
       const int32_t q = S.cand[(int64_t)k * N + i];
@@ -418,8 +504,24 @@ __global__ void __launch_bounds__(256) k_adj_pairs(DevState S, const double4* __
       const double r2 = dist_sq_exact(dx, dy, dz);
       const double rs = __dadd_rn(p.w, pq.w);
       if (!(r2 <= __dmul_rn(__dmul_rn(lt2, rs), rs))) continue;  // connect_proc :115-119
-      const bool both_old = attr_old(a) && attr_old(S.attr[q]);
-      const LawD w = aad_d(L, r2, rs, both_old);
+      const uint32_t aq = S.attr[q];
+      const uint32_t sq = attr_state(aq);
+      const bool both_old = attr_old(a) && attr_old(aq);
+      // the laws i applies while iterating q and q applies while iterating i
+      LawD w{0.0, 0.0, 0.0, 0.0};
+      if (st != ST_MEMB) {
+        const int law = law_of(st, (int32_t)i, pair_i, dermis_i, sq, q);
+        if (law != L_NONE) w = w + law_d(law, L, r2, rs, both_old, attr_sfm(a));
+      }
+      if (sq != ST_MEMB) {
+        int32_t pair_q = -1, dermis_q = -1;
+        if (sq == ST_FIX || sq == ST_MUSUME) {
+          pair_q = S.pair[q];
+          dermis_q = S.dermis[q];
+        }
+        const int law = law_of(sq, q, pair_q, dermis_q, st, (int32_t)i);
+        if (law != L_NONE) w = w + law_d(law, L, r2, rs, both_old, attr_sfm(aq));
+      }
       const D3 d = d3(dx, dy, dz);
       const D3 dl = li - xyz(lam[q]);
       mu += dt * (w.c * dl + (2.0 * w.dc_dr2 * dot(d, dl)) * d);
@@ -427,7 +529,21 @@ __global__ void __launch_bounds__(256) k_adj_pairs(DevState S, const double4* __
       g_spring += dt * w.c_spring * ld;
       g_eps += dt * w.c_eps * ld;
     }
-    if (attr_state(a) == ST_MEMB) {
+    // _pair_interaction (:637-641): the spring to the partner, from the
+    // higher index's rest length, in the separation of pair_sep
+    if (pair_i >= 0) {
+      const int32_t q = pair_i;
+      const double4 pq = S.pos_cur[q];
+      double dx, dy, dz;
+      pair_sep(p, pq, i > q, T, dx, dy, dz);
+      const D3 d = d3(dx, dy, dz);
+      const LawD w = pair_d(L, dist_sq_exact(dx, dy, dz), S.spr[i > q ? i : q]);
+      const D3 dl = li - xyz(lam[q]);
+      mu += dt * (w.c * dl + (2.0 * w.dc_dr2 * dot(d, dl)) * d);
+      g_spring += dt * w.c_spring * dot(li, d);
+    }
+    if (st == ST_DER && p.z < p.w) wall_back(L, dt, p.z, p.w, li.z, mu, g_eps);
+    if (st == ST_MEMB) {
       const int32_t j = (int32_t)i - T.pbase;
       const int32_t e = T.mbase + j;
       const int32_t NMX = T.nmx, NMY = T.nmy, jj = j % NMX, kk = j / NMX;

@@ -952,7 +952,6 @@ int epi_adjoint(epi_ctx* c, int32_t nsteps, int32_t K, const epi_loss* loss, dou
       !loss->target_z || loss->reserved != 0 || (loss->cells_only != 0 && loss->cells_only != 1))
     return EPI_ERR_INVALID_ARG;
   if (!c->loaded) return EPI_ERR_STATE;
-  if (!c->lc.simple) return EPI_ERR_UNSUPPORTED;
   EPI_GUARD_BEGIN
   int rc = set_device(c);
   if (rc) return rc;
@@ -1015,6 +1014,8 @@ int epi_adjoint(epi_ctx* c, int32_t nsteps, int32_t K, const epi_loss* loss, dou
       St.pos_cur = hist + (size_t)(t - t0) * n;
       launch_gate_check(St, c->lc, s);
       launch_rebuild(St, whole(c), c->scan, c->lc, s, nullptr);
+      // the dermis of FIX / MUSUME cells at X_t selects their membrane law
+      launch_dermis(St, c->nprep_memb, c->nprep, c->lc, s, nullptr);
       const AdjointBuffers B{lam[a], lam[a ^ 1], bend, madj, gmemb, gpart};
       launch_adjoint_step(St, B, c->lc, s);
       launch_tissue_sum(St, gpart, acc, c->lc, s);

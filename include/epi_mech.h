@@ -266,9 +266,9 @@ typedef struct epi_loss {
  * is recomputed before it is differentiated, so the device holds
  * ceil(nsteps / checkpoint_every) + checkpoint_every position sets.
  * Derivatives are evaluated in FP64 along the trajectory of the context's
- * precision. Square and triangular membranes; tissues must hold only
- * membrane and ALIVE / DEAD / AIR cells without pairs (else
- * EPI_ERR_UNSUPPORTED). loss or grad may be NULL. */
+ * precision. Square and triangular membranes and every cell state of the
+ * path (DER, FIX, MUSUME with their dermis springs, ALIVE / DEAD / AIR, pair
+ * springs). loss or grad may be NULL. */
 int epi_adjoint(epi_ctx* ctx, int32_t nsteps, int32_t checkpoint_every, const epi_loss* loss,
                 double* loss_out, double* grad);
 

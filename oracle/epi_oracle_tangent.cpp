@@ -20,9 +20,11 @@
 // an independent check of a hand-written reverse-mode adjoint.
 //
 // Scope: square or triangular membranes (the triangular bending of
-// tri_memb_bend, :451-508, restated from epi_oracle.c) plus ALIVE / DEAD /
-// AIR cells without pairs (the states of the synthetic tissues); other
-// tissues are rejected.
+// tri_memb_bend, :451-508, restated from epi_oracle.c) and every cell state
+// of the path: DER (CI_der_to_der and the wall), FIX and MUSUME (the
+// dermis springs, CI_fix_mu_to_fix_mu), ALIVE / DEAD / AIR, and the pair
+// springs of dividing cells (:129-183, 281-285, 549-641). The dermis of each
+// step comes from epi_oracle.c's connect, like the lists.
 #include "epi_oracle.h"
 
 #include <cmath>
@@ -76,7 +78,7 @@ inline double val(const Dual& a) { return a.v; }
 inline double val(double a) { return a; }
 using std::sqrt;
 
-enum { S_ALIVE = 0, S_DEAD = 1, S_AIR = 8, S_MEMB = 9 };
+enum { S_ALIVE = 0, S_DEAD = 1, S_FIX = 4, S_DER = 6, S_MUSUME = 7, S_AIR = 8, S_MEMB = 9 };
 inline bool is_aad(uint8_t s) { return s == S_ALIVE || s == S_AIR || s == S_DEAD; }
 
 template <class T>
@@ -87,8 +89,8 @@ inline T pow3(const T& v) { return v * v * v; }
 // Force constants; the three scaled families are T, the rest plain doubles.
 template <class T>
 struct Consts {
-  double dt, p_memb, lj_thresh, thresh_sp;
-  T eps_m, der_der_const, k_total, k_desmosome, kbend;
+  double dt, p_memb, lj_thresh, thresh_sp, delta_r, para_ljp2;
+  T eps_m, der_der_const, k_total, k_desmosome, kbend, kspring, kspring_d, kspring_division;
 };
 
 // vec3 (vec3.h:5-54) over T, operation by operation as epi_oracle.c's v3
@@ -133,8 +135,10 @@ struct Tissue {
   double lx, ly;
   Consts<T> P;
   std::vector<T> x, y, z, nx, ny, nz;
-  std::vector<double> radius, agek;
+  std::vector<double> radius, agek, spr;
   std::vector<uint8_t> state;
+  std::vector<int32_t> pair, rest_div, dermis;
+  std::vector<T> sfm;  // spring_force_to_memb of each MUSUME
   std::vector<int32_t> lat_l, lat_ll, lat_r, lat_b, lat_bb, lat_u;
   std::vector<T> nv, mv, dn, dm, ipn, ipm;
   std::vector<int32_t> off, idx;  // connection lists, the reference's push order
@@ -181,6 +185,45 @@ struct Tissue {
     T spf = P.k_desmosome;
     if (agek[a] > P.thresh_sp && agek[b] > P.thresh_sp) spf = P.k_total;
     return adhesion(a, b, spf);
+  }
+  // CI_der_to_der, :129-139
+  T ci_der_to_der(int32_t a, int32_t b) const {
+    const double rs = radius[a] + radius[b];
+    if (val(sqrt(dist_sq(a, b)) + P.delta_r) < rs) {
+      const T dist = sqrt(dist_sq(a, b));
+      const T dist2 = dist + P.delta_r;
+      const T lj6 = pow6(rs) / pow6(dist2);
+      return 4.0 * P.eps_m * lj6 * (lj6 - 1) / (dist * dist2) + P.para_ljp2;
+    } else if (is_near(a, b)) {
+      return T(P.para_ljp2);
+    }
+    const T dist = sqrt(dist_sq(a, b));
+    const T dist2 = dist + P.delta_r;
+    const T lj6 = pow6(rs) / pow6(dist2);
+    return 4.0 * P.eps_m * lj6 * (lj6 - 1) / (dist * dist) + P.para_ljp2;
+  }
+  // CI_fix_mu_to_fix_mu, :154-162
+  T ci_fixmu(int32_t a, int32_t b) const {
+    if (is_near(a, b)) return ljmain(a, b);
+    return adhesion(a, b, P.k_desmosome);
+  }
+  // CI_mu_to_memb, :164-172
+  T ci_mu_memb(int32_t a, int32_t b) const {
+    if (is_near(a, b)) return ljmain(a, b);
+    return adhesion(a, b, sfm[a]);
+  }
+  // CI_fix_to_memb, :174-183
+  T ci_fix_memb(int32_t a, int32_t b) const {
+    if (is_near(a, b)) return ljmain(a, b);
+    const T distlj = sqrt(dist_sq(a, b));
+    const T lj2 = distlj / (radius[a] + radius[b]);
+    return -(P.kspring / distlj) * (lj2 - 1.0);
+  }
+  // CI_pair, :281-285
+  T ci_pair(int32_t a, int32_t b) const {
+    const T dist = sqrt(dist_sq(a, b));
+    const T force = P.kspring_division * (dist - spr[a]);
+    return -force / dist;
   }
   // CI_memb_to_memb, :185-234
   T ci_memb_memb(int32_t a, int32_t b) const {
@@ -335,15 +378,63 @@ struct Tissue {
         if (state[o] == S_MEMB && m > o) apply(m, o, ci_memb_memb(m, o));
       }
     }
-    for (int32_t c = nmemb; c < n; ++c) {  // _AL_AIR_DE_interaction, :563-579
-      for (int32_t k = off[c]; k < off[c + 1]; ++k) {
-        const int32_t o = idx[k];
-        if (is_aad(state[o])) {
-          if (c > o) apply(c, o, ci_aad(c, o));
-        } else {
-          apply(c, o, ci_aad(c, o));
+    for (int32_t c = nmemb; c < n; ++c) {
+      const uint8_t sc = state[c];
+      if (sc == S_DER) {  // _DER_interaction, :549-561
+        if (val(z[c]) < radius[c]) wall(c);
+        for (int32_t k = off[c]; k < off[c + 1]; ++k) {
+          const int32_t o = idx[k];
+          if (state[o] == S_DER && c > o)
+            apply(c, o, ci_der_to_der(c, o));
+          else
+            apply(c, o, ljmain(c, o));
+        }
+      } else if (sc == S_FIX) {  // _FIX_interaction, :581-604
+        for (int32_t k = off[c]; k < off[c + 1]; ++k) {
+          const int32_t o = idx[k];
+          const uint8_t so = state[o];
+          if (so == S_FIX) {
+            if (pair[c] != o && c > o) apply(c, o, ci_fixmu(c, o));
+          } else if (so == S_MUSUME) {
+            if (pair[c] != o) apply(c, o, ci_fixmu(c, o));
+          } else if (so == S_MEMB) {
+            if (dermis[c] == o)
+              apply(c, o, ci_fix_memb(c, o));
+            else
+              apply(c, o, ljmain(c, o));
+          }
+        }
+      } else if (sc == S_MUSUME) {  // _MUSUME_interaction, :613-634
+        sfm[c] = T(0.0);
+        if (pair[c] >= 0 && state[pair[c]] == S_FIX)
+          sfm[c] = P.kspring;
+        else if (rest_div[c] > 0)
+          sfm[c] = P.kspring_d;
+        for (int32_t k = off[c]; k < off[c + 1]; ++k) {
+          const int32_t o = idx[k];
+          const uint8_t so = state[o];
+          if (so == S_MEMB) {
+            if (dermis[c] == o)
+              apply(c, o, ci_mu_memb(c, o));
+            else
+              apply(c, o, ljmain(c, o));
+          } else if (so == S_MUSUME && pair[c] != o && c > o) {
+            apply(c, o, ci_fixmu(c, o));
+          }
+        }
+      } else if (is_aad(sc)) {  // _AL_AIR_DE_interaction, :563-579
+        for (int32_t k = off[c]; k < off[c + 1]; ++k) {
+          const int32_t o = idx[k];
+          const uint8_t so = state[o];
+          if (is_aad(so)) {
+            if (c > o) apply(c, o, ci_aad(c, o));
+          } else if (so != S_DER) {
+            apply(c, o, ci_aad(c, o));
+          }
         }
       }
+      // _pair_interaction, :637-641
+      if (pair[c] >= 0 && c > pair[c]) apply(c, pair[c], ci_pair(c, pair[c]));
     }
   }
   // pos_copy + cell_pos_periodic_fix (cellmanager.cpp:19-26, 395-414)
@@ -379,9 +470,10 @@ Dual scaled<Dual>(double v, int dir) {
 template <class T>
 int run(ora_tissue* o, int32_t n, int32_t nmemb, int32_t nmx, int32_t nmy, double lx, double ly,
         const ora_params& p, const double* x, const double* y, const double* z,
-        const double* radius, const double* agek, const uint8_t* state, int32_t nsteps,
-        const double* tx, const double* ty, const double* tz, int32_t cells_only, T* loss,
-        double* ox, double* oy, double* oz) {
+        const double* radius, const double* agek, const double* spr, const uint8_t* state,
+        const int32_t* pair, const int32_t* rest_div, int32_t nsteps, const double* tx,
+        const double* ty, const double* tz, int32_t cells_only, T* loss, double* ox, double* oy,
+        double* oz) {
   Tissue<T> t;
   t.n = n; t.nmemb = nmemb; t.nmx = nmx; t.nmy = nmy; t.lx = lx; t.ly = ly;
   t.P.dt = p.dt; t.P.p_memb = p.p_memb; t.P.lj_thresh = p.lj_thresh; t.P.thresh_sp = p.thresh_sp;
@@ -390,11 +482,23 @@ int run(ora_tissue* o, int32_t n, int32_t nmemb, int32_t nmx, int32_t nmy, doubl
   t.P.k_desmosome = scaled<T>(p.k_desmosome, 0);
   t.P.eps_m = scaled<T>(p.eps_m, 1);
   t.P.kbend = scaled<T>(p.kbend, 2);
+  t.P.kspring = scaled<T>(p.kspring, 0);
+  t.P.kspring_d = scaled<T>(p.kspring_d, 0);
+  t.P.kspring_division = scaled<T>(p.kspring_division, 0);
+  t.P.delta_r = p.delta_r;
+  t.P.para_ljp2 = p.para_ljp2;
   t.x.assign(x, x + n); t.y.assign(y, y + n); t.z.assign(z, z + n);
   t.nx = t.x; t.ny = t.y; t.nz = t.z;
   t.radius.assign(radius, radius + n);
   t.agek.assign(agek, agek + n);
   t.state.assign(state, state + n);
+  t.spr.assign(spr, spr + n);
+  t.pair.assign((size_t)n, -1);
+  if (pair) t.pair.assign(pair, pair + n);
+  t.rest_div.assign((size_t)n, 0);
+  if (rest_div) t.rest_div.assign(rest_div, rest_div + n);
+  t.dermis.assign((size_t)n, -1);
+  t.sfm.assign((size_t)n, T(0.0));
   t.nv.assign(3 * (size_t)nmemb, T(0.0)); t.mv = t.nv;
   t.dn.assign(nmemb, T(0.0)); t.dm = t.dn; t.ipn = t.dn; t.ipm = t.dn;
   t.lat_l.resize(nmemb); t.lat_ll.resize(nmemb); t.lat_r.resize(nmemb);
@@ -419,6 +523,7 @@ int run(ora_tissue* o, int32_t n, int32_t nmemb, int32_t nmx, int32_t nmy, doubl
     const int64_t tot = ora_get_connections_raw(o, t.off.data(), nullptr, 0);
     t.idx.assign((size_t)(tot > 0 ? tot : 1), 0);
     ora_get_connections_raw(o, t.off.data(), t.idx.data(), tot);
+    ora_get_dermis(o, t.dermis.data());
   };
   fetch_lists();
   for (int32_t s = 0; s < nsteps; ++s) {
@@ -466,12 +571,9 @@ extern "C" int ora_tangent_gradient(
     const int32_t* pair, const int32_t* rest_div_times, int32_t lattice, int32_t nsteps,
     const double* tx, const double* ty, const double* tz, int32_t cells_only, int32_t use_dual,
     double* loss, double* grad3, double* out_x, double* out_y, double* out_z) {
-  if (n <= 0 || nsteps < 0 || !params14 || nder != 0) return ORA_ERR_INVALID_ARG;
-  for (int32_t i = 0; i < n; ++i) {
-    if (pair && pair[i] >= 0) return ORA_ERR_INVALID_ARG;
+  if (n <= 0 || nsteps < 0 || !params14) return ORA_ERR_INVALID_ARG;
+  for (int32_t i = 0; i < n; ++i)
     if ((i < nmemb) != (state[i] == S_MEMB)) return ORA_ERR_INVALID_ARG;
-    if (i >= nmemb && !is_aad(state[i])) return ORA_ERR_INVALID_ARG;
-  }
   ora_tissue* o = ora_new_lattice(n, nmemb, nder, nmx, nmy, lx, ly, lz, params14, x, y, z,
                                   radius, agek, spr_nat_len, state, pair, rest_div_times, lattice);
   if (!o) return ORA_ERR_INVALID_ARG;
@@ -480,15 +582,16 @@ extern "C" int ora_tangent_gradient(
   int rc;
   if (use_dual) {
     Dual L;
-    rc = run<Dual>(o, n, nmemb, nmx, nmy, lx, ly, p, x, y, z, radius, agek, state, nsteps, tx, ty,
-                   tz, cells_only, &L, out_x, out_y, out_z);
+    rc = run<Dual>(o, n, nmemb, nmx, nmy, lx, ly, p, x, y, z, radius, agek, spr_nat_len, state,
+                   pair, rest_div_times, nsteps, tx, ty, tz, cells_only, &L, out_x, out_y, out_z);
     if (rc == ORA_OK && loss) *loss = L.v;
     if (rc == ORA_OK && grad3)
       for (int k = 0; k < kDir; ++k) grad3[k] = L.d[k];
   } else {
     double L = 0;
-    rc = run<double>(o, n, nmemb, nmx, nmy, lx, ly, p, x, y, z, radius, agek, state, nsteps, tx,
-                     ty, tz, cells_only, &L, out_x, out_y, out_z);
+    rc = run<double>(o, n, nmemb, nmx, nmy, lx, ly, p, x, y, z, radius, agek, spr_nat_len, state,
+                     pair, rest_div_times, nsteps, tx, ty, tz, cells_only, &L, out_x, out_y,
+                     out_z);
     if (rc == ORA_OK && loss) *loss = L;
   }
   ora_free(o);

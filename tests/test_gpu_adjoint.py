@@ -7,7 +7,8 @@ bending), as the adjoint workload specifies. Gradient: d loss / d (s_spring,
 s_eps, s_bend), the multipliers of those constants at 1.
 
 Tissues: square membranes and a triangular one (TRI_MEMB, the reference's
-default lattice), under ALIVE / DEAD / AIR cells.
+default lattice), under ALIVE / DEAD / AIR cells, and tissues with every
+cell state and law (DER, FIX, MUSUME, pairs) on both lattices.
 
 Bars: FP64 adjoint vs the FP64 forward-mode reference gradient within 1e-6
 relative per component; vs central differences (h = 1e-4 relative) within
@@ -29,15 +30,15 @@ MIXED = capi.EPI_PREC_MIXED
 H = 1e-4
 
 
-def gpu_positions(t, steps, params=None, precision=FP64):
-    with capi.Context(precision=precision) as ctx:
+def gpu_positions(t, steps, params=None, precision=FP64, **cfg):
+    with capi.Context(precision=precision, **cfg) as ctx:
         ctx.upload([t], [params] if params is not None else None)
         ctx.step(steps)
         return ctx.positions()
 
 
-def gpu_adjoint(tissues, steps, targets, K=20, precision=FP64, params=None):
-    with capi.Context(precision=precision) as ctx:
+def gpu_adjoint(tissues, steps, targets, K=20, precision=FP64, params=None, **cfg):
+    with capi.Context(precision=precision, **cfg) as ctx:
         ctx.upload(tissues, params)
         tgt = [np.concatenate([tg[k] for tg in targets]) for k in range(3)]
         loss, grad = ctx.adjoint(steps, tgt, checkpoint_every=K)
@@ -45,8 +46,8 @@ def gpu_adjoint(tissues, steps, targets, K=20, precision=FP64, params=None):
     return loss, grad, end
 
 
-def target_of(t, steps):
-    return gpu_positions(t, steps, t.params.scaled(1.1, 1.1, 1.1))
+def target_of(t, steps, **cfg):
+    return gpu_positions(t, steps, t.params.scaled(1.1, 1.1, 1.1), **cfg)
 
 
 @pytest.mark.parametrize("factory,steps", [(T.config1, 200), (aged_tissue, 200),
@@ -117,13 +118,49 @@ def test_adjoint_mixed_precision_close_to_fp64(built):
     assert np.allclose(gmx, g64, rtol=1e-2, atol=0), (gmx, g64)
 
 
-def test_adjoint_rejects_unsupported_tissues_and_arguments(built):
-    t = T.mixed_state_tissue()
-    with capi.Context(precision=FP64, max_conn=96, max_cand=192) as ctx:
-        ctx.upload([t])
-        with pytest.raises(capi.EpiError) as e:
-            ctx.adjoint(5, (t.x, t.y, t.z))
-        assert e.value.code == capi.EPI_ERR_UNSUPPORTED
+MIXED_CFG = dict(max_conn=96, max_cand=192)
+
+
+def mixed_tri():
+    return T.mixed_state_tissue(lattice=T.TRIANGULAR)
+
+
+@pytest.mark.parametrize("factory", [T.mixed_state_tissue, mixed_tri])
+def test_adjoint_all_laws_matches_forward_mode_reference_gradient(built, factory):
+    """Every cell state and law: DER (CI_der_to_der, wall), FIX and MUSUME
+    with their dermis springs, pairs of dividing cells, old cells."""
+    t = factory()
+    steps = 60
+    target = target_of(t, steps, **MIXED_CFG)
+    loss, grad, _ = gpu_adjoint([t], steps, [target], **MIXED_CFG)
+    rloss, rgrad, _ = O.tangent_gradient(t, steps, target=target)
+    assert loss[0] == pytest.approx(rloss, rel=1e-9)
+    for k in range(3):
+        assert abs(grad[0, k] - rgrad[k]) <= 1e-6 * abs(rgrad[k]) + 1e-9 * np.max(np.abs(rgrad)), \
+            (k, grad[0], rgrad)
+
+
+@pytest.mark.parametrize("factory", [T.mixed_state_tissue, mixed_tri])
+def test_adjoint_all_laws_matches_central_differences(built, factory):
+    """Short run: DER laws jump where their branches meet, which central
+    differences must not straddle; the small bending component's bar adds
+    1e-6 of the largest component."""
+    t = factory()
+    steps = 10
+    target = target_of(t, steps, **MIXED_CFG)
+    _, grad, _ = gpu_adjoint([t], steps, [target], **MIXED_CFG)
+    g = grad[0]
+    for k in range(3):
+        e = [1.0, 1.0, 1.0]
+        e[k] = 1.0 + H
+        lp = min_image_loss(t, gpu_positions(t, steps, t.params.scaled(*e), **MIXED_CFG), target)
+        e[k] = 1.0 - H
+        lm = min_image_loss(t, gpu_positions(t, steps, t.params.scaled(*e), **MIXED_CFG), target)
+        fd = (lp - lm) / (2 * H)
+        assert abs(g[k] - fd) <= 1e-4 * abs(fd) + 1e-6 * np.max(np.abs(g)), (k, g[k], fd)
+
+
+def test_adjoint_rejects_invalid_arguments(built):
     t = T.config1()
     with capi.Context(precision=FP64) as ctx:
         ctx.upload([t])

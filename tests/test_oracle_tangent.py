@@ -48,7 +48,12 @@ def oracle_positions(t, steps, params=None):
     return ora.positions()
 
 
-@pytest.mark.parametrize("factory", [T.config1, aged_tissue, tri_tissue])
+def mixed_tri():
+    return T.mixed_state_tissue(lattice=T.TRIANGULAR)
+
+
+@pytest.mark.parametrize("factory", [T.config1, aged_tissue, tri_tissue, T.mixed_state_tissue,
+                                     mixed_tri])
 def test_tangent_value_path_is_the_oracle_bit_for_bit(built, factory):
     t = factory()
     ref = oracle_positions(t, STEPS)
@@ -75,6 +80,32 @@ def test_tangent_gradient_matches_central_differences(built, factory):
         assert abs(fd - grad[k]) <= 1e-5 * abs(grad[k]), (k, fd, grad[k])
 
 
-def test_tangent_rejects_states_outside_its_scope(built):
+@pytest.mark.parametrize("factory", [T.mixed_state_tissue, mixed_tri])
+def test_tangent_gradient_all_laws_matches_central_differences(built, factory):
+    """Every cell state and law (DER, FIX, MUSUME with their dermis springs,
+    pairs). Shorter run: DER pairs have laws that jump where their branches
+    meet (CI_der_to_der at r = r_i + r_j, ljmain at the connection cut-off),
+    which central differences must not straddle. The bending component is
+    small here, so its bar adds 1e-6 of the largest component."""
+    t = factory()
+    steps = 10
+    target = oracle_positions(t, steps, t.params.scaled(1.1, 1.1, 1.1))
+    loss, grad, pos = O.tangent_gradient(t, steps, target=target)
+    assert loss == pytest.approx(min_image_loss(t, pos, target), rel=1e-12)
+    for k in range(3):
+        e = [1.0, 1.0, 1.0]
+        e[k] = 1.0 + H
+        lp = min_image_loss(t, oracle_positions(t, steps, t.params.scaled(*e)), target)
+        e[k] = 1.0 - H
+        lm = min_image_loss(t, oracle_positions(t, steps, t.params.scaled(*e)), target)
+        fd = (lp - lm) / (2 * H)
+        assert abs(fd - grad[k]) <= 1e-5 * abs(grad[k]) + 1e-6 * np.max(np.abs(grad)), \
+            (k, fd, grad[k])
+
+
+def test_tangent_rejects_a_broken_layout(built):
+    t = T.config1()
+    t = t.copy()
+    t.state[0] = T.ALIVE  # a membrane slot that is not a membrane particle
     with pytest.raises(RuntimeError):
-        O.tangent_gradient(T.mixed_state_tissue(), 1)
+        O.tangent_gradient(t, 1)
