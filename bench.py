@@ -52,6 +52,10 @@ def workload(name: str, tissues: int = 512):
             return (T.config4()[:tissues],
                     f"first {tissues} tissues of the batched ensemble (config 4)")
         return T.config4(), "batched ensemble: 512 tissues, side {16..64}, 2-8 layers (config 4)"
+    if name == "tri_ensemble":
+        return (T.config4_tri()[:tissues],
+                f"batched ensemble of {tissues} tissues with triangular membranes (config 4 "
+                f"shapes, TRI_MEMB)")
     if name == "c2":
         return [T.config2()], "single tissue 64x64 membrane + 32,768 cells (config 2)"
     if name == "c3":
@@ -337,7 +341,8 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "c1", "c2", "c3"])
+    ap.add_argument("--workload", default="ensemble",
+                    choices=["ensemble", "tri_ensemble", "c1", "c2", "c3"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--skin", type=float, default=None,
                     help="candidate skin (default: chosen by the autotuner)")

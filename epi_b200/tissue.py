@@ -291,6 +291,31 @@ def config4(seed: int = 3, n_tissues: int = 512,
                            name=f"C4[{t}]") for t in indices]
 
 
+def tri_rows(side: int, spacing: float = 1.0) -> int:
+    """An even row count near `side` for a triangular membrane whose box
+    (rows * spacing * sqrt(3) / 2 in y) the reference's grid covers: it has
+    (int)(LY / 2 + 0.5) bins of 2.0 (cell_connection.cpp:22-26), so LY must
+    not round down."""
+    for rows in range(side + side % 2, side + 32, 2):
+        ly = rows * spacing * math.sqrt(3.0) / 2.0
+        if int(ly / 2.0 + 0.5) * 2.0 >= ly:
+            return rows
+    raise ValueError("no row count found")
+
+
+def config4_tri(seed: int = 3, n_tissues: int = 512,
+                indices: Optional[Sequence[int]] = None) -> List[Tissue]:
+    """The ensemble of config4 with triangular membranes (TRI_MEMB, the
+    reference's default lattice): same sides, layers and constants, rows =
+    tri_rows(side), cells on the same lattice."""
+    specs = config4_specs(seed, n_tissues)
+    if indices is None:
+        indices = range(n_tissues)
+    return [tri_layered_tissue(specs[t][0], tri_rows(specs[t][0]), specs[t][1],
+                               mix_seed(seed, t, 1), params=specs[t][2], name=f"C4T[{t}]")
+            for t in indices]
+
+
 def config5(seed: int = 4) -> Tissue:
     """Adjoint case: config-2 geometry (64x64 membrane, 32,768 cells)."""
     return layered_tissue(64, 8, seed, name="C5")
