@@ -91,6 +91,12 @@ def test_host_step_general_laws_and_aliased_arrays(built):
     assert_same(host_steps(tissues, 25, FP64, alias=True, **cfg), ref)
 
 
+def test_host_step_triangular_membranes(built):
+    tissues = [T.mixed_state_tissue(lattice=T.TRIANGULAR), T.tri_layered_tissue(16, 18, 2, 0)]
+    cfg = dict(max_conn=96, max_cand=192)
+    assert_same(host_steps(tissues, 20, MIXED, **cfg), three_call_steps(tissues, 20, MIXED, **cfg))
+
+
 def test_host_step_rejects_bad_arrays(built):
     t = T.config1(1)
     with capi.Context(precision=MIXED) as ctx:
