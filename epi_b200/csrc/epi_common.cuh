@@ -402,6 +402,30 @@ __host__ __device__ __forceinline__ int32_t tri_link(int32_t j, int k, int32_t N
   }
 }
 
+// tri_link as a step from (column, row): the same wiring with conditional
+// wraps instead of integer divisions (rows alternate their offset; NMY is
+// even, so the row wrap keeps the alternation).
+struct TriSite {
+  int32_t col, row;
+};
+__device__ __forceinline__ TriSite tri_step(TriSite s, int k, int32_t NMX, int32_t NMY) {
+  const bool even = (s.row & 1) == 0;
+  int32_t c = s.col, r = s.row;
+  switch (k) {
+    case 0: c += 1; break;
+    case 1: r -= 1; c += even ? 0 : 1; break;
+    case 2: r -= 1; c -= even ? 1 : 0; break;
+    case 3: c -= 1; break;
+    case 4: r += 1; c -= even ? 1 : 0; break;
+    default: r += 1; c += even ? 0 : 1; break;
+  }
+  c += c < 0 ? NMX : 0;
+  c -= c >= NMX ? NMX : 0;
+  r += r < 0 ? NMY : 0;
+  r -= r >= NMY ? NMY : 0;
+  return TriSite{c, r};
+}
+
 // The k-th lattice link of membrane particle j in connected_cell's push
 // order: square l, r, b, u (cellmanager.cpp:160-163), triangular memb[0..5].
 __device__ __forceinline__ int32_t lattice_link(const TissueDev& T, int32_t j, int k) {

@@ -722,21 +722,21 @@ __device__ __forceinline__ Vec3<R> v3_unit(const Vec3<R>& a) {
 
 // Triangular-membrane bending of particle j (tri_memb_bend, tri_bend_1 and
 // tri_bend_2, cell_interaction.cpp:451-508) from the offsets of its six
-// lattice neighbours n[i] = memb[i] and of the six second-ring sites
-// c[i] = memb[(i+1)%6]->memb[i]; the particle itself is the origin. Returns
+// lattice neighbours n[i] = memb[i] (indices nb[i]) and of the six
+// second-ring sites c[i] = memb[(i+1)%6]->memb[i] (indices ring[i]); the
+// particle itself is the origin. Returns
 // the sum dr before the DT * KBEND factor. The reference divides each term
 // by the norm of a normal it has already normalised in place
 // (vec3::normalize, vec3.h:40-44), i.e. by 1 up to rounding; that division
 // is left out.
 template <typename R, typename Off>
-__device__ __forceinline__ Vec3<R> tri_bending(const Off& off, int32_t j, int32_t NMX,
-                                               int32_t nm, int32_t pb) {
+__device__ __forceinline__ Vec3<R> tri_bending(const Off& off, const int32_t (&nb)[6],
+                                               const int32_t (&ring)[6]) {
   Vec3<R> n[6], c[6];
 #pragma unroll
-  for (int i = 0; i < 6; ++i) n[i] = off(pb + tri_link(j, i, NMX, nm));
+  for (int i = 0; i < 6; ++i) n[i] = off(nb[i]);
 #pragma unroll
-  for (int i = 0; i < 6; ++i)
-    c[i] = off(pb + tri_link(tri_link(j, (i + 1) % 6, NMX, nm), i, NMX, nm));
+  for (int i = 0; i < 6; ++i) c[i] = off(ring[i]);
   Vec3<R> dr{R(0), R(0), R(0)};
 #pragma unroll
   for (int i = 0; i < 6; ++i) {
@@ -799,8 +799,32 @@ __device__ __forceinline__ double3 memb_force(const DevState& S, int32_t i) {
     const double4 p = S.pos_cur[i];
     const SiteOffsets<R> off(S, i, p, T);
     double ax = 0.0, ay = 0.0, az = 0.0;
-    if (T.lattice == kLatticeTriangular) {
-      const Vec3<R> b = tri_bending<R>(off, j, NMX, T.nmemb, pb);
+    // lattice links in connected_cell's order (square: l, r, b, u)
+    int32_t nb[6];
+    const bool tri = T.lattice == kLatticeTriangular;
+    if (tri) {
+      const TriSite s0{jj, kk};
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        const TriSite a = tri_step(s0, k, NMX, NMY);
+        nb[k] = pb + a.row * NMX + a.col;
+      }
+    } else {
+      nb[0] = site(-1, 0);
+      nb[1] = site(1, 0);
+      nb[2] = site(0, -1);
+      nb[3] = site(0, 1);
+      nb[4] = nb[5] = nb[0];
+    }
+    if (tri) {
+      int32_t ring[6];
+      const TriSite s0{jj, kk};
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        const TriSite a = tri_step(tri_step(s0, (k + 1) % 6, NMX, NMY), k, NMX, NMY);
+        ring[k] = pb + a.row * NMX + a.col;
+      }
+      const Vec3<R> b = tri_bending<R>(off, nb, ring);
       const R s = R(dt * T.P.kbend);
       ax += double(s * b.x);
       ay += double(s * b.y);
@@ -846,7 +870,7 @@ __device__ __forceinline__ double3 memb_force(const DevState& S, int32_t i) {
       }
     }
     for (int k = 0; k < T.nadj; ++k) {
-      const int32_t q = pb + lattice_link(T, j, k);
+      const int32_t q = nb[k];
       const bool hi = i > q;
       R dx, dy, dz, rs, d2;
       if constexpr (sizeof(R) == 4) {
