@@ -345,7 +345,8 @@ __global__ void k_binsort(DevState S) {
   const int32_t nbg = S.rl_bpre[cnt];
   for (int32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < nbg; g += gridDim.x * blockDim.x) {
     const int32_t k = locate(S.rl_bpre, cnt, g);
-    const int32_t b = S.tissues[S.rl_list[k]].binbase + (g - S.rl_bpre[k]);
+    const TissueDev& T = S.tissues[S.rl_list[k]];
+    const int32_t b = T.binbase + (g - S.rl_bpre[k]);
     const int32_t s0 = S.starts[b], s1 = S.starts[b + 1];
     if (s1 <= s0) continue;
     S.counts[b] = 0;  // ready for the next binning
@@ -378,8 +379,11 @@ __global__ void k_binsort(DevState S) {
       const uint32_t gi = S.skey[s];
       const bool memb = attr_state(S.attr[gi]) == ST_MEMB;
       S.skey[s] = gi | (memb ? 0x80000000u : 0u);
+      // x and y as grid_init bins them (ref_bin): in [0, L)
       const double4 pg = S.pos_cur[gi];
-      S.spos[s] = make_float4((float)pg.x, (float)pg.y, (float)pg.z, (float)pg.w);
+      const double xc = 0.5 * T.lx - pdiff(0.5 * T.lx, pg.x, T.lx);
+      const double yc = 0.5 * T.ly - pdiff(0.5 * T.ly, pg.y, T.ly);
+      S.spos[s] = make_float4((float)xc, (float)yc, (float)pg.z, (float)pg.w);
     }
   }
 }
@@ -387,8 +391,11 @@ __global__ void k_binsort(DevState S) {
 // Bin ranges (inclusive) of the periodic window [x-R, x+R] along one axis:
 // at most two ranges, because the window may wrap once. Bin k holds
 // [k*AG, (k+1)*AG) of [0, L) (the last one is shortened; AG*AN > L).
+// off[r]: the image of range r's particles nearest to x is their binned
+// coordinate + off[r] (0, or +-L for the wrapped part of a split window).
 __device__ __forceinline__ int window_ranges(double x, double R, double L, int32_t an,
-                                             int32_t lo[2], int32_t hi[2]) {
+                                             int32_t lo[2], int32_t hi[2], double off[2]) {
+  off[0] = off[1] = 0.0;
   if (2.0 * R >= L) {
     lo[0] = 0;
     hi[0] = an - 1;
@@ -404,12 +411,14 @@ __device__ __forceinline__ int window_ranges(double x, double R, double L, int32
   if (a < 0.0) {
     lo[0] = 0; hi[0] = bin_of(b);
     lo[1] = bin_of(a + L); hi[1] = an - 1;
+    off[1] = -L;
     if (lo[1] <= hi[0]) { hi[0] = an - 1; return 1; }
     return 2;
   }
   if (b >= L) {
     lo[0] = bin_of(a); hi[0] = an - 1;
     lo[1] = 0; hi[1] = bin_of(b - L);
+    off[1] = L;
     if (hi[1] >= lo[0]) { lo[0] = 0; return 1; }
     return 2;
   }
@@ -425,12 +434,17 @@ __device__ __forceinline__ int window_ranges(double x, double R, double L, int32
 // is a superset for every pair it can connect (reach <= 1.2 * 3.2 < 2 * 2.0).
 // Candidates come out in column order (x ranges outer, y ranges inner), slot
 // order within a column: deterministic after k_binsort.
+// Slot positions are the grid's canonical [0, L) coordinates, so every
+// particle of a window's x (or y) range has the same nearest image: the
+// range's offset is folded into the particle's own coordinate (pxe, pye)
+// and no per-slot wrap is needed. Boxes below 2 (R + AG) keep the per-slot
+// minimum image (wrap_x, wrap_y): there an edge bin may hold the other image.
 struct SearchWindow {
   int32_t xlo[2], xhi[2], ylo[2], yhi[2];
   int nxr, nyr;
   int32_t z0, z1;
-  float px, py, pz, pw, flx, fly, fhx, fhy, flt, fskin;
-  bool memb_i;
+  float pxe[2], pye[2], pz, pw, flx, fly, fhx, fhy, flt, fskin;
+  bool memb_i, wrap_x, wrap_y;
 
   __device__ __forceinline__ SearchWindow(const DevState& S, const TissueDev& T, int32_t i) {
     constexpr double kInvAG = 1.0 / kAreaGrid;
@@ -442,16 +456,22 @@ struct SearchWindow {
     // float coordinates up to the box size (and the window widens with it).
     const double margin = 1e-4 + 5e-7 * (T.lx > T.ly ? T.lx : T.ly) + 5e-7 * T.lz;
     const double R = lt * (p.w + (memb_i ? T.rmax_nm : T.rmax)) + skin + margin + 1e-6;
-    nxr = window_ranges(p.x, R, T.lx, T.anx, xlo, xhi);
-    nyr = window_ranges(p.y, R, T.ly, T.any, ylo, yhi);
+    double offx[2], offy[2];
+    nxr = window_ranges(p.x, R, T.lx, T.anx, xlo, xhi, offx);
+    nyr = window_ranges(p.y, R, T.ly, T.any, ylo, yhi, offy);
+    wrap_x = !(T.lx > 2.0 * (R + kAreaGrid));
+    wrap_y = !(T.ly > 2.0 * (R + kAreaGrid));
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      pxe[r] = (float)(wrap_x ? p.x : p.x - offx[r]);
+      pye[r] = (float)(wrap_y ? p.y : p.y - offy[r]);
+    }
     // z bins are floor(max(z, 0) / AG) (ref_bin); the margin in R covers the
     // multiply-for-divide rounding, so [z - R, z + R] needs no extra bins
     z0 = (int32_t)floor((p.z - R) * kInvAG);
     z1 = (int32_t)floor((p.z + R) * kInvAG);
     z0 = z0 < 0 ? 0 : (z0 > T.anz - 1 ? T.anz - 1 : z0);
     z1 = z1 < 0 ? 0 : (z1 > T.anz - 1 ? T.anz - 1 : z1);
-    px = (float)p.x;
-    py = (float)p.y;
     pz = (float)p.z;
     pw = (float)p.w;
     flx = (float)T.lx;
@@ -461,13 +481,15 @@ struct SearchWindow {
     flt = (float)lt;
     fskin = (float)(skin + margin);
   }
-  // Is the particle in slot s (key, FP32 copy q) a candidate of i?
-  __device__ __forceinline__ bool hit(int32_t i, uint32_t key, const float4& q) const {
+  // Is the particle in slot s (key, FP32 copy q) of a column of x range xr
+  // and y range yr a candidate of i? (ex, ey: pxe[xr], pye[yr])
+  __device__ __forceinline__ bool hit(int32_t i, uint32_t key, const float4& q, float ex,
+                                      float ey) const {
     const int32_t j = (int32_t)(key & 0x7fffffffu);
     if (j == i || (memb_i && (key >> 31))) return false;
-    float dx = px - q.x, dy = py - q.y;
-    dx = dx > fhx ? dx - flx : (dx <= -fhx ? dx + flx : dx);
-    dy = dy > fhy ? dy - fly : (dy <= -fhy ? dy + fly : dy);
+    float dx = ex - q.x, dy = ey - q.y;
+    if (wrap_x) dx = dx > fhx ? dx - flx : (dx <= -fhx ? dx + flx : dx);
+    if (wrap_y) dy = dy > fhy ? dy - fly : (dy <= -fhy ? dy + fly : dy);
     const float dz = pz - q.z;
     const float reach = flt * (pw + q.w) + fskin;
     return dx * dx + dy * dy + dz * dz <= reach * reach;
@@ -506,8 +528,11 @@ __device__ __forceinline__ void cand_search_warps(const DevState& S, int32_t cnt
     for (int32_t c0 = 0; c0 < ncol; c0 += 32) {
       const int32_t c = c0 + lane;
       int32_t lo = 0, len = 0;
+      float cex = 0.f, cey = 0.f;
       if (c < ncol) {
         const int32_t cx = c / ncy, cy = c - cx * ncy;
+        cex = W.pxe[cx < nx0 ? 0 : 1];
+        cey = W.pye[cy < ny0 ? 0 : 1];
         const int32_t bx = cx < nx0 ? W.xlo[0] + cx : W.xlo[1] + (cx - nx0);
         const int32_t by = cy < ny0 ? W.ylo[0] + cy : W.ylo[1] + (cy - ny0);
         const int32_t col = T.binbase + (bx * T.any + by) * T.anz;
@@ -527,11 +552,12 @@ __device__ __forceinline__ void cand_search_warps(const DevState& S, int32_t cnt
           if (e <= f) k += step;
         }
         const int32_t s = __shfl_sync(0xffffffffu, lo, k) + (f - __shfl_sync(0xffffffffu, excl, k));
+        const float ex = __shfl_sync(0xffffffffu, cex, k), ey = __shfl_sync(0xffffffffu, cey, k);
         bool hit = false;
         uint32_t key = 0;
         if (f < total) {
           key = S.skey[s];
-          hit = W.hit(i, key, S.spos[s]);
+          hit = W.hit(i, key, S.spos[s], ex, ey);
         }
         const unsigned m = __ballot_sync(0xffffffffu, hit);
         if (hit) {
@@ -562,8 +588,10 @@ __device__ __forceinline__ void cand_search_threads(const DevState& S, int32_t c
     const int32_t any = T.any, anz = T.anz, binbase = T.binbase;
     int32_t count = 0;
     for (int xr = 0; xr < W.nxr; ++xr) {
+      const float ex = W.pxe[xr];
       for (int32_t bx = W.xlo[xr]; bx <= W.xhi[xr]; ++bx) {
         for (int yr = 0; yr < W.nyr; ++yr) {
+          const float ey = W.pye[yr];
           for (int32_t by = W.ylo[yr]; by <= W.yhi[yr]; ++by) {
             const int32_t col = binbase + (bx * any + by) * anz;
             const int32_t s_hi = S.starts[col + W.z1 + 1];
@@ -577,7 +605,7 @@ __device__ __forceinline__ void cand_search_threads(const DevState& S, int32_t c
               }
 #pragma unroll
               for (int u = 0; u < 4; ++u) {
-                if (s + u < s_hi && W.hit(i, key[u], q[u])) {
+                if (s + u < s_hi && W.hit(i, key[u], q[u], ex, ey)) {
                   if (count < cap) S.cand[(int64_t)count * N + i] = (int32_t)(key[u] & 0x7fffffffu);
                   ++count;
                 }
@@ -594,7 +622,7 @@ __device__ __forceinline__ void cand_search_threads(const DevState& S, int32_t c
 // Below this many gated particles the warp-per-particle search is faster.
 constexpr int32_t kWarpSearchMax = 48 * 1024;
 
-__global__ void k_cand_search(DevState S, int32_t clear_any) {
+__global__ void __launch_bounds__(256, 4) k_cand_search(DevState S, int32_t clear_any) {
   pdl_entry();
   count_launch(S.launches);
   const int32_t cnt = S.rl_count[0];
