@@ -344,8 +344,9 @@ cudaError_t capture_conditional_rebuild(epi_ctx* c, int cur) {
 }
 
 // The step graph of parity c->cur: one launch runs a whole sequence of steps.
-// A WHILE node repeats its body -- two steps (per step: the conditional
-// rebuild, the prepass and the fused step), then a one-thread kernel that
+// A WHILE node repeats its body -- two steps (per step: the membrane sums
+// forked beside the conditional rebuild, the dermis, the fused step), then a
+// one-thread kernel that
 // counts down the passes left (set before each launch) and sets the loop
 // condition -- so the device drives the loop and the host launches once.
 cudaError_t capture_step_graph(epi_ctx* c, cudaGraphExec_t* out) {
