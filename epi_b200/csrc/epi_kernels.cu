@@ -1411,11 +1411,14 @@ void launch_prepass(const DevState& S, int32_t m0, int32_t m1, int32_t f0, int32
 template <typename R, bool kSimple, bool kOld>
 void launch_step_v(const DevState& S, const Range& r, const LaunchCfg& lc, cudaStream_t s) {
   const int grid = blocks_for(r.p1 - r.p0, 256);
+  // resident 256-thread blocks per SM of each tuning variant: the FP64
+  // kernel needs more registers (4 blocks spill; 2 and 3 do not)
+  constexpr bool kF = sizeof(R) == 4;
   switch (lc.variant) {
-    case 2: launch_pdl(k_step<R, kSimple, kOld, 5>, grid, 256, s, S, r); break;
-    case 3: launch_pdl(k_step<R, kSimple, kOld, 6>, grid, 256, s, S, r); break;
-    case 4: launch_pdl(k_step<R, kSimple, kOld, 3>, grid, 256, s, S, r); break;
-    default: launch_pdl(k_step<R, kSimple, kOld, 4>, grid, 256, s, S, r); break;
+    case 2: launch_pdl(k_step<R, kSimple, kOld, kF ? 5 : 2>, grid, 256, s, S, r); break;
+    case 3: launch_pdl(k_step<R, kSimple, kOld, kF ? 6 : 4>, grid, 256, s, S, r); break;
+    case 4: launch_pdl(k_step<R, kSimple, kOld, kF ? 3 : 5>, grid, 256, s, S, r); break;
+    default: launch_pdl(k_step<R, kSimple, kOld, kF ? 4 : 3>, grid, 256, s, S, r); break;
   }
 }
 
