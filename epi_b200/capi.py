@@ -39,7 +39,7 @@ EXPORTED = [
     "epi_params_default", "epi_config_default", "epi_strerror", "epi_create", "epi_destroy",
     "epi_upload", "epi_connect", "epi_interact_commit", "epi_step", "epi_step_graph",
     "epi_step_per_tissue", "epi_sync", "epi_num_particles", "epi_download_positions",
-    "epi_upload_positions", "epi_step_host", "epi_get_connections", "epi_get_dermis", "epi_error_info",
+    "epi_upload_positions", "epi_step_host", "epi_step_host_async", "epi_get_connections", "epi_get_dermis", "epi_error_info",
     "epi_stream", "epi_rebuild_count", "epi_launch_count", "epi_time_kernels", "epi_autotune",
     "epi_field_init",
     "epi_field_step", "epi_field_get", "epi_field_set_ext", "epi_adjoint", "epi_connect_noalloc",
@@ -122,6 +122,7 @@ def lib():
         L.epi_download_positions.argtypes = [vp, _dp, _dp, _dp]
         L.epi_upload_positions.argtypes = [vp, _dp, _dp, _dp]
         L.epi_step_host.argtypes = [vp, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.epi_step_host_async.argtypes = [vp, _dp, _dp, _dp, _dp, _dp, _dp]
         L.epi_get_connections.argtypes = [vp, _ip, _ip, ctypes.c_int64,
                                           ctypes.POINTER(ctypes.c_int64)]
         L.epi_get_dermis.argtypes = [vp, _ip]
@@ -289,10 +290,12 @@ class Context:
                                           _ptr(y, ctypes.c_double), _ptr(z, ctypes.c_double)),
                "epi_upload_positions")
 
-    def step_host(self, pos_in, pos_out=None):
+    def step_host(self, pos_in, pos_out=None, wait: bool = True):
         """epi_step_host: one step of a batch whose positions are in host
         memory (x, y, z arrays in, new positions out; the same arrays may be
-        given for both). Pinned host arrays let the copies overlap."""
+        given for both). Pinned host arrays let the copies overlap. With
+        wait=False (epi_step_host_async) the call returns once the step is
+        queued; the arrays are valid after sync()."""
         x, y, z = pos_in
         for a in (x, y, z):
             if a.dtype != np.float64 or not a.flags.c_contiguous or a.shape != (self.n,):
@@ -300,8 +303,9 @@ class Context:
         if pos_out is None:
             pos_out = (np.empty(self.n), np.empty(self.n), np.empty(self.n))
         ox, oy, oz = pos_out
-        _check(lib().epi_step_host(self._h, *(_ptr(a, ctypes.c_double) for a in (x, y, z, ox, oy, oz))),
-               "epi_step_host")
+        fn = lib().epi_step_host if wait else lib().epi_step_host_async
+        _check(fn(self._h, *(_ptr(a, ctypes.c_double) for a in (x, y, z, ox, oy, oz))),
+               "epi_step_host" if wait else "epi_step_host_async")
         return pos_out
 
     def connections(self):

@@ -111,7 +111,7 @@ struct epi_ctx {
   double* stage = nullptr;        // 3n doubles: x | y | z for host transfers
   // epi_step_host: copy streams, per-chunk events, the outbound staging (3n)
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
-  std::vector<cudaEvent_t> ev_in, ev_done;
+  std::vector<cudaEvent_t> ev_in, ev_done, ev_d2h;
   double* stage_out = nullptr;
   DevStatus* status = nullptr;
   DevStatus* status_h = nullptr;  // pinned
@@ -700,8 +700,11 @@ void epi_destroy(epi_ctx* ctx) {
   if (ctx->loop_left) cudaFree(ctx->loop_left);
   if (ctx->launches) cudaFree(ctx->launches);
   if (ctx->status_h) cudaFreeHost(ctx->status_h);
+  if (ctx->copy_in) cudaStreamSynchronize(ctx->copy_in);
+  if (ctx->copy_out) cudaStreamSynchronize(ctx->copy_out);
   for (cudaEvent_t e : ctx->ev_in) cudaEventDestroy(e);
   for (cudaEvent_t e : ctx->ev_done) cudaEventDestroy(e);
+  for (cudaEvent_t e : ctx->ev_d2h) cudaEventDestroy(e);
   if (ctx->copy_in) cudaStreamDestroy(ctx->copy_in);
   if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
   if (ctx->aux) cudaStreamSynchronize(ctx->aux);
@@ -1300,6 +1303,8 @@ int epi_sync(epi_ctx* c) {
   EPI_GUARD_BEGIN
   int rc = set_device(c);
   if (rc) return rc;
+  // outbound copies of host steps run on their own stream
+  if (c->copy_out) EPI_CUDA(cudaStreamSynchronize(c->copy_out));
   return check_status(c);
   EPI_GUARD_END
 }
@@ -1354,16 +1359,14 @@ int epi_upload_positions(epi_ctx* c, const double* x, const double* y, const dou
 // group's inbound copies, its kernels and its outbound copies run on three
 // streams, so one group's copies overlap the next group's copies in the
 // other direction and the compute between them. Tissues never interact, so
-// the result equals the three calls'. Returns once the new positions are in
-// x_out, y_out, z_out (which may be the input arrays).
-int epi_step_host(epi_ctx* c, const double* x_in, const double* y_in, const double* z_in,
-                  double* x_out, double* y_out, double* z_out) {
-  if (!c || !x_in || !y_in || !z_in || !x_out || !y_out || !z_out) return EPI_ERR_INVALID_ARG;
-  if (!c->loaded) return EPI_ERR_STATE;
-  EPI_GUARD_BEGIN
-  int rc = set_device(c);
-  if (rc) return rc;
+// the result equals the three calls'. Successive calls pipeline: a group's
+// inbound copy and its unpack into the outbound staging wait only for the
+// previous call's outbound copy of the same group (the host arrays may be
+// the same for input and output, and the staging regions are reused).
+static int enqueue_host_step(epi_ctx* c, const double* x_in, const double* y_in,
+                             const double* z_in, double* x_out, double* y_out, double* z_out) {
   const int64_t n = c->n;
+  int rc;
   if (!c->copy_in)
     EPI_CUDA(cudaStreamCreateWithFlags(&c->copy_in, cudaStreamNonBlocking));
   if (!c->copy_out)
@@ -1372,11 +1375,13 @@ int epi_step_host(epi_ctx* c, const double* x_in, const double* y_in, const doub
   // groups: whole tissues, split at multiples of n / K particles
   const int K = std::min(kHostStepGroups, c->ntissues);
   while ((int)c->ev_in.size() < K) {
-    cudaEvent_t a, b;
+    cudaEvent_t a, b, d;
     EPI_CUDA(cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
     EPI_CUDA(cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
+    EPI_CUDA(cudaEventCreateWithFlags(&d, cudaEventDisableTiming));
     c->ev_in.push_back(a);
     c->ev_done.push_back(b);
+    c->ev_d2h.push_back(d);
   }
   std::vector<int> split{0};
   for (int t = 0, k = 1; t < c->ntissues && k < K; ++t) {
@@ -1389,10 +1394,10 @@ int epi_step_host(epi_ctx* c, const double* x_in, const double* y_in, const doub
   split.push_back(c->ntissues);
   double* in = c->stage;
   double* out = c->stage_out;
-  // the compute stream's earlier work (a previous step) precedes the copies
+  // the compute stream's earlier work (a previous step, an upload through
+  // the same inbound staging) precedes this step's inbound copies
   EPI_CUDA(cudaEventRecord(c->ev_done[0], c->stream));
   EPI_CUDA(cudaStreamWaitEvent(c->copy_in, c->ev_done[0], 0));
-  EPI_CUDA(cudaStreamWaitEvent(c->copy_out, c->ev_done[0], 0));
   const int cur = c->cur;
   const DevState S = make_state(c, cur);
   const DevState Snew = make_state(c, cur ^ 1);
@@ -1403,6 +1408,9 @@ int epi_step_host(epi_ctx* c, const double* x_in, const double* y_in, const doub
     const int32_t p0 = A.pbase, p1 = B.pbase + B.n;
     const size_t off = (size_t)p0, bytes = sizeof(double) * (size_t)(p1 - p0);
     const double* src[3] = {x_in, y_in, z_in};
+    // the previous call's outbound copy of this group may still write the
+    // host arrays this copy reads
+    EPI_CUDA(cudaStreamWaitEvent(c->copy_in, c->ev_d2h[g], 0));
     for (int k = 0; k < 3; ++k)
       EPI_CUDA(cudaMemcpyAsync(in + k * n + off, src[k] + off, bytes, cudaMemcpyHostToDevice,
                                c->copy_in));
@@ -1417,6 +1425,8 @@ int epi_step_host(epi_ctx* c, const double* x_in, const double* y_in, const doub
                    c->nprep_memb + HB.prep_f + HB.nfm, c->cfg.precision, c->lc, c->stream,
                    nullptr);
     launch_step(S, r, c->cfg.precision, c->lc, c->stream, nullptr);
+    // ... and may still read this group's outbound staging
+    EPI_CUDA(cudaStreamWaitEvent(c->stream, c->ev_d2h[g], 0));
     launch_unpack_range(Snew, out, out + n, out + 2 * n, p0, p1, c->lc, c->stream);
     EPI_CUDA(cudaEventRecord(c->ev_done[g], c->stream));
     EPI_CUDA(cudaStreamWaitEvent(c->copy_out, c->ev_done[g], 0));
@@ -1424,15 +1434,35 @@ int epi_step_host(epi_ctx* c, const double* x_in, const double* y_in, const doub
     for (int k = 0; k < 3; ++k)
       EPI_CUDA(cudaMemcpyAsync(dst[k] + off, out + k * n + off, bytes, cudaMemcpyDeviceToHost,
                                c->copy_out));
+    EPI_CUDA(cudaEventRecord(c->ev_d2h[g], c->copy_out));
   }
   c->cur ^= 1;
   c->posf_stale = false;
   c->lists_fresh = false;
-  // later work on the compute stream waits for the outbound copies
-  EPI_CUDA(cudaEventRecord(c->ev_in[0], c->copy_out));
-  EPI_CUDA(cudaStreamWaitEvent(c->stream, c->ev_in[0], 0));
+  return EPI_OK;
+}
+
+int epi_step_host(epi_ctx* c, const double* x_in, const double* y_in, const double* z_in,
+                  double* x_out, double* y_out, double* z_out) {
+  if (!c || !x_in || !y_in || !z_in || !x_out || !y_out || !z_out) return EPI_ERR_INVALID_ARG;
+  if (!c->loaded) return EPI_ERR_STATE;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  if ((rc = enqueue_host_step(c, x_in, y_in, z_in, x_out, y_out, z_out))) return rc;
   EPI_CUDA(cudaStreamSynchronize(c->copy_out));
   return check_status(c);
+  EPI_GUARD_END
+}
+
+int epi_step_host_async(epi_ctx* c, const double* x_in, const double* y_in, const double* z_in,
+                        double* x_out, double* y_out, double* z_out) {
+  if (!c || !x_in || !y_in || !z_in || !x_out || !y_out || !z_out) return EPI_ERR_INVALID_ARG;
+  if (!c->loaded) return EPI_ERR_STATE;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  return enqueue_host_step(c, x_in, y_in, z_in, x_out, y_out, z_out);
   EPI_GUARD_END
 }
 

@@ -174,6 +174,12 @@ int epi_upload_positions(epi_ctx* ctx, const double* x, const double* y, const d
  * memory should be pinned (page-locked) for the copies to overlap. */
 int epi_step_host(epi_ctx* ctx, const double* x_in, const double* y_in, const double* z_in,
                   double* x_out, double* y_out, double* z_out);
+/* epi_step_host without waiting: returns once the step is queued. Successive
+ * calls pipeline (a call's first copies overlap the previous call's last
+ * ones); the out arrays hold the new positions, and the in arrays may be
+ * reused, only after epi_sync (which also reports errors of queued steps). */
+int epi_step_host_async(epi_ctx* ctx, const double* x_in, const double* y_in,
+                        const double* z_in, double* x_out, double* y_out, double* z_out);
 /* Connection lists as CSR over all particles (offsets has n+1 entries). Each
  * row holds tissue-local indices sorted ascending; membrane rows include their
  * four lattice links, as connected_cell does (epi5_MT/cell.h:132). Writes at

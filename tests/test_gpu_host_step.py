@@ -97,6 +97,24 @@ def test_host_step_triangular_membranes(built):
     assert_same(host_steps(tissues, 20, MIXED, **cfg), three_call_steps(tissues, 20, MIXED, **cfg))
 
 
+def test_async_host_steps_equal_sync_ones(built):
+    """epi_step_host_async queued step after step on the same (aliased)
+    pinned arrays, one sync at the end: the same positions as synchronous
+    steps."""
+    tissues = T.config4(n_tissues=24)
+    steps = 12
+    ref, _, _ = host_steps(tissues, steps, MIXED, alias=True, max_conn=64)
+    with capi.Context(precision=MIXED, max_conn=64) as ctx:
+        ctx.upload(tissues)
+        keep = [pinned(a) for a in ctx.positions()]
+        pos = tuple(k[0] for k in keep)
+        for _ in range(steps):
+            ctx.step_host(pos, pos, wait=False)
+        ctx.sync()
+        for d in range(3):
+            assert np.array_equal(pos[d], ref[-1][d]), d
+
+
 def test_host_step_rejects_bad_arrays(built):
     t = T.config1(1)
     with capi.Context(precision=MIXED) as ctx:
