@@ -113,6 +113,9 @@ struct epi_ctx {
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
   std::vector<cudaEvent_t> ev_in, ev_done, ev_d2h;
   double* stage_out = nullptr;
+  // the last work queued on the compute stream was a host step (its inbound
+  // staging is then guarded per group, not by the whole stream)
+  bool after_host_step = false;
   DevStatus* status = nullptr;
   DevStatus* status_h = nullptr;  // pinned
   unsigned long long* rebuilds = nullptr;
@@ -437,7 +440,12 @@ int materialize(epi_ctx* c) {
   return rc;
 }
 
-int set_device(const epi_ctx* c) { return cuda_status(cudaSetDevice(c->cfg.device)); }
+// Every entry point starts here; any work it queues that is not a host step
+// ends a chain of host steps (see enqueue_host_step).
+int set_device(epi_ctx* c) {
+  c->after_host_step = false;
+  return cuda_status(cudaSetDevice(c->cfg.device));
+}
 
 #define EPI_GUARD_BEGIN try {
 #define EPI_GUARD_END             \
@@ -1363,7 +1371,7 @@ int epi_upload_positions(epi_ctx* c, const double* x, const double* y, const dou
 // inbound copy and its unpack into the outbound staging wait only for the
 // previous call's outbound copy of the same group (the host arrays may be
 // the same for input and output, and the staging regions are reused).
-static int enqueue_host_step(epi_ctx* c, const double* x_in, const double* y_in,
+static int enqueue_host_step(epi_ctx* c, bool chained, const double* x_in, const double* y_in,
                              const double* z_in, double* x_out, double* y_out, double* z_out) {
   const int64_t n = c->n;
   int rc;
@@ -1394,10 +1402,13 @@ static int enqueue_host_step(epi_ctx* c, const double* x_in, const double* y_in,
   split.push_back(c->ntissues);
   double* in = c->stage;
   double* out = c->stage_out;
-  // the compute stream's earlier work (a previous step, an upload through
-  // the same inbound staging) precedes this step's inbound copies
-  EPI_CUDA(cudaEventRecord(c->ev_done[0], c->stream));
-  EPI_CUDA(cudaStreamWaitEvent(c->copy_in, c->ev_done[0], 0));
+  // other earlier work on the compute stream (an upload through the same
+  // inbound staging, a step) precedes this step's inbound copies; after a
+  // host step the per-group waits below are enough
+  if (!chained) {
+    EPI_CUDA(cudaEventRecord(c->ev_done[0], c->stream));
+    EPI_CUDA(cudaStreamWaitEvent(c->copy_in, c->ev_done[0], 0));
+  }
   const int cur = c->cur;
   const DevState S = make_state(c, cur);
   const DevState Snew = make_state(c, cur ^ 1);
@@ -1439,6 +1450,7 @@ static int enqueue_host_step(epi_ctx* c, const double* x_in, const double* y_in,
   c->cur ^= 1;
   c->posf_stale = false;
   c->lists_fresh = false;
+  c->after_host_step = true;
   return EPI_OK;
 }
 
@@ -1447,9 +1459,10 @@ int epi_step_host(epi_ctx* c, const double* x_in, const double* y_in, const doub
   if (!c || !x_in || !y_in || !z_in || !x_out || !y_out || !z_out) return EPI_ERR_INVALID_ARG;
   if (!c->loaded) return EPI_ERR_STATE;
   EPI_GUARD_BEGIN
+  const bool chained = c->after_host_step;
   int rc = set_device(c);
   if (rc) return rc;
-  if ((rc = enqueue_host_step(c, x_in, y_in, z_in, x_out, y_out, z_out))) return rc;
+  if ((rc = enqueue_host_step(c, chained, x_in, y_in, z_in, x_out, y_out, z_out))) return rc;
   EPI_CUDA(cudaStreamSynchronize(c->copy_out));
   return check_status(c);
   EPI_GUARD_END
@@ -1460,9 +1473,10 @@ int epi_step_host_async(epi_ctx* c, const double* x_in, const double* y_in, cons
   if (!c || !x_in || !y_in || !z_in || !x_out || !y_out || !z_out) return EPI_ERR_INVALID_ARG;
   if (!c->loaded) return EPI_ERR_STATE;
   EPI_GUARD_BEGIN
+  const bool chained = c->after_host_step;
   int rc = set_device(c);
   if (rc) return rc;
-  return enqueue_host_step(c, x_in, y_in, z_in, x_out, y_out, z_out);
+  return enqueue_host_step(c, chained, x_in, y_in, z_in, x_out, y_out, z_out);
   EPI_GUARD_END
 }
 
