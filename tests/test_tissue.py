@@ -51,3 +51,21 @@ def test_reference_file_round_trip(tmp_path):
     # pairs are mutual, as the reference loader builds them
     paired = np.nonzero(t.pair >= 0)[0]
     assert np.all(t.pair[t.pair[paired]] == paired)
+
+
+def test_triangular_ensemble_fits_the_reference_grid():
+    """config4_tri: the config-4 shapes with triangular membranes. Each box
+    must be covered by the reference's grid ((int)(L / 2 + 0.5) bins of 2.0,
+    cell_connection.cpp:22-26), rows even (the lattice wiring alternates
+    row offsets), every position inside the box."""
+    specs = T.config4_specs(n_tissues=16)
+    ts = T.config4_tri(n_tissues=16)
+    for (side, layers, _), t in zip(specs, ts):
+        t.validate()
+        rows = T.tri_rows(side)
+        assert rows % 2 == 0 and rows >= side
+        assert t.nmemb == side * rows
+        for L in (t.lx, t.ly):
+            assert int(L / 2.0 + 0.5) * 2.0 >= L
+        x, y = np.asarray(t.x), np.asarray(t.y)
+        assert x.min() >= 0 and x.max() < t.lx and y.min() >= 0 and y.max() < t.ly
