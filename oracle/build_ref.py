@@ -41,7 +41,9 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
-REF_DIR = Path(os.environ.get("EPI_REFERENCE_DIR", "/root/reference")) / "epi5_MT"
+# The reference checkout: EPI_REFERENCE_DIR, else a "reference" directory
+# beside this repository.
+REF_DIR = Path(os.environ.get("EPI_REFERENCE_DIR", str(ROOT.parent / "reference"))) / "epi5_MT"
 OUT = HERE / "_ref"
 
 # The mechanics path's translation units plus cell_state_renew (the harness's

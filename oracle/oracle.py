@@ -29,8 +29,9 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "liboracle.so"
 REF_OUT = HERE / "_ref"
-# the reference checkout (present where the oracle is built, not on GPU hosts)
-REF_DIR = Path(os.environ.get("EPI_REFERENCE_DIR", "/root/reference"))
+# the reference checkout (present where the oracle is built, not on GPU
+# hosts): EPI_REFERENCE_DIR, else a "reference" directory beside this repository
+REF_DIR = Path(os.environ.get("EPI_REFERENCE_DIR", str(HERE.parent.parent / "reference")))
 
 _lib = None
 
@@ -204,6 +205,45 @@ def run_reference(t, nsteps: int, every: int, variant: str = "serial",
         if r.returncode != 0:
             raise RuntimeError(f"reference harness failed ({r.returncode}): {r.stderr[-2000:]}")
         return read_reference_frames(out)
+
+
+def read_gj_frames(path: str):
+    """Parse the gap-junction dumps of the harness (EPI_HARNESS_GJ): per frame
+    {step, dead (keys of removed cells per cell), off (CSR row offsets), idx,
+    checked, value}."""
+    data = open(path, "rb").read()
+    off = 0
+    frames = []
+    entry = np.dtype([("idx", "<i4"), ("checked", "<i4"), ("value", "<f8")])
+    while off < len(data):
+        tag, step, n = np.frombuffer(data, np.int32, 3, off)
+        assert tag == 0x504D4A47, "bad gap-junction frame tag"
+        off += 12
+        rows, dead, lens = [], np.zeros(n, np.int32), np.zeros(n, np.int64)
+        for i in range(n):
+            m, d = np.frombuffer(data, np.int32, 2, off)
+            off += 8
+            rows.append(np.frombuffer(data, entry, m, off))
+            off += 16 * int(m)
+            dead[i], lens[i] = d, m
+        allr = np.concatenate(rows) if rows else np.zeros(0, entry)
+        frames.append(dict(step=int(step), dead=dead,
+                           off=np.concatenate([[0], np.cumsum(lens)]),
+                           idx=allr["idx"].copy(), checked=allr["checked"].copy(),
+                           value=allr["value"].copy()))
+    return frames
+
+
+def run_reference_gj(t, nsteps: int, every: int, variant: str = "serial",
+                     env: Optional[dict] = None, mode: str = "run"):
+    """run_reference with the gap-junction maps dumped beside each frame:
+    returns (frames, gap-junction frames)."""
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "gj.bin")
+        e = dict(env or {})
+        e["EPI_HARNESS_GJ"] = path
+        frames = run_reference(t, nsteps, every, variant=variant, env=e, mode=mode)
+        return frames, read_gj_frames(path)
 
 
 def time_reference(t, warmup: int, steps: int, threads: Optional[int] = None):
