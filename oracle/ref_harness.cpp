@@ -63,6 +63,7 @@
 #include <random>
 #include <string>
 #include <unistd.h>
+#include <unordered_set>
 #include <vector>
 
 double genrand_real() {
@@ -165,6 +166,48 @@ void write_frame(std::FILE* f, CellManager& cman, int step) {
   std::fwrite(dermis.data(), 4, n, f);
 }
 
+// Gap-junction bookkeeping of every cell, as gj_refresh leaves it
+// (epi5_MT/cell_connection.cpp:133-152; read by ca2p.cpp:204-207): per cell,
+// the number of map keys that point to a live cell, the number that do not
+// (the reference keeps keys of removed cells until CellManager::clean_up),
+// then (partner index, value, checked) of the live ones sorted by index.
+// Keys of removed cells are never dereferenced.
+void write_gj(std::FILE* f, CellManager& cman, int step) {
+  const std::vector<Cell*> cells = cells_of(cman);
+  const int32_t n = static_cast<int32_t>(cells.size());
+  std::unordered_set<const Cell*> live(cells.begin(), cells.end());
+  const int32_t tag = 0x504d4a47;  // "GJMP"
+  std::fwrite(&tag, 4, 1, f);
+  std::fwrite(&step, 4, 1, f);
+  std::fwrite(&n, 4, 1, f);
+  for (int32_t i = 0; i < n; ++i) {
+    struct Entry {
+      int32_t idx;
+      int32_t checked;
+      double value;
+    };
+    std::vector<Entry> row;
+    int32_t dead = 0;
+    for (auto& kv : cells[i]->gj) {
+      if (!live.count(kv.first)) {
+        ++dead;
+        continue;
+      }
+      row.push_back({static_cast<int32_t>(kv.first->get_index()), kv.second.is_checked() ? 1 : 0,
+                     kv.second()});
+    }
+    std::sort(row.begin(), row.end(), [](const Entry& a, const Entry& b) { return a.idx < b.idx; });
+    const int32_t m = static_cast<int32_t>(row.size());
+    std::fwrite(&m, 4, 1, f);
+    std::fwrite(&dead, 4, 1, f);
+    for (const Entry& e : row) {
+      std::fwrite(&e.idx, 4, 1, f);
+      std::fwrite(&e.checked, 4, 1, f);
+      std::fwrite(&e.value, 8, 1, f);
+    }
+  }
+}
+
 // Highest z of a DEAD / ALIVE / MUSUME / FIX cell, 0 if none: the zzmax the
 // reference's loop computes before its maps (calc_zzmax, proc.cpp:34-43).
 double highest_cell_z(CellManager& cman) {
@@ -242,8 +285,13 @@ int main(int argc, char** argv) {
     }
     std::FILE* f = std::fopen(argv[4], "wb");
     if (!f) return 3;
+    // EPI_HARNESS_GJ=<path>: the gap-junction maps beside every frame
+    const char* gj_path = std::getenv("EPI_HARNESS_GJ");
+    std::FILE* g = gj_path ? std::fopen(gj_path, "wb") : nullptr;
+    if (gj_path && !g) return 3;
     check_capacity(*cman);
     write_frame(f, *cman, 0);
+    if (g) write_gj(g, *cman, 0);
     for (int s = 1; s <= nsteps; ++s) {
       if (dyn) {
         SilenceStdout quiet;  // state renewal reports every division / cornification
@@ -252,9 +300,13 @@ int main(int argc, char** argv) {
         one_step(*cman);
       }
       check_capacity(*cman);
-      if (s % every == 0 || s == nsteps) write_frame(f, *cman, s);
+      if (s % every == 0 || s == nsteps) {
+        write_frame(f, *cman, s);
+        if (g) write_gj(g, *cman, s);
+      }
     }
     std::fclose(f);
+    if (g) std::fclose(g);
     return 0;
   }
   if (mode == "field" && argc == 6) {

@@ -95,3 +95,38 @@ def test_dropin_triangular_build_matches_reference_frames(built):
         err = rel_pos_err((f["x"], f["y"], f["z"]), (g["x"], g["y"], g["z"]), t.lx, t.ly)
         assert err <= TOL_FP64, (s, err)
         assert lists_equal(f["conn_off"], f["conn_idx"], g["conn_off"], g["conn_idx"])
+
+
+@pytest.mark.parametrize("case", ["mixed", "renewal"])
+def test_dropin_gap_junction_bookkeeping_matches_reference(built, case):
+    """The gap-junction maps the drop-in's connect_cell leaves for the
+    chemistry (gj_refresh, cell_connection.cpp:133-152; read by
+    ca2p.cpp:204-207) equal the reference's: per cell the same partners,
+    values and marks. With state renewal, cells are removed and the reference
+    keeps their map keys (never dereferenced here); there the marked entries
+    and each cell's key count are compared."""
+    if case == "mixed":
+        t, mode, env, steps, every = T.mixed_state_tissue(), "run", {}, 300, 50
+    else:
+        t, mode, env, steps, every = (T.renewal_tissue(), "dyn", {"EPI_HARNESS_RNG": "zero"},
+                                      200, 20)
+    if O.reference_binary(t, "dropin") is None or O.reference_binary(t, "serial") is None:
+        pytest.skip("reference and drop-in harnesses not built (oracle/build_ref.py --dropin)")
+    _, ref = O.run_reference_gj(t, steps, every, mode=mode, env=env)
+    _, got = O.run_reference_gj(t, steps, every, variant="dropin", mode=mode,
+                                env=dict(env, EPI_MECH_PRECISION="fp64"))
+    assert [g["step"] for g in got] == [g["step"] for g in ref]
+    for a, b in zip(ref, got):
+        s = a["step"]
+        if case == "mixed":
+            for k in ("off", "idx", "checked", "value", "dead"):
+                assert np.array_equal(a[k], b[k]), (s, k)
+        else:
+            keys_a = np.diff(a["off"]) + a["dead"]
+            keys_b = np.diff(b["off"]) + b["dead"]
+            assert np.array_equal(keys_a, keys_b), s
+            row_a = np.repeat(np.arange(len(a["dead"])), np.diff(a["off"]))
+            row_b = np.repeat(np.arange(len(b["dead"])), np.diff(b["off"]))
+            ca, cb = a["checked"] == 1, b["checked"] == 1
+            for arr_a, arr_b in ((row_a, row_b), (a["idx"], b["idx"]), (a["value"], b["value"])):
+                assert np.array_equal(arr_a[ca], arr_b[cb]), s
