@@ -495,9 +495,9 @@ __global__ void __launch_bounds__(256) k_adj_pairs(DevState S, const double4* __
       pair_i = S.pair[i];
       if (st == ST_FIX || st == ST_MUSUME) dermis_i = S.dermis[i];
     }
-    const int32_t nc = S.ncand[i];
+    const int32_t nc = cand_count(S, i);
     for (int32_t k = 0; k < nc; ++k) {
-      const int32_t q = S.cand[(int64_t)k * N + i];
+      const int32_t q = T.pbase + (int32_t)cand_entry(S, i, k + 1);
       const double4 pq = S.pos_cur[q];
       const double dx = pdiff_h(p.x, pq.x, T.lx, T.hlx), dy = pdiff_h(p.y, pq.y, T.ly, T.hly);
       const double dz = p.z - pq.z;

@@ -93,8 +93,9 @@ struct epi_ctx {
   int32_t* pair = nullptr;
   double* spr = nullptr;
   int32_t* dermis = nullptr;
-  int32_t* cand = nullptr;
-  int32_t* ncand = nullptr;
+  uint4* cand = nullptr;  // candidate rows, cand_chunks 16-byte chunks per particle
+  int32_t cand16 = 1;     // 16-bit row entries (every tissue below 65,537 particles)
+  int32_t cand_chunks = 0;
   float4* bpos = nullptr;
   int32_t* nbr = nullptr;
   int32_t* nn = nullptr;
@@ -137,6 +138,14 @@ struct epi_ctx {
   int ext_cur = 0;
   double* zzmax = nullptr;
   int32_t* izb = nullptr;
+  // export buffers of epi_get_connections / epi_get_dermis, kept between
+  // calls (the drop-in exports every step) and grown on demand
+  int32_t* x_rowlen = nullptr;   // n
+  int32_t* x_rowoff = nullptr;   // n + 1
+  int32_t* x_partial = nullptr;  // scan partials
+  int32_t* x_idx = nullptr;      // x_idx_cap entries
+  int64_t x_idx_cap = 0;
+  int64_t x_n = 0;               // particles the row buffers hold
   // last error details
   DevStatus last{};
 };
@@ -181,13 +190,23 @@ void free_field(epi_ctx* c) {
   c->fd_h.clear();
 }
 
+void free_export(epi_ctx* c) {
+  void* ptrs[] = {c->x_rowlen, c->x_rowoff, c->x_partial, c->x_idx};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  c->x_rowlen = c->x_rowoff = c->x_partial = c->x_idx = nullptr;
+  c->x_idx_cap = 0;
+  c->x_n = 0;
+}
+
 void free_buffers(epi_ctx* c) {
   destroy_graphs(c);
   free_field(c);
+  free_export(c);
   if (c->agek) cudaFree(c->agek);
   c->agek = nullptr;
   void* ptrs[] = {c->tissues, c->pos[0], c->pos[1], c->posf[0], c->posf[1], c->attr, c->pair, c->spr, c->dermis,
-                  c->cand, c->ncand, c->bpos, c->nbr, c->nn, c->fmemb, c->bin,
+                  c->cand, c->bpos, c->nbr, c->nn, c->fmemb, c->bin,
                   c->rank, c->counts, c->starts, c->skey, c->spos, c->gate, c->rl, c->prep,
                   c->scan.partial, c->stage, c->stage_out};
   for (void* p : ptrs)
@@ -196,7 +215,7 @@ void free_buffers(epi_ctx* c) {
   c->pos[0] = c->pos[1] = nullptr;
   c->posf[0] = c->posf[1] = nullptr;
   c->attr = nullptr; c->pair = nullptr; c->spr = nullptr; c->dermis = nullptr;
-  c->cand = nullptr; c->ncand = nullptr; c->bpos = nullptr;
+  c->cand = nullptr; c->bpos = nullptr;
   c->nbr = nullptr; c->nn = nullptr; c->fmemb = nullptr;
   c->bin = nullptr; c->rank = nullptr; c->counts = nullptr; c->starts = nullptr;
   c->skey = nullptr; c->spos = nullptr; c->gate = nullptr; c->rl = nullptr; c->prep = nullptr;
@@ -217,7 +236,7 @@ DevState make_state(epi_ctx* c, int cur) {
   S.spr = c->spr;
   S.dermis = c->dermis;
   S.cand = c->cand;
-  S.ncand = c->ncand;
+  S.cand16 = c->cand16;
   S.bpos = c->bpos;
   S.nbr = c->nbr;
   S.nn = c->nn;
@@ -742,9 +761,19 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
   }
   if (n > (int64_t)0x7fffffff || nbins > (int64_t)0x7ffffff0 || ntissues >= (1 << 24))
     return EPI_ERR_UNSUPPORTED;
+  // Candidate rows hold tissue-local indices: 16-bit entries when every
+  // tissue has at most 65,536 particles, else 32-bit. Each row has room for
+  // the count and max_cand entries, and at least the chunks the step kernel
+  // loads up front (2 of 16-bit entries, 4 of 32-bit).
+  int32_t nmax = 0;
+  for (int t = 0; t < ntissues; ++t) nmax = std::max(nmax, tv[t].n);
+  const int32_t cand16 = nmax <= 65536 ? 1 : 0;
+  const int32_t per_chunk = cand16 ? 8 : 4;
+  const int32_t chunks = std::max((c->cfg.max_cand + 1 + per_chunk - 1) / per_chunk, cand16 ? 2 : 4);
   // A re-upload of the same shape (the per-step connect of an application
   // that renews cell state on the host) keeps the device buffers.
-  const bool reuse = c->loaded && c->ntissues == ntissues && c->n == n && c->nbins == nbins;
+  const bool reuse = c->loaded && c->ntissues == ntissues && c->n == n && c->nbins == nbins &&
+                     c->cand16 == cand16 && c->cand_chunks == chunks;
   const int32_t old_nprep = c->nprep;
   destroy_graphs(c);
   // The field grids depend on the tissue count and the grid size only: they
@@ -777,6 +806,8 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
   c->ntissues = ntissues;
   c->n = n;
   c->nbins = (int32_t)nbins;
+  c->cand16 = cand16;
+  c->cand_chunks = chunks;
   const std::vector<TissueDev> old_tissues = reuse ? c->tissues_h : std::vector<TissueDev>();
   c->tissues_h.assign(ntissues, TissueDev{});
   c->thost.assign(ntissues, TissueHost{});
@@ -861,7 +892,7 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
   c->nprep = c->nprep_memb + (int32_t)prep_f.size();
   std::vector<int32_t> prep(prep_m);
   prep.insert(prep.end(), prep_f.begin(), prep_f.end());
-  const size_t C = (size_t)c->cfg.max_conn, CC = (size_t)c->cfg.max_cand;
+  const size_t C = (size_t)c->cfg.max_conn, CC = (size_t)chunks;
   if (reuse && (int32_t)prep.size() > old_nprep) {
     cudaFree(c->prep);
     c->prep = nullptr;
@@ -875,7 +906,7 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
       (rc = dev_alloc(&c->posf[1], n)) || (rc = dev_alloc(&c->attr, n)) ||
       (rc = dev_alloc(&c->pair, n)) || (rc = dev_alloc(&c->spr, n)) ||
       (rc = dev_alloc(&c->dermis, n)) || (rc = dev_alloc(&c->cand, CC * n)) ||
-      (rc = dev_alloc(&c->ncand, n)) || (rc = dev_alloc(&c->bpos, n)) ||
+      (rc = dev_alloc(&c->bpos, n)) ||
       (rc = dev_alloc(&c->nbr, C * n)) || (rc = dev_alloc(&c->nn, n)) ||
       (rc = dev_alloc(&c->fmemb, n)) ||
       (rc = dev_alloc(&c->bin, n)) || (rc = dev_alloc(&c->rank, n)) ||
@@ -940,7 +971,7 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
   for (int64_t i = 0; i < n; ++i) c->h_radius[i] = pos[i].w;
   if (gates.empty()) {
     EPI_CUDA(cudaMemsetAsync(c->nn, 0, sizeof(int32_t) * n, s));
-    EPI_CUDA(cudaMemsetAsync(c->ncand, 0, sizeof(int32_t) * n, s));
+    EPI_CUDA(cudaMemsetAsync(c->cand, 0, sizeof(uint4) * n, s));  // row counts (chunk 0)
     EPI_CUDA(cudaMemsetAsync(c->dermis, 0xff, sizeof(int32_t) * n, s));
   }
   EPI_CUDA(cudaMemsetAsync(c->status, 0, sizeof(DevStatus), s));
@@ -1489,41 +1520,44 @@ int epi_get_connections(epi_ctx* c, int32_t* offsets, int32_t* idx, int64_t cap,
   if (rc) return rc;
   if ((rc = materialize(c))) return rc;
   const int32_t n = (int32_t)c->n;
-  int32_t *rowlen = nullptr, *rowoff = nullptr, *didx = nullptr, *partial = nullptr;
-  if ((rc = dev_alloc(&rowlen, n)) || (rc = dev_alloc(&rowoff, (size_t)n + 1))) {
-    cudaFree(rowlen);
-    return rc;
-  }
   ScanScratch sc;
   sc.capacity = (n + kScanTile - 1) / kScanTile + 1;
-  if ((rc = dev_alloc(&partial, sc.capacity))) {
-    cudaFree(rowlen);
-    cudaFree(rowoff);
-    return rc;
-  }
-  sc.partial = partial;
-  const DevState S = make_state(c, c->cur);
-  launch_rowlen(S, rowlen, n, c->stream);
-  launch_scan(rowlen, rowoff, n, 0, sc, nullptr, c->lc, c->stream);
-  cudaError_t e = cudaMemcpyAsync(offsets, rowoff, sizeof(int32_t) * ((size_t)n + 1),
-                                  cudaMemcpyDeviceToHost, c->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  const int64_t tot = e == cudaSuccess ? offsets[n] : 0;
-  if (total) *total = tot;
-  if (e == cudaSuccess && cap >= tot && tot > 0) {
-    e = cudaMalloc((void**)&didx, sizeof(int32_t) * tot);
-    if (e == cudaSuccess) {
-      launch_fill_csr(S, rowoff, didx, n, c->stream);
-      e = cudaMemcpyAsync(idx, didx, sizeof(int32_t) * tot, cudaMemcpyDeviceToHost, c->stream);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (c->x_n != c->n || !c->x_rowlen) {
+    free_export(c);
+    if ((rc = dev_alloc(&c->x_rowlen, n)) || (rc = dev_alloc(&c->x_rowoff, (size_t)n + 1)) ||
+        (rc = dev_alloc(&c->x_partial, sc.capacity))) {
+      free_export(c);
+      return rc;
     }
+    c->x_n = c->n;
   }
-  cudaFree(rowlen);
-  cudaFree(rowoff);
-  cudaFree(partial);
-  if (didx) cudaFree(didx);
-  EPI_CUDA(e);
-  if (cap < tot && cap > 0) return EPI_ERR_INVALID_ARG;
+  sc.partial = c->x_partial;
+  const DevState S = make_state(c, c->cur);
+  launch_rowlen(S, c->x_rowlen, n, c->stream);
+  launch_scan(c->x_rowlen, c->x_rowoff, n, 0, sc, nullptr, c->lc, c->stream);
+  EPI_CUDA(cudaMemcpyAsync(offsets, c->x_rowoff, sizeof(int32_t) * ((size_t)n + 1),
+                           cudaMemcpyDeviceToHost, c->stream));
+  EPI_CUDA(cudaStreamSynchronize(c->stream));
+  const int64_t tot = offsets[n];
+  if (total) *total = tot;
+  if (cap >= tot && tot > 0) {
+    if (c->x_idx_cap < tot) {
+      if (c->x_idx) cudaFree(c->x_idx);
+      c->x_idx = nullptr;
+      c->x_idx_cap = 0;
+      // room for the lists to grow by a quarter before the next reallocation
+      const int64_t want = tot + tot / 4;
+      if ((rc = dev_alloc(&c->x_idx, (size_t)want))) return rc;
+      c->x_idx_cap = want;
+    }
+    launch_fill_csr(S, c->x_rowoff, c->x_idx, n, c->stream);
+    EPI_CUDA(cudaMemcpyAsync(idx, c->x_idx, sizeof(int32_t) * tot, cudaMemcpyDeviceToHost,
+                             c->stream));
+  }
+  if (cap < tot && cap > 0) {
+    EPI_CUDA(cudaStreamSynchronize(c->stream));
+    return EPI_ERR_INVALID_ARG;
+  }
   return check_status(c);
   EPI_GUARD_END
 }
@@ -1535,14 +1569,20 @@ int epi_get_dermis(epi_ctx* c, int32_t* dermis) {
   int rc = set_device(c);
   if (rc) return rc;
   if ((rc = materialize(c))) return rc;
-  int32_t* d = nullptr;
-  if ((rc = dev_alloc(&d, c->n))) return rc;
-  launch_dermis_local(make_state(c, c->cur), d, (int32_t)c->n, c->stream);
-  cudaError_t e = cudaMemcpyAsync(dermis, d, sizeof(int32_t) * c->n, cudaMemcpyDeviceToHost,
-                                  c->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  cudaFree(d);
-  EPI_CUDA(e);
+  if (c->x_n != c->n || !c->x_rowlen) {
+    free_export(c);
+    const int32_t n = (int32_t)c->n;
+    if ((rc = dev_alloc(&c->x_rowlen, n)) || (rc = dev_alloc(&c->x_rowoff, (size_t)n + 1)) ||
+        (rc = dev_alloc(&c->x_partial, (n + kScanTile - 1) / kScanTile + 1))) {
+      free_export(c);
+      return rc;
+    }
+    c->x_n = c->n;
+  }
+  // the row-length buffer holds the local dermis indices (n entries)
+  launch_dermis_local(make_state(c, c->cur), c->x_rowlen, (int32_t)c->n, c->stream);
+  EPI_CUDA(cudaMemcpyAsync(dermis, c->x_rowlen, sizeof(int32_t) * c->n, cudaMemcpyDeviceToHost,
+                           c->stream));
   return check_status(c);
   EPI_GUARD_END
 }

@@ -8,10 +8,14 @@
 //              MUSUME membrane spring selector, bits 8-31 tissue id
 //   pair[N]    i32 global partner index or -1; spr[N] double spring rest length
 //   dermis[N]  i32 global index of the nearest connected MEMB (FIX/MUSUME)
-//   cand[N][C] i32 Verlet candidates (all partners within reach + skin at
-//              the last rebuild), one row per particle so that the G lanes
-//              sharing a particle in the step kernel read consecutive
-//              entries; ncand[N]
+//   cand[K][N] Verlet candidates (all partners within reach + skin at the
+//              last rebuild) in 16-byte chunks, chunk k of particle i at
+//              cand[k * N + i]: entry 0 is the count, entries 1.. the
+//              tissue-local candidate indices, 8 per chunk (16-bit) or 4
+//              (32-bit, when a tissue of the batch has 65,536 particles or
+//              more). A warp's loads of chunk k of 32 consecutive particles
+//              are one coalesced 512-byte request, and two loads give a
+//              thread its first 15 candidates without a dependent load.
 //   nbr[N][C]  i32 exact connection lists, materialised on request; nn[N].
 //              Membrane lattice links are implicit in both.
 //   sn/sm[N]   membrane bending scratch (unit vector + length to the right /
@@ -67,9 +71,9 @@ struct DevState {
   const double* spr;
   int32_t* dermis;
   // Verlet candidates: every partner within LJ_THRESH*(r_i+r_j) + skin at
-  // the last rebuild, column-major like nbr.
-  int32_t* cand;
-  int32_t* ncand;
+  // the last rebuild, chunked rows (see the layout above; cand_* below).
+  uint4* cand;
+  int32_t cand16;   // 1: 16-bit entries, 0: 32-bit entries
   float4* bpos;     // positions at the last rebuild (displacement check)
   int32_t* nbr;     // exact connection lists (materialised on request)
   int32_t* nn;
@@ -95,6 +99,30 @@ struct DevState {
   int32_t max_conn, max_cand;
   double skin;
 };
+
+// Candidate rows: entry e of particle i (entry 0: the count; entry k + 1:
+// candidate k, tissue-local). 16-bit entries: chunk e / 8, half e % 8;
+// 32-bit: chunk e / 4, word e % 4.
+__device__ __forceinline__ uint32_t cand_entry(const DevState& S, int64_t i, int32_t e) {
+  if (S.cand16) {
+    const uint16_t* c = reinterpret_cast<const uint16_t*>(S.cand + (int64_t)(e >> 3) * S.n_total + i);
+    return c[e & 7];
+  }
+  const uint32_t* c = reinterpret_cast<const uint32_t*>(S.cand + (int64_t)(e >> 2) * S.n_total + i);
+  return c[e & 3];
+}
+__device__ __forceinline__ void cand_set(const DevState& S, int64_t i, int32_t e, uint32_t v) {
+  if (S.cand16) {
+    uint16_t* c = reinterpret_cast<uint16_t*>(S.cand + (int64_t)(e >> 3) * S.n_total + i);
+    c[e & 7] = (uint16_t)v;
+  } else {
+    uint32_t* c = reinterpret_cast<uint32_t*>(S.cand + (int64_t)(e >> 2) * S.n_total + i);
+    c[e & 3] = v;
+  }
+}
+__device__ __forceinline__ int32_t cand_count(const DevState& S, int64_t i) {
+  return (int32_t)cand_entry(S, i, 0);
+}
 
 __device__ __forceinline__ uint32_t attr_state(uint32_t a) { return a & 15u; }
 __device__ __forceinline__ bool attr_old(uint32_t a) { return (a >> 4) & 1u; }

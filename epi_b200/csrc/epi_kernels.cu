@@ -499,7 +499,7 @@ struct SearchWindow {
 __device__ __forceinline__ void finish_search(const DevState& S, int32_t i, int32_t count) {
   const int32_t cap = S.max_cand;
   if (count > cap) raise_error(S.status, E_LIST_OVERFLOW, i, -1, (double)count);
-  S.ncand[i] = count < cap ? count : cap;
+  cand_set(S, i, 0, (uint32_t)(count < cap ? count : cap));
   const double4 p = S.pos_cur[i];
   S.bpos[i] = make_float4((float)p.x, (float)p.y, (float)p.z, 0.f);
 }
@@ -514,7 +514,6 @@ __device__ __forceinline__ void cand_search_warps(const DevState& S, int32_t cnt
   const unsigned lt_mask = (1u << lane) - 1u;
   const int32_t warps = (gridDim.x * blockDim.x) >> 5;
   const int32_t cap = S.max_cand;
-  const int64_t N = S.n_total;
   for (int32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ngated; g += warps) {
     int32_t t;
     const int32_t i = gated_particle(S, cnt, g, &t);
@@ -562,7 +561,7 @@ __device__ __forceinline__ void cand_search_warps(const DevState& S, int32_t cnt
         const unsigned m = __ballot_sync(0xffffffffu, hit);
         if (hit) {
           const int32_t kk = count + __popc(m & lt_mask);
-          if (kk < cap) S.cand[(int64_t)kk * N + i] = (int32_t)(key & 0x7fffffffu);
+          if (kk < cap) cand_set(S, i, kk + 1, (key & 0x7fffffffu) - (uint32_t)T.pbase);
         }
         count += __popc(m);
       }
@@ -577,7 +576,6 @@ __device__ __forceinline__ void cand_search_warps(const DevState& S, int32_t cnt
 // column-major candidate rows coalesced.
 __device__ __forceinline__ void cand_search_threads(const DevState& S, int32_t cnt,
                                                     int32_t ngated) {
-  const int64_t N = S.n_total;
   const int32_t cap = S.max_cand;
   for (int32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ngated;
        g += gridDim.x * blockDim.x) {
@@ -586,6 +584,7 @@ __device__ __forceinline__ void cand_search_threads(const DevState& S, int32_t c
     const TissueDev& T = S.tissues[t];
     const SearchWindow W(S, T, i);
     const int32_t any = T.any, anz = T.anz, binbase = T.binbase;
+    const uint32_t pbase = (uint32_t)T.pbase;
     int32_t count = 0;
     for (int xr = 0; xr < W.nxr; ++xr) {
       const float ex = W.pxe[xr];
@@ -606,7 +605,7 @@ __device__ __forceinline__ void cand_search_threads(const DevState& S, int32_t c
 #pragma unroll
               for (int u = 0; u < 4; ++u) {
                 if (s + u < s_hi && W.hit(i, key[u], q[u], ex, ey)) {
-                  if (count < cap) S.cand[(int64_t)count * N + i] = (int32_t)(key[u] & 0x7fffffffu);
+                  if (count < cap) cand_set(S, i, count + 1, (key[u] & 0x7fffffffu) - pbase);
                   ++count;
                 }
               }
@@ -662,12 +661,12 @@ __global__ void k_dermis(DevState S, int32_t f0, int32_t f1) {
     const int32_t i = S.prep[e];
     const TissueDev& T = S.tissues[attr_tissue(S.attr[i])];
     const double4 p = S.pos_cur[i];
-    const int32_t nc = S.ncand[i];
+    const int32_t nc = cand_count(S, i);
     const double lt = T.P.lj_thresh;
     int32_t best = -1;
     double bestd = T.lx * T.lx;
     for (int32_t k = 0; k < nc; ++k) {
-      const int32_t q = S.cand[(int64_t)k * S.n_total + i];
+      const int32_t q = T.pbase + (int32_t)cand_entry(S, i, k + 1);
       if (attr_state(S.attr[q]) != ST_MEMB) continue;
       const double4 pq = S.pos_cur[q];
       const double d2 =
@@ -990,7 +989,8 @@ struct Particle {
       : S(S_), i(i_), a(__ldg(&S_.attr[i_])), t(attr_tissue(a)), st(attr_state(a)),
         T(S_.tissues[t]), L(T.laws<R>()), p(S_.pos_cur[i_]),
         lt2(T.P.lj_thresh * T.P.lj_thresh), dt(R(T.P.dt)) {
-    if (kFloatPos) pf = S.posf_cur[i];
+    // the FP32 copy of the particle itself, as every writer of posf forms it
+    if (kFloatPos) pf = make_float4((float)p.x, (float)p.y, (float)p.z, (float)p.w);
     if (!kSimple && st != ST_MEMB) {
       pair_i = __ldg(&S.pair[i]);
       if (st == ST_FIX || st == ST_MUSUME) dermis_i = __ldg(&S.dermis[i]);
@@ -1150,11 +1150,6 @@ struct Particle {
   }
 };
 
-// One thread per particle. The candidate chain index -> position is
-// software-pipelined: indices are loaded two candidates ahead (they stream
-// from HBM), positions one ahead (gathers from L1/L2), so neither latency is
-// paid serially per candidate. kMinBlocks bounds the registers so that that
-// many 256-thread blocks stay resident per SM.
 template <typename Pos>
 __device__ __forceinline__ const Pos* gather_source(const DevState& S);
 template <>
@@ -1166,35 +1161,64 @@ __device__ __forceinline__ const float4* gather_source<float4>(const DevState& S
   return S.posf_cur;
 }
 
-template <typename R, bool kSimple, bool kOld, int kMinBlocks>
+// Entry e of a candidate row from its first chunks held in registers (e a
+// constant once the caller's loop is unrolled). 16-bit entries: half e % 2
+// of word (e % 8) / 2 of chunk e / 8; 32-bit: word e % 4 of chunk e / 4.
+template <bool k16, int NC>
+__device__ __forceinline__ uint32_t row_entry(const uint4 (&c)[NC], int e) {
+  const uint4& ch = c[k16 ? e / 8 : e / 4];
+  const int w = k16 ? (e % 8) / 2 : e % 4;
+  const uint32_t word = w == 0 ? ch.x : (w == 1 ? ch.y : (w == 2 ? ch.z : ch.w));
+  return k16 ? ((e & 1) ? word >> 16 : word & 0xffffu) : word;
+}
+
+// One thread per particle. The first chunks of the particle's candidate row
+// (15 candidates with 16-bit entries, 15 with 32-bit) are loaded up front,
+// independent of each other and of the particle's own data, so the index
+// stream costs one memory latency per particle rather than one per
+// candidate. The neighbours' positions are then gathered kG at a time (all
+// kG loads issued before the first is used). Rows longer than that (rare)
+// finish with one load per entry. kMinBlocks bounds the registers so that
+// that many 256-thread blocks stay resident per SM.
+template <typename R, bool kSimple, bool kOld, int kMinBlocks, bool k16>
 __global__ void __launch_bounds__(256, kMinBlocks) k_step(DevState S, Range r) {
   pdl_entry();
   count_launch(S.launches);
   const int64_t i = r.p0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= r.p1) return;
   const int64_t N = S.n_total;
-  const int32_t nc = __ldg(&S.ncand[i]);
-  const int32_t* cp = S.cand + i;  // column-major: entry k at cp[k * N]
-  int32_t q1 = nc > 1 ? __ldg(cp + N) : 0;
-  int32_t q2 = nc > 2 ? __ldg(cp + 2 * N) : 0;
+  constexpr int kChunks = k16 ? 2 : 4;               // chunks loaded up front
+  constexpr int kPre = kChunks * (k16 ? 8 : 4) - 1;  // candidates they hold
+  constexpr int kG = sizeof(R) == 4 ? 4 : 2;         // gathers in flight
+  uint4 c[kChunks];
+#pragma unroll
+  for (int k = 0; k < kChunks; ++k) c[k] = __ldg(S.cand + k * N + i);
   using Part = Particle<R, kSimple, kOld>;
   using Pos = typename Part::Pos;
   Part P(S, (int32_t)i);
-  const Pos* src = gather_source<Pos>(S);
-  int32_t q0 = nc > 0 ? __ldg(cp) : 0;
-  Pos p0 = src[q0];
-  cp += 3 * N;
-  for (int32_t k = 0; k < nc; ++k) {
-    const int32_t q = q0;
-    const Pos pq = p0;
-    q0 = q1;
-    q1 = q2;
-    if (k + 3 < nc) {
-      q2 = __ldg(cp);
-      cp += N;
+  const int32_t pbase = P.T.pbase;
+  const Pos* src = gather_source<Pos>(S) + pbase;
+  const int32_t nc = (int32_t)row_entry<k16>(c, 0);
+#pragma unroll
+  for (int b = 1; b <= kPre; b += kG) {
+    if (b > nc) break;
+    int32_t q[kG];
+    Pos pq[kG];
+#pragma unroll
+    for (int u = 0; u < kG; ++u) {
+      q[u] = 0;
+      if (b + u <= kPre) {
+        q[u] = (int32_t)row_entry<k16>(c, b + u);
+        if (b + u <= nc) pq[u] = src[q[u]];
+      }
     }
-    if (k + 1 < nc) p0 = src[q0];
-    P.candidate(q, pq);
+#pragma unroll
+    for (int u = 0; u < kG; ++u)
+      if (b + u <= kPre && b + u <= nc) P.candidate(pbase + q[u], pq[u]);
+  }
+  for (int32_t e = kPre + 1; e <= nc; ++e) {
+    const int32_t q = (int32_t)cand_entry(S, i, e);
+    P.candidate(pbase + q, src[q]);
   }
   P.finish();
 }
@@ -1205,11 +1229,11 @@ __global__ void k_exact_lists(DevState S, Range r) {
     const uint32_t a = S.attr[i];
     const TissueDev& T = S.tissues[attr_tissue(a)];
     const double4 p = S.pos_cur[i];
-    const int32_t nc = S.ncand[i];
+    const int32_t nc = cand_count(S, i);
     const double lt = T.P.lj_thresh;
     int32_t count = 0;
     for (int32_t k = 0; k < nc; ++k) {
-      const int32_t q = S.cand[(int64_t)k * S.n_total + i];
+      const int32_t q = T.pbase + (int32_t)cand_entry(S, i, k + 1);
       const double4 pq = S.pos_cur[q];
       const double d2 =
           dist_sq_exact(pdiff(p.x, pq.x, T.lx), pdiff(p.y, pq.y, T.ly), p.z - pq.z);
@@ -1408,18 +1432,24 @@ void launch_prepass(const DevState& S, int32_t m0, int32_t m1, int32_t f0, int32
   launch_dermis(S, f0, f1, lc, s, tm);
 }
 
-template <typename R, bool kSimple, bool kOld>
-void launch_step_v(const DevState& S, const Range& r, const LaunchCfg& lc, cudaStream_t s) {
+template <typename R, bool kSimple, bool kOld, bool k16>
+void launch_step_w(const DevState& S, const Range& r, const LaunchCfg& lc, cudaStream_t s) {
   const int grid = blocks_for(r.p1 - r.p0, 256);
   // resident 256-thread blocks per SM of each tuning variant: the FP64
   // kernel needs more registers (4 blocks spill; 2 and 3 do not)
   constexpr bool kF = sizeof(R) == 4;
   switch (lc.variant) {
-    case 2: launch_pdl(k_step<R, kSimple, kOld, kF ? 5 : 2>, grid, 256, s, S, r); break;
-    case 3: launch_pdl(k_step<R, kSimple, kOld, kF ? 6 : 4>, grid, 256, s, S, r); break;
-    case 4: launch_pdl(k_step<R, kSimple, kOld, kF ? 3 : 5>, grid, 256, s, S, r); break;
-    default: launch_pdl(k_step<R, kSimple, kOld, kF ? 4 : 3>, grid, 256, s, S, r); break;
+    case 2: launch_pdl(k_step<R, kSimple, kOld, kF ? 5 : 2, k16>, grid, 256, s, S, r); break;
+    case 3: launch_pdl(k_step<R, kSimple, kOld, kF ? 6 : 4, k16>, grid, 256, s, S, r); break;
+    case 4: launch_pdl(k_step<R, kSimple, kOld, kF ? 3 : 5, k16>, grid, 256, s, S, r); break;
+    default: launch_pdl(k_step<R, kSimple, kOld, kF ? 4 : 3, k16>, grid, 256, s, S, r); break;
   }
+}
+
+template <typename R, bool kSimple, bool kOld>
+void launch_step_v(const DevState& S, const Range& r, const LaunchCfg& lc, cudaStream_t s) {
+  if (S.cand16) launch_step_w<R, kSimple, kOld, true>(S, r, lc, s);
+  else launch_step_w<R, kSimple, kOld, false>(S, r, lc, s);
 }
 
 template <typename R>
