@@ -78,11 +78,18 @@ __global__ void na_bin(Args A) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.n) return;
   const double x = A.x[i], y = A.y[i], z = A.z[i];
-  const int32_t aix = (int32_t)((0.5 * A.lx - pdiff(0.5 * A.lx, x, A.lx)) / kAreaGrid);
-  const int32_t aiy = (int32_t)((0.5 * A.ly - pdiff(0.5 * A.ly, y, A.ly)) / kAreaGrid);
-  const int32_t aiz = (int32_t)(fmax(z, 0.0) / kAreaGrid);
-  bool bad = !isfinite(x) || !isfinite(y) || !isfinite(z) || aix >= A.anx || aiy >= A.any ||
-             aiz >= A.anz || aix < 0 || aiy < 0 || aiz < 0;
+  // Coordinates are converted to bin numbers only once they are finite and
+  // within a few boxes of the grid, so every conversion is in int32 range.
+  const double big = 4.0 * (A.lx + A.ly + A.lz);
+  bool bad = !isfinite(x) || !isfinite(y) || !isfinite(z) || fabs(x) > big || fabs(y) > big ||
+             fabs(z) > big;
+  int32_t aix = 0, aiy = 0, aiz = 0;
+  if (!bad) {
+    aix = (int32_t)((0.5 * A.lx - pdiff(0.5 * A.lx, x, A.lx)) / kAreaGrid);
+    aiy = (int32_t)((0.5 * A.ly - pdiff(0.5 * A.ly, y, A.ly)) / kAreaGrid);
+    aiz = (int32_t)(fmax(z, 0.0) / kAreaGrid);
+    bad = aix >= A.anx || aiy >= A.any || aiz >= A.anz || aix < 0 || aiy < 0 || aiz < 0;
+  }
   if (!bad && i >= A.nmemb) {  // connect_proc's assert for the searching cells (:95-99)
     const int32_t cx = (int32_t)(x / kAreaGrid), cy = (int32_t)(y / kAreaGrid),
                   cz = (int32_t)(z / kAreaGrid);
@@ -191,6 +198,16 @@ __global__ void na_sort_rows(Args A) {
   }
 }
 
+// Launches kernel k with `grid` blocks of kThreads threads on stream s and
+// returns that launch's own status.
+cudaError_t launch(void (*k)(Args), int grid, cudaStream_t s, const Args& A) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)kThreads);
+  cfg.stream = s;
+  return cudaLaunchKernelEx(&cfg, k, A);
+}
+
 // Device address of the scratch array, looked up once per device.
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
@@ -254,13 +271,16 @@ extern "C" int epi_connect_noalloc(const double* x, const double* y, const doubl
     const int nb = A.anx * A.any * A.anz;
     const int g = (std::max(n, nb) + kThreads - 1) / kThreads;
     const int gp = (n + kThreads - 1) / kThreads;
-    na_init<<<g, kThreads, 0, s>>>(A);
-    na_bin<<<gp, kThreads, 0, s>>>(A);
-    na_scan<<<1, kThreads, 0, s>>>(A);
-    na_scatter<<<gp, kThreads, 0, s>>>(A);
-    if (n > nmemb) na_connect<<<(n - nmemb + kThreads - 1) / kThreads, kThreads, 0, s>>>(A);
-    na_sort_rows<<<gp, kThreads, 0, s>>>(A);
-    return cudaGetLastError() == cudaSuccess ? EPI_OK : EPI_ERR_CUDA;
+    // Each launch reports its own status, so an error that earlier, unrelated
+    // work left pending on this thread is neither reported here nor cleared.
+    cudaError_t e = launch(na_init, g, s, A);
+    if (e == cudaSuccess) e = launch(na_bin, gp, s, A);
+    if (e == cudaSuccess) e = launch(na_scan, 1, s, A);
+    if (e == cudaSuccess) e = launch(na_scatter, gp, s, A);
+    if (e == cudaSuccess && n > nmemb)
+      e = launch(na_connect, (n - nmemb + kThreads - 1) / kThreads, s, A);
+    if (e == cudaSuccess) e = launch(na_sort_rows, gp, s, A);
+    return e == cudaSuccess ? EPI_OK : EPI_ERR_CUDA;
   } catch (...) {
     return EPI_ERR_CUDA;
   }

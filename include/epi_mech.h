@@ -293,10 +293,13 @@ int epi_adjoint(epi_ctx* ctx, int32_t nsteps, int32_t checkpoint_every, const ep
  * the work is queued on `stream` (a cudaStream_t; NULL = the default stream)
  * and nothing is synchronised. When the stream reaches it: count[i] is the
  * length of connected_cell for particle i (membrane rows include their four
- * lattice links) and row i holds the first min(count[i], max_conn) partner
- * indices sorted ascending; count[i] > max_conn means the row overflowed;
- * count[i] = -1 means particle i is outside the grid (the reference's range
- * assert). The connection set is connect_proc's (cell_connection.cpp:70-129).
+ * lattice links) and, when count[i] <= max_conn, row i holds its partner
+ * indices sorted ascending. count[i] > max_conn means the row overflowed:
+ * the row then holds an unspecified subset of max_conn partners (which ones
+ * depends on thread timing); treat it as an error, as the context API's
+ * EPI_ERR_LIST_OVERFLOW. count[i] = -1 means particle i is outside the grid
+ * (the reference's range assert); no searched connection lists it (membrane
+ * rows still list their lattice links). The connection set is connect_proc's (cell_connection.cpp:70-129).
  *
  * Limits: n <= EPI_NOALLOC_MAX_PARTICLES and ANX*ANY*ANZ <=
  * EPI_NOALLOC_MAX_BINS (ANX = (int)(lx/2 + 0.5), ANY likewise, ANZ =
