@@ -89,6 +89,38 @@ def rank_workload(name: str, tissues: int, world: int, rank: int):
     return every, sum(t.n for t in every), len(every), desc, every
 
 
+def rank_tissue_ids(name: str, tissues: int, world: int, rank: int):
+    """Job ids of this rank's tissues, in the order rank_workload returns
+    them: the ensemble's shard, or the rank's own replica of a single-tissue
+    workload (job id = rank; the replicas are ordered by rank)."""
+    if name == "ensemble" and world > 1:
+        specs = T.config4_specs(n_tissues=tissues * world)
+        sizes = [side * side * (1 + layers) for side, layers, _ in specs]
+        return shard_tissues(sizes, world)[rank]
+    if world > 1:
+        return [rank]
+    every, _ = workload(name, tissues)
+    return list(range(len(every)))
+
+
+def gather_positions(ctx, mine, ids, dist):
+    """The job's final positions on rank 0 in job order (bench.py's result
+    gather, after the timed region): (tissues, particles, checksum) there,
+    None elsewhere. Single-tissue replicas count once per rank."""
+    from epi_b200.ensemble import gather_results, split_by_tissue
+    per = split_by_tissue(ctx.positions(), [t.n for t in mine])
+    if dist is None:
+        allr = per
+    else:
+        allr = gather_results(ids if len(ids) == len(per) else list(range(len(per))), per, dist)
+    if allr is None:
+        return None
+    total = sum(len(r[0]) for r in allr)
+    checksum = float(sum(np.sum(a) for r in allr for a in r))
+    return {"tissues": len(allr), "particles": total, "sum_of_coordinates": checksum,
+            "order": "job order (tissue ids of the whole job)"}
+
+
 # --------------------------------------------------------------------------
 # clocks during the timed region (NVML)
 # --------------------------------------------------------------------------
@@ -327,6 +359,38 @@ def field_check(capi, device: int, steps: int, with_cpu: bool):
     return out
 
 
+def dropin_check(workloads, steps: int, warmup: int):
+    """The drop-in inside the reference's own step loop: epi5_MT's harness
+    (cell_interaction -> pos_copy -> cell_pos_periodic_fix -> connect_cell,
+    proc.cpp:22-32) built with epi_b200/shim in place of its two mechanics
+    files, against the same harness built with the reference's own mechanics;
+    both OpenMP builds on all host threads, steady_clock median per step. The
+    drop-in's step includes every host<->device copy and the write-back of
+    connected_cell, the gap-junction maps and dermis."""
+    from oracle import oracle as O
+    out = {}
+    for name, t in workloads:
+        try:
+            ref = O.time_reference(t, warmup, steps, threads=os.cpu_count())
+            gpu = O.time_reference(t, warmup, steps, threads=os.cpu_count(),
+                                   variant="dropin_omp")
+            out[name] = {"particles": t.n, "steps": steps, "warmup": warmup,
+                         "reference_ms_per_step": ref["median_s"] * 1e3,
+                         "dropin_ms_per_step": gpu["median_s"] * 1e3,
+                         "host_threads": ref["threads"],
+                         "speedup": ref["median_s"] / gpu["median_s"]}
+        except Exception as e:  # harness builds missing on this host
+            out[name] = {"unavailable": str(e)[:200]}
+    return out
+
+
+def cfg_skin(tuned, args):
+    """The candidate skin the headline run used."""
+    if tuned:
+        return tuned["skin"]
+    return args.skin if args.skin is not None else 0.1
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -354,6 +418,8 @@ def main():
     ap.add_argument("--tune-steps", type=int, default=128, help="timed steps per autotuner trial")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--plain-steps", type=int, default=3)
+    ap.add_argument("--fp64-batched-steps", type=int, default=None,
+                    help="timed steps of the FP64-forces batched run (default: --steps; 0: skip)")
     ap.add_argument("--ref-particles", type=int, default=120000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="timed region only (profiling)")
@@ -361,10 +427,16 @@ def main():
                     help="steps of the adjoint workload (0: skip)")
     ap.add_argument("--field-steps", type=int, default=50,
                     help="timed steps of the cell-map / stimulus part (0: skip)")
+    ap.add_argument("--dropin-steps", type=int, default=10,
+                    help="timed steps of the drop-in inside the reference's loop (0: skip)")
+    ap.add_argument("--dropin-c3", action="store_true",
+                    help="also time the drop-in on the 1.1M-particle tissue")
     ap.add_argument("--accuracy-steps", type=int, default=1000,
                     help="steps of the mixed-vs-FP64 position error check (0: skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 0)
+    if args.fp64_batched_steps is None:
+        args.fp64_batched_steps = args.steps
 
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -437,6 +509,11 @@ def main():
     value = n_all * args.steps / (ms * 1e-3)
 
     extras = {}
+    # every rank's final positions, assembled on rank 0 in job order
+    gathered = gather_positions(ctx, mine,
+                                rank_tissue_ids(args.workload, args.tissues, world, rank), dist)
+    if gathered is not None:
+        extras["gathered"] = gathered
     if not args.no_extras:
         # per-kernel device time (events around each kernel class, not captured)
         tk = ctx.time_kernels(5)
@@ -550,7 +627,40 @@ def main():
                 pms = float(t.item())
             plain = n_all * args.plain_steps / (pms * 1e-3)
             extras["fp64_plain"] = {"value": plain, "unit": UNIT, "steps": args.plain_steps,
+                                    "path": "FP64 forces, one launch sequence per tissue, "
+                                            "no graph",
                                     "speedup": value / plain}
+
+        # FP64 forces on the same batch, graph and step count as the headline:
+        # what the precision pattern alone buys (batching and launch
+        # amortisation are the same on both sides)
+        if args.fp64_batched_steps > 0 and args.precision == "mixed":
+            with capi.Context(precision=capi.EPI_PREC_FP64, max_conn=64, device=local,
+                              skin=cfg_skin(tuned, args)) as bc:
+                bc.upload(mine)
+                if args.warmup:
+                    bc.step(args.warmup, args.mode)
+                bs = torch.cuda.ExternalStream(bc.stream_handle())
+                torch.cuda.synchronize()
+                barrier()
+                h0 = torch.cuda.Event(enable_timing=True)
+                h1 = torch.cuda.Event(enable_timing=True)
+                h0.record(bs)
+                bc.step(args.fp64_batched_steps, args.mode)
+                h1.record(bs)
+                h1.synchronize()
+                barrier()
+                bms = h0.elapsed_time(h1)
+            if dist is not None:
+                t = torch.tensor([bms], device="cuda", dtype=torch.float64)
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                bms = float(t.item())
+            batched = n_all * args.fp64_batched_steps / (bms * 1e-3)
+            extras["fp64_batched"] = {
+                "value": batched, "unit": UNIT, "steps": args.fp64_batched_steps,
+                "warmup": args.warmup,
+                "path": "FP64 forces, same batch, graph and skin as the headline",
+                "speedup": value / batched}
 
     if world == 1 and not args.no_extras:
         if args.accuracy_steps > 0:
@@ -560,12 +670,16 @@ def main():
         if args.field_steps > 0:
             extras["field"] = field_check(capi, local, args.field_steps,
                                           not args.no_cpu_baseline)
+        if args.dropin_steps > 0 and not args.no_cpu_baseline:
+            wl = [("c2", T.config2())]
+            if args.dropin_c3:
+                wl.append(("c3", T.config3()))
+            extras["dropin"] = dropin_check(wl, args.dropin_steps, 2)
 
     if rank == 0:
         cfg = {"workload": desc, "tissues": n_tissues_all, "particles": n_all,
                "mean_connections": kbar, "precision": args.precision,
-               "skin": (tuned["skin"] if tuned else
-                        (args.skin if args.skin is not None else 0.1)),
+               "skin": cfg_skin(tuned, args),
                "variant": tuned["variant"] if tuned else (args.variant or 1),
                "autotune": tuned,
                "tissues_rebuilt_per_step": rebuilds_timed / max(args.steps, 1),

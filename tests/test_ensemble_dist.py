@@ -122,3 +122,58 @@ def test_weak_scaling_job_per_rank():
     # a single tissue runs as one replica per rank
     mine, n_job1, nt1, _, _ = bench.rank_workload("c1", per, world, 1)
     assert len(mine) == 1 and nt1 == world and n_job1 == world * mine[0].n
+
+
+def _gather_rank_main(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    from oracle import oracle as O
+    from epi_b200.ensemble import gather_results, split_by_tissue
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        job = _gather_job()
+        mine = shard_tissues([t.n for t in job], world)[rank]
+        # this rank's shard stepped as one batch (the oracle stands in for the
+        # rank's GPU context), its positions split back into tissues
+        xs, ys, zs = [], [], []
+        for i in mine:
+            ora = O.OracleTissue(job[i])
+            assert ora.step(5) == 0
+            x, y, z = ora.positions()
+            xs.append(x), ys.append(y), zs.append(z)
+        cat = [np.concatenate(a) for a in (xs, ys, zs)]
+        per = split_by_tissue(cat, [job[i].n for i in mine])
+        res = gather_results(mine, per, dist)
+        out[rank] = res
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def _gather_job():
+    return [T.config1(s) for s in range(3)] + [T.layered_tissue(16 + 8 * (s % 2), 2, s)
+                                               for s in range(3)]
+
+
+def test_two_rank_result_gather_is_in_job_order():
+    """bench.py's multi-GPU job returns its results to rank 0: each rank's
+    per-tissue positions (and adjoint gradients alike) assembled in job order
+    equal the tissues run one batch on one device, tissue by tissue."""
+    world = 2
+    port = 29900 + (os.getpid() % 90)
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(_gather_rank_main, args=(world, port, out), nprocs=world, join=True)
+        res = dict(out)
+    assert res[1] is None
+    got = res[0]
+    job = _gather_job()
+    assert len(got) == len(job)
+    from oracle import oracle as O
+    for t, r in zip(job, got):
+        ora = O.OracleTissue(t)
+        assert ora.step(5) == 0
+        for a, b in zip(ora.positions(), r):
+            assert np.array_equal(a, b)
