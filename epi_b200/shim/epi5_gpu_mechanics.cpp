@@ -23,6 +23,12 @@
 // reference's asserts and aborts do. EPI_MECH_PRECISION=fp64 selects FP64
 // forces (default: FP32 forces, FP64 sums and positions); EPI_MECH_DEVICE
 // selects the GPU.
+//
+// The host work around the library calls -- gathering the cells, writing
+// connected_cell, the gap-junction maps and dermis back, storing the new
+// positions -- touches each cell's own members only, so built with OpenMP
+// (-fopenmp) its per-cell loops run on all host threads; without it they
+// run serially and give the same result.
 #include "cell.h"
 #include "cell_connection.h"
 #include "cell_interaction.h"
@@ -51,6 +57,7 @@ class GpuMechanics {
     check(epi_get_connections(ctx_, off_.data(), idx_.data(), total, &total), "connect_cell");
     dermis_.assign(n, -1);
     check(epi_get_dermis(ctx_, dermis_.data()), "connect_cell");
+#pragma omp parallel for schedule(static)
     for (int32_t i = 0; i < n; ++i) {
       Cell* c = cells_[i];
       if (c->state == MEMB) {
@@ -69,16 +76,15 @@ class GpuMechanics {
           c->connected_cell.push_back(cells_[idx_[k]]);
       }
     }
-    // gj_refresh (cell_connection.cpp:133-152): mark the connected, reset the rest
-    for (Cell* c : cells_) {
+    // gj_refresh (cell_connection.cpp:133-152): mark the connected, reset the
+    // rest; and set_dermis (:178-185), FIX and MUSUME only
+#pragma omp parallel for schedule(static)
+    for (int32_t i = 0; i < n; ++i) {
+      Cell* c = cells_[i];
       for (auto& kv : c->gj) kv.second.uncheck();
       c->connected_cell.foreach([&](Cell* o) { c->gj[o].check(); });
       for (auto& kv : c->gj)
         if (!kv.second.is_checked()) kv.second.reset();
-    }
-    // set_dermis (cell_connection.cpp:178-185): FIX and MUSUME only
-    for (int32_t i = 0; i < n; ++i) {
-      Cell* c = cells_[i];
       if (c->state == FIX || c->state == MUSUME)
         c->set_dermis(dermis_[i] >= 0 ? cells_[dermis_[i]] : nullptr);
     }
@@ -90,6 +96,7 @@ class GpuMechanics {
     const int32_t n = view_.n;
     nx_.resize(n); ny_.resize(n); nz_.resize(n);
     check(epi_download_positions(ctx_, nx_.data(), ny_.data(), nz_.data()), "cell_interaction");
+#pragma omp parallel for schedule(static)
     for (int32_t i = 0; i < n; ++i) {
       Cell* c = cells_[i];
       // The reference runs cell_state_renew between pos_copy and
@@ -153,6 +160,7 @@ class GpuMechanics {
     x_.resize(n); y_.resize(n); z_.resize(n); r_.resize(n); agek_.resize(n); spr_.resize(n);
     state_.resize(n); pair_.resize(n); rest_.resize(n);
     int32_t nmemb = 0, nder = 0;
+#pragma omp parallel for schedule(static) reduction(+ : nmemb, nder)
     for (size_t i = 0; i < n; ++i) {
       const Cell* c = cells_[i];
       x_[i] = c->x();

@@ -208,8 +208,11 @@ def build(name: str, variant: str, jobs: int = 8) -> Path:
         flags = ["-O2", "-ffp-contract=off"]
     elif variant == "omp":
         flags = ["-O3", "-march=x86-64-v3", "-fopenmp", "-DEPI_TBB_SHIM_OPENMP"]
-    elif variant == "dropin":
-        flags = ["-O2", "-ffp-contract=off"]
+    elif variant in ("dropin", "dropin_omp"):
+        # dropin_omp: the timed build (the reference's own loops and the
+        # drop-in's host loops on all threads, as the omp build)
+        flags = (["-O2", "-ffp-contract=off"] if variant == "dropin" else
+                 ["-O3", "-march=x86-64-v3", "-fopenmp", "-DEPI_TBB_SHIM_OPENMP"])
         inc += ["-I", str(ROOT / "include")]
         srcs = [s for s in srcs if s.name not in DROPIN_REPLACED] + [DROPIN_SHIM]
         # relative rpath: the binary sits three levels below the repository root
@@ -242,7 +245,7 @@ def main(argv):
     variants = ["serial", "omp"]
     if "--dropin" in argv:
         argv = [a for a in argv if a != "--dropin"]
-        variants.append("dropin")
+        variants += ["dropin", "dropin_omp"]
     names = argv or list(GEOMETRIES)
     if not available():
         print(f"reference sources not found under {REF_DIR}; nothing built")

@@ -246,13 +246,16 @@ def run_reference_gj(t, nsteps: int, every: int, variant: str = "serial",
         return frames, read_gj_frames(path)
 
 
-def time_reference(t, warmup: int, steps: int, threads: Optional[int] = None):
-    """Time the OpenMP build of the reference on `t`; returns its JSON summary."""
+def time_reference(t, warmup: int, steps: int, threads: Optional[int] = None,
+                   variant: str = "omp", env: Optional[dict] = None):
+    """Time the OpenMP build of the reference on `t` (or another build: the
+    drop-in's is "dropin_omp"); returns its JSON summary."""
     import json
-    exe = reference_binary(t, "omp")
+    exe = reference_binary(t, variant)
     if exe is None:
-        raise FileNotFoundError("compiled reference harness (omp) not built for this geometry")
-    env = dict(os.environ)
+        raise FileNotFoundError(f"compiled reference harness ({variant}) not built for this "
+                                f"geometry")
+    env = dict(os.environ, **(env or {}))
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)
     with tempfile.TemporaryDirectory() as d:
