@@ -416,6 +416,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default skin / variant instead of epi_autotune's choice")
     ap.add_argument("--tune-steps", type=int, default=128, help="timed steps per autotuner trial")
+    ap.add_argument("--retune", action="store_true",
+                    help="run the autotuner even when its choice for this batch is cached")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--fp64-batched-steps", type=int, default=None,
@@ -465,13 +467,14 @@ def main():
     tuned = None
     if args.skin is None and args.variant is None and not args.no_autotune:
         # tune on the state the timed region starts from (after the warm-up's
-        # relaxation of the jittered start), then warm up again below
+        # relaxation of the jittered start), then warm up again below; a
+        # choice cached for this batch shape is reused (epi_b200/autotune.py)
         if args.warmup:
             ctx.step(args.warmup, args.mode)
-        skin, variant, trial_ms = ctx.autotune(args.tune_steps)
-        tuned = {"skin": skin, "variant": variant, "trial_ms_per_step": trial_ms,
-                 "trial_steps": args.tune_steps,
-                 "grid": "skin {0.05,0.08,0.1,0.15,0.2,0.3} x step-kernel variant 1..4"}
+        from epi_b200.autotune import tuned as autotuned
+        tuned = autotuned(ctx, mine, args.tune_steps, device=local, retune=args.retune)
+        tuned["grid"] = ("skin {0.05,0.08,0.1,0.15,0.2,0.3} x step-kernel variant 1..6, "
+                         "then search switch {8192,16384,49152,131072}")
     off, _ = ctx.connections()
     kbar = float(off[-1]) / max(n_mine, 1)  # mean connected_cell length incl. lattice links
     nmemb_mine = sum(t.nmemb for t in mine)
@@ -680,7 +683,8 @@ def main():
         cfg = {"workload": desc, "tissues": n_tissues_all, "particles": n_all,
                "mean_connections": kbar, "precision": args.precision,
                "skin": cfg_skin(tuned, args),
-               "variant": tuned["variant"] if tuned else (args.variant or 1),
+               "variant": tuned["variant"] if tuned else (args.variant or 3),
+               "search_switch": ctx.config()["search_switch"] or 49152,
                "autotune": tuned,
                "tissues_rebuilt_per_step": rebuilds_timed / max(args.steps, 1),
                "rebuilt_fraction_per_step": rebuilds_timed / max(args.steps, 1) / len(mine),

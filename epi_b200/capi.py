@@ -41,7 +41,7 @@ EXPORTED = [
     "epi_step_per_tissue", "epi_sync", "epi_num_particles", "epi_download_positions",
     "epi_upload_positions", "epi_step_host", "epi_step_host_async", "epi_get_connections", "epi_get_dermis", "epi_error_info",
     "epi_stream", "epi_rebuild_count", "epi_launch_count", "epi_time_kernels", "epi_autotune",
-    "epi_field_init",
+    "epi_get_config", "epi_set_tuning", "epi_field_init",
     "epi_field_step", "epi_field_get", "epi_field_set_ext", "epi_adjoint", "epi_connect_noalloc",
 ]
 
@@ -89,7 +89,7 @@ class ConfigC(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("precision", ctypes.c_int32),
                 ("max_conn", ctypes.c_int32), ("max_cand", ctypes.c_int32),
                 ("skin", ctypes.c_double), ("variant", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+                ("search_switch", ctypes.c_int32)]
 
 
 _lib = None
@@ -134,6 +134,8 @@ def lib():
         L.epi_time_kernels.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, _dp, _ip,
                                        ctypes.POINTER(ctypes.c_char_p), _ip]
         L.epi_autotune.argtypes = [vp, ctypes.c_int32, _dp, _ip, _dp]
+        L.epi_get_config.argtypes = [vp, ctypes.POINTER(ConfigC)]
+        L.epi_set_tuning.argtypes = [vp, ctypes.c_double, ctypes.c_int32, ctypes.c_int32]
         L.epi_field_init.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
         L.epi_field_step.argtypes = [vp, ctypes.c_int32]
         L.epi_field_get.argtypes = [vp, ctypes.c_int32, _ip, _up, _dp, _dp]
@@ -371,6 +373,17 @@ class Context:
                                  _ptr(loss, ctypes.c_double), _ptr(grad, ctypes.c_double)),
                "epi_adjoint")
         return loss, grad.reshape(nt, 3)
+
+    def config(self) -> dict:
+        """epi_get_config: the context's configuration (after autotune: its choice)."""
+        cfg = ConfigC()
+        _check(lib().epi_get_config(self._h, ctypes.byref(cfg)), "epi_get_config")
+        return {k: getattr(cfg, k) for k, _ in ConfigC._fields_}
+
+    def set_tuning(self, skin: float, variant: int, search_switch: int = 0):
+        """epi_set_tuning: apply a tuning chosen earlier (e.g. cached)."""
+        _check(lib().epi_set_tuning(self._h, float(skin), int(variant), int(search_switch)),
+               "epi_set_tuning")
 
     def autotune(self, trial_steps: int = 64):
         """epi_autotune: returns (skin, variant, ms per step of the best trial)

@@ -53,6 +53,9 @@ namespace {
 
 // epi_step_host splits the batch into at most this many groups of tissues.
 constexpr int kHostStepGroups = 8;
+// Rebuilt particles from which the candidate search takes one thread per
+// particle (epi_config.search_switch = 0).
+constexpr int kDefaultSearchSwitch = 48 * 1024;
 
 // Host-side bookkeeping of one tissue in the batch.
 struct TissueHost {
@@ -70,7 +73,8 @@ struct epi_ctx {
   // the membrane sums run on `aux` beside the candidate rebuild (fork / join)
   cudaStream_t aux = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  LaunchCfg lc{148, 256, 0, 0, 0};
+  cudaEvent_t ev_cond = nullptr;  // split step: the rebuild work list is built
+  LaunchCfg lc{148, 256, 0, 0, 0, kDefaultSearchSwitch};
   bool loaded = false;
   bool lists_fresh = false;  // nbr / nn / dermis match the current positions
   int32_t ntissues = 0;
@@ -107,7 +111,8 @@ struct epi_ctx {
   uint32_t* skey = nullptr;
   float4* spos = nullptr;
   int32_t* gate = nullptr;
-  int32_t* rl = nullptr;    // rebuild work list: [count | list (T) | ppre (T+1) | bpre (T+1)]
+  // rebuild work list: [count | list (T) | ppre (T+1) | bpre (T+1) | marks (T)]
+  int32_t* rl = nullptr;
   int32_t* prep = nullptr;
   double* stage = nullptr;        // 3n doubles: x | y | z for host transfers
   // epi_step_host: copy streams, per-chunk events, the outbound staging (3n)
@@ -252,6 +257,7 @@ DevState make_state(epi_ctx* c, int cur) {
   S.rl_list = c->rl ? c->rl + 1 : nullptr;
   S.rl_ppre = c->rl ? c->rl + 1 + c->ntissues : nullptr;
   S.rl_bpre = c->rl ? c->rl + 2 + 2 * c->ntissues : nullptr;
+  S.rl_mark = c->rl ? c->rl + 3 + 3 * c->ntissues : nullptr;
   S.ntissues = c->ntissues;
   S.prep = c->prep;
   S.nprep = c->nprep;
@@ -331,12 +337,38 @@ void enqueue_step(epi_ctx* c, int& cur, Timer* tm) {
   cur ^= 1;
 }
 
+// The step graph's split schedule: whether the step of the tissues that need
+// no candidate rebuild may run beside the rebuild of the others. It may when
+// the batch has no FIX / MUSUME cell (their dermis is found after the
+// rebuild, and the step reads it) and the step kernel is not the persistent
+// one (whose blocks would hold every SM while the rebuild waits for room).
+bool split_step(const epi_ctx* c) {
+  return c->nprep == c->nprep_memb && (c->lc.variant == 3 || c->lc.variant == 4);
+}
+// Blocks per SM of the rebuild's grid-stride kernels: in the split schedule
+// they share the GPU with the step, so they take a quarter of their usual
+// grid and leave most SMs to it.
+constexpr int kRebuildPerSmSplit = 2;
+
+// Skin, step-kernel variant and candidate-search switch of the context; the
+// captured graphs hold all three, so they are dropped.
+void apply_tuning(epi_ctx* c, double skin, int32_t variant, int32_t search_switch) {
+  c->cfg.skin = skin;
+  c->cfg.variant = variant;
+  c->cfg.search_switch = search_switch;
+  c->lc.variant = variant == 0 ? 3 : variant;
+  c->lc.search_switch = search_switch > 0 ? search_switch : kDefaultSearchSwitch;
+  destroy_graphs(c);
+}
+
 // Appends to the graph being captured on c->stream a conditional (IF) node
 // whose body, captured on c->side, is the candidate rebuild; a one-block
 // kernel before it builds the rebuild work list and sets the condition to
 // "the list is not empty", so steps that need no rebuild launch none of the
-// rebuild's kernels.
-cudaError_t capture_conditional_rebuild(epi_ctx* c, int cur) {
+// rebuild's kernels. side_step: right after the work list, the step of the
+// particles of the tissues not on it is forked onto c->aux (after the
+// membrane sums already queued there), to run beside the rebuild.
+cudaError_t capture_conditional_rebuild(epi_ctx* c, int cur, bool side_step = false) {
   cudaStreamCaptureStatus st;
   cudaGraph_t g;
   const cudaGraphNode_t* deps = nullptr;
@@ -346,6 +378,14 @@ cudaError_t capture_conditional_rebuild(epi_ctx* c, int cur) {
   cudaGraphConditionalHandle h;
   if ((e = cudaGraphConditionalHandleCreate(&h, g, 0, 0)) != cudaSuccess) return e;
   launch_rebuild_condition(make_state(c, cur), whole(c), h, c->stream);
+  if (side_step) {
+    if ((e = cudaEventRecord(c->ev_cond, c->stream)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(c->aux, c->ev_cond, 0)) != cudaSuccess) return e;
+    Range r = whole(c);
+    r.skip_listed = 1;
+    launch_step(make_state(c, cur), r, c->cfg.precision, c->lc, c->aux, nullptr);
+    if ((e = cudaEventRecord(c->ev_join, c->aux)) != cudaSuccess) return e;
+  }
   if ((e = cudaStreamGetCaptureInfo(c->stream, &st, nullptr, &g, &deps, &nd)) != cudaSuccess)
     return e;
   cudaGraphNodeParams p{};
@@ -359,7 +399,9 @@ cudaError_t capture_conditional_rebuild(epi_ctx* c, int cur) {
   if ((e = cudaStreamBeginCaptureToGraph(c->side, body, nullptr, nullptr, 0,
                                          cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
     return e;
-  launch_rebuild(make_state(c, cur), whole(c), c->scan, c->lc, c->side, nullptr, true);
+  LaunchCfg lc = c->lc;
+  if (side_step) lc.rebuild_per_sm = kRebuildPerSmSplit;
+  launch_rebuild(make_state(c, cur), whole(c), c->scan, lc, c->side, nullptr, true);
   if ((e = cudaStreamEndCapture(c->side, &body)) != cudaSuccess) return e;
   return cudaStreamUpdateCaptureDependencies(c->stream, &node, 1,
                                              cudaStreamSetCaptureDependencies);
@@ -392,13 +434,20 @@ cudaError_t capture_step_graph(epi_ctx* c, cudaGraphExec_t* out) {
                                       cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
       int cur = c->cur;
+      const bool split = split_step(c);
       for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
         e = fork_memb(c, cur, nullptr);
-        if (e == cudaSuccess) e = capture_conditional_rebuild(c, cur);
+        if (e == cudaSuccess) e = capture_conditional_rebuild(c, cur, split);
         if (e != cudaSuccess) break;
-        dermis_all(c, cur, nullptr);
-        if ((e = join_memb(c)) != cudaSuccess) break;
-        launch_step(make_state(c, cur), whole(c), c->cfg.precision, c->lc, c->stream, nullptr);
+        if (split) {
+          // the side stream's membrane sums and step, then the rebuilt tissues
+          if ((e = cudaStreamWaitEvent(c->stream, c->ev_join, 0)) != cudaSuccess) break;
+          launch_step_listed(make_state(c, cur), c->cfg.precision, c->lc, c->stream);
+        } else {
+          dermis_all(c, cur, nullptr);
+          if ((e = join_memb(c)) != cudaSuccess) break;
+          launch_step(make_state(c, cur), whole(c), c->cfg.precision, c->lc, c->stream, nullptr);
+        }
         cur ^= 1;
       }
       if (e == cudaSuccess) launch_loop_tick(c->loop_left, hw, c->launches, c->stream);
@@ -638,7 +687,7 @@ void epi_config_default(epi_config* c) {
   c->max_cand = 96;
   c->skin = 0.1;
   c->variant = 0;
-  c->reserved = 0;
+  c->search_switch = 0;
 }
 
 const char* epi_strerror(int s) {
@@ -671,9 +720,9 @@ int epi_create(epi_ctx** out, const epi_config* cfg) {
   if (c.max_conn <= 0 || c.max_conn > 400 || c.max_cand < c.max_conn || c.max_cand > 1024)
     return EPI_ERR_INVALID_ARG;
   if (!(c.skin > 0) || c.skin > 2.0) return EPI_ERR_INVALID_ARG;
-  if (c.variant < 0 || c.variant > 4) return EPI_ERR_INVALID_ARG;
+  if (c.variant < 0 || c.variant > 6) return EPI_ERR_INVALID_ARG;
   if (c.precision != EPI_PREC_FP64 && c.precision != EPI_PREC_MIXED) return EPI_ERR_INVALID_ARG;
-  if (c.reserved != 0) return EPI_ERR_INVALID_ARG;
+  if (c.search_switch < 0) return EPI_ERR_INVALID_ARG;
   int ndev = 0;
   const cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev <= 0) return EPI_ERR_NO_DEVICE;
@@ -681,7 +730,8 @@ int epi_create(epi_ctx** out, const epi_config* cfg) {
   EPI_CUDA(cudaSetDevice(c.device));
   epi_ctx* ctx = new epi_ctx();
   ctx->cfg = c;
-  ctx->lc.variant = c.variant;
+  ctx->lc.variant = c.variant == 0 ? 3 : c.variant;
+  ctx->lc.search_switch = c.search_switch > 0 ? c.search_switch : kDefaultSearchSwitch;
   int sms = 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device) == cudaSuccess &&
       sms > 0)
@@ -700,6 +750,8 @@ int epi_create(epi_ctx** out, const epi_config* cfg) {
     rc = cuda_status(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
   if (rc == EPI_OK)
     rc = cuda_status(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+  if (rc == EPI_OK)
+    rc = cuda_status(cudaEventCreateWithFlags(&ctx->ev_cond, cudaEventDisableTiming));
   if (rc == EPI_OK) rc = dev_alloc(&ctx->status, 1);
   if (rc == EPI_OK) rc = cuda_status(cudaMallocHost((void**)&ctx->status_h, sizeof(DevStatus)));
   if (rc == EPI_OK) rc = cuda_status(cudaMemset(ctx->status, 0, sizeof(DevStatus)));
@@ -737,6 +789,7 @@ void epi_destroy(epi_ctx* ctx) {
   if (ctx->aux) cudaStreamSynchronize(ctx->aux);
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+  if (ctx->ev_cond) cudaEventDestroy(ctx->ev_cond);
   if (ctx->aux) cudaStreamDestroy(ctx->aux);
   if (ctx->side) cudaStreamDestroy(ctx->side);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -901,19 +954,21 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
       return rc;
     }
   }
-  if (!reuse && ((rc = dev_alloc(&c->tissues, ntissues)) || (rc = dev_alloc(&c->pos[0], n)) ||
-      (rc = dev_alloc(&c->pos[1], n)) || (rc = dev_alloc(&c->posf[0], n)) ||
-      (rc = dev_alloc(&c->posf[1], n)) || (rc = dev_alloc(&c->attr, n)) ||
+  // buffers the step kernel streams by whole tiles are padded (kStepTilePad)
+  const int64_t np = padded_particles(n);
+  if (!reuse && ((rc = dev_alloc(&c->tissues, ntissues)) || (rc = dev_alloc(&c->pos[0], np)) ||
+      (rc = dev_alloc(&c->pos[1], np)) || (rc = dev_alloc(&c->posf[0], n)) ||
+      (rc = dev_alloc(&c->posf[1], n)) || (rc = dev_alloc(&c->attr, np)) ||
       (rc = dev_alloc(&c->pair, n)) || (rc = dev_alloc(&c->spr, n)) ||
-      (rc = dev_alloc(&c->dermis, n)) || (rc = dev_alloc(&c->cand, CC * n)) ||
-      (rc = dev_alloc(&c->bpos, n)) ||
+      (rc = dev_alloc(&c->dermis, n)) || (rc = dev_alloc(&c->cand, CC * n + kStepTilePad)) ||
+      (rc = dev_alloc(&c->bpos, np)) ||
       (rc = dev_alloc(&c->nbr, C * n)) || (rc = dev_alloc(&c->nn, n)) ||
-      (rc = dev_alloc(&c->fmemb, n)) ||
+      (rc = dev_alloc(&c->fmemb, np)) ||
       (rc = dev_alloc(&c->bin, n)) || (rc = dev_alloc(&c->rank, n)) ||
       (rc = dev_alloc(&c->counts, nbins)) || (rc = dev_alloc(&c->starts, nbins + 1)) ||
       (rc = dev_alloc(&c->skey, n)) || (rc = dev_alloc(&c->spos, n)) ||
       (rc = dev_alloc(&c->gate, (size_t)ntissues + 1)) ||
-      (rc = dev_alloc(&c->rl, 3 + 3 * (size_t)ntissues)) ||
+      (rc = dev_alloc(&c->rl, 3 + 4 * (size_t)ntissues)) ||
       (rc = dev_alloc(&c->prep, prep.size())) || (rc = dev_alloc(&c->stage, 3 * (size_t)n)) ||
       (rc = dev_alloc(&c->agek, n)))) {
     free_buffers(c);
@@ -1250,7 +1305,7 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
   int rc = set_device(c);
   if (rc) return rc;
   static const double kSkins[] = {0.05, 0.08, 0.1, 0.15, 0.2, 0.3};
-  static const int32_t kVariants[] = {1, 2, 3, 4};
+  static const int32_t kVariants[] = {1, 2, 3, 4, 5, 6};
   constexpr int32_t kWarm = 4;  // the first step after a restore rebuilds every tissue
   const size_t pbytes = sizeof(double4) * (size_t)c->n;
   cudaStream_t s = c->stream;
@@ -1278,26 +1333,33 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
     c->lists_fresh = false;
     return EPI_OK;
   };
-  auto apply = [&](double skin, int32_t variant) {
-    c->cfg.skin = skin;
-    c->cfg.variant = variant;
-    c->lc.variant = variant;
-    destroy_graphs(c);  // the graphs hold the skin and the kernel instantiation
+  auto apply = [&](double skin, int32_t variant, int32_t search_switch) {
+    apply_tuning(c, skin, variant, search_switch);
+  };
+  // one trial: ms per trial (INFINITY when the rows overflowed)
+  auto trial = [&](double* ms_out) -> int {
+    int r;
+    if ((r = restore())) return r;
+    if ((r = enqueue_graph_steps(c, kWarm))) return r;
+    EPI_CUDA(cudaEventRecord(ev[0], s));
+    if ((r = enqueue_graph_steps(c, trial_steps))) return r;
+    EPI_CUDA(cudaEventRecord(ev[1], s));
+    *ms_out = INFINITY;
+    // a skin whose candidate rows overflow max_cand fails here: skip it
+    if (check_status(c) != EPI_OK) return EPI_OK;
+    float ms = 0;
+    EPI_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    *ms_out = ms;
+    return EPI_OK;
   };
   double best = INFINITY, best_skin = c->cfg.skin;
   int32_t best_variant = c->cfg.variant;
+  const int32_t switch0 = c->cfg.search_switch;
   for (double skin : kSkins) {
     for (int32_t variant : kVariants) {
-      apply(skin, variant);
-      if ((rc = restore())) return rc;
-      if ((rc = enqueue_graph_steps(c, kWarm))) return rc;
-      EPI_CUDA(cudaEventRecord(ev[0], s));
-      if ((rc = enqueue_graph_steps(c, trial_steps))) return rc;
-      EPI_CUDA(cudaEventRecord(ev[1], s));
-      // a skin whose candidate rows overflow max_cand fails here: skip it
-      if (check_status(c) != EPI_OK) continue;
-      float ms = 0;
-      EPI_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+      apply(skin, variant, switch0);
+      double ms;
+      if ((rc = trial(&ms))) return rc;
       if (ms < best) {
         best = ms;
         best_skin = skin;
@@ -1305,13 +1367,50 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
       }
     }
   }
-  apply(best_skin, best_variant);
+  // then the candidate search's switch between its two forms
+  static const int32_t kSwitches[] = {8192, 16384, 49152, 131072};
+  int32_t best_switch = switch0;
+  if (std::isfinite(best)) {
+    for (int32_t sw : kSwitches) {
+      apply(best_skin, best_variant, sw);
+      double ms;
+      if ((rc = trial(&ms))) return rc;
+      if (ms < best) {
+        best = ms;
+        best_switch = sw;
+      }
+    }
+  }
+  apply(best_skin, best_variant, best_switch);
   if ((rc = restore())) return rc;
   if ((rc = check_status(c))) return rc;
   if (skin_out) *skin_out = best_skin;
   if (variant_out) *variant_out = best_variant;
   if (ms_out) *ms_out = std::isfinite(best) ? best / trial_steps : -1.0;
   return std::isfinite(best) ? EPI_OK : EPI_ERR_LIST_OVERFLOW;
+  EPI_GUARD_END
+}
+
+int epi_get_config(epi_ctx* c, epi_config* out) {
+  if (!c || !out) return EPI_ERR_INVALID_ARG;
+  *out = c->cfg;
+  return EPI_OK;
+}
+
+int epi_set_tuning(epi_ctx* c, double skin, int32_t variant, int32_t search_switch) {
+  if (!c || !(skin > 0) || skin > 2.0 || variant < 0 || variant > 6 || search_switch < 0)
+    return EPI_ERR_INVALID_ARG;
+  EPI_GUARD_BEGIN
+  int rc = set_device(c);
+  if (rc) return rc;
+  apply_tuning(c, skin, variant, search_switch);
+  if (c->loaded) {
+    // candidates were built for the old skin: rebuild every tissue's
+    launch_set_gates(make_state(c, c->cur), c->ntissues, c->stream);
+    c->lists_fresh = false;
+    return check_status(c);
+  }
+  return EPI_OK;
   EPI_GUARD_END
 }
 

@@ -172,8 +172,14 @@ __device__ __forceinline__ int32_t ref_bin(const TissueDev& T, double x, double 
 // index back to (tissue, local index) by binary search in the prefix sums.
 // With nothing gated the list is empty and each kernel exits at once.
 // ---------------------------------------------------------------------------
+// Each tissue of [t0, t1) is marked (rl_mark) while it is on the list, so
+// a step kernel running beside the rebuild can leave those tissues out.
+// For the whole batch the "some tissue" word is cleared once the list is
+// built: the step kernels set it again for the next step.
 __device__ __forceinline__ void gate_compact(const DevState& S, int32_t t0, int32_t t1) {
+  const bool whole = t0 == 0 && t1 == S.ntissues;
   if (S.gate[0] == 0) {
+    for (int32_t t = t0 + (int32_t)threadIdx.x; t < t1; t += blockDim.x) S.rl_mark[t] = 0;
     if (threadIdx.x == 0) {
       S.rl_count[0] = 0;
       S.rl_ppre[0] = 0;
@@ -181,10 +187,13 @@ __device__ __forceinline__ void gate_compact(const DevState& S, int32_t t0, int3
     }
     return;
   }
+  __syncthreads();  // every thread has read gate[0] before it is cleared
+  if (whole && threadIdx.x == 0) S.gate[0] = 0;
   int32_t cc = 0, cp = 0, cb = 0;
   for (int32_t base = t0; base < t1; base += kScanThreads) {
     const int32_t t = base + threadIdx.x;
     const bool g = t < t1 && S.gate[1 + t] != 0;
+    if (t < t1) S.rl_mark[t] = g ? 1 : 0;
     int32_t np = 0, nb = 0;
     if (g) {
       const TissueDev& T = S.tissues[t];
@@ -212,14 +221,11 @@ __device__ __forceinline__ void gate_compact(const DevState& S, int32_t t0, int3
 }
 
 // Once the work list is built nothing of the rebuild reads the flags: clear
-// the listed tissues' flags (and the "some tissue" word for a whole-batch
-// rebuild) and count the rebuilds. Run by one block of the candidate search.
-__device__ __forceinline__ void gate_clear(const DevState& S, int32_t cnt, int32_t clear_any) {
+// the listed tissues' flags and count the rebuilds. Run by one block of the
+// candidate search. (gate_compact cleared the "some tissue" word.)
+__device__ __forceinline__ void gate_clear(const DevState& S, int32_t cnt) {
   for (int32_t k = threadIdx.x; k < cnt; k += blockDim.x) S.gate[1 + S.rl_list[k]] = 0;
-  if (threadIdx.x == 0) {
-    if (cnt) atomicAdd(S.rebuilds, (unsigned long long)cnt);
-    if (clear_any) S.gate[0] = 0;
-  }
+  if (threadIdx.x == 0 && cnt) atomicAdd(S.rebuilds, (unsigned long long)cnt);
 }
 
 __global__ void k_gate_compact(DevState S, int32_t t0, int32_t t1) {
@@ -570,6 +576,42 @@ __device__ __forceinline__ void cand_search_warps(const DevState& S, int32_t cnt
   }
 }
 
+// A thread's candidate row written a whole 16-byte chunk at a time: entries
+// collect in a register chunk that is stored when full or at the end (chunk 0
+// is stored with a zero count; the caller stores the count afterwards).
+struct RowWriter {
+  const DevState& S;
+  const int64_t i;
+  const bool k16;
+  uint32_t w0 = 0, w1 = 0, w2 = 0, w3 = 0;
+  int32_t e = 1;  // next entry (entry 0 is the count)
+  __device__ __forceinline__ RowWriter(const DevState& S_, int64_t i_)
+      : S(S_), i(i_), k16(S_.cand16 != 0) {}
+  __device__ __forceinline__ void put(uint32_t v) {
+    const int per = k16 ? 8 : 4;
+    const int slot = e & (per - 1);
+    const int word = k16 ? slot >> 1 : slot;
+    const uint32_t sh = k16 ? (uint32_t)(slot & 1) * 16u : 0u;
+    const uint32_t m = k16 ? 0xffffu << sh : 0xffffffffu;
+    const uint32_t val = (k16 ? (v & 0xffffu) : v) << sh;
+    w0 = word == 0 ? (w0 & ~m) | val : w0;
+    w1 = word == 1 ? (w1 & ~m) | val : w1;
+    w2 = word == 2 ? (w2 & ~m) | val : w2;
+    w3 = word == 3 ? (w3 & ~m) | val : w3;
+    ++e;
+    if ((e & (per - 1)) == 0) flush();
+  }
+  __device__ __forceinline__ void flush() {
+    const int per = k16 ? 8 : 4;
+    S.cand[(int64_t)((e - 1) / per) * S.n_total + i] = make_uint4(w0, w1, w2, w3);
+    w0 = w1 = w2 = w3 = 0;
+  }
+  __device__ __forceinline__ void close() {
+    const int per = k16 ? 8 : 4;
+    if ((e & (per - 1)) != 0) flush();
+  }
+};
+
 // Many gated particles: one thread per particle. A particle sweeps about a
 // hundred slots (bins of 2.0 hold about six particles), four at a time so
 // their loads overlap; a warp keeps 32 particles in flight and writes the
@@ -585,6 +627,7 @@ __device__ __forceinline__ void cand_search_threads(const DevState& S, int32_t c
     const SearchWindow W(S, T, i);
     const int32_t any = T.any, anz = T.anz, binbase = T.binbase;
     const uint32_t pbase = (uint32_t)T.pbase;
+    RowWriter row(S, i);
     int32_t count = 0;
     for (int xr = 0; xr < W.nxr; ++xr) {
       const float ex = W.pxe[xr];
@@ -605,7 +648,7 @@ __device__ __forceinline__ void cand_search_threads(const DevState& S, int32_t c
 #pragma unroll
               for (int u = 0; u < 4; ++u) {
                 if (s + u < s_hi && W.hit(i, key[u], q[u], ex, ey)) {
-                  if (count < cap) cand_set(S, i, count + 1, (key[u] & 0x7fffffffu) - pbase);
+                  if (count < cap) row.put((key[u] & 0x7fffffffu) - pbase);
                   ++count;
                 }
               }
@@ -614,21 +657,22 @@ __device__ __forceinline__ void cand_search_threads(const DevState& S, int32_t c
         }
       }
     }
+    row.close();
     finish_search(S, i, count);
   }
 }
 
-// Below this many gated particles the warp-per-particle search is faster.
-constexpr int32_t kWarpSearchMax = 48 * 1024;
-
-__global__ void __launch_bounds__(256, 4) k_cand_search(DevState S, int32_t clear_any) {
+// Below `thread_from` gated particles the warp-per-particle search (which
+// keeps the GPU busy with few particles) runs, from there on one thread per
+// particle. Both emit every row in the same order.
+__global__ void __launch_bounds__(256, 4) k_cand_search(DevState S, int32_t thread_from) {
   pdl_entry();
   count_launch(S.launches);
   const int32_t cnt = S.rl_count[0];
-  if (blockIdx.x == 0) gate_clear(S, cnt, clear_any);
+  if (blockIdx.x == 0) gate_clear(S, cnt);
   if (cnt == 0) return;
   const int32_t ngated = S.rl_ppre[cnt];
-  if (ngated < kWarpSearchMax) cand_search_warps(S, cnt, ngated);
+  if (ngated < thread_from) cand_search_warps(S, cnt, ngated);
   else cand_search_threads(S, cnt, ngated);
 }
 
@@ -982,12 +1026,26 @@ struct Particle {
   const R dt;
   int32_t pair_i = -1, dermis_i = -1;
   double ax = 0.0, ay = 0.0, az = 0.0;
+  // the first too-strong interaction of this particle (|coef| > 1000): kept
+  // in registers and reported by finish(), so the candidate loop stores
+  // nothing and the tissue's constants stay in registers across it
+  int32_t bad_a = -1, bad_b = -1;
+  double bad_v = 0.0;
+  __device__ __forceinline__ void note_bad(R c, int32_t x, int32_t y) {
+    if (fabs(c) > R(1000) && bad_a < 0) {
+      bad_a = x;
+      bad_b = y;
+      bad_v = double(c);
+    }
+  }
   // the particle's FP32 copy (mixed path only)
   float4 pf = make_float4(0.f, 0.f, 0.f, 0.f);
 
-  __device__ __forceinline__ Particle(const DevState& S_, int32_t i_)
-      : S(S_), i(i_), a(__ldg(&S_.attr[i_])), t(attr_tissue(a)), st(attr_state(a)),
-        T(S_.tissues[t]), L(T.laws<R>()), p(S_.pos_cur[i_]),
+  // a_: the particle's attribute word, p_: its current position
+  __device__ __forceinline__ Particle(const DevState& S_, int32_t i_, uint32_t a_,
+                                     const double4& p_)
+      : S(S_), i(i_), a(a_), t(attr_tissue(a)), st(attr_state(a)),
+        T(S_.tissues[t]), L(T.laws<R>()), p(p_),
         lt2(T.P.lj_thresh * T.P.lj_thresh), dt(R(T.P.dt)) {
     // the FP32 copy of the particle itself, as every writer of posf forms it
     if (kFloatPos) pf = make_float4((float)p.x, (float)p.y, (float)p.z, (float)p.w);
@@ -1052,7 +1110,7 @@ struct Particle {
       const bool both_old = kOld && attr_old(a) && attr_old(__ldg(&S.attr[q]));
       if constexpr (sizeof(R) == 4) coef = L.aad_fused(d2, rs, both_old);
       else coef = L.aad(d2, rs, both_old);
-      if (fabs(coef) > R(1000)) raise_error(S.status, E_COEF_RANGE, i, q, double(coef));
+      note_bad(coef, i, q);
     } else {
       const uint32_t aq = __ldg(&S.attr[q]);
       const uint32_t sq = attr_state(aq);
@@ -1063,7 +1121,7 @@ struct Particle {
         const int law = law_of(st, i, pair_i, dermis_i, sq, q);
         if (law != L_NONE) {
           const R c = eval_law<R>(law, L, d2, rs, both_old, attr_sfm(a));
-          if (fabs(c) > R(1000)) raise_error(S.status, E_COEF_RANGE, i, q, double(c));
+          note_bad(c, i, q);
           coef += c;
         }
       }
@@ -1077,7 +1135,7 @@ struct Particle {
         const int law = law_of(sq, q, pair_q, dermis_q, st, i);
         if (law != L_NONE) {
           const R c = eval_law<R>(law, L, d2, rs, both_old, attr_sfm(aq));
-          if (fabs(c) > R(1000)) raise_error(S.status, E_COEF_RANGE, q, i, double(c));
+          note_bad(c, q, i);
           coef += c;
         }
       }
@@ -1089,9 +1147,11 @@ struct Particle {
     az += double(sdt * dz);
   }
 
-  __device__ __forceinline__ void finish() {
+  // b: the position of the tissue's last candidate rebuild; f: the membrane
+  // sums (membrane particles only)
+  __device__ __forceinline__ void finish(const float4& b, const double4& f) {
+    if (bad_a >= 0) raise_error(S.status, E_COEF_RANGE, bad_a, bad_b, bad_v);
     if (st == ST_MEMB) {
-      const double4 f = S.fmemb[i];
       ax += f.x;
       ay += f.y;
       az += f.z;
@@ -1135,7 +1195,6 @@ struct Particle {
     S.pos_nxt[i] = make_double4(nx, ny, nz, p.w);
     if (kFloatPos) S.posf_nxt[i] = make_float4((float)nx, (float)ny, (float)nz, (float)p.w);
     // Candidate validity: rebuild the tissue once a particle moved skin/2.
-    const float4 b = S.bpos[i];
     double ex = nx - (double)b.x, ey = ny - (double)b.y;
     if (ex > hlx) ex -= lx;
     else if (ex < -hlx) ex += lx;
@@ -1172,30 +1231,14 @@ __device__ __forceinline__ uint32_t row_entry(const uint4 (&c)[NC], int e) {
   return k16 ? ((e & 1) ? word >> 16 : word & 0xffffu) : word;
 }
 
-// One thread per particle. The first chunks of the particle's candidate row
-// (15 candidates with 16-bit entries, 15 with 32-bit) are loaded up front,
-// independent of each other and of the particle's own data, so the index
-// stream costs one memory latency per particle rather than one per
-// candidate. The neighbours' positions are then gathered kG at a time (all
-// kG loads issued before the first is used). Rows longer than that (rare)
-// finish with one load per entry. kMinBlocks bounds the registers so that
-// that many 256-thread blocks stay resident per SM.
-template <typename R, bool kSimple, bool kOld, int kMinBlocks, bool k16>
-__global__ void __launch_bounds__(256, kMinBlocks) k_step(DevState S, Range r) {
-  pdl_entry();
-  count_launch(S.launches);
-  const int64_t i = r.p0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= r.p1) return;
-  const int64_t N = S.n_total;
-  constexpr int kChunks = k16 ? 2 : 4;               // chunks loaded up front
-  constexpr int kPre = kChunks * (k16 ? 8 : 4) - 1;  // candidates they hold
-  constexpr int kG = sizeof(R) == 4 ? 4 : 2;         // gathers in flight
-  uint4 c[kChunks];
-#pragma unroll
-  for (int k = 0; k < kChunks; ++k) c[k] = __ldg(S.cand + k * N + i);
-  using Part = Particle<R, kSimple, kOld>;
+// The candidates of particle i, from the first chunks of its row in c (kPre
+// entries after the count) and the rest of the row from memory, passed to
+// P.candidate with their positions. Positions are gathered kG at a time:
+// all kG loads are issued before the first is used.
+template <bool k16, int kPre, int kG, typename Part, int NC>
+__device__ __forceinline__ void gather_candidates(const DevState& S, Part& P, const uint4 (&c)[NC],
+                                                  int64_t i) {
   using Pos = typename Part::Pos;
-  Part P(S, (int32_t)i);
   const int32_t pbase = P.T.pbase;
   const Pos* src = gather_source<Pos>(S) + pbase;
   const int32_t nc = (int32_t)row_entry<k16>(c, 0);
@@ -1220,7 +1263,206 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_step(DevState S, Range r) {
     const int32_t q = (int32_t)cand_entry(S, i, e);
     P.candidate(pbase + q, src[q]);
   }
-  P.finish();
+}
+
+// One thread per particle. The first chunks of the particle's candidate row
+// (15 candidates with 16-bit entries, 15 with 32-bit) are loaded up front,
+// independent of each other and of the particle's own data, so the index
+// stream costs one memory latency per particle rather than one per
+// candidate. The neighbours' positions are then gathered kG at a time (all
+// kG loads issued before the first is used). Rows longer than that (rare)
+// finish with one load per entry. kMinBlocks bounds the registers so that
+// that many 256-thread blocks stay resident per SM.
+// One particle of the step (skip_listed: nothing for a particle whose tissue
+// is on the rebuild work list).
+template <typename R, bool kSimple, bool kOld, bool k16>
+__device__ __forceinline__ void step_particle(const DevState& S, int64_t i, bool skip_listed) {
+  const int64_t N = S.n_total;
+  constexpr int kChunks = k16 ? 2 : 4;               // chunks loaded up front
+  constexpr int kPre = kChunks * (k16 ? 8 : 4) - 1;  // candidates they hold
+  constexpr int kG = sizeof(R) == 4 ? 4 : 2;         // gathers in flight
+  uint4 c[kChunks];
+#pragma unroll
+  for (int k = 0; k < kChunks; ++k) c[k] = __ldg(S.cand + k * N + i);
+  const uint32_t a = __ldg(&S.attr[i]);
+  if (skip_listed && S.rl_mark[attr_tissue(a)]) return;
+  using Part = Particle<R, kSimple, kOld>;
+  Part P(S, (int32_t)i, a, S.pos_cur[i]);
+  const float4 bp = S.bpos[i];
+  const double4 fm = P.st == ST_MEMB ? S.fmemb[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+  gather_candidates<k16, kPre, kG>(S, P, c, i);
+  P.finish(bp, fm);
+}
+
+template <typename R, bool kSimple, bool kOld, int kMinBlocks, bool k16>
+__global__ void __launch_bounds__(256, kMinBlocks) k_step(DevState S, Range r) {
+  pdl_entry();
+  count_launch(S.launches);
+  const int64_t i = r.p0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= r.p1) return;
+  step_particle<R, kSimple, kOld, k16>(S, i, r.skip_listed != 0);
+}
+
+// The particles of the tissues on the rebuild work list, after their
+// rebuild: a grid-stride loop over the listed particles.
+template <typename R, bool kSimple, bool kOld, int kMinBlocks, bool k16>
+__global__ void __launch_bounds__(256, kMinBlocks) k_step_listed(DevState S) {
+  pdl_entry();
+  count_launch(S.launches);
+  GATED_PARTICLES(g, cnt) {
+    int32_t t;
+    const int32_t i = gated_particle(S, cnt, g, &t);
+    step_particle<R, kSimple, kOld, k16>(S, i, false);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The step as a persistent kernel with its per-particle input stream staged
+// in shared memory by the bulk-copy engine. A block takes tiles of kT
+// consecutive particles (tile t: particles [t kT, (t + 1) kT)) in turn; while
+// its threads work on one tile, bulk copies (cp.async.bulk, completion counted
+// on an mbarrier) bring the next tile's candidate chunks, positions, membrane
+// sums, rebuild positions and attribute words into the other half of a
+// double buffer. The threads then wait only on their neighbours' position
+// gathers, which hit L1 / L2; the streamed inputs are read once, so their
+// copies carry an L2 evict-first policy and leave L2 to the gathered FP32
+// copies. Allocations are padded to whole tiles (kStepTilePad), so a tile's
+// copies never leave their buffers; particles of a tile outside the launch
+// range are skipped.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Waits for phase `parity` of the barrier to complete; gives up (false)
+// after kWaitTries unsuccessful tries (each try may block for a while).
+constexpr uint32_t kWaitTries = 1u << 22;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (uint32_t k = 0; k < kWaitTries; ++k)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ uint64_t l2_evict_first() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+// global -> shared bulk copy of `bytes` (a multiple of 16, both addresses
+// 16-byte aligned), completion counted on bar
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes,
+                                          uint64_t* bar, uint64_t pol) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint "
+      "[%0], [%1], %2, [%3], %4;" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
+      : "memory");
+}
+
+template <int kT, int kChunks>
+struct StepTile {
+  uint4 c[kChunks][kT];  // candidate chunks 0 .. kChunks - 1
+  double4 pos[kT];
+  double4 fmemb[kT];
+  float4 bpos[kT];
+  uint32_t attr[kT];
+};
+
+// Resident blocks per SM the staged kernel's registers are held to.
+template <typename R, int kT>
+constexpr int staged_min_blocks() {
+  return sizeof(R) == 4 ? (kT == 128 ? 7 : 3) : (kT == 128 ? 5 : 2);
+}
+
+template <typename R, bool kSimple, bool kOld, bool k16, int kT>
+__global__ void __launch_bounds__(kT, staged_min_blocks<R, kT>())
+    k_step_staged(DevState S, Range r) {
+  pdl_entry();
+  count_launch(S.launches);
+  constexpr int kChunks = k16 ? 2 : 4;
+  constexpr int kPre = kChunks * (k16 ? 8 : 4) - 1;
+  constexpr int kG = sizeof(R) == 4 ? 4 : 2;
+  using Tile = StepTile<kT, kChunks>;
+  constexpr uint32_t kBytes = (uint32_t)sizeof(Tile);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Tile* buf = reinterpret_cast<Tile*>(smem_raw);
+  __shared__ uint64_t bar[2];
+  const int64_t t_lo = r.p0 / kT, t_hi = (r.p1 + kT - 1) / kT;
+  const int64_t first = t_lo + blockIdx.x;
+  if (first >= t_hi) return;
+  const int64_t N = S.n_total;
+  const int tid = threadIdx.x;
+  uint64_t pol = 0;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    pol = l2_evict_first();
+  }
+  __syncthreads();
+  auto issue = [&](int64_t t, int s) {
+    const int64_t i0 = t * kT;
+    Tile& d = buf[s];
+    mbar_expect_tx(&bar[s], kBytes);
+#pragma unroll
+    for (int k = 0; k < kChunks; ++k)
+      bulk_load(d.c[k], S.cand + k * N + i0, 16 * kT, &bar[s], pol);
+    bulk_load(d.pos, S.pos_cur + i0, 32 * kT, &bar[s], pol);
+    bulk_load(d.fmemb, S.fmemb + i0, 32 * kT, &bar[s], pol);
+    bulk_load(d.bpos, S.bpos + i0, 16 * kT, &bar[s], pol);
+    bulk_load(d.attr, S.attr + i0, 4 * kT, &bar[s], pol);
+  };
+  if (tid == 0) issue(first, 0);
+  using Part = Particle<R, kSimple, kOld>;
+  int it = 0;
+  for (int64_t t = first; t < t_hi; t += gridDim.x, ++it) {
+    const int s = it & 1;
+    const int64_t next = t + gridDim.x;
+    // the other half was released by the barrier that ended the last tile
+    if (tid == 0 && next < t_hi) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(next, s ^ 1);
+    }
+    const bool ok = mbar_wait(&bar[s], (uint32_t)(it >> 1) & 1u);
+    if (!__syncthreads_and(ok)) {
+      // the copies never completed: report, let the other half's copies
+      // (if any) land, and stop
+      if (tid == 0) {
+        raise_error(S.status, E_TIMEOUT, (int32_t)(t * kT), -1, 0.0);
+        if (next < t_hi) (void)mbar_wait(&bar[s ^ 1], (uint32_t)((it + 1) >> 1) & 1u);
+      }
+      return;
+    }
+    const int64_t i = t * kT + tid;
+    if (i >= r.p0 && i < r.p1) {
+      const Tile& d = buf[s];
+      uint4 c[kChunks];
+#pragma unroll
+      for (int k = 0; k < kChunks; ++k) c[k] = d.c[k][tid];
+      Part P(S, (int32_t)i, d.attr[tid], d.pos[tid]);
+      gather_candidates<k16, kPre, kG>(S, P, c, i);
+      P.finish(d.bpos[tid], d.fmemb[tid]);
+    }
+    __syncthreads();  // this half is free for the copies of tile t + 2 gridDim.x
+  }
 }
 
 // connect_cell's lists (for export): the exact predicate over the candidates.
@@ -1382,7 +1624,7 @@ void launch_scan(const int32_t* in, int32_t* out, int32_t n, int32_t init,
 void launch_rebuild(const DevState& S, const Range& r, const ScanScratch&,
                     const LaunchCfg& lc, cudaStream_t s, Timer* tm, bool listed) {
   const int B = lc.block;
-  const int grid = lc.num_sms * 8;
+  const int grid = lc.num_sms * lc.rebuild_per_sm;
   if (!listed) {
     timer_begin(tm, KC_GATE, s);
     launch_pdl(k_gate_compact, 1, kScanThreads, s, S, r.t0, r.t1);
@@ -1400,9 +1642,8 @@ void launch_rebuild(const DevState& S, const Range& r, const ScanScratch&,
   launch_pdl(k_scatter, grid, B, s, S);
   launch_pdl(k_binsort, grid, B, s, S);
   timer_end(tm, KC_REBUILD_SORT, s);
-  const bool whole = r.t0 == 0 && r.t1 == S.ntissues;
   timer_begin(tm, KC_REBUILD_SEARCH, s);
-  launch_pdl(k_cand_search, grid, B, s, S, (int32_t)(whole ? 1 : 0));
+  launch_pdl(k_cand_search, grid, B, s, S, (int32_t)lc.search_switch);
   timer_end(tm, KC_REBUILD_SEARCH, s);
 }
 
@@ -1432,16 +1673,50 @@ void launch_prepass(const DevState& S, int32_t m0, int32_t m1, int32_t f0, int32
   launch_dermis(S, f0, f1, lc, s, tm);
 }
 
+// The staged kernel: dynamic shared memory for two tiles, a persistent grid
+// of as many blocks as fit on the GPU at once (found once per instantiation).
+template <typename R, bool kSimple, bool kOld, bool k16, int kT>
+void launch_step_staged(const DevState& S, const Range& r, const LaunchCfg& lc, cudaStream_t s) {
+  auto kern = k_step_staged<R, kSimple, kOld, k16, kT>;
+  constexpr int smem = 2 * (int)sizeof(StepTile<kT, k16 ? 2 : 4>);
+  static int per_sm = 0;
+  if (per_sm == 0) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kT, smem) != cudaSuccess || b < 1)
+      b = 1;
+    per_sm = b;
+  }
+  const int64_t tiles = (r.p1 + kT - 1) / kT - r.p0 / kT;
+  const int64_t cap = (int64_t)lc.num_sms * per_sm;
+  const int grid = (int)(tiles < cap ? tiles : cap);
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)kT);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kern, S, r);
+}
+
+// Tuning variants: 1 and 2, the staged kernel with tiles of 128 and 256
+// particles; 3 (default) and 4, one thread per particle with
+// register-pipelined loads at two register budgets (FP32: 4 and 3 resident
+// 256-thread blocks per SM; FP64: 3 and 2, below which it spills); 5 and 6,
+// the kernels of 3 and 4 (the step graph schedules them differently).
 template <typename R, bool kSimple, bool kOld, bool k16>
 void launch_step_w(const DevState& S, const Range& r, const LaunchCfg& lc, cudaStream_t s) {
   const int grid = blocks_for(r.p1 - r.p0, 256);
-  // resident 256-thread blocks per SM of each tuning variant: the FP64
-  // kernel needs more registers (4 blocks spill; 2 and 3 do not)
   constexpr bool kF = sizeof(R) == 4;
   switch (lc.variant) {
-    case 2: launch_pdl(k_step<R, kSimple, kOld, kF ? 5 : 2, k16>, grid, 256, s, S, r); break;
-    case 3: launch_pdl(k_step<R, kSimple, kOld, kF ? 6 : 4, k16>, grid, 256, s, S, r); break;
-    case 4: launch_pdl(k_step<R, kSimple, kOld, kF ? 3 : 5, k16>, grid, 256, s, S, r); break;
+    case 1: launch_step_staged<R, kSimple, kOld, k16, 128>(S, r, lc, s); break;
+    case 2: launch_step_staged<R, kSimple, kOld, k16, 256>(S, r, lc, s); break;
+    case 4:
+    case 6: launch_pdl(k_step<R, kSimple, kOld, kF ? 3 : 2, k16>, grid, 256, s, S, r); break;
     default: launch_pdl(k_step<R, kSimple, kOld, kF ? 4 : 3, k16>, grid, 256, s, S, r); break;
   }
 }
@@ -1450,6 +1725,33 @@ template <typename R, bool kSimple, bool kOld>
 void launch_step_v(const DevState& S, const Range& r, const LaunchCfg& lc, cudaStream_t s) {
   if (S.cand16) launch_step_w<R, kSimple, kOld, true>(S, r, lc, s);
   else launch_step_w<R, kSimple, kOld, false>(S, r, lc, s);
+}
+
+template <typename R, bool kSimple, bool kOld>
+void launch_step_listed_v(const DevState& S, const LaunchCfg& lc, cudaStream_t s) {
+  constexpr bool kF = sizeof(R) == 4;
+  const int grid = lc.num_sms * (kF ? 4 : 3);
+  if (S.cand16)
+    launch_pdl(k_step_listed<R, kSimple, kOld, kF ? 4 : 3, true>, grid, 256, s, S);
+  else
+    launch_pdl(k_step_listed<R, kSimple, kOld, kF ? 4 : 3, false>, grid, 256, s, S);
+}
+
+template <typename R>
+void launch_step_listed_r(const DevState& S, const LaunchCfg& lc, cudaStream_t s) {
+  if (lc.simple && lc.any_old)
+    launch_step_listed_v<R, true, true>(S, lc, s);
+  else if (lc.simple)
+    launch_step_listed_v<R, true, false>(S, lc, s);
+  else
+    launch_step_listed_v<R, false, true>(S, lc, s);
+}
+
+void launch_step_listed(const DevState& S, int precision, const LaunchCfg& lc, cudaStream_t s) {
+  if (precision == 1)
+    launch_step_listed_r<float>(S, lc, s);
+  else
+    launch_step_listed_r<double>(S, lc, s);
 }
 
 template <typename R>

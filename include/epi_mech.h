@@ -120,11 +120,21 @@ typedef struct epi_config {
                          extra); the reference allows 400 (define.h:80) */
   int32_t max_cand;   /* candidates per particle (>= max_conn) */
   double skin;        /* candidate margin, > 0 (default 0.1) */
-  int32_t variant;    /* step-kernel register budget: 0 = default (1);
-                         1..4 = 4, 5, 6, 3 resident 256-thread blocks per SM.
-                         Same formulas; the compiler may fuse multiply-adds
-                         differently, so results agree to rounding. */
-  int32_t reserved;   /* must be 0 */
+  int32_t variant;    /* step-kernel form: 0 = default (3); 1, 2 = one
+                         persistent kernel whose per-particle inputs are
+                         staged in shared memory by bulk copies, tiles of 128
+                         / 256 particles; 3, 4 = one thread per particle with
+                         register-pipelined loads, 4 / 3 resident 256-thread
+                         blocks per SM (FP64: 3 / 2), whose step of the tissues
+                         that need no candidate rebuild runs beside the others'
+                         rebuild in the step graph (when the batch has no FIX
+                         or MUSUME cell); 5, 6 = the kernels of 3, 4 after the
+                         rebuild. Same formulas; the compiler may fuse
+                         multiply-adds differently, so results agree to
+                         rounding. */
+  int32_t search_switch; /* candidate search: rebuilds of at least this many
+                         particles take one thread per particle, smaller ones
+                         one warp per particle; 0 = default (49152) */
 } epi_config;
 
 typedef struct epi_ctx epi_ctx;
@@ -214,15 +224,28 @@ int epi_time_kernels(epi_ctx* ctx, int32_t nsteps, int32_t max_classes, double* 
 
 /* Autotuner. Times short graph-replayed trials of the uploaded batch for
  * every candidate skin in {0.05, 0.08, 0.1, 0.15, 0.2, 0.3} and step-kernel
- * variant 1..4 (4 warm-up steps, then trial_steps timed with CUDA events),
- * and keeps the fastest pair in the context's configuration. Skins whose
- * candidate rows would overflow max_cand are skipped. The simulation state
- * is left as it was (positions are restored after every trial), and neither
- * choice changes results beyond multiply-add rounding (connection sets are
- * exact for every skin). Writes the choice and the best trial's time per
- * step; any output may be NULL. No counterpart in the reference. */
+ * variant 1..6 (4 warm-up steps, then trial_steps timed with CUDA events),
+ * then, for the fastest pair, the candidate-search switch in {8192, 16384,
+ * 49152, 131072} rebuilt particles, and keeps the fastest choice in the
+ * context's configuration. Skins whose candidate rows would overflow
+ * max_cand are skipped. The simulation state is left as it was (positions
+ * are restored after every trial), and no choice changes results beyond
+ * multiply-add rounding (connection sets are exact for every skin, and both
+ * search forms emit candidates in the same order). Writes the skin, variant
+ * and the best trial's time per step (any output may be NULL);
+ * epi_get_config returns the whole choice. No counterpart in the
+ * reference. */
 int epi_autotune(epi_ctx* ctx, int32_t trial_steps, double* skin, int32_t* variant,
                  double* ms_per_step);
+
+/* The context's configuration (after epi_autotune: its choice). */
+int epi_get_config(epi_ctx* ctx, epi_config* out);
+
+/* Applies a tuning chosen earlier (for instance a cached epi_autotune
+ * result for the same batch shape): skin, variant and search switch, with
+ * epi_config's ranges. Every tissue's candidates are rebuilt before the
+ * next step. No counterpart in the reference. */
+int epi_set_tuning(epi_ctx* ctx, double skin, int32_t variant, int32_t search_switch);
 
 /* ---- cell maps and external-stimulus diffusion -----------------------------
  * The rest of the reference's per-step loop before its chemistry

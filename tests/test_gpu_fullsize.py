@@ -4,7 +4,8 @@ CPU side.
 * 1.1M-particle tissue (256x256 membrane + 1,048,576 cells), FP64: the
   initial connection lists bit-exact against the oracle; after a few steps
   positions within 1e-10 of the oracle's and the lists bit-exact against the
-  oracle's lists at the GPU's positions; the mixed path within 1e-5.
+  oracle's lists at the GPU's positions; the mixed path within 1e-5. Over
+  the workload's 200 steps, the same bars against the compiled reference.
 * 512-tissue ensemble (6.56M particles), mixed precision, graph-replayed:
   every sampled tissue of the batch bit-identical to the same tissue run
   alone. The batch's rebuilds take the thread-per-particle candidate search
@@ -53,6 +54,44 @@ def test_large_tissue_vs_oracle(built):
         mpos = ctx.positions()
     err = rel_pos_err(mpos, opos, t.lx, t.ly)
     assert err <= TOL_MIXED, err
+
+
+def test_large_tissue_200_steps_vs_reference(built):
+    """The 1.1M-particle tissue over its workload's 200 steps against the
+    compiled reference (its OpenMP build on the host's threads; the serial
+    oracle would take a quarter of an hour): FP64 positions within 1e-10 at
+    steps 100 and 200, lists bit-exact there against the reference's and
+    against the oracle's connect at the GPU's positions; the mixed path
+    within 1e-5 at step 200."""
+    t = T.config3()
+    if O.reference_binary(t, "omp") is None:
+        pytest.skip("compiled reference (omp) not built for the 256 x 256 geometry")
+    frames = {f["step"]: f for f in O.run_reference(t, 200, 100, variant="omp")}
+    assert sorted(frames) == [0, 100, 200]
+    with capi.Context(precision=FP64, max_conn=64, max_cand=128) as ctx:
+        ctx.upload([t])
+        done = 0
+        for s in (100, 200):
+            ctx.step(s - done, "graph")
+            done = s
+            f = frames[s]
+            pos = ctx.positions()
+            err = rel_pos_err(pos, (f["x"], f["y"], f["z"]), t.lx, t.ly)
+            assert err <= TOL_FP64, (s, err)
+            off, idx = ctx.connections()
+            assert lists_equal(off, idx, f["conn_off"], f["conn_idx"]), \
+                (s, list_diff_summary(off, idx, f["conn_off"], f["conn_idx"]))
+            ora = O.OracleTissue(t)
+            ora.set_positions(*pos)
+            assert ora.connect() == 0
+            ooff, oidx = ora.connections()
+            assert lists_equal(off, idx, ooff, oidx), s
+    with capi.Context(precision=MIXED, max_conn=64, max_cand=128) as ctx:
+        ctx.upload([t])
+        ctx.step(200, "graph")
+        f = frames[200]
+        err = rel_pos_err(ctx.positions(), (f["x"], f["y"], f["z"]), t.lx, t.ly)
+        assert err <= TOL_MIXED, err
 
 
 def test_full_ensemble_batch_equals_single_tissue_runs(built):
