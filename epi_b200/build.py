@@ -15,6 +15,9 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libepi_mech.so"
+# the bounds-checked build (-DEPI_CHECK): every index derived from stored data
+# is checked before use (EPI_ERR_CHECK); for tests, not for timing
+LIB_CHECK = PKG / "libepi_mech_check.so"
 
 SOURCES = ["epi_kernels.cu", "epi_adjoint.cu", "epi_field.cu", "epi_capi.cu", "epi_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -40,16 +43,34 @@ def _stale(out: Path) -> bool:
     return out.stat().st_mtime < max(p.stat().st_mtime for p in deps)
 
 
-def build_library(force: bool = False, verbose: bool = False) -> Path:
-    if not force and not _stale(LIB):
-        return LIB
-    cmd = compile_command(LIB, ("-Xptxas", "-v") if verbose else ())
+def _run(cmd):
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("nvcc failed:\n" + r.stderr[-6000:])
+    return r.stderr
+
+
+def build_library(force: bool = False, verbose: bool = False, check: bool = False) -> Path:
+    """Compiles the translation units in parallel (one nvcc each), then links
+    them into the shared library."""
+    from concurrent.futures import ThreadPoolExecutor
+    out = LIB_CHECK if check else LIB
+    if not force and not _stale(out):
+        return out
+    extra = (("-Xptxas", "-v") if verbose else ()) + (("-DEPI_CHECK",) if check else ())
+    objdir = PKG / "_build" / ("check" if check else "release")
+    objdir.mkdir(parents=True, exist_ok=True)
+    common = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+              "-I", str(ROOT / "include"), "-I", str(CSRC), *extra]
+    jobs = [(common + ["-c", str(CSRC / src), "-o", str(objdir / (src + ".o"))])
+            for src in SOURCES]
+    with ThreadPoolExecutor(max_workers=len(jobs)) as ex:
+        logs = list(ex.map(_run, jobs))
+    _run([nvcc(), *ARCH, "--shared", "-o", str(out),
+          *[str(objdir / (src + ".o")) for src in SOURCES]])
     if verbose:
-        print(r.stderr)
-    return LIB
+        print("".join(logs))
+    return out
 
 
 if __name__ == "__main__":

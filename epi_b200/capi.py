@@ -7,6 +7,7 @@ the C ABI a C or C++ caller uses. The library must be built in-tree
 from __future__ import annotations
 
 import ctypes
+import os
 from pathlib import Path
 from typing import List, Optional, Sequence
 
@@ -14,7 +15,10 @@ import numpy as np
 
 from .tissue import Params, Tissue
 
-LIB_PATH = Path(__file__).resolve().parent / "libepi_mech.so"
+# EPI_MECH_LIB selects another build of the same library, e.g. the
+# bounds-checked libepi_mech_check.so the tests run.
+LIB_PATH = Path(os.environ.get("EPI_MECH_LIB",
+                               Path(__file__).resolve().parent / "libepi_mech.so"))
 
 EPI_OK = 0
 EPI_ERR_INVALID_ARG = 1
@@ -30,6 +34,7 @@ EPI_ERR_NONFINITE = 10
 EPI_ERR_TIMEOUT = 11
 EPI_ERR_STATE = 12
 EPI_ERR_UNSUPPORTED = 13
+EPI_ERR_CHECK = 14
 
 EPI_PREC_FP64 = 0
 EPI_PREC_MIXED = 1

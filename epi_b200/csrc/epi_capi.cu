@@ -7,6 +7,8 @@
 #include "epi_mech.h"
 #include "epi_kernels.h"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -50,6 +52,15 @@ void timer_end(Timer* tm, int cls, cudaStream_t s) {
 }  // namespace epi
 
 namespace {
+
+// NVTX range over a scope: every entry point and the phases it queues show
+// up by name on a profiler's timeline (no cost without a tool attached).
+struct Nvtx {
+  explicit Nvtx(const char* name) { nvtxRangePushA(name); }
+  ~Nvtx() { nvtxRangePop(); }
+  Nvtx(const Nvtx&) = delete;
+  Nvtx& operator=(const Nvtx&) = delete;
+};
 
 // epi_step_host splits the batch into at most this many groups of tissues.
 constexpr int kHostStepGroups = 8;
@@ -329,11 +340,20 @@ void dermis_all(epi_ctx* c, int cur, Timer* tm) {
 // at the next synchronising call.
 void enqueue_step(epi_ctx* c, int& cur, Timer* tm) {
   ensure_posf(c);
-  (void)fork_memb(c, cur, tm);
-  launch_rebuild(make_state(c, cur), whole(c), c->scan, c->lc, c->stream, tm);
+  {
+    Nvtx r("membrane sums");
+    (void)fork_memb(c, cur, tm);
+  }
+  {
+    Nvtx r("candidate rebuild");
+    launch_rebuild(make_state(c, cur), whole(c), c->scan, c->lc, c->stream, tm);
+  }
   dermis_all(c, cur, tm);
   (void)join_memb(c);
-  launch_step(make_state(c, cur), whole(c), c->cfg.precision, c->lc, c->stream, tm);
+  {
+    Nvtx r("interaction + commit");
+    launch_step(make_state(c, cur), whole(c), c->cfg.precision, c->lc, c->stream, tm);
+  }
   cur ^= 1;
 }
 
@@ -706,6 +726,7 @@ const char* epi_strerror(int s) {
     case EPI_ERR_TIMEOUT: return "bounded device wait timed out";
     case EPI_ERR_STATE: return "call out of order";
     case EPI_ERR_UNSUPPORTED: return "unsupported geometry";
+    case EPI_ERR_CHECK: return "index check failed (bounds-checked build)";
     default: return "unknown status";
   }
 }
@@ -799,6 +820,7 @@ void epi_destroy(epi_ctx* ctx) {
 int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const epi_params* params) {
   if (!c || ntissues <= 0 || !tv) return EPI_ERR_INVALID_ARG;
   EPI_GUARD_BEGIN
+  Nvtx nvtx_range("epi_upload");
   int rc = set_device(c);
   if (rc) return rc;
   int64_t n = 0;
@@ -1051,6 +1073,7 @@ int epi_adjoint(epi_ctx* c, int32_t nsteps, int32_t K, const epi_loss* loss, dou
     return EPI_ERR_INVALID_ARG;
   if (!c->loaded) return EPI_ERR_STATE;
   EPI_GUARD_BEGIN
+  Nvtx nvtx_range("epi_adjoint");
   int rc = set_device(c);
   if (rc) return rc;
   const size_t n = (size_t)c->n;
@@ -1141,6 +1164,7 @@ int epi_field_init(epi_ctx* c, int32_t nx, int32_t ny, int32_t nz) {
   if (!c || nx < 3 || ny < 3 || nz < 3) return EPI_ERR_INVALID_ARG;
   if (!c->loaded) return EPI_ERR_STATE;
   EPI_GUARD_BEGIN
+  Nvtx nvtx_range("epi_field_init");
   int rc = set_device(c);
   if (rc) return rc;
   free_field(c);
@@ -1186,6 +1210,7 @@ int epi_field_step(epi_ctx* c, int32_t nsteps) {
   if (!c || nsteps < 0) return EPI_ERR_INVALID_ARG;
   if (!c->loaded || !c->field_on) return EPI_ERR_STATE;
   EPI_GUARD_BEGIN
+  Nvtx nvtx_range("epi_field_step");
   int rc = set_device(c);
   if (rc) return rc;
   for (int32_t k = 0; k < nsteps; ++k) {
@@ -1256,6 +1281,7 @@ int epi_connect(epi_ctx* c) {
   if (!c) return EPI_ERR_INVALID_ARG;
   if (!c->loaded) return EPI_ERR_STATE;
   EPI_GUARD_BEGIN
+  Nvtx nvtx_range("epi_connect");
   int rc = set_device(c);
   if (rc) return rc;
   return materialize(c);
@@ -1266,6 +1292,7 @@ int epi_interact_commit(epi_ctx* c) {
   if (!c) return EPI_ERR_INVALID_ARG;
   if (!c->loaded) return EPI_ERR_STATE;
   EPI_GUARD_BEGIN
+  Nvtx nvtx_range("epi_interact_commit");
   int rc = set_device(c);
   if (rc) return rc;
   enqueue_step(c, c->cur, nullptr);
@@ -1278,6 +1305,7 @@ int epi_step(epi_ctx* c, int32_t nsteps) {
   if (!c || nsteps < 0) return EPI_ERR_INVALID_ARG;
   if (!c->loaded) return EPI_ERR_STATE;
   EPI_GUARD_BEGIN
+  Nvtx nvtx_range("epi_step");
   int rc = set_device(c);
   if (rc) return rc;
   for (int32_t k = 0; k < nsteps; ++k) enqueue_step(c, c->cur, nullptr);
@@ -1290,6 +1318,7 @@ int epi_step_graph(epi_ctx* c, int32_t nsteps) {
   if (!c || nsteps < 0) return EPI_ERR_INVALID_ARG;
   if (!c->loaded) return EPI_ERR_STATE;
   EPI_GUARD_BEGIN
+  Nvtx nvtx_range("epi_step_graph");
   int rc = set_device(c);
   if (rc) return rc;
   if ((rc = enqueue_graph_steps(c, nsteps))) return rc;
@@ -1302,6 +1331,7 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
   if (!c || trial_steps < 2) return EPI_ERR_INVALID_ARG;
   if (!c->loaded) return EPI_ERR_STATE;
   EPI_GUARD_BEGIN
+  Nvtx nvtx_range("epi_autotune");
   int rc = set_device(c);
   if (rc) return rc;
   static const double kSkins[] = {0.05, 0.08, 0.1, 0.15, 0.2, 0.3};
@@ -1401,6 +1431,7 @@ int epi_set_tuning(epi_ctx* c, double skin, int32_t variant, int32_t search_swit
   if (!c || !(skin > 0) || skin > 2.0 || variant < 0 || variant > 6 || search_switch < 0)
     return EPI_ERR_INVALID_ARG;
   EPI_GUARD_BEGIN
+  Nvtx nvtx_range("epi_set_tuning");
   int rc = set_device(c);
   if (rc) return rc;
   apply_tuning(c, skin, variant, search_switch);
@@ -1418,6 +1449,7 @@ int epi_step_per_tissue(epi_ctx* c, int32_t nsteps) {
   if (!c || nsteps < 0) return EPI_ERR_INVALID_ARG;
   if (!c->loaded) return EPI_ERR_STATE;
   EPI_GUARD_BEGIN
+  Nvtx nvtx_range("epi_step_per_tissue");
   int rc = set_device(c);
   if (rc) return rc;
   ensure_posf(c);
@@ -1457,6 +1489,7 @@ int epi_download_positions(epi_ctx* c, double* x, double* y, double* z) {
   if (!c || !x || !y || !z) return EPI_ERR_INVALID_ARG;
   if (!c->loaded) return EPI_ERR_STATE;
   EPI_GUARD_BEGIN
+  Nvtx nvtx_range("epi_download_positions");
   int rc = set_device(c);
   if (rc) return rc;
   const int64_t n = c->n;
@@ -1473,6 +1506,7 @@ int epi_upload_positions(epi_ctx* c, const double* x, const double* y, const dou
   if (!c || !x || !y || !z) return EPI_ERR_INVALID_ARG;
   if (!c->loaded) return EPI_ERR_STATE;
   EPI_GUARD_BEGIN
+  Nvtx nvtx_range("epi_upload_positions");
   int rc = set_device(c);
   if (rc) return rc;
   const int64_t n = c->n;
@@ -1552,9 +1586,12 @@ static int enqueue_host_step(epi_ctx* c, bool chained, const double* x_in, const
     // the previous call's outbound copy of this group may still write the
     // host arrays this copy reads
     EPI_CUDA(cudaStreamWaitEvent(c->copy_in, c->ev_d2h[g], 0));
-    for (int k = 0; k < 3; ++k)
-      EPI_CUDA(cudaMemcpyAsync(in + k * n + off, src[k] + off, bytes, cudaMemcpyHostToDevice,
-                               c->copy_in));
+    {
+      Nvtx r("host step: positions in");
+      for (int k = 0; k < 3; ++k)
+        EPI_CUDA(cudaMemcpyAsync(in + k * n + off, src[k] + off, bytes, cudaMemcpyHostToDevice,
+                                 c->copy_in));
+    }
     EPI_CUDA(cudaEventRecord(c->ev_in[g], c->copy_in));
     EPI_CUDA(cudaStreamWaitEvent(c->stream, c->ev_in[g], 0));
     launch_pack_gate(S, in, in + n, in + 2 * n, p0, p1, c->lc, c->stream);
@@ -1572,9 +1609,12 @@ static int enqueue_host_step(epi_ctx* c, bool chained, const double* x_in, const
     EPI_CUDA(cudaEventRecord(c->ev_done[g], c->stream));
     EPI_CUDA(cudaStreamWaitEvent(c->copy_out, c->ev_done[g], 0));
     double* dst[3] = {x_out, y_out, z_out};
-    for (int k = 0; k < 3; ++k)
-      EPI_CUDA(cudaMemcpyAsync(dst[k] + off, out + k * n + off, bytes, cudaMemcpyDeviceToHost,
-                               c->copy_out));
+    {
+      Nvtx r("host step: positions out");
+      for (int k = 0; k < 3; ++k)
+        EPI_CUDA(cudaMemcpyAsync(dst[k] + off, out + k * n + off, bytes, cudaMemcpyDeviceToHost,
+                                 c->copy_out));
+    }
     EPI_CUDA(cudaEventRecord(c->ev_d2h[g], c->copy_out));
   }
   c->cur ^= 1;
@@ -1589,6 +1629,7 @@ int epi_step_host(epi_ctx* c, const double* x_in, const double* y_in, const doub
   if (!c || !x_in || !y_in || !z_in || !x_out || !y_out || !z_out) return EPI_ERR_INVALID_ARG;
   if (!c->loaded) return EPI_ERR_STATE;
   EPI_GUARD_BEGIN
+  Nvtx nvtx_range("epi_step_host");
   const bool chained = c->after_host_step;
   int rc = set_device(c);
   if (rc) return rc;
@@ -1603,6 +1644,7 @@ int epi_step_host_async(epi_ctx* c, const double* x_in, const double* y_in, cons
   if (!c || !x_in || !y_in || !z_in || !x_out || !y_out || !z_out) return EPI_ERR_INVALID_ARG;
   if (!c->loaded) return EPI_ERR_STATE;
   EPI_GUARD_BEGIN
+  Nvtx nvtx_range("epi_step_host_async");
   const bool chained = c->after_host_step;
   int rc = set_device(c);
   if (rc) return rc;
@@ -1615,6 +1657,7 @@ int epi_get_connections(epi_ctx* c, int32_t* offsets, int32_t* idx, int64_t cap,
   if (!c || !offsets || cap < 0 || (cap > 0 && !idx)) return EPI_ERR_INVALID_ARG;
   if (!c->loaded) return EPI_ERR_STATE;
   EPI_GUARD_BEGIN
+  Nvtx nvtx_range("epi_get_connections");
   int rc = set_device(c);
   if (rc) return rc;
   if ((rc = materialize(c))) return rc;
@@ -1665,6 +1708,7 @@ int epi_get_dermis(epi_ctx* c, int32_t* dermis) {
   if (!c || !dermis) return EPI_ERR_INVALID_ARG;
   if (!c->loaded) return EPI_ERR_STATE;
   EPI_GUARD_BEGIN
+  Nvtx nvtx_range("epi_get_dermis");
   int rc = set_device(c);
   if (rc) return rc;
   if ((rc = materialize(c))) return rc;
@@ -1742,6 +1786,7 @@ int epi_time_kernels(epi_ctx* c, int32_t nsteps, int32_t max_classes, double* ms
   if (!c || nsteps < 0 || !ms || !launches || max_classes < KC_COUNT) return EPI_ERR_INVALID_ARG;
   if (!c->loaded) return EPI_ERR_STATE;
   EPI_GUARD_BEGIN
+  Nvtx nvtx_range("epi_time_kernels");
   int rc = set_device(c);
   if (rc) return rc;
   Timer tm;

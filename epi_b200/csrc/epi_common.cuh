@@ -35,8 +35,22 @@ enum State : uint32_t {
 
 enum ErrCode : int32_t {
   E_OK = 0, E_BIN_RANGE = 5, E_BIN_OVERFLOW = 6, E_LIST_OVERFLOW = 7, E_COEF_RANGE = 8,
-  E_MEMB_COEF_RANGE = 9, E_NONFINITE = 10, E_TIMEOUT = 11, E_UNSUPPORTED = 13
+  E_MEMB_COEF_RANGE = 9, E_NONFINITE = 10, E_TIMEOUT = 11, E_UNSUPPORTED = 13, E_CHECK = 14
 };
+
+// The bounds-checked build (-DEPI_CHECK, libepi_mech_check.so): every index a
+// kernel derives from stored data (candidate entries, bin slots, lattice
+// sites, pair and dermis partners) is checked against the range it must lie
+// in before it is used; a failed check records E_CHECK with the particle and
+// the index, and the access is skipped. The release build compiles the
+// checks away. It stands in for a memory checker, which this build does not
+// rely on.
+#ifdef EPI_CHECK
+#define EPI_CHECKED(ok, status, a, b) \
+  ((ok) ? true : (raise_error((status), E_CHECK, (a), (b), 0.0), false))
+#else
+#define EPI_CHECKED(ok, status, a, b) true
+#endif
 
 constexpr double kAreaGrid = 2.0 + 1e-7;  // AREA_GRID, cell_connection.cpp:16-19
 constexpr int kBinCap = 200;              // N3, cell_connection.cpp:28
@@ -101,30 +115,6 @@ struct DevState {
   double skin;
 };
 
-// Candidate rows: entry e of particle i (entry 0: the count; entry k + 1:
-// candidate k, tissue-local). 16-bit entries: chunk e / 8, half e % 8;
-// 32-bit: chunk e / 4, word e % 4.
-__device__ __forceinline__ uint32_t cand_entry(const DevState& S, int64_t i, int32_t e) {
-  if (S.cand16) {
-    const uint16_t* c = reinterpret_cast<const uint16_t*>(S.cand + (int64_t)(e >> 3) * S.n_total + i);
-    return c[e & 7];
-  }
-  const uint32_t* c = reinterpret_cast<const uint32_t*>(S.cand + (int64_t)(e >> 2) * S.n_total + i);
-  return c[e & 3];
-}
-__device__ __forceinline__ void cand_set(const DevState& S, int64_t i, int32_t e, uint32_t v) {
-  if (S.cand16) {
-    uint16_t* c = reinterpret_cast<uint16_t*>(S.cand + (int64_t)(e >> 3) * S.n_total + i);
-    c[e & 7] = (uint16_t)v;
-  } else {
-    uint32_t* c = reinterpret_cast<uint32_t*>(S.cand + (int64_t)(e >> 2) * S.n_total + i);
-    c[e & 3] = v;
-  }
-}
-__device__ __forceinline__ int32_t cand_count(const DevState& S, int64_t i) {
-  return (int32_t)cand_entry(S, i, 0);
-}
-
 __device__ __forceinline__ uint32_t attr_state(uint32_t a) { return a & 15u; }
 __device__ __forceinline__ bool attr_old(uint32_t a) { return (a >> 4) & 1u; }
 __device__ __forceinline__ uint32_t attr_sfm(uint32_t a) { return (a >> 5) & 3u; }
@@ -138,6 +128,33 @@ __device__ __forceinline__ void raise_error(DevStatus* s, int32_t code, int32_t 
     s->b = b;
     s->v = v;
   }
+}
+
+// Candidate rows: entry e of particle i (entry 0: the count; entry k + 1:
+// candidate k, tissue-local). 16-bit entries: chunk e / 8, half e % 8;
+// 32-bit: chunk e / 4, word e % 4.
+__device__ __forceinline__ uint32_t cand_entry(const DevState& S, int64_t i, int32_t e) {
+  if (S.cand16) {
+    const uint16_t* c = reinterpret_cast<const uint16_t*>(S.cand + (int64_t)(e >> 3) * S.n_total + i);
+    return c[e & 7];
+  }
+  const uint32_t* c = reinterpret_cast<const uint32_t*>(S.cand + (int64_t)(e >> 2) * S.n_total + i);
+  return c[e & 3];
+}
+__device__ __forceinline__ void cand_set(const DevState& S, int64_t i, int32_t e, uint32_t v) {
+  if (!EPI_CHECKED(e >= 0 && e <= S.max_cand && (e == 0 || v < 65536u || !S.cand16), S.status,
+                   (int32_t)i, e))
+    return;
+  if (S.cand16) {
+    uint16_t* c = reinterpret_cast<uint16_t*>(S.cand + (int64_t)(e >> 3) * S.n_total + i);
+    c[e & 7] = (uint16_t)v;
+  } else {
+    uint32_t* c = reinterpret_cast<uint32_t*>(S.cand + (int64_t)(e >> 2) * S.n_total + i);
+    c[e & 3] = v;
+  }
+}
+__device__ __forceinline__ int32_t cand_count(const DevState& S, int64_t i) {
+  return (int32_t)cand_entry(S, i, 0);
 }
 
 // Minimum-image difference, p_diff_x / p_diff_y (epi5_MT/utils.h:25-41).

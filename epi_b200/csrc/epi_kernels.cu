@@ -31,6 +31,12 @@
 
 namespace epi {
 
+#ifdef EPI_CHECK
+constexpr bool kCheck = true;
+#else
+constexpr bool kCheck = false;
+#endif
+
 const char* const kKernelClassNames[KC_COUNT] = {
     "step", "prepass", "rebuild_bin", "rebuild_scan", "rebuild_sort", "rebuild_search", "gate"};
 
@@ -337,7 +343,10 @@ __global__ void k_scatter(DevState S) {
     const int32_t i = gated_particle(S, cnt, g, &t);
     const int32_t b = S.bin[i];
     if (b < 0) continue;
-    S.skey[S.starts[b] + S.rank[i]] = (uint32_t)i;
+    const int32_t slot = S.starts[b] + S.rank[i];
+    const TissueDev& T = S.tissues[t];
+    if (!EPI_CHECKED(slot >= T.pbase && slot < T.pbase + T.n, S.status, i, slot)) continue;
+    S.skey[slot] = (uint32_t)i;
   }
 }
 
@@ -383,6 +392,9 @@ __global__ void k_binsort(DevState S) {
     }
     for (int32_t s = s0; s < s1; ++s) {
       const uint32_t gi = S.skey[s];
+      if (!EPI_CHECKED(gi >= (uint32_t)T.pbase && gi < (uint32_t)(T.pbase + T.n), S.status,
+                       (int32_t)gi, s))
+        continue;
       const bool memb = attr_state(S.attr[gi]) == ST_MEMB;
       S.skey[s] = gi | (memb ? 0x80000000u : 0u);
       // x and y as grid_init bins them (ref_bin): in [0, L)
@@ -865,7 +877,8 @@ __device__ __forceinline__ double3 memb_force(const DevState& S, int32_t i) {
       c -= c >= NMX ? NMX : 0;
       w += w < 0 ? NMY : 0;
       w -= w >= NMY ? NMY : 0;
-      return pb + w * NMX + c;
+      const int32_t q = pb + w * NMX + c;
+      return EPI_CHECKED(q >= pb && q < pb + T.nmemb, S.status, i, q) ? q : i;
     };
     const double4 p = S.pos_cur[i];
     const SiteOffsets<R> off(S, i, p, T);
@@ -1052,6 +1065,12 @@ struct Particle {
     if (!kSimple && st != ST_MEMB) {
       pair_i = __ldg(&S.pair[i]);
       if (st == ST_FIX || st == ST_MUSUME) dermis_i = __ldg(&S.dermis[i]);
+      if (!EPI_CHECKED(pair_i < T.pbase + T.n && (pair_i >= T.pbase || pair_i == -1), S.status,
+                       i, pair_i))
+        pair_i = -1;
+      if (!EPI_CHECKED(dermis_i < T.pbase + T.n && (dermis_i >= T.pbase || dermis_i == -1),
+                       S.status, i, dermis_i))
+        dermis_i = -1;
     }
   }
 
@@ -1252,15 +1271,18 @@ __device__ __forceinline__ void gather_candidates(const DevState& S, Part& P, co
       q[u] = 0;
       if (b + u <= kPre) {
         q[u] = (int32_t)row_entry<k16>(c, b + u);
-        if (b + u <= nc) pq[u] = src[q[u]];
+        if (b + u <= nc && EPI_CHECKED(q[u] < P.T.n, S.status, (int32_t)i, q[u]))
+          pq[u] = src[q[u]];
       }
     }
 #pragma unroll
     for (int u = 0; u < kG; ++u)
-      if (b + u <= kPre && b + u <= nc) P.candidate(pbase + q[u], pq[u]);
+      if (b + u <= kPre && b + u <= nc && (q[u] < P.T.n || !kCheck))
+        P.candidate(pbase + q[u], pq[u]);
   }
   for (int32_t e = kPre + 1; e <= nc; ++e) {
     const int32_t q = (int32_t)cand_entry(S, i, e);
+    if (!EPI_CHECKED(q < P.T.n, S.status, (int32_t)i, q)) continue;
     P.candidate(pbase + q, src[q]);
   }
 }

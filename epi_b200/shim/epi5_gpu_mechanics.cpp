@@ -50,11 +50,20 @@ class GpuMechanics {
     gather(cman);
     check(epi_upload(ctx(), 1, &view_, &params_), "connect_cell");
     const int32_t n = view_.n;
-    off_.assign(n + 1, 0);
+    off_.resize(n + 1);
+    // one export per step: the index buffer keeps the last step's size plus
+    // a margin, and only a list that outgrew it asks a second time
+    if (idx_.size() < 8 * (size_t)n) idx_.resize(8 * (size_t)n);
     int64_t total = 0;
-    check(epi_get_connections(ctx_, off_.data(), nullptr, 0, &total), "connect_cell");
-    idx_.assign(total > 0 ? total : 1, 0);
-    check(epi_get_connections(ctx_, off_.data(), idx_.data(), total, &total), "connect_cell");
+    const int rc = epi_get_connections(ctx_, off_.data(), idx_.data(), (int64_t)idx_.size(),
+                                       &total);
+    if (rc == EPI_ERR_INVALID_ARG && total > (int64_t)idx_.size()) {
+      idx_.resize((size_t)(total + total / 4));
+      check(epi_get_connections(ctx_, off_.data(), idx_.data(), (int64_t)idx_.size(), &total),
+            "connect_cell");
+    } else {
+      check(rc, "connect_cell");
+    }
     dermis_.assign(n, -1);
     check(epi_get_dermis(ctx_, dermis_.data()), "connect_cell");
 #pragma omp parallel for schedule(static)

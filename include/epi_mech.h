@@ -49,7 +49,9 @@ typedef enum epi_status {
   EPI_ERR_NONFINITE = 10,       /* a position became NaN or infinite */
   EPI_ERR_TIMEOUT = 11,         /* a bounded device-side wait gave up */
   EPI_ERR_STATE = 12,           /* call out of order (e.g. step before upload) */
-  EPI_ERR_UNSUPPORTED = 13      /* geometry outside what the library implements */
+  EPI_ERR_UNSUPPORTED = 13,     /* geometry outside what the library implements */
+  EPI_ERR_CHECK = 14            /* an index check of the bounds-checked build failed
+                                   (libepi_mech_check.so, built with -DEPI_CHECK) */
 } epi_status;
 
 /* Force-law constants of one tissue. Defaults (epi_params_default) are the

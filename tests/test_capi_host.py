@@ -29,7 +29,7 @@ def test_library_exports_every_declared_function(built):
 
 
 def test_strerror_covers_every_status(built):
-    for code in range(0, 14):
+    for code in range(0, 15):
         s = capi.strerror(code)
         assert s and "unknown" not in s
     assert "unknown" in capi.strerror(99)
