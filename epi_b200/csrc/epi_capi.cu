@@ -84,7 +84,6 @@ struct epi_ctx {
   // the membrane sums run on `aux` beside the candidate rebuild (fork / join)
   cudaStream_t aux = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  cudaEvent_t ev_cond = nullptr;  // split step: the rebuild work list is built
   LaunchCfg lc{148, 256, 0, 0, 0, kDefaultSearchSwitch};
   bool loaded = false;
   bool lists_fresh = false;  // nbr / nn / dermis match the current positions
@@ -122,8 +121,7 @@ struct epi_ctx {
   uint32_t* skey = nullptr;
   float4* spos = nullptr;
   int32_t* gate = nullptr;
-  // rebuild work list: [count | list (T) | ppre (T+1) | bpre (T+1) | marks (T)]
-  int32_t* rl = nullptr;
+  int32_t* rl = nullptr;    // rebuild work list: [count | list (T) | ppre (T+1) | bpre (T+1)]
   int32_t* prep = nullptr;
   double* stage = nullptr;        // 3n doubles: x | y | z for host transfers
   // epi_step_host: copy streams, per-chunk events, the outbound staging (3n)
@@ -268,7 +266,6 @@ DevState make_state(epi_ctx* c, int cur) {
   S.rl_list = c->rl ? c->rl + 1 : nullptr;
   S.rl_ppre = c->rl ? c->rl + 1 + c->ntissues : nullptr;
   S.rl_bpre = c->rl ? c->rl + 2 + 2 * c->ntissues : nullptr;
-  S.rl_mark = c->rl ? c->rl + 3 + 3 * c->ntissues : nullptr;
   S.ntissues = c->ntissues;
   S.prep = c->prep;
   S.nprep = c->nprep;
@@ -357,19 +354,6 @@ void enqueue_step(epi_ctx* c, int& cur, Timer* tm) {
   cur ^= 1;
 }
 
-// The step graph's split schedule: whether the step of the tissues that need
-// no candidate rebuild may run beside the rebuild of the others. It may when
-// the batch has no FIX / MUSUME cell (their dermis is found after the
-// rebuild, and the step reads it) and the step kernel is not the persistent
-// one (whose blocks would hold every SM while the rebuild waits for room).
-bool split_step(const epi_ctx* c) {
-  return c->nprep == c->nprep_memb && (c->lc.variant == 3 || c->lc.variant == 4);
-}
-// Blocks per SM of the rebuild's grid-stride kernels: in the split schedule
-// they share the GPU with the step, so they take a quarter of their usual
-// grid and leave most SMs to it.
-constexpr int kRebuildPerSmSplit = 2;
-
 // Skin, step-kernel variant and candidate-search switch of the context; the
 // captured graphs hold all three, so they are dropped.
 void apply_tuning(epi_ctx* c, double skin, int32_t variant, int32_t search_switch) {
@@ -385,10 +369,8 @@ void apply_tuning(epi_ctx* c, double skin, int32_t variant, int32_t search_switc
 // whose body, captured on c->side, is the candidate rebuild; a one-block
 // kernel before it builds the rebuild work list and sets the condition to
 // "the list is not empty", so steps that need no rebuild launch none of the
-// rebuild's kernels. side_step: right after the work list, the step of the
-// particles of the tissues not on it is forked onto c->aux (after the
-// membrane sums already queued there), to run beside the rebuild.
-cudaError_t capture_conditional_rebuild(epi_ctx* c, int cur, bool side_step = false) {
+// rebuild's kernels.
+cudaError_t capture_conditional_rebuild(epi_ctx* c, int cur) {
   cudaStreamCaptureStatus st;
   cudaGraph_t g;
   const cudaGraphNode_t* deps = nullptr;
@@ -398,14 +380,6 @@ cudaError_t capture_conditional_rebuild(epi_ctx* c, int cur, bool side_step = fa
   cudaGraphConditionalHandle h;
   if ((e = cudaGraphConditionalHandleCreate(&h, g, 0, 0)) != cudaSuccess) return e;
   launch_rebuild_condition(make_state(c, cur), whole(c), h, c->stream);
-  if (side_step) {
-    if ((e = cudaEventRecord(c->ev_cond, c->stream)) != cudaSuccess) return e;
-    if ((e = cudaStreamWaitEvent(c->aux, c->ev_cond, 0)) != cudaSuccess) return e;
-    Range r = whole(c);
-    r.skip_listed = 1;
-    launch_step(make_state(c, cur), r, c->cfg.precision, c->lc, c->aux, nullptr);
-    if ((e = cudaEventRecord(c->ev_join, c->aux)) != cudaSuccess) return e;
-  }
   if ((e = cudaStreamGetCaptureInfo(c->stream, &st, nullptr, &g, &deps, &nd)) != cudaSuccess)
     return e;
   cudaGraphNodeParams p{};
@@ -419,9 +393,7 @@ cudaError_t capture_conditional_rebuild(epi_ctx* c, int cur, bool side_step = fa
   if ((e = cudaStreamBeginCaptureToGraph(c->side, body, nullptr, nullptr, 0,
                                          cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
     return e;
-  LaunchCfg lc = c->lc;
-  if (side_step) lc.rebuild_per_sm = kRebuildPerSmSplit;
-  launch_rebuild(make_state(c, cur), whole(c), c->scan, lc, c->side, nullptr, true);
+  launch_rebuild(make_state(c, cur), whole(c), c->scan, c->lc, c->side, nullptr, true);
   if ((e = cudaStreamEndCapture(c->side, &body)) != cudaSuccess) return e;
   return cudaStreamUpdateCaptureDependencies(c->stream, &node, 1,
                                              cudaStreamSetCaptureDependencies);
@@ -454,20 +426,13 @@ cudaError_t capture_step_graph(epi_ctx* c, cudaGraphExec_t* out) {
                                       cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
       int cur = c->cur;
-      const bool split = split_step(c);
       for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
         e = fork_memb(c, cur, nullptr);
-        if (e == cudaSuccess) e = capture_conditional_rebuild(c, cur, split);
+        if (e == cudaSuccess) e = capture_conditional_rebuild(c, cur);
         if (e != cudaSuccess) break;
-        if (split) {
-          // the side stream's membrane sums and step, then the rebuilt tissues
-          if ((e = cudaStreamWaitEvent(c->stream, c->ev_join, 0)) != cudaSuccess) break;
-          launch_step_listed(make_state(c, cur), c->cfg.precision, c->lc, c->stream);
-        } else {
-          dermis_all(c, cur, nullptr);
-          if ((e = join_memb(c)) != cudaSuccess) break;
-          launch_step(make_state(c, cur), whole(c), c->cfg.precision, c->lc, c->stream, nullptr);
-        }
+        dermis_all(c, cur, nullptr);
+        if ((e = join_memb(c)) != cudaSuccess) break;
+        launch_step(make_state(c, cur), whole(c), c->cfg.precision, c->lc, c->stream, nullptr);
         cur ^= 1;
       }
       if (e == cudaSuccess) launch_loop_tick(c->loop_left, hw, c->launches, c->stream);
@@ -741,7 +706,7 @@ int epi_create(epi_ctx** out, const epi_config* cfg) {
   if (c.max_conn <= 0 || c.max_conn > 400 || c.max_cand < c.max_conn || c.max_cand > 1024)
     return EPI_ERR_INVALID_ARG;
   if (!(c.skin > 0) || c.skin > 2.0) return EPI_ERR_INVALID_ARG;
-  if (c.variant < 0 || c.variant > 6) return EPI_ERR_INVALID_ARG;
+  if (c.variant < 0 || c.variant > 4) return EPI_ERR_INVALID_ARG;
   if (c.precision != EPI_PREC_FP64 && c.precision != EPI_PREC_MIXED) return EPI_ERR_INVALID_ARG;
   if (c.search_switch < 0) return EPI_ERR_INVALID_ARG;
   int ndev = 0;
@@ -771,8 +736,6 @@ int epi_create(epi_ctx** out, const epi_config* cfg) {
     rc = cuda_status(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
   if (rc == EPI_OK)
     rc = cuda_status(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
-  if (rc == EPI_OK)
-    rc = cuda_status(cudaEventCreateWithFlags(&ctx->ev_cond, cudaEventDisableTiming));
   if (rc == EPI_OK) rc = dev_alloc(&ctx->status, 1);
   if (rc == EPI_OK) rc = cuda_status(cudaMallocHost((void**)&ctx->status_h, sizeof(DevStatus)));
   if (rc == EPI_OK) rc = cuda_status(cudaMemset(ctx->status, 0, sizeof(DevStatus)));
@@ -810,7 +773,6 @@ void epi_destroy(epi_ctx* ctx) {
   if (ctx->aux) cudaStreamSynchronize(ctx->aux);
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
-  if (ctx->ev_cond) cudaEventDestroy(ctx->ev_cond);
   if (ctx->aux) cudaStreamDestroy(ctx->aux);
   if (ctx->side) cudaStreamDestroy(ctx->side);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -976,21 +938,19 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
       return rc;
     }
   }
-  // buffers the step kernel streams by whole tiles are padded (kStepTilePad)
-  const int64_t np = padded_particles(n);
-  if (!reuse && ((rc = dev_alloc(&c->tissues, ntissues)) || (rc = dev_alloc(&c->pos[0], np)) ||
-      (rc = dev_alloc(&c->pos[1], np)) || (rc = dev_alloc(&c->posf[0], n)) ||
-      (rc = dev_alloc(&c->posf[1], n)) || (rc = dev_alloc(&c->attr, np)) ||
+  if (!reuse && ((rc = dev_alloc(&c->tissues, ntissues)) || (rc = dev_alloc(&c->pos[0], n)) ||
+      (rc = dev_alloc(&c->pos[1], n)) || (rc = dev_alloc(&c->posf[0], n)) ||
+      (rc = dev_alloc(&c->posf[1], n)) || (rc = dev_alloc(&c->attr, n)) ||
       (rc = dev_alloc(&c->pair, n)) || (rc = dev_alloc(&c->spr, n)) ||
-      (rc = dev_alloc(&c->dermis, n)) || (rc = dev_alloc(&c->cand, CC * n + kStepTilePad)) ||
-      (rc = dev_alloc(&c->bpos, np)) ||
+      (rc = dev_alloc(&c->dermis, n)) || (rc = dev_alloc(&c->cand, CC * n)) ||
+      (rc = dev_alloc(&c->bpos, n)) ||
       (rc = dev_alloc(&c->nbr, C * n)) || (rc = dev_alloc(&c->nn, n)) ||
-      (rc = dev_alloc(&c->fmemb, np)) ||
+      (rc = dev_alloc(&c->fmemb, n)) ||
       (rc = dev_alloc(&c->bin, n)) || (rc = dev_alloc(&c->rank, n)) ||
       (rc = dev_alloc(&c->counts, nbins)) || (rc = dev_alloc(&c->starts, nbins + 1)) ||
       (rc = dev_alloc(&c->skey, n)) || (rc = dev_alloc(&c->spos, n)) ||
       (rc = dev_alloc(&c->gate, (size_t)ntissues + 1)) ||
-      (rc = dev_alloc(&c->rl, 3 + 4 * (size_t)ntissues)) ||
+      (rc = dev_alloc(&c->rl, 3 + 3 * (size_t)ntissues)) ||
       (rc = dev_alloc(&c->prep, prep.size())) || (rc = dev_alloc(&c->stage, 3 * (size_t)n)) ||
       (rc = dev_alloc(&c->agek, n)))) {
     free_buffers(c);
@@ -1335,7 +1295,7 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
   int rc = set_device(c);
   if (rc) return rc;
   static const double kSkins[] = {0.05, 0.08, 0.1, 0.15, 0.2, 0.3};
-  static const int32_t kVariants[] = {1, 2, 3, 4, 5, 6};
+  static const int32_t kVariants[] = {1, 2, 3, 4};
   constexpr int32_t kWarm = 4;  // the first step after a restore rebuilds every tissue
   const size_t pbytes = sizeof(double4) * (size_t)c->n;
   cudaStream_t s = c->stream;
@@ -1428,7 +1388,7 @@ int epi_get_config(epi_ctx* c, epi_config* out) {
 }
 
 int epi_set_tuning(epi_ctx* c, double skin, int32_t variant, int32_t search_switch) {
-  if (!c || !(skin > 0) || skin > 2.0 || variant < 0 || variant > 6 || search_switch < 0)
+  if (!c || !(skin > 0) || skin > 2.0 || variant < 0 || variant > 4 || search_switch < 0)
     return EPI_ERR_INVALID_ARG;
   EPI_GUARD_BEGIN
   Nvtx nvtx_range("epi_set_tuning");

@@ -103,7 +103,6 @@ struct DevState {
   int32_t* rl_list;   // their ids
   int32_t* rl_ppre;   // prefix sums of their particle counts (count + 1 entries)
   int32_t* rl_bpre;   // prefix sums of their bin counts
-  int32_t* rl_mark;   // per tissue: 1 while it is on the current work list
   int32_t ntissues;
   const int32_t* prep;  // membrane particles, then FIX/MUSUME cells
   int32_t nprep, nprep_memb;

@@ -178,14 +178,11 @@ __device__ __forceinline__ int32_t ref_bin(const TissueDev& T, double x, double 
 // index back to (tissue, local index) by binary search in the prefix sums.
 // With nothing gated the list is empty and each kernel exits at once.
 // ---------------------------------------------------------------------------
-// Each tissue of [t0, t1) is marked (rl_mark) while it is on the list, so
-// a step kernel running beside the rebuild can leave those tissues out.
 // For the whole batch the "some tissue" word is cleared once the list is
-// built: the step kernels set it again for the next step.
+// built: the step kernel sets it again for the next step.
 __device__ __forceinline__ void gate_compact(const DevState& S, int32_t t0, int32_t t1) {
   const bool whole = t0 == 0 && t1 == S.ntissues;
   if (S.gate[0] == 0) {
-    for (int32_t t = t0 + (int32_t)threadIdx.x; t < t1; t += blockDim.x) S.rl_mark[t] = 0;
     if (threadIdx.x == 0) {
       S.rl_count[0] = 0;
       S.rl_ppre[0] = 0;
@@ -199,7 +196,6 @@ __device__ __forceinline__ void gate_compact(const DevState& S, int32_t t0, int3
   for (int32_t base = t0; base < t1; base += kScanThreads) {
     const int32_t t = base + threadIdx.x;
     const bool g = t < t1 && S.gate[1 + t] != 0;
-    if (t < t1) S.rl_mark[t] = g ? 1 : 0;
     int32_t np = 0, nb = 0;
     if (g) {
       const TissueDev& T = S.tissues[t];
@@ -1295,10 +1291,9 @@ __device__ __forceinline__ void gather_candidates(const DevState& S, Part& P, co
 // kG loads issued before the first is used). Rows longer than that (rare)
 // finish with one load per entry. kMinBlocks bounds the registers so that
 // that many 256-thread blocks stay resident per SM.
-// One particle of the step (skip_listed: nothing for a particle whose tissue
-// is on the rebuild work list).
+// One particle of the step.
 template <typename R, bool kSimple, bool kOld, bool k16>
-__device__ __forceinline__ void step_particle(const DevState& S, int64_t i, bool skip_listed) {
+__device__ __forceinline__ void step_particle(const DevState& S, int64_t i) {
   const int64_t N = S.n_total;
   constexpr int kChunks = k16 ? 2 : 4;               // chunks loaded up front
   constexpr int kPre = kChunks * (k16 ? 8 : 4) - 1;  // candidates they hold
@@ -1307,12 +1302,94 @@ __device__ __forceinline__ void step_particle(const DevState& S, int64_t i, bool
 #pragma unroll
   for (int k = 0; k < kChunks; ++k) c[k] = __ldg(S.cand + k * N + i);
   const uint32_t a = __ldg(&S.attr[i]);
-  if (skip_listed && S.rl_mark[attr_tissue(a)]) return;
   using Part = Particle<R, kSimple, kOld>;
   Part P(S, (int32_t)i, a, S.pos_cur[i]);
   const float4 bp = S.bpos[i];
   const double4 fm = P.st == ST_MEMB ? S.fmemb[i] : make_double4(0.0, 0.0, 0.0, 0.0);
   gather_candidates<k16, kPre, kG>(S, P, c, i);
+  P.finish(bp, fm);
+}
+
+// The same loop with the gathers copied into shared memory asynchronously
+// (cp.async, cached in L1): a thread issues the copies of kS neighbours'
+// positions at once -- all 15 candidates its first two chunks hold when
+// kS = 15 -- holding no register for data in flight, waits once for its own
+// copies, then evaluates the candidates from its own slots (thread t's slot
+// k at slots[k * kStepThreads + t]: conflict-free, no barrier needed).
+constexpr int kStepThreads = 256;
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+template <typename Pos>
+__device__ __forceinline__ void cp_async_pos(Pos* dst, const Pos* src) {
+#pragma unroll
+  for (int h = 0; h < (int)(sizeof(Pos) / 16); ++h)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(smem_u32(
+                     reinterpret_cast<char*>(dst) + 16 * h)),
+                 "l"(reinterpret_cast<const char*>(src) + 16 * h)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+template <bool k16, int kPre, int kS, typename Part, int NC>
+__device__ __forceinline__ void gather_candidates_async(const DevState& S, Part& P,
+                                                        const uint4 (&c)[NC], int64_t i,
+                                                        typename Part::Pos* slots) {
+  using Pos = typename Part::Pos;
+  const int32_t pbase = P.T.pbase;
+  const Pos* src = gather_source<Pos>(S) + pbase;
+  const int32_t nc = (int32_t)row_entry<k16>(c, 0);
+#pragma unroll
+  for (int b = 1; b <= kPre; b += kS) {
+    if (b > nc) break;
+#pragma unroll
+    for (int u = 0; u < kS; ++u) {
+      const int e = b + u;
+      if (e <= kPre && e <= nc) {
+        const int32_t q = (int32_t)row_entry<k16>(c, e);
+        if (EPI_CHECKED(q < P.T.n, S.status, (int32_t)i, q))
+          cp_async_pos(slots + u * kStepThreads, src + q);
+      }
+    }
+    cp_async_wait_all();
+#pragma unroll
+    for (int u = 0; u < kS; ++u) {
+      const int e = b + u;
+      if (e <= kPre && e <= nc) {
+        const int32_t q = (int32_t)row_entry<k16>(c, e);
+        if (q < P.T.n || !kCheck) P.candidate(pbase + q, slots[u * kStepThreads]);
+      }
+    }
+  }
+  for (int32_t e = kPre + 1; e <= nc; ++e) {
+    const int32_t q = (int32_t)cand_entry(S, i, e);
+    if (!EPI_CHECKED(q < P.T.n, S.status, (int32_t)i, q)) continue;
+    P.candidate(pbase + q, src[q]);
+  }
+}
+
+template <typename R, bool kSimple, bool kOld, int kMinBlocks, bool k16, int kS>
+__global__ void __launch_bounds__(kStepThreads, kMinBlocks) k_step_async(DevState S, Range r) {
+  pdl_entry();
+  count_launch(S.launches);
+  using Part = Particle<R, kSimple, kOld>;
+  using Pos = typename Part::Pos;
+  extern __shared__ __align__(16) unsigned char gather_smem[];
+  Pos* slots = reinterpret_cast<Pos*>(gather_smem) + threadIdx.x;
+  const int64_t i = r.p0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= r.p1) return;
+  const int64_t N = S.n_total;
+  constexpr int kChunks = k16 ? 2 : 4;
+  constexpr int kPre = kChunks * (k16 ? 8 : 4) - 1;
+  uint4 c[kChunks];
+#pragma unroll
+  for (int k = 0; k < kChunks; ++k) c[k] = __ldg(S.cand + k * N + i);
+  Part P(S, (int32_t)i, __ldg(&S.attr[i]), S.pos_cur[i]);
+  const float4 bp = S.bpos[i];
+  const double4 fm = P.st == ST_MEMB ? S.fmemb[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+  gather_candidates_async<k16, kPre, kS>(S, P, c, i, slots);
   P.finish(bp, fm);
 }
 
@@ -1322,170 +1399,9 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_step(DevState S, Range r) {
   count_launch(S.launches);
   const int64_t i = r.p0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= r.p1) return;
-  step_particle<R, kSimple, kOld, k16>(S, i, r.skip_listed != 0);
+  step_particle<R, kSimple, kOld, k16>(S, i);
 }
 
-// The particles of the tissues on the rebuild work list, after their
-// rebuild: a grid-stride loop over the listed particles.
-template <typename R, bool kSimple, bool kOld, int kMinBlocks, bool k16>
-__global__ void __launch_bounds__(256, kMinBlocks) k_step_listed(DevState S) {
-  pdl_entry();
-  count_launch(S.launches);
-  GATED_PARTICLES(g, cnt) {
-    int32_t t;
-    const int32_t i = gated_particle(S, cnt, g, &t);
-    step_particle<R, kSimple, kOld, k16>(S, i, false);
-  }
-}
-
-// ---------------------------------------------------------------------------
-// The step as a persistent kernel with its per-particle input stream staged
-// in shared memory by the bulk-copy engine. A block takes tiles of kT
-// consecutive particles (tile t: particles [t kT, (t + 1) kT)) in turn; while
-// its threads work on one tile, bulk copies (cp.async.bulk, completion counted
-// on an mbarrier) bring the next tile's candidate chunks, positions, membrane
-// sums, rebuild positions and attribute words into the other half of a
-// double buffer. The threads then wait only on their neighbours' position
-// gathers, which hit L1 / L2; the streamed inputs are read once, so their
-// copies carry an L2 evict-first policy and leave L2 to the gathered FP32
-// copies. Allocations are padded to whole tiles (kStepTilePad), so a tile's
-// copies never leave their buffers; particles of a tile outside the launch
-// range are skipped.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t done;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(done)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return done != 0;
-}
-// Waits for phase `parity` of the barrier to complete; gives up (false)
-// after kWaitTries unsuccessful tries (each try may block for a while).
-constexpr uint32_t kWaitTries = 1u << 22;
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (uint32_t k = 0; k < kWaitTries; ++k)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-__device__ __forceinline__ uint64_t l2_evict_first() {
-  uint64_t pol;
-  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
-  return pol;
-}
-// global -> shared bulk copy of `bytes` (a multiple of 16, both addresses
-// 16-byte aligned), completion counted on bar
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes,
-                                          uint64_t* bar, uint64_t pol) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint "
-      "[%0], [%1], %2, [%3], %4;" ::"r"(smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
-      : "memory");
-}
-
-template <int kT, int kChunks>
-struct StepTile {
-  uint4 c[kChunks][kT];  // candidate chunks 0 .. kChunks - 1
-  double4 pos[kT];
-  double4 fmemb[kT];
-  float4 bpos[kT];
-  uint32_t attr[kT];
-};
-
-// Resident blocks per SM the staged kernel's registers are held to.
-template <typename R, int kT>
-constexpr int staged_min_blocks() {
-  return sizeof(R) == 4 ? (kT == 128 ? 7 : 3) : (kT == 128 ? 5 : 2);
-}
-
-template <typename R, bool kSimple, bool kOld, bool k16, int kT>
-__global__ void __launch_bounds__(kT, staged_min_blocks<R, kT>())
-    k_step_staged(DevState S, Range r) {
-  pdl_entry();
-  count_launch(S.launches);
-  constexpr int kChunks = k16 ? 2 : 4;
-  constexpr int kPre = kChunks * (k16 ? 8 : 4) - 1;
-  constexpr int kG = sizeof(R) == 4 ? 4 : 2;
-  using Tile = StepTile<kT, kChunks>;
-  constexpr uint32_t kBytes = (uint32_t)sizeof(Tile);
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  Tile* buf = reinterpret_cast<Tile*>(smem_raw);
-  __shared__ uint64_t bar[2];
-  const int64_t t_lo = r.p0 / kT, t_hi = (r.p1 + kT - 1) / kT;
-  const int64_t first = t_lo + blockIdx.x;
-  if (first >= t_hi) return;
-  const int64_t N = S.n_total;
-  const int tid = threadIdx.x;
-  uint64_t pol = 0;
-  if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    pol = l2_evict_first();
-  }
-  __syncthreads();
-  auto issue = [&](int64_t t, int s) {
-    const int64_t i0 = t * kT;
-    Tile& d = buf[s];
-    mbar_expect_tx(&bar[s], kBytes);
-#pragma unroll
-    for (int k = 0; k < kChunks; ++k)
-      bulk_load(d.c[k], S.cand + k * N + i0, 16 * kT, &bar[s], pol);
-    bulk_load(d.pos, S.pos_cur + i0, 32 * kT, &bar[s], pol);
-    bulk_load(d.fmemb, S.fmemb + i0, 32 * kT, &bar[s], pol);
-    bulk_load(d.bpos, S.bpos + i0, 16 * kT, &bar[s], pol);
-    bulk_load(d.attr, S.attr + i0, 4 * kT, &bar[s], pol);
-  };
-  if (tid == 0) issue(first, 0);
-  using Part = Particle<R, kSimple, kOld>;
-  int it = 0;
-  for (int64_t t = first; t < t_hi; t += gridDim.x, ++it) {
-    const int s = it & 1;
-    const int64_t next = t + gridDim.x;
-    // the other half was released by the barrier that ended the last tile
-    if (tid == 0 && next < t_hi) {
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue(next, s ^ 1);
-    }
-    const bool ok = mbar_wait(&bar[s], (uint32_t)(it >> 1) & 1u);
-    if (!__syncthreads_and(ok)) {
-      // the copies never completed: report, let the other half's copies
-      // (if any) land, and stop
-      if (tid == 0) {
-        raise_error(S.status, E_TIMEOUT, (int32_t)(t * kT), -1, 0.0);
-        if (next < t_hi) (void)mbar_wait(&bar[s ^ 1], (uint32_t)((it + 1) >> 1) & 1u);
-      }
-      return;
-    }
-    const int64_t i = t * kT + tid;
-    if (i >= r.p0 && i < r.p1) {
-      const Tile& d = buf[s];
-      uint4 c[kChunks];
-#pragma unroll
-      for (int k = 0; k < kChunks; ++k) c[k] = d.c[k][tid];
-      Part P(S, (int32_t)i, d.attr[tid], d.pos[tid]);
-      gather_candidates<k16, kPre, kG>(S, P, c, i);
-      P.finish(d.bpos[tid], d.fmemb[tid]);
-    }
-    __syncthreads();  // this half is free for the copies of tile t + 2 gridDim.x
-  }
-}
 
 // connect_cell's lists (for export): the exact predicate over the candidates.
 __global__ void k_exact_lists(DevState S, Range r) {
@@ -1646,7 +1562,7 @@ void launch_scan(const int32_t* in, int32_t* out, int32_t n, int32_t init,
 void launch_rebuild(const DevState& S, const Range& r, const ScanScratch&,
                     const LaunchCfg& lc, cudaStream_t s, Timer* tm, bool listed) {
   const int B = lc.block;
-  const int grid = lc.num_sms * lc.rebuild_per_sm;
+  const int grid = lc.num_sms * 8;
   if (!listed) {
     timer_begin(tm, KC_GATE, s);
     launch_pdl(k_gate_compact, 1, kScanThreads, s, S, r.t0, r.t1);
@@ -1695,26 +1611,20 @@ void launch_prepass(const DevState& S, int32_t m0, int32_t m1, int32_t f0, int32
   launch_dermis(S, f0, f1, lc, s, tm);
 }
 
-// The staged kernel: dynamic shared memory for two tiles, a persistent grid
-// of as many blocks as fit on the GPU at once (found once per instantiation).
-template <typename R, bool kSimple, bool kOld, bool k16, int kT>
-void launch_step_staged(const DevState& S, const Range& r, const LaunchCfg& lc, cudaStream_t s) {
-  auto kern = k_step_staged<R, kSimple, kOld, k16, kT>;
-  constexpr int smem = 2 * (int)sizeof(StepTile<kT, k16 ? 2 : 4>);
-  static int per_sm = 0;
-  if (per_sm == 0) {
+// The asynchronous-gather kernel with kS shared-memory slots per thread.
+template <typename R, bool kSimple, bool kOld, bool k16, int kS, int kMinBlocks>
+void launch_step_async(const DevState& S, const Range& r, cudaStream_t s) {
+  using Pos = typename std::conditional<sizeof(R) == 4, float4, double4>::type;
+  auto kern = k_step_async<R, kSimple, kOld, kMinBlocks, k16, kS>;
+  constexpr int smem = kS * kStepThreads * (int)sizeof(Pos);
+  static bool configured = false;
+  if (!configured) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kT, smem) != cudaSuccess || b < 1)
-      b = 1;
-    per_sm = b;
+    configured = true;
   }
-  const int64_t tiles = (r.p1 + kT - 1) / kT - r.p0 / kT;
-  const int64_t cap = (int64_t)lc.num_sms * per_sm;
-  const int grid = (int)(tiles < cap ? tiles : cap);
   cudaLaunchConfig_t cfg{};
-  cfg.gridDim = dim3((unsigned)grid);
-  cfg.blockDim = dim3((unsigned)kT);
+  cfg.gridDim = dim3((unsigned)blocks_for(r.p1 - r.p0, kStepThreads));
+  cfg.blockDim = dim3((unsigned)kStepThreads);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
@@ -1725,20 +1635,19 @@ void launch_step_staged(const DevState& S, const Range& r, const LaunchCfg& lc, 
   cudaLaunchKernelEx(&cfg, kern, S, r);
 }
 
-// Tuning variants: 1 and 2, the staged kernel with tiles of 128 and 256
-// particles; 3 (default) and 4, one thread per particle with
-// register-pipelined loads at two register budgets (FP32: 4 and 3 resident
-// 256-thread blocks per SM; FP64: 3 and 2, below which it spills); 5 and 6,
-// the kernels of 3 and 4 (the step graph schedules them differently).
+// Tuning variants: 1 and 2, gathers copied asynchronously into shared
+// memory, 8 (FP64: 4) and 15 (FP64: 8) slots per thread; 3 (default) and 4,
+// gathers into registers four (FP64: two) at a time, at two register budgets
+// (FP32: 4 and 3 resident 256-thread blocks per SM; FP64: 3 and 2, below
+// which it spills).
 template <typename R, bool kSimple, bool kOld, bool k16>
 void launch_step_w(const DevState& S, const Range& r, const LaunchCfg& lc, cudaStream_t s) {
   const int grid = blocks_for(r.p1 - r.p0, 256);
   constexpr bool kF = sizeof(R) == 4;
   switch (lc.variant) {
-    case 1: launch_step_staged<R, kSimple, kOld, k16, 128>(S, r, lc, s); break;
-    case 2: launch_step_staged<R, kSimple, kOld, k16, 256>(S, r, lc, s); break;
-    case 4:
-    case 6: launch_pdl(k_step<R, kSimple, kOld, kF ? 3 : 2, k16>, grid, 256, s, S, r); break;
+    case 1: launch_step_async<R, kSimple, kOld, k16, kF ? 8 : 4, kF ? 4 : 3>(S, r, s); break;
+    case 2: launch_step_async<R, kSimple, kOld, k16, kF ? 15 : 8, 3>(S, r, s); break;
+    case 4: launch_pdl(k_step<R, kSimple, kOld, kF ? 3 : 2, k16>, grid, 256, s, S, r); break;
     default: launch_pdl(k_step<R, kSimple, kOld, kF ? 4 : 3, k16>, grid, 256, s, S, r); break;
   }
 }
@@ -1747,33 +1656,6 @@ template <typename R, bool kSimple, bool kOld>
 void launch_step_v(const DevState& S, const Range& r, const LaunchCfg& lc, cudaStream_t s) {
   if (S.cand16) launch_step_w<R, kSimple, kOld, true>(S, r, lc, s);
   else launch_step_w<R, kSimple, kOld, false>(S, r, lc, s);
-}
-
-template <typename R, bool kSimple, bool kOld>
-void launch_step_listed_v(const DevState& S, const LaunchCfg& lc, cudaStream_t s) {
-  constexpr bool kF = sizeof(R) == 4;
-  const int grid = lc.num_sms * (kF ? 4 : 3);
-  if (S.cand16)
-    launch_pdl(k_step_listed<R, kSimple, kOld, kF ? 4 : 3, true>, grid, 256, s, S);
-  else
-    launch_pdl(k_step_listed<R, kSimple, kOld, kF ? 4 : 3, false>, grid, 256, s, S);
-}
-
-template <typename R>
-void launch_step_listed_r(const DevState& S, const LaunchCfg& lc, cudaStream_t s) {
-  if (lc.simple && lc.any_old)
-    launch_step_listed_v<R, true, true>(S, lc, s);
-  else if (lc.simple)
-    launch_step_listed_v<R, true, false>(S, lc, s);
-  else
-    launch_step_listed_v<R, false, true>(S, lc, s);
-}
-
-void launch_step_listed(const DevState& S, int precision, const LaunchCfg& lc, cudaStream_t s) {
-  if (precision == 1)
-    launch_step_listed_r<float>(S, lc, s);
-  else
-    launch_step_listed_r<double>(S, lc, s);
 }
 
 template <typename R>

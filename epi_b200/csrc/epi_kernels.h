@@ -10,18 +10,7 @@ struct Range {
   int32_t p0, p1;  // particles
   int32_t b0, b1;  // bins
   int32_t t0, t1;  // tissues
-  // step kernels: 0 every particle of the range; 1 only those of tissues not
-  // on the rebuild work list (rl_mark), which may step beside the rebuild
-  int32_t skip_listed = 0;
 };
-
-// Per-particle buffers the staged step kernel copies by whole tiles (pos,
-// fmemb, bpos, attr) hold a multiple of this many entries, and the candidate
-// rows this many chunks more than their columns need.
-constexpr int64_t kStepTilePad = 256;
-inline int64_t padded_particles(int64_t n) {
-  return (n + kStepTilePad - 1) / kStepTilePad * kStepTilePad;
-}
 
 struct ScanScratch {
   int32_t* partial;  // ceil(n / kScanTile) entries
@@ -36,7 +25,6 @@ struct LaunchCfg {
   int any_old;      // some cell is older than THRESH_SP
   int variant;      // step-kernel instantiation (pipeline depth / residency), see epi_config
   int search_switch;  // rebuilt particles from which the search takes a thread per particle
-  int rebuild_per_sm = 8;  // blocks per SM of the rebuild's grid-stride kernels
 };
 
 // Kernel classes, for per-class timing.
@@ -78,9 +66,6 @@ void launch_dermis(const DevState& S, int32_t f0, int32_t f1, const LaunchCfg& l
 // skin/2 since their last rebuild.
 void launch_step(const DevState& S, const Range& r, int precision, const LaunchCfg& lc,
                  cudaStream_t s, Timer* tm);
-// The step for the particles of the tissues on the rebuild work list only
-// (after their rebuild; the rest stepped with skip_listed beside it).
-void launch_step_listed(const DevState& S, int precision, const LaunchCfg& lc, cudaStream_t s);
 // Exact connection lists (connect_cell's result) into S.nbr / S.nn.
 void launch_exact_lists(const DevState& S, const Range& r, const LaunchCfg& lc,
                         cudaStream_t s);

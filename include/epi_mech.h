@@ -122,16 +122,12 @@ typedef struct epi_config {
                          extra); the reference allows 400 (define.h:80) */
   int32_t max_cand;   /* candidates per particle (>= max_conn) */
   double skin;        /* candidate margin, > 0 (default 0.1) */
-  int32_t variant;    /* step-kernel form: 0 = default (3); 1, 2 = one
-                         persistent kernel whose per-particle inputs are
-                         staged in shared memory by bulk copies, tiles of 128
-                         / 256 particles; 3, 4 = one thread per particle with
-                         register-pipelined loads, 4 / 3 resident 256-thread
-                         blocks per SM (FP64: 3 / 2), whose step of the tissues
-                         that need no candidate rebuild runs beside the others'
-                         rebuild in the step graph (when the batch has no FIX
-                         or MUSUME cell); 5, 6 = the kernels of 3, 4 after the
-                         rebuild. Same formulas; the compiler may fuse
+  int32_t variant;    /* step-kernel form: 0 = default (3); 1, 2 = the
+                         neighbours' positions copied asynchronously into
+                         shared memory, 8 / 15 per thread at once (FP64: 4 /
+                         8); 3, 4 = gathered into registers four at a time
+                         (FP64: two), 4 / 3 resident 256-thread blocks per SM
+                         (FP64: 3 / 2). Same formulas; the compiler may fuse
                          multiply-adds differently, so results agree to
                          rounding. */
   int32_t search_switch; /* candidate search: rebuilds of at least this many
@@ -226,7 +222,7 @@ int epi_time_kernels(epi_ctx* ctx, int32_t nsteps, int32_t max_classes, double* 
 
 /* Autotuner. Times short graph-replayed trials of the uploaded batch for
  * every candidate skin in {0.05, 0.08, 0.1, 0.15, 0.2, 0.3} and step-kernel
- * variant 1..6 (4 warm-up steps, then trial_steps timed with CUDA events),
+ * variant 1..4 (4 warm-up steps, then trial_steps timed with CUDA events),
  * then, for the fastest pair, the candidate-search switch in {8192, 16384,
  * 49152, 131072} rebuilt particles, and keeps the fastest choice in the
  * context's configuration. Skins whose candidate rows would overflow

@@ -160,11 +160,11 @@ def test_batch_with_scaled_params_vs_oracle(built):
         base += t.n
 
 
-@pytest.mark.parametrize("variant", [None, 3, 4])
+@pytest.mark.parametrize("variant", [None, 1, 2])
 @pytest.mark.parametrize("precision", [FP64, MIXED])
 def test_graph_and_per_tissue_launches_are_bit_identical(built, precision, variant):
-    """Variants 3 and 4 capture the split schedule: the step of the tissues
-    that need no rebuild runs beside the others' rebuild, then theirs."""
+    """Also for the step-kernel forms whose gathers go through shared memory
+    (variants 1 and 2)."""
     ts = [T.config1(1), T.layered_tissue(24, 2, 4), T.config1(7)]
     ref = run_gpu(ts, 21, precision, "eager")
     for mode in ("graph", "per_tissue"):
@@ -201,7 +201,7 @@ def test_simple_and_general_step_kernels_agree(built):
     assert np.array_equal(idx_b[: off_s[-1]], idx_s)
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4])
 def test_step_kernel_variants_agree(built, variant):
     """Register-budget variants run the same formulas in the same order; only
     the compiler's multiply-add fusion may differ (FP64: rounding level)."""
