@@ -94,7 +94,8 @@ class ConfigC(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("precision", ctypes.c_int32),
                 ("max_conn", ctypes.c_int32), ("max_cand", ctypes.c_int32),
                 ("skin", ctypes.c_double), ("variant", ctypes.c_int32),
-                ("search_switch", ctypes.c_int32)]
+                ("search_switch", ctypes.c_int32), ("rebuild_form", ctypes.c_int32),
+                ("search_lanes", ctypes.c_int32)]
 
 
 _lib = None
@@ -140,7 +141,8 @@ def lib():
                                        ctypes.POINTER(ctypes.c_char_p), _ip]
         L.epi_autotune.argtypes = [vp, ctypes.c_int32, _dp, _ip, _dp]
         L.epi_get_config.argtypes = [vp, ctypes.POINTER(ConfigC)]
-        L.epi_set_tuning.argtypes = [vp, ctypes.c_double, ctypes.c_int32, ctypes.c_int32]
+        L.epi_set_tuning.argtypes = [vp, ctypes.c_double, ctypes.c_int32, ctypes.c_int32,
+                                     ctypes.c_int32, ctypes.c_int32]
         L.epi_field_init.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
         L.epi_field_step.argtypes = [vp, ctypes.c_int32]
         L.epi_field_get.argtypes = [vp, ctypes.c_int32, _ip, _up, _dp, _dp]
@@ -182,7 +184,8 @@ class Context:
 
     def __init__(self, precision: int = EPI_PREC_MIXED, max_conn: int = 64, device: int = 0,
                  max_cand: Optional[int] = None, skin: Optional[float] = None,
-                 variant: Optional[int] = None):
+                 variant: Optional[int] = None, rebuild_form: Optional[int] = None,
+                 search_switch: Optional[int] = None, search_lanes: Optional[int] = None):
         L = lib()
         cfg = ConfigC()
         L.epi_config_default(ctypes.byref(cfg))
@@ -193,6 +196,12 @@ class Context:
             cfg.skin = skin
         if variant is not None:
             cfg.variant = variant
+        if rebuild_form is not None:
+            cfg.rebuild_form = rebuild_form
+        if search_switch is not None:
+            cfg.search_switch = search_switch
+        if search_lanes is not None:
+            cfg.search_lanes = search_lanes
         cfg.device = device
         h = ctypes.c_void_p()
         _check(L.epi_create(ctypes.byref(h), ctypes.byref(cfg)), "epi_create")
@@ -385,10 +394,11 @@ class Context:
         _check(lib().epi_get_config(self._h, ctypes.byref(cfg)), "epi_get_config")
         return {k: getattr(cfg, k) for k, _ in ConfigC._fields_}
 
-    def set_tuning(self, skin: float, variant: int, search_switch: int = 0):
+    def set_tuning(self, skin: float, variant: int, search_switch: int = 0,
+                   rebuild_form: int = 0, search_lanes: int = 0):
         """epi_set_tuning: apply a tuning chosen earlier (e.g. cached)."""
-        _check(lib().epi_set_tuning(self._h, float(skin), int(variant), int(search_switch)),
-               "epi_set_tuning")
+        _check(lib().epi_set_tuning(self._h, float(skin), int(variant), int(search_switch),
+                                    int(rebuild_form), int(search_lanes)), "epi_set_tuning")
 
     def autotune(self, trial_steps: int = 64):
         """epi_autotune: returns (skin, variant, ms per step of the best trial)

@@ -340,9 +340,57 @@ __global__ void k_scatter(DevState S) {
     const int32_t b = S.bin[i];
     if (b < 0) continue;
     const int32_t slot = S.starts[b] + S.rank[i];
-    const TissueDev& T = S.tissues[t];
-    if (!EPI_CHECKED(slot >= T.pbase && slot < T.pbase + T.n, S.status, i, slot)) continue;
+    if (!EPI_CHECKED(slot >= S.tissues[t].pbase && slot < S.tissues[t].pbase + S.tissues[t].n,
+                     S.status, i, slot))
+      continue;
     S.skey[slot] = (uint32_t)i;
+  }
+}
+
+// Sorts the particles of one bin (slots [s0, s1)) by index -- the
+// deterministic order the candidate search emits them in -- then tags
+// membrane particles and writes the sorted FP32 copy of their positions (x
+// and y as grid_init bins them, in [0, L)). Bins hold a few to a few dozen
+// particles: up to 24 are sorted in registers.
+__device__ __forceinline__ void sort_bin(const DevState& S, const TissueDev& T, int32_t s0,
+                                         int32_t s1) {
+  constexpr int kLocal = 24;  // a bin holds about 8 particles at unit density
+  if (s1 - s0 <= kLocal) {
+    uint32_t key[kLocal];
+    const int m = s1 - s0;
+    for (int k = 0; k < m; ++k) {
+      const uint32_t v = S.skey[s0 + k];
+      int q = k - 1;
+      while (q >= 0 && key[q] > v) {
+        key[q + 1] = key[q];
+        --q;
+      }
+      key[q + 1] = v;
+    }
+    for (int k = 0; k < m; ++k) S.skey[s0 + k] = key[k];
+  } else {
+    for (int32_t s = s0 + 1; s < s1; ++s) {
+      const uint32_t v = S.skey[s];
+      int32_t q = s - 1;
+      while (q >= s0 && S.skey[q] > v) {
+        S.skey[q + 1] = S.skey[q];
+        --q;
+      }
+      S.skey[q + 1] = v;
+    }
+  }
+  for (int32_t s = s0; s < s1; ++s) {
+    const uint32_t gi = S.skey[s];
+    if (!EPI_CHECKED(gi >= (uint32_t)T.pbase && gi < (uint32_t)(T.pbase + T.n), S.status,
+                     (int32_t)gi, s))
+      continue;
+    const bool memb = attr_state(S.attr[gi]) == ST_MEMB;
+    S.skey[s] = gi | (memb ? 0x80000000u : 0u);
+    // x and y as grid_init bins them (ref_bin): in [0, L)
+    const double4 pg = S.pos_cur[gi];
+    const double xc = 0.5 * T.lx - pdiff(0.5 * T.lx, pg.x, T.lx);
+    const double yc = 0.5 * T.ly - pdiff(0.5 * T.ly, pg.y, T.ly);
+    S.spos[s] = make_float4((float)xc, (float)yc, (float)pg.z, (float)pg.w);
   }
 }
 
@@ -361,44 +409,106 @@ __global__ void k_binsort(DevState S) {
     const int32_t s0 = S.starts[b], s1 = S.starts[b + 1];
     if (s1 <= s0) continue;
     S.counts[b] = 0;  // ready for the next binning
-    constexpr int kLocal = 24;  // a bin holds about 8 particles at unit density
-    if (s1 - s0 <= kLocal) {
-      uint32_t key[kLocal];
-      const int m = s1 - s0;
-      for (int k = 0; k < m; ++k) {
-        const uint32_t v = S.skey[s0 + k];
-        int q = k - 1;
-        while (q >= 0 && key[q] > v) {
-          key[q + 1] = key[q];
-          --q;
-        }
-        key[q + 1] = v;
+    sort_bin(S, T, s0, s1);
+  }
+}
+
+// The counting sort of one gated tissue per block, all in one kernel:
+// binning with the bin counts in shared memory (ranks from shared-memory
+// atomics), the scan of the counts into bin offsets, the scatter into
+// sorted order and the per-bin sort, separated by block barriers. It
+// replaces k_bin, k_scan_tissue, k_scatter and k_binsort (four launches and
+// their grid-wide dependencies) when every tissue of the batch has at most
+// kFusedMaxBins bins. The tissue's particles are binned four at a time so
+// their position loads overlap.
+constexpr int kFusedThreads = 1024;
+constexpr int32_t kFusedMaxBins = kFusedRebuildMaxBins;  // 64 KB of counts in shared memory
+
+__global__ void __launch_bounds__(kFusedThreads) k_rebuild_tissue(DevState S) {
+  pdl_entry();
+  count_launch(S.launches);
+  extern __shared__ int32_t s_cnt[];  // bin counts, then offsets; nb + 1 entries
+  const int32_t cnt = S.rl_count[0];
+  for (int32_t k = blockIdx.x; k < cnt; k += gridDim.x) {
+    const TissueDev& T = S.tissues[S.rl_list[k]];
+    const int32_t nb = T.anx * T.any * T.anz;
+    for (int32_t b = threadIdx.x; b <= nb; b += blockDim.x) s_cnt[b] = 0;
+    __syncthreads();
+    // grid_init (cell_connection.cpp:38-62): the bin of every particle
+    for (int32_t j0 = 0; j0 < T.n; j0 += 4 * kFusedThreads) {
+      double4 p[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int32_t j = j0 + u * kFusedThreads + (int32_t)threadIdx.x;
+        if (j < T.n) p[u] = S.pos_cur[T.pbase + j];
       }
-      for (int k = 0; k < m; ++k) S.skey[s0 + k] = key[k];
-    } else {
-      for (int32_t s = s0 + 1; s < s1; ++s) {
-        const uint32_t v = S.skey[s];
-        int32_t q = s - 1;
-        while (q >= s0 && S.skey[q] > v) {
-          S.skey[q + 1] = S.skey[q];
-          --q;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int32_t j = j0 + u * kFusedThreads + (int32_t)threadIdx.x;
+        if (j >= T.n) continue;
+        const int32_t i = T.pbase + j;
+        int32_t lb = -1;
+        if (!isfinite(p[u].x) || !isfinite(p[u].y) || !isfinite(p[u].z)) {
+          raise_error(S.status, E_NONFINITE, i, -1, p[u].x);
+        } else {
+          lb = ref_bin(T, p[u].x, p[u].y, p[u].z, attr_state(S.attr[i]) == ST_MEMB);
+          if (lb < 0) raise_error(S.status, E_BIN_RANGE, i, -1, p[u].z);
         }
-        S.skey[q + 1] = v;
+        S.bin[i] = lb;
+        if (lb >= 0) {
+          const int32_t rk = atomicAdd(&s_cnt[lb], 1);
+          if (rk + 1 >= kBinCap)
+            raise_error(S.status, E_BIN_OVERFLOW, i, T.binbase + lb, (double)(rk + 1));
+          S.rank[i] = rk;
+        }
       }
     }
-    for (int32_t s = s0; s < s1; ++s) {
-      const uint32_t gi = S.skey[s];
-      if (!EPI_CHECKED(gi >= (uint32_t)T.pbase && gi < (uint32_t)(T.pbase + T.n), S.status,
-                       (int32_t)gi, s))
-        continue;
-      const bool memb = attr_state(S.attr[gi]) == ST_MEMB;
-      S.skey[s] = gi | (memb ? 0x80000000u : 0u);
-      // x and y as grid_init bins them (ref_bin): in [0, L)
-      const double4 pg = S.pos_cur[gi];
-      const double xc = 0.5 * T.lx - pdiff(0.5 * T.lx, pg.x, T.lx);
-      const double yc = 0.5 * T.ly - pdiff(0.5 * T.ly, pg.y, T.ly);
-      S.spos[s] = make_float4((float)xc, (float)yc, (float)pg.z, (float)pg.w);
+    __syncthreads();
+    // bin offsets: exclusive scan of the counts, offset by the tissue's first
+    // particle; entry nb is the tissue's end
+    int32_t carry = T.pbase;
+    constexpr int32_t kTile = kFusedThreads * kScanItems;
+    for (int32_t base = 0; base < nb; base += kTile) {
+      const int32_t b0 = base + (int32_t)threadIdx.x * kScanItems;
+      int32_t v[kScanItems];
+      int32_t sum = 0;
+#pragma unroll
+      for (int q = 0; q < kScanItems; ++q) {
+        v[q] = b0 + q < nb ? s_cnt[b0 + q] : 0;
+        sum += v[q];
+      }
+      int32_t tot;
+      int32_t run = carry + block_excl_scan_n<kFusedThreads>(sum, &tot);
+#pragma unroll
+      for (int q = 0; q < kScanItems; ++q) {
+        if (b0 + q < nb) {
+          s_cnt[b0 + q] = run;
+          S.starts[T.binbase + b0 + q] = run;
+        }
+        run += v[q];
+      }
+      carry += tot;
     }
+    if (threadIdx.x == 0) {
+      s_cnt[nb] = carry;
+      S.starts[T.binbase + nb] = carry;
+    }
+    __syncthreads();
+    // scatter into bin order
+    for (int32_t j = threadIdx.x; j < T.n; j += blockDim.x) {
+      const int32_t i = T.pbase + j;
+      const int32_t lb = S.bin[i];
+      if (lb < 0) continue;
+      const int32_t slot = s_cnt[lb] + S.rank[i];
+      if (!EPI_CHECKED(slot >= T.pbase && slot < T.pbase + T.n, S.status, i, slot)) continue;
+      S.skey[slot] = (uint32_t)i;
+    }
+    __syncthreads();
+    for (int32_t b = threadIdx.x; b < nb; b += blockDim.x) {
+      const int32_t s0 = s_cnt[b], s1 = s_cnt[b + 1];
+      if (s1 > s0) sort_bin(S, T, s0, s1);
+    }
+    __syncthreads();
   }
 }
 
@@ -518,17 +628,25 @@ __device__ __forceinline__ void finish_search(const DevState& S, int32_t i, int3
   S.bpos[i] = make_float4((float)p.x, (float)p.y, (float)p.z, 0.f);
 }
 
-// Few gated particles (a tissue or two): one warp per particle, so the GPU
-// has work for all its warps. Each lane fetches the slot range of one bin
-// column; a warp scan lays the ranges end to end, the warp sweeps the
-// concatenation 32 slots at a time, and ballots keep the slot order.
-__device__ __forceinline__ void cand_search_warps(const DevState& S, int32_t cnt,
-                                                  int32_t ngated) {
+// G lanes per particle (G = 32: one warp; 4, 8, 16: several particles per
+// warp). The group's lanes fetch the slot ranges of G bin columns at a time;
+// a scan within the group lays the ranges end to end, the group sweeps the
+// concatenation G slots at a time, and ballots keep the slot order, so every
+// G emits the same rows in the same order. With few gated particles G = 32
+// keeps the GPU busy; with many, smaller groups divide the divergence of
+// ragged windows among fewer lanes than whole warps do.
+template <int G>
+__device__ __forceinline__ void cand_search_groups(const DevState& S, int32_t cnt,
+                                                   int32_t ngated) {
+  static_assert(G == 4 || G == 8 || G == 16 || G == 32, "group of 4 to 32 lanes");
   const int lane = threadIdx.x & 31;
-  const unsigned lt_mask = (1u << lane) - 1u;
-  const int32_t warps = (gridDim.x * blockDim.x) >> 5;
+  const int gl = lane & (G - 1);          // lane within the group
+  const int gbase = lane & ~(G - 1);      // the group's first lane
+  const unsigned gmask = G == 32 ? 0xffffffffu : ((0xffffffffu >> (32 - G)) << gbase);
+  const unsigned lt_mask = (1u << gl) - 1u;
+  const int32_t groups = (gridDim.x * blockDim.x) / G;
   const int32_t cap = S.max_cand;
-  for (int32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ngated; g += warps) {
+  for (int32_t g = (blockIdx.x * blockDim.x + threadIdx.x) / G; g < ngated; g += groups) {
     int32_t t;
     const int32_t i = gated_particle(S, cnt, g, &t);
     const TissueDev& T = S.tissues[t];
@@ -538,8 +656,8 @@ __device__ __forceinline__ void cand_search_warps(const DevState& S, int32_t cnt
     const int32_t ncy = ny0 + (W.nyr > 1 ? W.yhi[1] - W.ylo[1] + 1 : 0);
     const int32_t ncol = ncx * ncy;  // column c = cx * ncy + cy
     int32_t count = 0;
-    for (int32_t c0 = 0; c0 < ncol; c0 += 32) {
-      const int32_t c = c0 + lane;
+    for (int32_t c0 = 0; c0 < ncol; c0 += G) {
+      const int32_t c = c0 + gl;
       int32_t lo = 0, len = 0;
       float cex = 0.f, cey = 0.f;
       if (c < ncol) {
@@ -552,27 +670,32 @@ __device__ __forceinline__ void cand_search_warps(const DevState& S, int32_t cnt
         lo = S.starts[col + W.z0];
         len = S.starts[col + W.z1 + 1] - lo;
       }
-      const int32_t incl = warp_incl_scan(len);
+      int32_t incl = len;
+#pragma unroll
+      for (int o = 1; o < G; o <<= 1) {
+        const int32_t v = __shfl_up_sync(gmask, incl, o, G);
+        if (gl >= o) incl += v;
+      }
       const int32_t excl = incl - len;
-      const int32_t total = __shfl_sync(0xffffffffu, incl, 31);
-      for (int32_t base = 0; base < total; base += 32) {
-        const int32_t f = base + lane;
-        // the last column whose range starts at or before f (k + step <= 31)
+      const int32_t total = __shfl_sync(gmask, incl, G - 1, G);
+      for (int32_t base = 0; base < total; base += G) {
+        const int32_t f = base + gl;
+        // the last column whose range starts at or before f (k + step <= G - 1)
         int32_t k = 0;
 #pragma unroll
-        for (int32_t step = 16; step > 0; step >>= 1) {
-          const int32_t e = __shfl_sync(0xffffffffu, excl, k + step);
+        for (int32_t step = G / 2; step > 0; step >>= 1) {
+          const int32_t e = __shfl_sync(gmask, excl, k + step, G);
           if (e <= f) k += step;
         }
-        const int32_t s = __shfl_sync(0xffffffffu, lo, k) + (f - __shfl_sync(0xffffffffu, excl, k));
-        const float ex = __shfl_sync(0xffffffffu, cex, k), ey = __shfl_sync(0xffffffffu, cey, k);
+        const int32_t s = __shfl_sync(gmask, lo, k, G) + (f - __shfl_sync(gmask, excl, k, G));
+        const float ex = __shfl_sync(gmask, cex, k, G), ey = __shfl_sync(gmask, cey, k, G);
         bool hit = false;
         uint32_t key = 0;
         if (f < total) {
           key = S.skey[s];
           hit = W.hit(i, key, S.spos[s], ex, ey);
         }
-        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        const unsigned m = (__ballot_sync(gmask, hit) & gmask) >> gbase;
         if (hit) {
           const int32_t kk = count + __popc(m & lt_mask);
           if (kk < cap) cand_set(S, i, kk + 1, (key & 0x7fffffffu) - (uint32_t)T.pbase);
@@ -580,7 +703,7 @@ __device__ __forceinline__ void cand_search_warps(const DevState& S, int32_t cnt
         count += __popc(m);
       }
     }
-    if (lane == 0) finish_search(S, i, count);
+    if (gl == 0) finish_search(S, i, count);
   }
 }
 
@@ -670,17 +793,22 @@ __device__ __forceinline__ void cand_search_threads(const DevState& S, int32_t c
   }
 }
 
-// Below `thread_from` gated particles the warp-per-particle search (which
-// keeps the GPU busy with few particles) runs, from there on one thread per
-// particle. Both emit every row in the same order.
-__global__ void __launch_bounds__(256, 4) k_cand_search(DevState S, int32_t thread_from) {
+// Below `large_from` gated particles the search takes a warp per particle
+// (which keeps the GPU busy with few particles), from there on `lanes`
+// lanes per particle (1: one thread, scanning its window alone). Every form
+// emits every row in the same order.
+__global__ void __launch_bounds__(256, 4) k_cand_search(DevState S, int32_t large_from,
+                                                        int32_t lanes) {
   pdl_entry();
   count_launch(S.launches);
   const int32_t cnt = S.rl_count[0];
   if (blockIdx.x == 0) gate_clear(S, cnt);
   if (cnt == 0) return;
   const int32_t ngated = S.rl_ppre[cnt];
-  if (ngated < thread_from) cand_search_warps(S, cnt, ngated);
+  if (ngated < large_from) cand_search_groups<32>(S, cnt, ngated);
+  else if (lanes == 4) cand_search_groups<4>(S, cnt, ngated);
+  else if (lanes == 8) cand_search_groups<8>(S, cnt, ngated);
+  else if (lanes == 16) cand_search_groups<16>(S, cnt, ngated);
   else cand_search_threads(S, cnt, ngated);
 }
 
@@ -1568,20 +1696,44 @@ void launch_rebuild(const DevState& S, const Range& r, const ScanScratch&,
     launch_pdl(k_gate_compact, 1, kScanThreads, s, S, r.t0, r.t1);
     timer_end(tm, KC_GATE, s);
   }
-  timer_begin(tm, KC_REBUILD_BIN, s);
-  launch_pdl(k_bin, grid, B, s, S);
-  timer_end(tm, KC_REBUILD_BIN, s);
-  timer_begin(tm, KC_REBUILD_SCAN, s);
   const int nt = r.t1 - r.t0;
-  launch_pdl(k_scan_tissue, nt < lc.num_sms * 4 ? (nt > 0 ? nt : 1) : lc.num_sms * 4,
-             kTissueScanThreads, s, S);
-  timer_end(tm, KC_REBUILD_SCAN, s);
-  timer_begin(tm, KC_REBUILD_SORT, s);
-  launch_pdl(k_scatter, grid, B, s, S);
-  launch_pdl(k_binsort, grid, B, s, S);
-  timer_end(tm, KC_REBUILD_SORT, s);
+  if (lc.fused_rebuild) {
+    // one block per gated tissue: bin, scan, scatter and sort in one launch
+    static bool configured = false;
+    constexpr int smem = (kFusedMaxBins + 1) * (int)sizeof(int32_t);
+    if (!configured) {
+      cudaFuncSetAttribute(k_rebuild_tissue, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      configured = true;
+    }
+    timer_begin(tm, KC_REBUILD_BIN, s);
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)(nt < lc.num_sms ? (nt > 0 ? nt : 1) : lc.num_sms));
+    cfg.blockDim = dim3((unsigned)kFusedThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_rebuild_tissue, S);
+    timer_end(tm, KC_REBUILD_BIN, s);
+  } else {
+    timer_begin(tm, KC_REBUILD_BIN, s);
+    launch_pdl(k_bin, grid, B, s, S);
+    timer_end(tm, KC_REBUILD_BIN, s);
+    timer_begin(tm, KC_REBUILD_SCAN, s);
+    launch_pdl(k_scan_tissue, nt < lc.num_sms * 4 ? (nt > 0 ? nt : 1) : lc.num_sms * 4,
+               kTissueScanThreads, s, S);
+    timer_end(tm, KC_REBUILD_SCAN, s);
+    timer_begin(tm, KC_REBUILD_SORT, s);
+    launch_pdl(k_scatter, grid, B, s, S);
+    launch_pdl(k_binsort, grid, B, s, S);
+    timer_end(tm, KC_REBUILD_SORT, s);
+  }
   timer_begin(tm, KC_REBUILD_SEARCH, s);
-  launch_pdl(k_cand_search, grid, B, s, S, (int32_t)lc.search_switch);
+  launch_pdl(k_cand_search, grid, B, s, S, (int32_t)lc.search_switch,
+             (int32_t)lc.search_lanes);
   timer_end(tm, KC_REBUILD_SEARCH, s);
 }
 
@@ -1638,8 +1790,7 @@ void launch_step_async(const DevState& S, const Range& r, cudaStream_t s) {
 // Tuning variants: 1 and 2, gathers copied asynchronously into shared
 // memory, 8 (FP64: 4) and 15 (FP64: 8) slots per thread; 3 (default) and 4,
 // gathers into registers four (FP64: two) at a time, at two register budgets
-// (FP32: 4 and 3 resident 256-thread blocks per SM; FP64: 3 and 2, below
-// which it spills).
+// (3 and 4 resident 256-thread blocks per SM; FP64: 3 and 2).
 template <typename R, bool kSimple, bool kOld, bool k16>
 void launch_step_w(const DevState& S, const Range& r, const LaunchCfg& lc, cudaStream_t s) {
   const int grid = blocks_for(r.p1 - r.p0, 256);
@@ -1647,8 +1798,8 @@ void launch_step_w(const DevState& S, const Range& r, const LaunchCfg& lc, cudaS
   switch (lc.variant) {
     case 1: launch_step_async<R, kSimple, kOld, k16, kF ? 8 : 4, kF ? 4 : 3>(S, r, s); break;
     case 2: launch_step_async<R, kSimple, kOld, k16, kF ? 15 : 8, 3>(S, r, s); break;
-    case 4: launch_pdl(k_step<R, kSimple, kOld, kF ? 3 : 2, k16>, grid, 256, s, S, r); break;
-    default: launch_pdl(k_step<R, kSimple, kOld, kF ? 4 : 3, k16>, grid, 256, s, S, r); break;
+    case 4: launch_pdl(k_step<R, kSimple, kOld, kF ? 4 : 2, k16>, grid, 256, s, S, r); break;
+    default: launch_pdl(k_step<R, kSimple, kOld, 3, k16>, grid, 256, s, S, r); break;
   }
 }
 

@@ -69,5 +69,8 @@ def test_checked_build_reports_nothing_and_matches_release(built):
         gx, gy, gz, goff, gidx = got[k]
         rx, ry, rz, roff, ridx = ref[k]
         assert goff == roff and gidx == ridx, k
+        # the two builds may contract multiply-adds differently: rounding
+        # level in FP64, FP32 rounding level of the forces in the mixed path
+        tol = 1e-12 if k.split("/")[1] == str(capi.EPI_PREC_FP64) else 1e-8
         for a, b in ((gx, rx), (gy, ry), (gz, rz)):
-            assert np.max(np.abs(np.array(a) - np.array(b))) <= 1e-12, k
+            assert np.max(np.abs(np.array(a) - np.array(b))) <= tol, k

@@ -217,6 +217,28 @@ def test_step_kernel_variants_agree(built, variant):
     assert np.array_equal(ref[1], got[1]) and np.array_equal(ref[2], got[2])
 
 
+@pytest.mark.parametrize("precision", [FP64, MIXED])
+def test_rebuild_forms_and_search_paths_are_bit_identical(built, precision):
+    """The counting sort in one kernel (a block per rebuilt tissue) or in four,
+    and the candidate search by warps, groups of 4, 8 or 16 lanes or single
+    threads, emit the same candidate rows in the same order: the steps agree
+    bit for bit."""
+    ts = [T.mixed_state_tissue(), T.config1(3), T.layered_tissue(24, 3, 5)]
+    runs = []
+    for form, switch, lanes in ((1, 1 << 30, 8), (2, 1 << 30, 8), (1, 1, 1), (2, 1, 4),
+                                (1, 1, 8), (1, 1, 16)):
+        with capi.Context(precision=precision, max_conn=96, max_cand=192, rebuild_form=form,
+                          search_switch=switch, search_lanes=lanes) as ctx:
+            ctx.upload(ts)
+            ctx.step(30, "graph")
+            runs.append((ctx.positions(), ctx.connections(), ctx.dermis()))
+    for pos, (off, idx), der in runs[1:]:
+        for a, b in zip(runs[0][0], pos):
+            assert np.array_equal(a, b)
+        assert np.array_equal(runs[0][1][0], off) and np.array_equal(runs[0][1][1], idx)
+        assert np.array_equal(runs[0][2], der)
+
+
 def test_repeat_runs_are_deterministic(built):
     t = T.config2()
     a = run_gpu([t], 20, MIXED)
