@@ -64,12 +64,9 @@ struct Nvtx {
 
 // epi_step_host splits the batch into at most this many groups of tissues.
 constexpr int kHostStepGroups = 8;
-// Rebuilt particles from which the candidate search takes fewer lanes per
-// particle than a warp (epi_config.search_switch = 0), and how many
-// (epi_config.search_lanes = 0).
+// Rebuilt particles from which the candidate search takes one thread per
+// particle (epi_config.search_switch = 0).
 constexpr int kDefaultSearchSwitch = 48 * 1024;
-constexpr int kDefaultSearchLanes = 8;
-bool valid_lanes(int32_t v) { return v == 0 || v == 1 || v == 4 || v == 8 || v == 16; }
 
 // Host-side bookkeeping of one tissue in the batch.
 struct TissueHost {
@@ -363,19 +360,17 @@ void enqueue_step(epi_ctx* c, int& cur, Timer* tm) {
 void set_rebuild_form(epi_ctx* c) {
   int32_t nb_max = 0;
   for (const TissueDev& T : c->tissues_h) nb_max = std::max(nb_max, T.anx * T.any * T.anz);
-  c->lc.fused_rebuild = c->cfg.rebuild_form != 2 && nb_max <= kFusedRebuildMaxBins ? 1 : 0;
+  c->lc.fused_rebuild = c->cfg.rebuild_form == 1 && nb_max <= kFusedRebuildMaxBins ? 1 : 0;
 }
 
 // Skin, step-kernel variant, candidate-search switch and rebuild form of the
 // context; the captured graphs hold them, so they are dropped.
 void apply_tuning(epi_ctx* c, double skin, int32_t variant, int32_t search_switch,
-                  int32_t rebuild_form, int32_t search_lanes) {
+                  int32_t rebuild_form) {
   c->cfg.skin = skin;
   c->cfg.variant = variant;
   c->cfg.search_switch = search_switch;
   c->cfg.rebuild_form = rebuild_form;
-  c->cfg.search_lanes = search_lanes;
-  c->lc.search_lanes = search_lanes > 0 ? search_lanes : kDefaultSearchLanes;
   c->lc.variant = variant == 0 ? 3 : variant;
   c->lc.search_switch = search_switch > 0 ? search_switch : kDefaultSearchSwitch;
   set_rebuild_form(c);
@@ -691,7 +686,7 @@ void epi_config_default(epi_config* c) {
   c->variant = 0;
   c->search_switch = 0;
   c->rebuild_form = 0;
-  c->search_lanes = 0;
+  c->reserved = 0;
 }
 
 const char* epi_strerror(int s) {
@@ -728,7 +723,7 @@ int epi_create(epi_ctx** out, const epi_config* cfg) {
   if (c.variant < 0 || c.variant > 4) return EPI_ERR_INVALID_ARG;
   if (c.precision != EPI_PREC_FP64 && c.precision != EPI_PREC_MIXED) return EPI_ERR_INVALID_ARG;
   if (c.search_switch < 0 || c.rebuild_form < 0 || c.rebuild_form > 2) return EPI_ERR_INVALID_ARG;
-  if (!valid_lanes(c.search_lanes)) return EPI_ERR_INVALID_ARG;
+  if (c.reserved != 0) return EPI_ERR_INVALID_ARG;
   int ndev = 0;
   const cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev <= 0) return EPI_ERR_NO_DEVICE;
@@ -738,7 +733,6 @@ int epi_create(epi_ctx** out, const epi_config* cfg) {
   ctx->cfg = c;
   ctx->lc.variant = c.variant == 0 ? 3 : c.variant;
   ctx->lc.search_switch = c.search_switch > 0 ? c.search_switch : kDefaultSearchSwitch;
-  ctx->lc.search_lanes = c.search_lanes > 0 ? c.search_lanes : kDefaultSearchLanes;
   int sms = 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device) == cudaSuccess &&
       sms > 0)
@@ -1345,9 +1339,8 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
     c->lists_fresh = false;
     return EPI_OK;
   };
-  auto apply = [&](double skin, int32_t variant, int32_t search_switch, int32_t form,
-                   int32_t lanes) {
-    apply_tuning(c, skin, variant, search_switch, form, lanes);
+  auto apply = [&](double skin, int32_t variant, int32_t search_switch, int32_t form) {
+    apply_tuning(c, skin, variant, search_switch, form);
   };
   // one trial: ms per trial (INFINITY when the rows overflowed)
   auto trial = [&](double* ms_out) -> int {
@@ -1368,10 +1361,9 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
   double best = INFINITY, best_skin = c->cfg.skin;
   int32_t best_variant = c->cfg.variant;
   const int32_t switch0 = c->cfg.search_switch, form0 = c->cfg.rebuild_form;
-  const int32_t lanes0 = c->cfg.search_lanes;
   for (double skin : kSkins) {
     for (int32_t variant : kVariants) {
-      apply(skin, variant, switch0, form0, lanes0);
+      apply(skin, variant, switch0, form0);
       double ms;
       if ((rc = trial(&ms))) return rc;
       if (ms < best) {
@@ -1381,12 +1373,12 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
       }
     }
   }
-  // then the counting sort's form, the lanes per particle of large
-  // candidate searches and the switch to them
-  int32_t best_form = form0, best_switch = switch0, best_lanes = lanes0;
+  // then the counting sort's form and the candidate search's switch from a
+  // warp to a thread per particle
+  int32_t best_form = form0, best_switch = switch0;
   if (std::isfinite(best)) {
     for (int32_t form : {1, 2}) {
-      apply(best_skin, best_variant, switch0, form, lanes0);
+      apply(best_skin, best_variant, switch0, form);
       double ms;
       if ((rc = trial(&ms))) return rc;
       if (ms < best) {
@@ -1394,18 +1386,9 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
         best_form = form;
       }
     }
-    for (int32_t lanes : {1, 4, 8, 16}) {
-      apply(best_skin, best_variant, switch0, best_form, lanes);
-      double ms;
-      if ((rc = trial(&ms))) return rc;
-      if (ms < best) {
-        best = ms;
-        best_lanes = lanes;
-      }
-    }
     static const int32_t kSwitches[] = {8192, 16384, 49152, 131072};
     for (int32_t sw : kSwitches) {
-      apply(best_skin, best_variant, sw, best_form, best_lanes);
+      apply(best_skin, best_variant, sw, best_form);
       double ms;
       if ((rc = trial(&ms))) return rc;
       if (ms < best) {
@@ -1414,7 +1397,7 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
       }
     }
   }
-  apply(best_skin, best_variant, best_switch, best_form, best_lanes);
+  apply(best_skin, best_variant, best_switch, best_form);
   if ((rc = restore())) return rc;
   if ((rc = check_status(c))) return rc;
   if (skin_out) *skin_out = best_skin;
@@ -1431,15 +1414,15 @@ int epi_get_config(epi_ctx* c, epi_config* out) {
 }
 
 int epi_set_tuning(epi_ctx* c, double skin, int32_t variant, int32_t search_switch,
-                   int32_t rebuild_form, int32_t search_lanes) {
+                   int32_t rebuild_form) {
   if (!c || !(skin > 0) || skin > 2.0 || variant < 0 || variant > 4 || search_switch < 0 ||
-      rebuild_form < 0 || rebuild_form > 2 || !valid_lanes(search_lanes))
+      rebuild_form < 0 || rebuild_form > 2)
     return EPI_ERR_INVALID_ARG;
   EPI_GUARD_BEGIN
   Nvtx nvtx_range("epi_set_tuning");
   int rc = set_device(c);
   if (rc) return rc;
-  apply_tuning(c, skin, variant, search_switch, rebuild_form, search_lanes);
+  apply_tuning(c, skin, variant, search_switch, rebuild_form);
   if (c->loaded) {
     // candidates were built for the old skin: rebuild every tissue's
     launch_set_gates(make_state(c, c->cur), c->ntissues, c->stream);

@@ -628,13 +628,13 @@ __device__ __forceinline__ void finish_search(const DevState& S, int32_t i, int3
   S.bpos[i] = make_float4((float)p.x, (float)p.y, (float)p.z, 0.f);
 }
 
-// G lanes per particle (G = 32: one warp; 4, 8, 16: several particles per
-// warp). The group's lanes fetch the slot ranges of G bin columns at a time;
-// a scan within the group lays the ranges end to end, the group sweeps the
-// concatenation G slots at a time, and ballots keep the slot order, so every
-// G emits the same rows in the same order. With few gated particles G = 32
-// keeps the GPU busy; with many, smaller groups divide the divergence of
-// ragged windows among fewer lanes than whole warps do.
+// Few gated particles (a tissue or two): G = 32 lanes (one warp) per
+// particle, so the GPU has work for all its warps. The group's lanes fetch
+// the slot ranges of G bin columns at a time; a scan within the group lays
+// the ranges end to end, the group sweeps the concatenation G slots at a
+// time, and ballots keep the slot order. (Groups of 4 to 16 lanes emit the
+// same rows; they measured slower than one thread per particle for large
+// rebuilds, whose window set-up they repeat on every lane.)
 template <int G>
 __device__ __forceinline__ void cand_search_groups(const DevState& S, int32_t cnt,
                                                    int32_t ngated) {
@@ -793,22 +793,17 @@ __device__ __forceinline__ void cand_search_threads(const DevState& S, int32_t c
   }
 }
 
-// Below `large_from` gated particles the search takes a warp per particle
-// (which keeps the GPU busy with few particles), from there on `lanes`
-// lanes per particle (1: one thread, scanning its window alone). Every form
-// emits every row in the same order.
-__global__ void __launch_bounds__(256, 4) k_cand_search(DevState S, int32_t large_from,
-                                                        int32_t lanes) {
+// Below `thread_from` gated particles the warp-per-particle search (which
+// keeps the GPU busy with few particles) runs, from there on one thread per
+// particle. Both emit every row in the same order.
+__global__ void __launch_bounds__(256, 4) k_cand_search(DevState S, int32_t thread_from) {
   pdl_entry();
   count_launch(S.launches);
   const int32_t cnt = S.rl_count[0];
   if (blockIdx.x == 0) gate_clear(S, cnt);
   if (cnt == 0) return;
   const int32_t ngated = S.rl_ppre[cnt];
-  if (ngated < large_from) cand_search_groups<32>(S, cnt, ngated);
-  else if (lanes == 4) cand_search_groups<4>(S, cnt, ngated);
-  else if (lanes == 8) cand_search_groups<8>(S, cnt, ngated);
-  else if (lanes == 16) cand_search_groups<16>(S, cnt, ngated);
+  if (ngated < thread_from) cand_search_groups<32>(S, cnt, ngated);
   else cand_search_threads(S, cnt, ngated);
 }
 
@@ -1732,8 +1727,7 @@ void launch_rebuild(const DevState& S, const Range& r, const ScanScratch&,
     timer_end(tm, KC_REBUILD_SORT, s);
   }
   timer_begin(tm, KC_REBUILD_SEARCH, s);
-  launch_pdl(k_cand_search, grid, B, s, S, (int32_t)lc.search_switch,
-             (int32_t)lc.search_lanes);
+  launch_pdl(k_cand_search, grid, B, s, S, (int32_t)lc.search_switch);
   timer_end(tm, KC_REBUILD_SEARCH, s);
 }
 

@@ -24,8 +24,7 @@ struct LaunchCfg {
   int simple;       // batch holds only ALIVE / DEAD / AIR / MEMB, no pairs
   int any_old;      // some cell is older than THRESH_SP
   int variant;      // step-kernel instantiation (pipeline depth / residency), see epi_config
-  int search_switch;  // rebuilt particles from which the search takes search_lanes per particle
-  int search_lanes = 8;  // lanes per particle of large rebuilds' search (1, 4, 8, 16)
+  int search_switch;  // rebuilt particles from which the search takes a thread per particle
   int fused_rebuild = 0;  // every tissue has at most 16,384 bins: one counting-sort kernel
 };
 // Bins a tissue may have for the one-kernel counting sort (k_rebuild_tissue).

@@ -131,18 +131,13 @@ typedef struct epi_config {
                          multiply-adds differently, so results agree to
                          rounding. */
   int32_t search_switch; /* candidate search: rebuilds of at least this many
-                         particles take search_lanes lanes per particle,
-                         smaller ones one warp per particle; 0 = default
-                         (49152) */
+                         particles take one thread per particle, smaller ones
+                         one warp per particle; 0 = default (49152) */
   int32_t rebuild_form; /* counting sort of a candidate rebuild: 0 = default
-                         (1 when every tissue has at most 16,384 grid bins,
-                         else 2); 1 = one kernel, one block per rebuilt tissue
-                         (tissues with more bins take 2); 2 = four kernels
-                         over all rebuilt particles */
-  int32_t search_lanes; /* lanes per particle of the candidate search for
-                         rebuilds from search_switch on: 0 = default (8); 1
-                         (a thread scans its particle's window alone), 4, 8 or
-                         16 */
+                         (2); 1 = one kernel, one block per rebuilt tissue
+                         (when every tissue has at most 16,384 grid bins, else
+                         2); 2 = four kernels over all rebuilt particles */
+  int32_t reserved;   /* must be 0 */
 } epi_config;
 
 typedef struct epi_ctx epi_ctx;
@@ -234,9 +229,9 @@ int epi_time_kernels(epi_ctx* ctx, int32_t nsteps, int32_t max_classes, double* 
  * every candidate skin in {0.05, 0.08, 0.1, 0.15, 0.2, 0.3} and step-kernel
  * variant 1..4 (4 warm-up steps, then trial_steps timed with CUDA events),
  * then, for the fastest pair, the counting sort's form (one kernel or
- * four), the lanes per particle of large searches (1, 4, 8, 16) and the
- * switch to them in {8192, 16384, 49152, 131072} rebuilt particles, and
- * keeps the fastest choice in the context's configuration. Skins whose candidate rows would overflow
+ * four) and the candidate search's switch from a warp to a thread per
+ * particle in {8192, 16384, 49152, 131072} rebuilt particles, and keeps the
+ * fastest choice in the context's configuration. Skins whose candidate rows would overflow
  * max_cand are skipped. The simulation state is left as it was (positions
  * are restored after every trial), and no choice changes results beyond
  * multiply-add rounding (connection sets are exact for every skin, and both
@@ -251,11 +246,11 @@ int epi_autotune(epi_ctx* ctx, int32_t trial_steps, double* skin, int32_t* varia
 int epi_get_config(epi_ctx* ctx, epi_config* out);
 
 /* Applies a tuning chosen earlier (for instance a cached epi_autotune
- * result for the same batch shape): skin, variant, search switch, rebuild
- * form and search lanes, with epi_config's ranges. Every tissue's candidates are rebuilt before the
+ * result for the same batch shape): skin, variant, search switch and
+ * rebuild form, with epi_config's ranges. Every tissue's candidates are rebuilt before the
  * next step. No counterpart in the reference. */
 int epi_set_tuning(epi_ctx* ctx, double skin, int32_t variant, int32_t search_switch,
-                   int32_t rebuild_form, int32_t search_lanes);
+                   int32_t rebuild_form);
 
 /* ---- cell maps and external-stimulus diffusion -----------------------------
  * The rest of the reference's per-step loop before its chemistry

@@ -62,14 +62,14 @@ def test_create_rejects_bad_arguments(built):
     assert L.epi_create(ctypes.byref(h), ctypes.byref(cfg)) == capi.EPI_ERR_INVALID_ARG
     cfg = capi.ConfigC(0, 1, 64, 96, 0.1, 0, 0, 3, 0)  # unknown rebuild form
     assert L.epi_create(ctypes.byref(h), ctypes.byref(cfg)) == capi.EPI_ERR_INVALID_ARG
-    cfg = capi.ConfigC(0, 1, 64, 96, 0.1, 0, 0, 0, 5)  # 5 lanes per particle
+    cfg = capi.ConfigC(0, 1, 64, 96, 0.1, 0, 0, 0, 5)  # reserved must be 0
     assert L.epi_create(ctypes.byref(h), ctypes.byref(cfg)) == capi.EPI_ERR_INVALID_ARG
     cfg = capi.ConfigC(0, 1, 500, 600, 0.1, 0, 0, 0, 0)  # beyond the reference's 400 connections
     assert L.epi_create(ctypes.byref(h), ctypes.byref(cfg)) == capi.EPI_ERR_INVALID_ARG
     assert L.epi_step(None, 1) == capi.EPI_ERR_INVALID_ARG
     assert L.epi_sync(None) == capi.EPI_ERR_INVALID_ARG
     assert L.epi_get_config(None, ctypes.byref(cfg)) == capi.EPI_ERR_INVALID_ARG
-    assert L.epi_set_tuning(None, 0.1, 3, 0, 0, 0) == capi.EPI_ERR_INVALID_ARG
+    assert L.epi_set_tuning(None, 0.1, 3, 0, 0) == capi.EPI_ERR_INVALID_ARG
 
 
 def _has_gpu():

@@ -220,15 +220,13 @@ def test_step_kernel_variants_agree(built, variant):
 @pytest.mark.parametrize("precision", [FP64, MIXED])
 def test_rebuild_forms_and_search_paths_are_bit_identical(built, precision):
     """The counting sort in one kernel (a block per rebuilt tissue) or in four,
-    and the candidate search by warps, groups of 4, 8 or 16 lanes or single
-    threads, emit the same candidate rows in the same order: the steps agree
-    bit for bit."""
+    and the candidate search by warps or by threads, emit the same candidate
+    rows in the same order: the steps agree bit for bit."""
     ts = [T.mixed_state_tissue(), T.config1(3), T.layered_tissue(24, 3, 5)]
     runs = []
-    for form, switch, lanes in ((1, 1 << 30, 8), (2, 1 << 30, 8), (1, 1, 1), (2, 1, 4),
-                                (1, 1, 8), (1, 1, 16)):
+    for form, switch in ((1, 1 << 30), (2, 1 << 30), (1, 1), (2, 1)):
         with capi.Context(precision=precision, max_conn=96, max_cand=192, rebuild_form=form,
-                          search_switch=switch, search_lanes=lanes) as ctx:
+                          search_switch=switch) as ctx:
             ctx.upload(ts)
             ctx.step(30, "graph")
             runs.append((ctx.positions(), ctx.connections(), ctx.dermis()))
