@@ -134,6 +134,11 @@ struct epi_ctx {
   DevStatus* status = nullptr;
   DevStatus* status_h = nullptr;  // pinned
   unsigned long long* rebuilds = nullptr;
+  // adaptive skin: per-tissue skin, last rebuild step, largest row; step count
+  float* tskin = nullptr;
+  int32_t* tlast = nullptr;
+  int32_t* tcmax = nullptr;
+  int32_t* stepno = nullptr;
   int32_t* loop_left = nullptr;  // passes left in the step graph's device loop
   unsigned long long* launches = nullptr;  // step-sequence kernels executed
   ScanScratch scan{};
@@ -220,12 +225,14 @@ void free_buffers(epi_ctx* c) {
   if (c->agek) cudaFree(c->agek);
   c->agek = nullptr;
   void* ptrs[] = {c->tissues, c->pos[0], c->pos[1], c->posf[0], c->posf[1], c->attr, c->pair, c->spr, c->dermis,
+                  c->tskin, c->tlast, c->tcmax, c->stepno,
                   c->cand, c->bpos, c->nbr, c->nn, c->fmemb, c->bin,
                   c->rank, c->counts, c->starts, c->skey, c->spos, c->gate, c->rl, c->prep,
                   c->scan.partial, c->stage, c->stage_out};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   c->tissues = nullptr;
+  c->tskin = nullptr; c->tlast = nullptr; c->tcmax = nullptr; c->stepno = nullptr;
   c->pos[0] = c->pos[1] = nullptr;
   c->posf[0] = c->posf[1] = nullptr;
   c->attr = nullptr; c->pair = nullptr; c->spr = nullptr; c->dermis = nullptr;
@@ -272,6 +279,11 @@ DevState make_state(epi_ctx* c, int cur) {
   S.nprep_memb = c->nprep_memb;
   S.status = c->status;
   S.rebuilds = c->rebuilds;
+  S.tskin = c->tskin;
+  S.tlast = c->tlast;
+  S.tcmax = c->tcmax;
+  S.stepno = c->stepno;
+  S.adapt_skin = c->cfg.adapt_skin;
   S.launches = c->launches;
   S.n_total = c->n;
   S.max_conn = c->cfg.max_conn;
@@ -354,26 +366,46 @@ void enqueue_step(epi_ctx* c, int& cur, Timer* tm) {
   cur ^= 1;
 }
 
-// The counting sort's form for the batch: one kernel (a block per tissue)
-// when the configuration allows it and every tissue's bins fit its shared
-// memory.
-void set_rebuild_form(epi_ctx* c) {
-  int32_t nb_max = 0;
-  for (const TissueDev& T : c->tissues_h) nb_max = std::max(nb_max, T.anx * T.any * T.anz);
-  c->lc.fused_rebuild = c->cfg.rebuild_form == 1 && nb_max <= kFusedRebuildMaxBins ? 1 : 0;
+// Every tissue's skin to the configured one, no rebuild yet (its first one
+// keeps the configured skin), the step count to 0.
+cudaError_t reset_skins(epi_ctx* c) {
+  if (!c->tskin) return cudaSuccess;
+  const std::vector<float> sk((size_t)c->ntissues, (float)c->cfg.skin);
+  const std::vector<int32_t> never((size_t)c->ntissues, -(1 << 30));
+  cudaError_t e = cudaMemcpyAsync(c->tskin, sk.data(), sizeof(float) * sk.size(),
+                                  cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(c->tlast, never.data(), sizeof(int32_t) * never.size(),
+                        cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->tcmax, 0, sizeof(int32_t) * c->ntissues, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->stepno, 0, sizeof(int32_t), c->stream);
+  // the host vector must outlive the copy
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  return e;
 }
 
-// Skin, step-kernel variant, candidate-search switch and rebuild form of the
-// context; the captured graphs hold them, so they are dropped.
+// Whether the step graph puts the candidate rebuild in a conditional node
+// that skips its kernels on steps with nothing to rebuild: by default for a
+// single tissue (most of its steps rebuild nothing), not for a batch (some
+// tissue rebuilds at almost every step, and the node costs more than the
+// kernels' early exit).
+bool conditional_rebuild(const epi_ctx* c) {
+  return c->cfg.rebuild_gate == 1 || (c->cfg.rebuild_gate == 0 && c->ntissues == 1);
+}
+
+// Skin, step-kernel variant, candidate-search switch, rebuild node and
+// adaptive skin of the context; the captured graphs hold them, so they are
+// dropped.
 void apply_tuning(epi_ctx* c, double skin, int32_t variant, int32_t search_switch,
-                  int32_t rebuild_form) {
+                  int32_t rebuild_gate, int32_t adapt_skin) {
   c->cfg.skin = skin;
   c->cfg.variant = variant;
   c->cfg.search_switch = search_switch;
-  c->cfg.rebuild_form = rebuild_form;
+  c->cfg.rebuild_gate = rebuild_gate;
+  c->cfg.adapt_skin = adapt_skin;
+  (void)reset_skins(c);
   c->lc.variant = variant == 0 ? 3 : variant;
   c->lc.search_switch = search_switch > 0 ? search_switch : kDefaultSearchSwitch;
-  set_rebuild_form(c);
   destroy_graphs(c);
 }
 
@@ -440,7 +472,12 @@ cudaError_t capture_step_graph(epi_ctx* c, cudaGraphExec_t* out) {
       int cur = c->cur;
       for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
         e = fork_memb(c, cur, nullptr);
-        if (e == cudaSuccess) e = capture_conditional_rebuild(c, cur);
+        if (e == cudaSuccess) {
+          if (conditional_rebuild(c))
+            e = capture_conditional_rebuild(c, cur);
+          else
+            launch_rebuild(make_state(c, cur), whole(c), c->scan, c->lc, c->stream, nullptr);
+        }
         if (e != cudaSuccess) break;
         dermis_all(c, cur, nullptr);
         if ((e = join_memb(c)) != cudaSuccess) break;
@@ -685,7 +722,8 @@ void epi_config_default(epi_config* c) {
   c->skin = 0.1;
   c->variant = 0;
   c->search_switch = 0;
-  c->rebuild_form = 0;
+  c->rebuild_gate = 0;
+  c->adapt_skin = 1;
   c->reserved = 0;
 }
 
@@ -722,8 +760,9 @@ int epi_create(epi_ctx** out, const epi_config* cfg) {
   if (!(c.skin > 0) || c.skin > 2.0) return EPI_ERR_INVALID_ARG;
   if (c.variant < 0 || c.variant > 4) return EPI_ERR_INVALID_ARG;
   if (c.precision != EPI_PREC_FP64 && c.precision != EPI_PREC_MIXED) return EPI_ERR_INVALID_ARG;
-  if (c.search_switch < 0 || c.rebuild_form < 0 || c.rebuild_form > 2) return EPI_ERR_INVALID_ARG;
+  if (c.search_switch < 0 || c.rebuild_gate < 0 || c.rebuild_gate > 2) return EPI_ERR_INVALID_ARG;
   if (c.reserved != 0) return EPI_ERR_INVALID_ARG;
+  if (c.adapt_skin != 0 && c.adapt_skin != 1) return EPI_ERR_INVALID_ARG;
   int ndev = 0;
   const cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev <= 0) return EPI_ERR_NO_DEVICE;
@@ -939,7 +978,6 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
     binbase += T.anx * T.any * T.anz + 1;  // + sentinel (end offset of the tissue)
   }
   c->lc.simple = simple ? 1 : 0;
-  set_rebuild_form(c);
   c->lc.any_old = any_old ? 1 : 0;
   c->nprep_memb = (int32_t)prep_m.size();
   c->nprep = c->nprep_memb + (int32_t)prep_f.size();
@@ -967,6 +1005,8 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
       (rc = dev_alloc(&c->skey, n)) || (rc = dev_alloc(&c->spos, n)) ||
       (rc = dev_alloc(&c->gate, (size_t)ntissues + 1)) ||
       (rc = dev_alloc(&c->rl, 3 + 3 * (size_t)ntissues)) ||
+      (rc = dev_alloc(&c->tskin, ntissues)) || (rc = dev_alloc(&c->tlast, ntissues)) ||
+      (rc = dev_alloc(&c->tcmax, ntissues)) || (rc = dev_alloc(&c->stepno, 1)) ||
       (rc = dev_alloc(&c->prep, prep.size())) || (rc = dev_alloc(&c->stage, 3 * (size_t)n)) ||
       (rc = dev_alloc(&c->agek, n)))) {
     free_buffers(c);
@@ -1028,6 +1068,9 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
     EPI_CUDA(cudaMemsetAsync(c->dermis, 0xff, sizeof(int32_t) * n, s));
   }
   EPI_CUDA(cudaMemsetAsync(c->status, 0, sizeof(DevStatus), s));
+  // adaptive skin: a new batch starts every tissue at the configured skin (a
+  // same-shape re-upload keeps what the tissues adapted to)
+  if (!reuse) EPI_CUDA(reset_skins(c));
   c->cur = 0;
   c->loaded = true;
   if (gates.empty()) {
@@ -1339,8 +1382,9 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
     c->lists_fresh = false;
     return EPI_OK;
   };
-  auto apply = [&](double skin, int32_t variant, int32_t search_switch, int32_t form) {
-    apply_tuning(c, skin, variant, search_switch, form);
+  auto apply = [&](double skin, int32_t variant, int32_t search_switch, int32_t form,
+                   int32_t adapt) {
+    apply_tuning(c, skin, variant, search_switch, form, adapt);
   };
   // one trial: ms per trial (INFINITY when the rows overflowed)
   auto trial = [&](double* ms_out) -> int {
@@ -1360,10 +1404,11 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
   };
   double best = INFINITY, best_skin = c->cfg.skin;
   int32_t best_variant = c->cfg.variant;
-  const int32_t switch0 = c->cfg.search_switch, form0 = c->cfg.rebuild_form;
+  const int32_t switch0 = c->cfg.search_switch, form0 = c->cfg.rebuild_gate;
+  const int32_t adapt0 = c->cfg.adapt_skin;
   for (double skin : kSkins) {
     for (int32_t variant : kVariants) {
-      apply(skin, variant, switch0, form0);
+      apply(skin, variant, switch0, form0, adapt0);
       double ms;
       if ((rc = trial(&ms))) return rc;
       if (ms < best) {
@@ -1373,12 +1418,22 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
       }
     }
   }
-  // then the counting sort's form and the candidate search's switch from a
-  // warp to a thread per particle
-  int32_t best_form = form0, best_switch = switch0;
+  // then adaptive or fixed skins, the rebuild in a conditional graph node or
+  // not, and the candidate search's switch from a warp to a thread per
+  // particle
+  int32_t best_form = form0, best_switch = switch0, best_adapt = adapt0;
   if (std::isfinite(best)) {
+    for (int32_t adapt : {0, 1}) {
+      apply(best_skin, best_variant, switch0, form0, adapt);
+      double ms;
+      if ((rc = trial(&ms))) return rc;
+      if (ms < best) {
+        best = ms;
+        best_adapt = adapt;
+      }
+    }
     for (int32_t form : {1, 2}) {
-      apply(best_skin, best_variant, switch0, form);
+      apply(best_skin, best_variant, switch0, form, best_adapt);
       double ms;
       if ((rc = trial(&ms))) return rc;
       if (ms < best) {
@@ -1388,7 +1443,7 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
     }
     static const int32_t kSwitches[] = {8192, 16384, 49152, 131072};
     for (int32_t sw : kSwitches) {
-      apply(best_skin, best_variant, sw, best_form);
+      apply(best_skin, best_variant, sw, best_form, best_adapt);
       double ms;
       if ((rc = trial(&ms))) return rc;
       if (ms < best) {
@@ -1397,7 +1452,7 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
       }
     }
   }
-  apply(best_skin, best_variant, best_switch, best_form);
+  apply(best_skin, best_variant, best_switch, best_form, best_adapt);
   if ((rc = restore())) return rc;
   if ((rc = check_status(c))) return rc;
   if (skin_out) *skin_out = best_skin;
@@ -1414,15 +1469,15 @@ int epi_get_config(epi_ctx* c, epi_config* out) {
 }
 
 int epi_set_tuning(epi_ctx* c, double skin, int32_t variant, int32_t search_switch,
-                   int32_t rebuild_form) {
+                   int32_t rebuild_gate, int32_t adapt_skin) {
   if (!c || !(skin > 0) || skin > 2.0 || variant < 0 || variant > 4 || search_switch < 0 ||
-      rebuild_form < 0 || rebuild_form > 2)
+      rebuild_gate < 0 || rebuild_gate > 2 || (adapt_skin != 0 && adapt_skin != 1))
     return EPI_ERR_INVALID_ARG;
   EPI_GUARD_BEGIN
   Nvtx nvtx_range("epi_set_tuning");
   int rc = set_device(c);
   if (rc) return rc;
-  apply_tuning(c, skin, variant, search_switch, rebuild_form);
+  apply_tuning(c, skin, variant, search_switch, rebuild_gate, adapt_skin);
   if (c->loaded) {
     // candidates were built for the old skin: rebuild every tissue's
     launch_set_gates(make_state(c, c->cur), c->ntissues, c->stream);

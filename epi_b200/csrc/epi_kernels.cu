@@ -180,8 +180,38 @@ __device__ __forceinline__ int32_t ref_bin(const TissueDev& T, double x, double 
 // ---------------------------------------------------------------------------
 // For the whole batch the "some tissue" word is cleared once the list is
 // built: the step kernel sets it again for the next step.
+// Adaptive skin (when S.adapt_skin): at its rebuild, a tissue that rebuilt
+// fewer than kSkinGrowBelow steps before takes a skin 1.5 times wider (up to
+// kSkinMaxFactor times the configured one, and only while its largest
+// candidate row stays below half the row capacity); one that went more than
+// kSkinShrinkAbove steps without a rebuild returns towards the configured
+// skin. Wider skins cost candidates per step and save rebuilds; the
+// connections, and the order of the connected pairs in a row, do not depend
+// on the skin, so results are the same.
+constexpr int32_t kSkinGrowBelow = 16, kSkinShrinkAbove = 128;
+constexpr float kSkinMaxFactor = 3.f;
+
+__device__ __forceinline__ void adapt_skin_of(const DevState& S, int32_t t, int32_t step) {
+  const int32_t interval = step - S.tlast[t];
+  float sk = S.tskin[t];
+  const float base = (float)S.skin;
+  if (interval < kSkinGrowBelow && 2 * S.tcmax[t] <= S.max_cand)
+    sk = fminf(sk * 1.5f, kSkinMaxFactor * base);
+  else if (interval > kSkinShrinkAbove)
+    sk = fmaxf(sk / 1.5f, base);
+  S.tskin[t] = sk;
+  S.tlast[t] = step;
+  S.tcmax[t] = 0;
+}
+
 __device__ __forceinline__ void gate_compact(const DevState& S, int32_t t0, int32_t t1) {
   const bool whole = t0 == 0 && t1 == S.ntissues;
+  // one count per step: the call for the batch's first tissues
+  const int32_t step = S.stepno[0] + 1;
+  if (t0 == 0) {
+    __syncthreads();  // every thread has read the count
+    if (threadIdx.x == 0) S.stepno[0] = step;
+  }
   if (S.gate[0] == 0) {
     if (threadIdx.x == 0) {
       S.rl_count[0] = 0;
@@ -201,6 +231,7 @@ __device__ __forceinline__ void gate_compact(const DevState& S, int32_t t0, int3
       const TissueDev& T = S.tissues[t];
       np = T.n;
       nb = T.anx * T.any * T.anz;
+      if (S.adapt_skin) adapt_skin_of(S, t, step);
     }
     int32_t tc, tp, tb;
     const int32_t oc = block_excl_scan(g ? 1 : 0, &tc);
@@ -413,105 +444,6 @@ __global__ void k_binsort(DevState S) {
   }
 }
 
-// The counting sort of one gated tissue per block, all in one kernel:
-// binning with the bin counts in shared memory (ranks from shared-memory
-// atomics), the scan of the counts into bin offsets, the scatter into
-// sorted order and the per-bin sort, separated by block barriers. It
-// replaces k_bin, k_scan_tissue, k_scatter and k_binsort (four launches and
-// their grid-wide dependencies) when every tissue of the batch has at most
-// kFusedMaxBins bins. The tissue's particles are binned four at a time so
-// their position loads overlap.
-constexpr int kFusedThreads = 1024;
-constexpr int32_t kFusedMaxBins = kFusedRebuildMaxBins;  // 64 KB of counts in shared memory
-
-__global__ void __launch_bounds__(kFusedThreads) k_rebuild_tissue(DevState S) {
-  pdl_entry();
-  count_launch(S.launches);
-  extern __shared__ int32_t s_cnt[];  // bin counts, then offsets; nb + 1 entries
-  const int32_t cnt = S.rl_count[0];
-  for (int32_t k = blockIdx.x; k < cnt; k += gridDim.x) {
-    const TissueDev& T = S.tissues[S.rl_list[k]];
-    const int32_t nb = T.anx * T.any * T.anz;
-    for (int32_t b = threadIdx.x; b <= nb; b += blockDim.x) s_cnt[b] = 0;
-    __syncthreads();
-    // grid_init (cell_connection.cpp:38-62): the bin of every particle
-    for (int32_t j0 = 0; j0 < T.n; j0 += 4 * kFusedThreads) {
-      double4 p[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int32_t j = j0 + u * kFusedThreads + (int32_t)threadIdx.x;
-        if (j < T.n) p[u] = S.pos_cur[T.pbase + j];
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int32_t j = j0 + u * kFusedThreads + (int32_t)threadIdx.x;
-        if (j >= T.n) continue;
-        const int32_t i = T.pbase + j;
-        int32_t lb = -1;
-        if (!isfinite(p[u].x) || !isfinite(p[u].y) || !isfinite(p[u].z)) {
-          raise_error(S.status, E_NONFINITE, i, -1, p[u].x);
-        } else {
-          lb = ref_bin(T, p[u].x, p[u].y, p[u].z, attr_state(S.attr[i]) == ST_MEMB);
-          if (lb < 0) raise_error(S.status, E_BIN_RANGE, i, -1, p[u].z);
-        }
-        S.bin[i] = lb;
-        if (lb >= 0) {
-          const int32_t rk = atomicAdd(&s_cnt[lb], 1);
-          if (rk + 1 >= kBinCap)
-            raise_error(S.status, E_BIN_OVERFLOW, i, T.binbase + lb, (double)(rk + 1));
-          S.rank[i] = rk;
-        }
-      }
-    }
-    __syncthreads();
-    // bin offsets: exclusive scan of the counts, offset by the tissue's first
-    // particle; entry nb is the tissue's end
-    int32_t carry = T.pbase;
-    constexpr int32_t kTile = kFusedThreads * kScanItems;
-    for (int32_t base = 0; base < nb; base += kTile) {
-      const int32_t b0 = base + (int32_t)threadIdx.x * kScanItems;
-      int32_t v[kScanItems];
-      int32_t sum = 0;
-#pragma unroll
-      for (int q = 0; q < kScanItems; ++q) {
-        v[q] = b0 + q < nb ? s_cnt[b0 + q] : 0;
-        sum += v[q];
-      }
-      int32_t tot;
-      int32_t run = carry + block_excl_scan_n<kFusedThreads>(sum, &tot);
-#pragma unroll
-      for (int q = 0; q < kScanItems; ++q) {
-        if (b0 + q < nb) {
-          s_cnt[b0 + q] = run;
-          S.starts[T.binbase + b0 + q] = run;
-        }
-        run += v[q];
-      }
-      carry += tot;
-    }
-    if (threadIdx.x == 0) {
-      s_cnt[nb] = carry;
-      S.starts[T.binbase + nb] = carry;
-    }
-    __syncthreads();
-    // scatter into bin order
-    for (int32_t j = threadIdx.x; j < T.n; j += blockDim.x) {
-      const int32_t i = T.pbase + j;
-      const int32_t lb = S.bin[i];
-      if (lb < 0) continue;
-      const int32_t slot = s_cnt[lb] + S.rank[i];
-      if (!EPI_CHECKED(slot >= T.pbase && slot < T.pbase + T.n, S.status, i, slot)) continue;
-      S.skey[slot] = (uint32_t)i;
-    }
-    __syncthreads();
-    for (int32_t b = threadIdx.x; b < nb; b += blockDim.x) {
-      const int32_t s0 = s_cnt[b], s1 = s_cnt[b + 1];
-      if (s1 > s0) sort_bin(S, T, s0, s1);
-    }
-    __syncthreads();
-  }
-}
-
 // Bin ranges (inclusive) of the periodic window [x-R, x+R] along one axis:
 // at most two ranges, because the window may wrap once. Bin k holds
 // [k*AG, (k+1)*AG) of [0, L) (the last one is shortened; AG*AN > L).
@@ -575,7 +507,7 @@ struct SearchWindow {
     memb_i = attr_state(S.attr[i]) == ST_MEMB;
     const double4 p = S.pos_cur[i];
     const double lt = T.P.lj_thresh;
-    const double skin = S.skin;
+    const double skin = skin_of(S, attr_tissue(S.attr[i]));
     // Candidates are compared in float: the margin covers the rounding of
     // float coordinates up to the box size (and the window widens with it).
     const double margin = 1e-4 + 5e-7 * (T.lx > T.ly ? T.lx : T.ly) + 5e-7 * T.lz;
@@ -624,6 +556,7 @@ __device__ __forceinline__ void finish_search(const DevState& S, int32_t i, int3
   const int32_t cap = S.max_cand;
   if (count > cap) raise_error(S.status, E_LIST_OVERFLOW, i, -1, (double)count);
   cand_set(S, i, 0, (uint32_t)(count < cap ? count : cap));
+  if (S.adapt_skin) atomicMax(&S.tcmax[attr_tissue(S.attr[i])], count);
   const double4 p = S.pos_cur[i];
   S.bpos[i] = make_float4((float)p.x, (float)p.y, (float)p.z, 0.f);
 }
@@ -1339,7 +1272,7 @@ struct Particle {
     if (ey > hly) ey -= ly;
     else if (ey < -hly) ey += ly;
     const double ez = nz - (double)b.z;
-    const double lim = 0.5 * S.skin - 1e-3;  // margin covers the float rounding of bpos
+    const double lim = 0.5 * skin_of(S, t) - 1e-3;  // margin covers the float rounding of bpos
     if (!(ex * ex + ey * ey + ez * ez <= lim * lim)) {
       S.gate[1 + t] = 1;
       S.gate[0] = 1;
@@ -1638,7 +1571,7 @@ __global__ void k_pack_gate(DevState S, const double* x, const double* y, const 
     if (ey > T.hly) ey -= T.ly;
     else if (ey < -T.hly) ey += T.ly;
     const double ez = p.z - (double)b.z;
-    const double lim = 0.5 * S.skin - 1e-3;
+    const double lim = 0.5 * skin_of(S, t) - 1e-3;
     if (!(ex * ex + ey * ey + ez * ez <= lim * lim)) {
       S.gate[1 + t] = 1;
       S.gate[0] = 1;
@@ -1691,41 +1624,18 @@ void launch_rebuild(const DevState& S, const Range& r, const ScanScratch&,
     launch_pdl(k_gate_compact, 1, kScanThreads, s, S, r.t0, r.t1);
     timer_end(tm, KC_GATE, s);
   }
+  timer_begin(tm, KC_REBUILD_BIN, s);
+  launch_pdl(k_bin, grid, B, s, S);
+  timer_end(tm, KC_REBUILD_BIN, s);
+  timer_begin(tm, KC_REBUILD_SCAN, s);
   const int nt = r.t1 - r.t0;
-  if (lc.fused_rebuild) {
-    // one block per gated tissue: bin, scan, scatter and sort in one launch
-    static bool configured = false;
-    constexpr int smem = (kFusedMaxBins + 1) * (int)sizeof(int32_t);
-    if (!configured) {
-      cudaFuncSetAttribute(k_rebuild_tissue, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-      configured = true;
-    }
-    timer_begin(tm, KC_REBUILD_BIN, s);
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3((unsigned)(nt < lc.num_sms ? (nt > 0 ? nt : 1) : lc.num_sms));
-    cfg.blockDim = dim3((unsigned)kFusedThreads);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_rebuild_tissue, S);
-    timer_end(tm, KC_REBUILD_BIN, s);
-  } else {
-    timer_begin(tm, KC_REBUILD_BIN, s);
-    launch_pdl(k_bin, grid, B, s, S);
-    timer_end(tm, KC_REBUILD_BIN, s);
-    timer_begin(tm, KC_REBUILD_SCAN, s);
-    launch_pdl(k_scan_tissue, nt < lc.num_sms * 4 ? (nt > 0 ? nt : 1) : lc.num_sms * 4,
-               kTissueScanThreads, s, S);
-    timer_end(tm, KC_REBUILD_SCAN, s);
-    timer_begin(tm, KC_REBUILD_SORT, s);
-    launch_pdl(k_scatter, grid, B, s, S);
-    launch_pdl(k_binsort, grid, B, s, S);
-    timer_end(tm, KC_REBUILD_SORT, s);
-  }
+  launch_pdl(k_scan_tissue, nt < lc.num_sms * 4 ? (nt > 0 ? nt : 1) : lc.num_sms * 4,
+             kTissueScanThreads, s, S);
+  timer_end(tm, KC_REBUILD_SCAN, s);
+  timer_begin(tm, KC_REBUILD_SORT, s);
+  launch_pdl(k_scatter, grid, B, s, S);
+  launch_pdl(k_binsort, grid, B, s, S);
+  timer_end(tm, KC_REBUILD_SORT, s);
   timer_begin(tm, KC_REBUILD_SEARCH, s);
   launch_pdl(k_cand_search, grid, B, s, S, (int32_t)lc.search_switch);
   timer_end(tm, KC_REBUILD_SEARCH, s);

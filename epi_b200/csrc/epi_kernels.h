@@ -25,10 +25,7 @@ struct LaunchCfg {
   int any_old;      // some cell is older than THRESH_SP
   int variant;      // step-kernel instantiation (pipeline depth / residency), see epi_config
   int search_switch;  // rebuilt particles from which the search takes a thread per particle
-  int fused_rebuild = 0;  // every tissue has at most 16,384 bins: one counting-sort kernel
 };
-// Bins a tissue may have for the one-kernel counting sort (k_rebuild_tissue).
-constexpr int32_t kFusedRebuildMaxBins = 16384;
 
 // Kernel classes, for per-class timing.
 enum KernelClass : int {
