@@ -48,19 +48,19 @@ def tuned(ctx, tissues: Sequence, trial_steps: int = 128, cache: Optional[Path] 
           device: int = 0, retune: bool = False) -> dict:
     """Applies the cached choice for this batch shape to ctx, or runs
     epi_autotune and stores its choice. Returns {skin, variant,
-    search_switch, rebuild_gate, adapt_skin, trial_ms_per_step, cached}."""
+    search_switch, rebuild_gate, trial_ms_per_step, cached}."""
     path = Path(cache or os.environ.get("EPI_AUTOTUNE_CACHE", DEFAULT_CACHE))
     key = shape_key(tissues, ctx.precision, gpu_name(device))
     db = _load(path)
     hit = db.get(key)
     if hit and not retune:
         ctx.set_tuning(hit["skin"], hit["variant"], hit["search_switch"],
-                       hit.get("rebuild_gate", 0), hit.get("adapt_skin", 1))
+                       hit.get("rebuild_gate", 0))
         return dict(hit, cached=True)
     skin, variant, ms = ctx.autotune(trial_steps)
     cfg = ctx.config()
     rec = {"skin": skin, "variant": variant, "search_switch": int(cfg["search_switch"]),
-           "rebuild_gate": int(cfg["rebuild_gate"]), "adapt_skin": int(cfg["adapt_skin"]),
+           "rebuild_gate": int(cfg["rebuild_gate"]),
            "trial_ms_per_step": ms, "trial_steps": trial_steps}
     db[key] = rec
     try:

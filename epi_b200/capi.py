@@ -95,7 +95,7 @@ class ConfigC(ctypes.Structure):
                 ("max_conn", ctypes.c_int32), ("max_cand", ctypes.c_int32),
                 ("skin", ctypes.c_double), ("variant", ctypes.c_int32),
                 ("search_switch", ctypes.c_int32), ("rebuild_gate", ctypes.c_int32),
-                ("adapt_skin", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("reserved", ctypes.c_int32)]
 
 
 _lib = None
@@ -142,7 +142,7 @@ def lib():
         L.epi_autotune.argtypes = [vp, ctypes.c_int32, _dp, _ip, _dp]
         L.epi_get_config.argtypes = [vp, ctypes.POINTER(ConfigC)]
         L.epi_set_tuning.argtypes = [vp, ctypes.c_double, ctypes.c_int32, ctypes.c_int32,
-                                     ctypes.c_int32, ctypes.c_int32]
+                                     ctypes.c_int32]
         L.epi_field_init.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
         L.epi_field_step.argtypes = [vp, ctypes.c_int32]
         L.epi_field_get.argtypes = [vp, ctypes.c_int32, _ip, _up, _dp, _dp]
@@ -185,7 +185,7 @@ class Context:
     def __init__(self, precision: int = EPI_PREC_MIXED, max_conn: int = 64, device: int = 0,
                  max_cand: Optional[int] = None, skin: Optional[float] = None,
                  variant: Optional[int] = None, rebuild_gate: Optional[int] = None,
-                 search_switch: Optional[int] = None, adapt_skin: Optional[int] = None):
+                 search_switch: Optional[int] = None):
         L = lib()
         cfg = ConfigC()
         L.epi_config_default(ctypes.byref(cfg))
@@ -200,8 +200,6 @@ class Context:
             cfg.rebuild_gate = rebuild_gate
         if search_switch is not None:
             cfg.search_switch = search_switch
-        if adapt_skin is not None:
-            cfg.adapt_skin = adapt_skin
         cfg.device = device
         h = ctypes.c_void_p()
         _check(L.epi_create(ctypes.byref(h), ctypes.byref(cfg)), "epi_create")
@@ -395,10 +393,10 @@ class Context:
         return {k: getattr(cfg, k) for k, _ in ConfigC._fields_}
 
     def set_tuning(self, skin: float, variant: int, search_switch: int = 0,
-                   rebuild_gate: int = 0, adapt_skin: int = 1):
+                   rebuild_gate: int = 0):
         """epi_set_tuning: apply a tuning chosen earlier (e.g. cached)."""
         _check(lib().epi_set_tuning(self._h, float(skin), int(variant), int(search_switch),
-                                    int(rebuild_gate), int(adapt_skin)), "epi_set_tuning")
+                                    int(rebuild_gate)), "epi_set_tuning")
 
     def autotune(self, trial_steps: int = 64):
         """epi_autotune: returns (skin, variant, ms per step of the best trial)

@@ -661,7 +661,7 @@ __global__ void k_gate_check(DevState S) {
     if (ey > T.hly) ey -= T.ly;
     else if (ey < -T.hly) ey += T.ly;
     const double ez = p.z - (double)b.z;
-    const double lim = 0.5 * skin_of(S, t) - 1e-3;
+    const double lim = 0.5 * S.skin - 1e-3;
     if (!(ex * ex + ey * ey + ez * ez <= lim * lim)) {
       S.gate[1 + t] = 1;
       S.gate[0] = 1;

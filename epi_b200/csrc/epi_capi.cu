@@ -134,11 +134,6 @@ struct epi_ctx {
   DevStatus* status = nullptr;
   DevStatus* status_h = nullptr;  // pinned
   unsigned long long* rebuilds = nullptr;
-  // adaptive skin: per-tissue skin, last rebuild step, largest row; step count
-  float* tskin = nullptr;
-  int32_t* tlast = nullptr;
-  int32_t* tcmax = nullptr;
-  int32_t* stepno = nullptr;
   int32_t* loop_left = nullptr;  // passes left in the step graph's device loop
   unsigned long long* launches = nullptr;  // step-sequence kernels executed
   ScanScratch scan{};
@@ -225,14 +220,12 @@ void free_buffers(epi_ctx* c) {
   if (c->agek) cudaFree(c->agek);
   c->agek = nullptr;
   void* ptrs[] = {c->tissues, c->pos[0], c->pos[1], c->posf[0], c->posf[1], c->attr, c->pair, c->spr, c->dermis,
-                  c->tskin, c->tlast, c->tcmax, c->stepno,
                   c->cand, c->bpos, c->nbr, c->nn, c->fmemb, c->bin,
                   c->rank, c->counts, c->starts, c->skey, c->spos, c->gate, c->rl, c->prep,
                   c->scan.partial, c->stage, c->stage_out};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   c->tissues = nullptr;
-  c->tskin = nullptr; c->tlast = nullptr; c->tcmax = nullptr; c->stepno = nullptr;
   c->pos[0] = c->pos[1] = nullptr;
   c->posf[0] = c->posf[1] = nullptr;
   c->attr = nullptr; c->pair = nullptr; c->spr = nullptr; c->dermis = nullptr;
@@ -279,11 +272,6 @@ DevState make_state(epi_ctx* c, int cur) {
   S.nprep_memb = c->nprep_memb;
   S.status = c->status;
   S.rebuilds = c->rebuilds;
-  S.tskin = c->tskin;
-  S.tlast = c->tlast;
-  S.tcmax = c->tcmax;
-  S.stepno = c->stepno;
-  S.adapt_skin = c->cfg.adapt_skin;
   S.launches = c->launches;
   S.n_total = c->n;
   S.max_conn = c->cfg.max_conn;
@@ -366,24 +354,6 @@ void enqueue_step(epi_ctx* c, int& cur, Timer* tm) {
   cur ^= 1;
 }
 
-// Every tissue's skin to the configured one, no rebuild yet (its first one
-// keeps the configured skin), the step count to 0.
-cudaError_t reset_skins(epi_ctx* c) {
-  if (!c->tskin) return cudaSuccess;
-  const std::vector<float> sk((size_t)c->ntissues, (float)c->cfg.skin);
-  const std::vector<int32_t> never((size_t)c->ntissues, -(1 << 30));
-  cudaError_t e = cudaMemcpyAsync(c->tskin, sk.data(), sizeof(float) * sk.size(),
-                                  cudaMemcpyHostToDevice, c->stream);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(c->tlast, never.data(), sizeof(int32_t) * never.size(),
-                        cudaMemcpyHostToDevice, c->stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(c->tcmax, 0, sizeof(int32_t) * c->ntissues, c->stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(c->stepno, 0, sizeof(int32_t), c->stream);
-  // the host vector must outlive the copy
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  return e;
-}
-
 // Whether the step graph puts the candidate rebuild in a conditional node
 // that skips its kernels on steps with nothing to rebuild: by default for a
 // single tissue (most of its steps rebuild nothing), not for a batch (some
@@ -393,17 +363,14 @@ bool conditional_rebuild(const epi_ctx* c) {
   return c->cfg.rebuild_gate == 1 || (c->cfg.rebuild_gate == 0 && c->ntissues == 1);
 }
 
-// Skin, step-kernel variant, candidate-search switch, rebuild node and
-// adaptive skin of the context; the captured graphs hold them, so they are
-// dropped.
+// Skin, step-kernel variant, candidate-search switch and rebuild node of the
+// context; the captured graphs hold them, so they are dropped.
 void apply_tuning(epi_ctx* c, double skin, int32_t variant, int32_t search_switch,
-                  int32_t rebuild_gate, int32_t adapt_skin) {
+                  int32_t rebuild_gate) {
   c->cfg.skin = skin;
   c->cfg.variant = variant;
   c->cfg.search_switch = search_switch;
   c->cfg.rebuild_gate = rebuild_gate;
-  c->cfg.adapt_skin = adapt_skin;
-  (void)reset_skins(c);
   c->lc.variant = variant == 0 ? 3 : variant;
   c->lc.search_switch = search_switch > 0 ? search_switch : kDefaultSearchSwitch;
   destroy_graphs(c);
@@ -723,7 +690,6 @@ void epi_config_default(epi_config* c) {
   c->variant = 0;
   c->search_switch = 0;
   c->rebuild_gate = 0;
-  c->adapt_skin = 1;
   c->reserved = 0;
 }
 
@@ -762,7 +728,6 @@ int epi_create(epi_ctx** out, const epi_config* cfg) {
   if (c.precision != EPI_PREC_FP64 && c.precision != EPI_PREC_MIXED) return EPI_ERR_INVALID_ARG;
   if (c.search_switch < 0 || c.rebuild_gate < 0 || c.rebuild_gate > 2) return EPI_ERR_INVALID_ARG;
   if (c.reserved != 0) return EPI_ERR_INVALID_ARG;
-  if (c.adapt_skin != 0 && c.adapt_skin != 1) return EPI_ERR_INVALID_ARG;
   int ndev = 0;
   const cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev <= 0) return EPI_ERR_NO_DEVICE;
@@ -1005,8 +970,6 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
       (rc = dev_alloc(&c->skey, n)) || (rc = dev_alloc(&c->spos, n)) ||
       (rc = dev_alloc(&c->gate, (size_t)ntissues + 1)) ||
       (rc = dev_alloc(&c->rl, 3 + 3 * (size_t)ntissues)) ||
-      (rc = dev_alloc(&c->tskin, ntissues)) || (rc = dev_alloc(&c->tlast, ntissues)) ||
-      (rc = dev_alloc(&c->tcmax, ntissues)) || (rc = dev_alloc(&c->stepno, 1)) ||
       (rc = dev_alloc(&c->prep, prep.size())) || (rc = dev_alloc(&c->stage, 3 * (size_t)n)) ||
       (rc = dev_alloc(&c->agek, n)))) {
     free_buffers(c);
@@ -1068,9 +1031,6 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
     EPI_CUDA(cudaMemsetAsync(c->dermis, 0xff, sizeof(int32_t) * n, s));
   }
   EPI_CUDA(cudaMemsetAsync(c->status, 0, sizeof(DevStatus), s));
-  // adaptive skin: a new batch starts every tissue at the configured skin (a
-  // same-shape re-upload keeps what the tissues adapted to)
-  if (!reuse) EPI_CUDA(reset_skins(c));
   c->cur = 0;
   c->loaded = true;
   if (gates.empty()) {
@@ -1382,9 +1342,8 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
     c->lists_fresh = false;
     return EPI_OK;
   };
-  auto apply = [&](double skin, int32_t variant, int32_t search_switch, int32_t form,
-                   int32_t adapt) {
-    apply_tuning(c, skin, variant, search_switch, form, adapt);
+  auto apply = [&](double skin, int32_t variant, int32_t search_switch, int32_t gate) {
+    apply_tuning(c, skin, variant, search_switch, gate);
   };
   // one trial: ms per trial (INFINITY when the rows overflowed)
   auto trial = [&](double* ms_out) -> int {
@@ -1405,10 +1364,9 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
   double best = INFINITY, best_skin = c->cfg.skin;
   int32_t best_variant = c->cfg.variant;
   const int32_t switch0 = c->cfg.search_switch, form0 = c->cfg.rebuild_gate;
-  const int32_t adapt0 = c->cfg.adapt_skin;
   for (double skin : kSkins) {
     for (int32_t variant : kVariants) {
-      apply(skin, variant, switch0, form0, adapt0);
+      apply(skin, variant, switch0, form0);
       double ms;
       if ((rc = trial(&ms))) return rc;
       if (ms < best) {
@@ -1418,22 +1376,12 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
       }
     }
   }
-  // then adaptive or fixed skins, the rebuild in a conditional graph node or
-  // not, and the candidate search's switch from a warp to a thread per
-  // particle
-  int32_t best_form = form0, best_switch = switch0, best_adapt = adapt0;
+  // then the rebuild in a conditional graph node or not, and the candidate
+  // search's switch from a warp to a thread per particle
+  int32_t best_form = form0, best_switch = switch0;
   if (std::isfinite(best)) {
-    for (int32_t adapt : {0, 1}) {
-      apply(best_skin, best_variant, switch0, form0, adapt);
-      double ms;
-      if ((rc = trial(&ms))) return rc;
-      if (ms < best) {
-        best = ms;
-        best_adapt = adapt;
-      }
-    }
     for (int32_t form : {1, 2}) {
-      apply(best_skin, best_variant, switch0, form, best_adapt);
+      apply(best_skin, best_variant, switch0, form);
       double ms;
       if ((rc = trial(&ms))) return rc;
       if (ms < best) {
@@ -1443,7 +1391,7 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
     }
     static const int32_t kSwitches[] = {8192, 16384, 49152, 131072};
     for (int32_t sw : kSwitches) {
-      apply(best_skin, best_variant, sw, best_form, best_adapt);
+      apply(best_skin, best_variant, sw, best_form);
       double ms;
       if ((rc = trial(&ms))) return rc;
       if (ms < best) {
@@ -1452,7 +1400,7 @@ int epi_autotune(epi_ctx* c, int32_t trial_steps, double* skin_out, int32_t* var
       }
     }
   }
-  apply(best_skin, best_variant, best_switch, best_form, best_adapt);
+  apply(best_skin, best_variant, best_switch, best_form);
   if ((rc = restore())) return rc;
   if ((rc = check_status(c))) return rc;
   if (skin_out) *skin_out = best_skin;
@@ -1469,15 +1417,15 @@ int epi_get_config(epi_ctx* c, epi_config* out) {
 }
 
 int epi_set_tuning(epi_ctx* c, double skin, int32_t variant, int32_t search_switch,
-                   int32_t rebuild_gate, int32_t adapt_skin) {
+                   int32_t rebuild_gate) {
   if (!c || !(skin > 0) || skin > 2.0 || variant < 0 || variant > 4 || search_switch < 0 ||
-      rebuild_gate < 0 || rebuild_gate > 2 || (adapt_skin != 0 && adapt_skin != 1))
+      rebuild_gate < 0 || rebuild_gate > 2)
     return EPI_ERR_INVALID_ARG;
   EPI_GUARD_BEGIN
   Nvtx nvtx_range("epi_set_tuning");
   int rc = set_device(c);
   if (rc) return rc;
-  apply_tuning(c, skin, variant, search_switch, rebuild_gate, adapt_skin);
+  apply_tuning(c, skin, variant, search_switch, rebuild_gate);
   if (c->loaded) {
     // candidates were built for the old skin: rebuild every tissue's
     launch_set_gates(make_state(c, c->cur), c->ntissues, c->stream);

@@ -111,21 +111,8 @@ struct DevState {
   unsigned long long* launches;  // kernels of the step sequence executed so far
   int64_t n_total;  // column stride of cand / nbr
   int32_t max_conn, max_cand;
-  double skin;       // the configured candidate skin
-  // Adaptive skin: each tissue's own skin (rows and the displacement test use
-  // it), the step of its last rebuild, its largest candidate row at that
-  // rebuild, and the step count (advanced by the rebuild condition).
-  float* tskin;
-  int32_t* tlast;
-  int32_t* tcmax;
-  int32_t* stepno;
-  int32_t adapt_skin;
+  double skin;
 };
-
-// The candidate skin of tissue t.
-__device__ __forceinline__ double skin_of(const DevState& S, int32_t t) {
-  return (double)S.tskin[t];
-}
 
 __device__ __forceinline__ uint32_t attr_state(uint32_t a) { return a & 15u; }
 __device__ __forceinline__ bool attr_old(uint32_t a) { return (a >> 4) & 1u; }

@@ -180,38 +180,8 @@ __device__ __forceinline__ int32_t ref_bin(const TissueDev& T, double x, double 
 // ---------------------------------------------------------------------------
 // For the whole batch the "some tissue" word is cleared once the list is
 // built: the step kernel sets it again for the next step.
-// Adaptive skin (when S.adapt_skin): at its rebuild, a tissue that rebuilt
-// fewer than kSkinGrowBelow steps before takes a skin 1.5 times wider (up to
-// kSkinMaxFactor times the configured one, and only while its largest
-// candidate row stays below half the row capacity); one that went more than
-// kSkinShrinkAbove steps without a rebuild returns towards the configured
-// skin. Wider skins cost candidates per step and save rebuilds; the
-// connections, and the order of the connected pairs in a row, do not depend
-// on the skin, so results are the same.
-constexpr int32_t kSkinGrowBelow = 16, kSkinShrinkAbove = 128;
-constexpr float kSkinMaxFactor = 3.f;
-
-__device__ __forceinline__ void adapt_skin_of(const DevState& S, int32_t t, int32_t step) {
-  const int32_t interval = step - S.tlast[t];
-  float sk = S.tskin[t];
-  const float base = (float)S.skin;
-  if (interval < kSkinGrowBelow && 2 * S.tcmax[t] <= S.max_cand)
-    sk = fminf(sk * 1.5f, kSkinMaxFactor * base);
-  else if (interval > kSkinShrinkAbove)
-    sk = fmaxf(sk / 1.5f, base);
-  S.tskin[t] = sk;
-  S.tlast[t] = step;
-  S.tcmax[t] = 0;
-}
-
 __device__ __forceinline__ void gate_compact(const DevState& S, int32_t t0, int32_t t1) {
   const bool whole = t0 == 0 && t1 == S.ntissues;
-  // one count per step: the call for the batch's first tissues
-  const int32_t step = S.stepno[0] + 1;
-  if (t0 == 0) {
-    __syncthreads();  // every thread has read the count
-    if (threadIdx.x == 0) S.stepno[0] = step;
-  }
   if (S.gate[0] == 0) {
     if (threadIdx.x == 0) {
       S.rl_count[0] = 0;
@@ -231,7 +201,6 @@ __device__ __forceinline__ void gate_compact(const DevState& S, int32_t t0, int3
       const TissueDev& T = S.tissues[t];
       np = T.n;
       nb = T.anx * T.any * T.anz;
-      if (S.adapt_skin) adapt_skin_of(S, t, step);
     }
     int32_t tc, tp, tb;
     const int32_t oc = block_excl_scan(g ? 1 : 0, &tc);
@@ -507,7 +476,7 @@ struct SearchWindow {
     memb_i = attr_state(S.attr[i]) == ST_MEMB;
     const double4 p = S.pos_cur[i];
     const double lt = T.P.lj_thresh;
-    const double skin = skin_of(S, attr_tissue(S.attr[i]));
+    const double skin = S.skin;
     // Candidates are compared in float: the margin covers the rounding of
     // float coordinates up to the box size (and the window widens with it).
     const double margin = 1e-4 + 5e-7 * (T.lx > T.ly ? T.lx : T.ly) + 5e-7 * T.lz;
@@ -556,7 +525,6 @@ __device__ __forceinline__ void finish_search(const DevState& S, int32_t i, int3
   const int32_t cap = S.max_cand;
   if (count > cap) raise_error(S.status, E_LIST_OVERFLOW, i, -1, (double)count);
   cand_set(S, i, 0, (uint32_t)(count < cap ? count : cap));
-  if (S.adapt_skin) atomicMax(&S.tcmax[attr_tissue(S.attr[i])], count);
   const double4 p = S.pos_cur[i];
   S.bpos[i] = make_float4((float)p.x, (float)p.y, (float)p.z, 0.f);
 }
@@ -1272,7 +1240,7 @@ struct Particle {
     if (ey > hly) ey -= ly;
     else if (ey < -hly) ey += ly;
     const double ez = nz - (double)b.z;
-    const double lim = 0.5 * skin_of(S, t) - 1e-3;  // margin covers the float rounding of bpos
+    const double lim = 0.5 * S.skin - 1e-3;  // margin covers the float rounding of bpos
     if (!(ex * ex + ey * ey + ez * ez <= lim * lim)) {
       S.gate[1 + t] = 1;
       S.gate[0] = 1;
@@ -1571,7 +1539,7 @@ __global__ void k_pack_gate(DevState S, const double* x, const double* y, const 
     if (ey > T.hly) ey -= T.ly;
     else if (ey < -T.hly) ey += T.ly;
     const double ez = p.z - (double)b.z;
-    const double lim = 0.5 * skin_of(S, t) - 1e-3;
+    const double lim = 0.5 * S.skin - 1e-3;
     if (!(ex * ex + ey * ey + ez * ez <= lim * lim)) {
       S.gate[1 + t] = 1;
       S.gate[0] = 1;

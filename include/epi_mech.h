@@ -138,13 +138,6 @@ typedef struct epi_config {
                          sit in a conditional node that skips them on steps
                          with nothing to rebuild; 2 = they are always launched
                          (and exit at once when nothing is listed) */
-  int32_t adapt_skin; /* 1 (default): each tissue adapts its own skin at its
-                         rebuilds -- 1.5 times wider after rebuilding again
-                         within 16 steps (up to 3 times `skin`, while its
-                         candidate rows stay below half of max_cand), back
-                         towards `skin` after 128 steps without one; 0: every
-                         tissue keeps `skin`. Connections and results do not
-                         depend on it. */
   int32_t reserved;   /* must be 0 */
 } epi_config;
 
@@ -236,10 +229,10 @@ int epi_time_kernels(epi_ctx* ctx, int32_t nsteps, int32_t max_classes, double* 
 /* Autotuner. Times short graph-replayed trials of the uploaded batch for
  * every candidate skin in {0.05, 0.08, 0.1, 0.15, 0.2, 0.3} and step-kernel
  * variant 1..4 (4 warm-up steps, then trial_steps timed with CUDA events),
- * then, for the fastest pair, adaptive or fixed skins, the rebuild in a
- * conditional graph node or not, and the candidate search's switch from a
- * warp to a thread per particle in {8192, 16384, 49152, 131072} rebuilt
- * particles, and keeps the fastest choice in the context's configuration. Skins whose candidate rows would overflow
+ * then, for the fastest pair, the rebuild in a conditional graph node or
+ * not, and the candidate search's switch from a warp to a thread per
+ * particle in {8192, 16384, 49152, 131072} rebuilt particles, and keeps the
+ * fastest choice in the context's configuration. Skins whose candidate rows would overflow
  * max_cand are skipped. The simulation state is left as it was (positions
  * are restored after every trial), and no choice changes results beyond
  * multiply-add rounding (connection sets are exact for every skin, and both
@@ -254,11 +247,11 @@ int epi_autotune(epi_ctx* ctx, int32_t trial_steps, double* skin, int32_t* varia
 int epi_get_config(epi_ctx* ctx, epi_config* out);
 
 /* Applies a tuning chosen earlier (for instance a cached epi_autotune
- * result for the same batch shape): skin, variant, search switch, rebuild
- * node and adaptive skin, with epi_config's ranges. Every tissue's candidates are rebuilt before the
+ * result for the same batch shape): skin, variant, search switch and
+ * rebuild node, with epi_config's ranges. Every tissue's candidates are rebuilt before the
  * next step. No counterpart in the reference. */
 int epi_set_tuning(epi_ctx* ctx, double skin, int32_t variant, int32_t search_switch,
-                   int32_t rebuild_gate, int32_t adapt_skin);
+                   int32_t rebuild_gate);
 
 /* ---- cell maps and external-stimulus diffusion -----------------------------
  * The rest of the reference's per-step loop before its chemistry

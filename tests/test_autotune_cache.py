@@ -19,10 +19,10 @@ class FakeCtx:
         return 0.15, 4, 0.42
 
     def config(self):
-        return {"search_switch": 16384, "rebuild_gate": 2, "adapt_skin": 1}
+        return {"search_switch": 16384, "rebuild_gate": 2}
 
-    def set_tuning(self, skin, variant, switch, form, adapt):
-        self.tuned_with = (skin, variant, switch, form, adapt)
+    def set_tuning(self, skin, variant, switch, gate):
+        self.tuned_with = (skin, variant, switch, gate)
 
 
 def test_cache_tunes_once_per_shape(tmp_path, monkeypatch):
@@ -35,7 +35,7 @@ def test_cache_tunes_once_per_shape(tmp_path, monkeypatch):
     assert (first["skin"], first["variant"], first["search_switch"]) == (0.15, 4, 16384)
     b = FakeCtx()
     again = A.tuned(b, [T.config1(s) for s in range(3)], 16, cache=cache)
-    assert b.autotuned == 0 and again["cached"] and b.tuned_with == (0.15, 4, 16384, 2, 1)
+    assert b.autotuned == 0 and again["cached"] and b.tuned_with == (0.15, 4, 16384, 2)
     # another shape, another precision, another GPU: tuned anew
     c = FakeCtx()
     A.tuned(c, ts[:2], 16, cache=cache)

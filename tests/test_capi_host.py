@@ -44,34 +44,32 @@ def test_default_params_equal_reference_constants(built):
 def test_create_rejects_bad_arguments(built):
     L = capi.lib()
     assert L.epi_create(None, None) == capi.EPI_ERR_INVALID_ARG
-    cfg = capi.ConfigC(0, 7, 64, 96, 0.3, 0, 0, 0, 0, 0)  # unknown precision
+    cfg = capi.ConfigC(0, 7, 64, 96, 0.3, 0, 0, 0, 0)  # unknown precision
     h = ctypes.c_void_p()
     assert L.epi_create(ctypes.byref(h), ctypes.byref(cfg)) in (
         capi.EPI_ERR_INVALID_ARG, capi.EPI_ERR_NO_DEVICE)
-    cfg = capi.ConfigC(0, 1, 64, 32, 0.3, 0, 0, 0, 0, 0)  # fewer candidates than connections
+    cfg = capi.ConfigC(0, 1, 64, 32, 0.3, 0, 0, 0, 0)  # fewer candidates than connections
     assert L.epi_create(ctypes.byref(h), ctypes.byref(cfg)) in (
         capi.EPI_ERR_INVALID_ARG, capi.EPI_ERR_NO_DEVICE)
-    cfg = capi.ConfigC(0, 1, 64, 96, -1.0, 0, 0, 0, 0, 0)  # negative skin
+    cfg = capi.ConfigC(0, 1, 64, 96, -1.0, 0, 0, 0, 0)  # negative skin
     assert L.epi_create(ctypes.byref(h), ctypes.byref(cfg)) in (
         capi.EPI_ERR_INVALID_ARG, capi.EPI_ERR_NO_DEVICE)
-    cfg = capi.ConfigC(0, 1, 64, 96, 0.1, 9, 0, 0, 0, 0)  # unknown step-kernel variant
+    cfg = capi.ConfigC(0, 1, 64, 96, 0.1, 9, 0, 0, 0)  # unknown step-kernel variant
     assert L.epi_create(ctypes.byref(h), ctypes.byref(cfg)) in (
         capi.EPI_ERR_INVALID_ARG, capi.EPI_ERR_NO_DEVICE)
     # argument checks come before the device query: exact codes without a GPU
-    cfg = capi.ConfigC(0, 1, 64, 96, 0.1, 0, -5, 0, 0, 0)  # negative search switch
+    cfg = capi.ConfigC(0, 1, 64, 96, 0.1, 0, -5, 0, 0)  # negative search switch
     assert L.epi_create(ctypes.byref(h), ctypes.byref(cfg)) == capi.EPI_ERR_INVALID_ARG
-    cfg = capi.ConfigC(0, 1, 64, 96, 0.1, 0, 0, 3, 0, 0)  # unknown rebuild node
+    cfg = capi.ConfigC(0, 1, 64, 96, 0.1, 0, 0, 3, 0)  # unknown rebuild node
     assert L.epi_create(ctypes.byref(h), ctypes.byref(cfg)) == capi.EPI_ERR_INVALID_ARG
-    cfg = capi.ConfigC(0, 1, 64, 96, 0.1, 0, 0, 0, 5, 0)  # adaptive skin is 0 or 1
+    cfg = capi.ConfigC(0, 1, 64, 96, 0.1, 0, 0, 0, 7)  # reserved must be 0
     assert L.epi_create(ctypes.byref(h), ctypes.byref(cfg)) == capi.EPI_ERR_INVALID_ARG
-    cfg = capi.ConfigC(0, 1, 64, 96, 0.1, 0, 0, 0, 1, 7)  # reserved must be 0
-    assert L.epi_create(ctypes.byref(h), ctypes.byref(cfg)) == capi.EPI_ERR_INVALID_ARG
-    cfg = capi.ConfigC(0, 1, 500, 600, 0.1, 0, 0, 0, 0, 0)  # beyond the reference's 400 connections
+    cfg = capi.ConfigC(0, 1, 500, 600, 0.1, 0, 0, 0, 0)  # beyond the reference's 400 connections
     assert L.epi_create(ctypes.byref(h), ctypes.byref(cfg)) == capi.EPI_ERR_INVALID_ARG
     assert L.epi_step(None, 1) == capi.EPI_ERR_INVALID_ARG
     assert L.epi_sync(None) == capi.EPI_ERR_INVALID_ARG
     assert L.epi_get_config(None, ctypes.byref(cfg)) == capi.EPI_ERR_INVALID_ARG
-    assert L.epi_set_tuning(None, 0.1, 3, 0, 0, 1) == capi.EPI_ERR_INVALID_ARG
+    assert L.epi_set_tuning(None, 0.1, 3, 0, 0) == capi.EPI_ERR_INVALID_ARG
 
 
 def _has_gpu():

@@ -237,26 +237,6 @@ def test_rebuild_nodes_and_search_paths_are_bit_identical(built, precision):
         assert np.array_equal(runs[0][2], der)
 
 
-@pytest.mark.parametrize("precision", [FP64, MIXED])
-def test_adaptive_skin_changes_nothing_but_the_rebuilds(built, precision):
-    """Per-tissue adaptive skins change when tissues rebuild, never which
-    pairs connect nor the order of the connected pairs in a row: the steps
-    agree bit for bit with fixed skins, while the batch rebuilds less."""
-    ts = [T.config1(s) for s in range(4)] + [T.layered_tissue(24, 3, 5)]
-    runs = []
-    for adapt in (0, 1):
-        with capi.Context(precision=precision, max_conn=64, adapt_skin=adapt) as ctx:
-            ctx.upload(ts)
-            r0 = ctx.rebuild_count()
-            ctx.step(120, "graph")
-            runs.append((ctx.positions(), ctx.connections(), ctx.rebuild_count() - r0))
-    (p0, (o0, i0), rb0), (p1, (o1, i1), rb1) = runs
-    for a, b in zip(p0, p1):
-        assert np.array_equal(a, b)
-    assert np.array_equal(o0, o1) and np.array_equal(i0, i1)
-    assert rb1 <= rb0
-
-
 def test_repeat_runs_are_deterministic(built):
     t = T.config2()
     a = run_gpu([t], 20, MIXED)
