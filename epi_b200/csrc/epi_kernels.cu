@@ -508,16 +508,21 @@ struct SearchWindow {
   }
   // Is the particle in slot s (key, FP32 copy q) of a column of x range xr
   // and y range yr a candidate of i? (ex, ey: pxe[xr], pye[yr])
-  __device__ __forceinline__ bool hit(int32_t i, uint32_t key, const float4& q, float ex,
-                                      float ey) const {
+  // kWrap = false: only for windows with neither wrap_x nor wrap_y.
+  template <bool kWrap>
+  __device__ __forceinline__ bool hit_t(int32_t i, uint32_t key, const float4& q, float ex,
+                                        float ey) const {
     const int32_t j = (int32_t)(key & 0x7fffffffu);
     if (j == i || (memb_i && (key >> 31))) return false;
     float dx = ex - q.x, dy = ey - q.y;
-    if (wrap_x) dx = dx > fhx ? dx - flx : (dx <= -fhx ? dx + flx : dx);
-    if (wrap_y) dy = dy > fhy ? dy - fly : (dy <= -fhy ? dy + fly : dy);
+    if (kWrap && wrap_x) dx = dx > fhx ? dx - flx : (dx <= -fhx ? dx + flx : dx);
+    if (kWrap && wrap_y) dy = dy > fhy ? dy - fly : (dy <= -fhy ? dy + fly : dy);
     const float dz = pz - q.z;
     const float reach = flt * (pw + q.w) + fskin;
     return dx * dx + dy * dy + dz * dz <= reach * reach;
+  }  __device__ __forceinline__ bool hit(int32_t i, uint32_t key, const float4& q, float ex,
+                                      float ey) const {
+    return hit_t<true>(i, key, q, ex, ey);
   }
 };
 
@@ -563,8 +568,8 @@ __device__ __forceinline__ void cand_search_groups(const DevState& S, int32_t cn
       float cex = 0.f, cey = 0.f;
       if (c < ncol) {
         const int32_t cx = c / ncy, cy = c - cx * ncy;
-        cex = W.pxe[cx < nx0 ? 0 : 1];
-        cey = W.pye[cy < ny0 ? 0 : 1];
+        cex = cx < nx0 ? W.pxe[0] : W.pxe[1];
+        cey = cy < ny0 ? W.pye[0] : W.pye[1];
         const int32_t bx = cx < nx0 ? W.xlo[0] + cx : W.xlo[1] + (cx - nx0);
         const int32_t by = cy < ny0 ? W.ylo[0] + cy : W.ylo[1] + (cy - ny0);
         const int32_t col = T.binbase + (bx * T.any + by) * T.anz;
@@ -609,94 +614,140 @@ __device__ __forceinline__ void cand_search_groups(const DevState& S, int32_t cn
 }
 
 // A thread's candidate row written a whole 16-byte chunk at a time: entries
-// collect in a register chunk that is stored when full or at the end (chunk 0
-// is stored with a zero count; the caller stores the count afterwards).
+// are shifted into a register chunk from the top (the oldest reaches slot 0
+// after a chunk's worth of entries) and the chunk is stored when full or at
+// the end. Chunk 0 starts with a zero in the count slot; the caller stores
+// the count afterwards.
+template <bool k16>
 struct RowWriter {
-  const DevState& S;
-  const int64_t i;
-  const bool k16;
+  static constexpr int kPer = k16 ? 8 : 4;  // entries per chunk
   uint32_t w0 = 0, w1 = 0, w2 = 0, w3 = 0;
   int32_t e = 1;  // next entry (entry 0 is the count)
-  __device__ __forceinline__ RowWriter(const DevState& S_, int64_t i_)
-      : S(S_), i(i_), k16(S_.cand16 != 0) {}
-  __device__ __forceinline__ void put(uint32_t v) {
-    const int per = k16 ? 8 : 4;
-    const int slot = e & (per - 1);
-    const int word = k16 ? slot >> 1 : slot;
-    const uint32_t sh = k16 ? (uint32_t)(slot & 1) * 16u : 0u;
-    const uint32_t m = k16 ? 0xffffu << sh : 0xffffffffu;
-    const uint32_t val = (k16 ? (v & 0xffffu) : v) << sh;
-    w0 = word == 0 ? (w0 & ~m) | val : w0;
-    w1 = word == 1 ? (w1 & ~m) | val : w1;
-    w2 = word == 2 ? (w2 & ~m) | val : w2;
-    w3 = word == 3 ? (w3 & ~m) | val : w3;
+  __device__ __forceinline__ void shift_in(uint32_t v) {
+    if (k16) {
+      w0 = __funnelshift_r(w0, w1, 16);
+      w1 = __funnelshift_r(w1, w2, 16);
+      w2 = __funnelshift_r(w2, w3, 16);
+      w3 = __funnelshift_r(w3, v, 16);
+    } else {
+      w0 = w1;
+      w1 = w2;
+      w2 = w3;
+      w3 = v;
+    }
+  }
+  __device__ __forceinline__ void put(const DevState& S, int64_t i, uint32_t v) {
+    if (!EPI_CHECKED(!k16 || v < 65536u, S.status, (int32_t)i, e)) return;
+    shift_in(v);
     ++e;
-    if ((e & (per - 1)) == 0) flush();
+    if ((e & (kPer - 1)) == 0)
+      S.cand[(int64_t)(e / kPer - 1) * S.n_total + i] = make_uint4(w0, w1, w2, w3);
   }
-  __device__ __forceinline__ void flush() {
-    const int per = k16 ? 8 : 4;
-    S.cand[(int64_t)((e - 1) / per) * S.n_total + i] = make_uint4(w0, w1, w2, w3);
-    w0 = w1 = w2 = w3 = 0;
-  }
-  __device__ __forceinline__ void close() {
-    const int per = k16 ? 8 : 4;
-    if ((e & (per - 1)) != 0) flush();
+  __device__ __forceinline__ void close(const DevState& S, int64_t i) {
+    const int n = e & (kPer - 1);
+    if (n == 0) return;
+    for (int k = n; k < kPer; ++k) shift_in(0u);
+    S.cand[(int64_t)(e / kPer) * S.n_total + i] = make_uint4(w0, w1, w2, w3);
   }
 };
 
-// Many gated particles: one thread per particle. A particle sweeps about a
-// hundred slots (bins of 2.0 hold about six particles), four at a time so
-// their loads overlap; a warp keeps 32 particles in flight and writes the
-// column-major candidate rows coalesced.
+// One particle's candidate search by one thread. The window's columns
+// (x ranges outer, y ranges inner) are walked as one flat sequence of
+// slots, two per iteration: a lane moves on to its next column whenever it
+// has used up the current one, so the lanes of a warp stay in step however
+// their columns' slot counts differ. Each column's slot range is fetched one
+// column ahead, so opening a column waits on no load. kWrap: the box is too
+// small for the folded images (per-slot minimum image).
+template <bool k16, bool kWrap>
+__device__ __forceinline__ void search_particle(const DevState& S, const TissueDev& T,
+                                                const SearchWindow& W, int32_t i) {
+  const int32_t cap = S.max_cand;
+  const int32_t nx0 = W.xhi[0] - W.xlo[0] + 1, ny0 = W.yhi[0] - W.ylo[0] + 1;
+  const int32_t ncx = nx0 + (W.nxr > 1 ? W.xhi[1] - W.xlo[1] + 1 : 0);
+  const int32_t ncy = ny0 + (W.nyr > 1 ? W.yhi[1] - W.ylo[1] + 1 : 0);
+  const int32_t any = T.any, anz = T.anz, binbase = T.binbase;
+  const uint32_t pbase = (uint32_t)T.pbase;
+  RowWriter<k16> row;
+  int32_t count = 0;
+  // the column after the current one: its slot range and folded coordinates
+  int32_t cx = 0, cy = 0;  // the column to fetch next
+  int32_t ns = 0, nhi = 0;
+  float nex = 0.f, ney = 0.f;
+  bool nvalid = false;
+  auto fetch = [&]() {
+    nvalid = cx < ncx;
+    if (!nvalid) return;
+    const int32_t bx = cx < nx0 ? W.xlo[0] + cx : W.xlo[1] + (cx - nx0);
+    const int32_t by = cy < ny0 ? W.ylo[0] + cy : W.ylo[1] + (cy - ny0);
+    nex = cx < nx0 ? W.pxe[0] : W.pxe[1];
+    ney = cy < ny0 ? W.pye[0] : W.pye[1];
+    const int32_t col = binbase + (bx * any + by) * anz;
+    ns = S.starts[col + W.z0];
+    nhi = S.starts[col + W.z1 + 1];
+    if (++cy == ncy) {
+      cy = 0;
+      ++cx;
+    }
+  };
+  fetch();
+  int32_t s = 0, s_hi = 0;
+  float ex = 0.f, ey = 0.f;
+  for (;;) {
+    bool live = true;
+    while (s >= s_hi) {  // open the next column
+      if (!nvalid) {
+        live = false;
+        break;
+      }
+      s = ns;
+      s_hi = nhi;
+      ex = nex;
+      ey = ney;
+      fetch();
+    }
+    if (!live) break;
+    const bool two = s + 1 < s_hi;
+    const uint32_t k0 = S.skey[s];
+    const float4 q0 = S.spos[s];
+    const uint32_t k1 = two ? S.skey[s + 1] : 0u;
+    const float4 q1 = two ? S.spos[s + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const bool h0 = W.template hit_t<kWrap>(i, k0, q0, ex, ey);
+    const bool h1 = two && W.template hit_t<kWrap>(i, k1, q1, ex, ey);
+    if (h0) {
+      if (count < cap) row.put(S, i, (k0 & 0x7fffffffu) - pbase);
+      ++count;
+    }
+    if (h1) {
+      if (count < cap) row.put(S, i, (k1 & 0x7fffffffu) - pbase);
+      ++count;
+    }
+    s += 2;
+  }
+  row.close(S, i);
+  finish_search(S, i, count);
+}
+
+// Many gated particles: one thread per particle (about a hundred slots each:
+// bins of 2.0 hold about six particles); a warp keeps 32 particles in flight
+// and writes the column-major candidate rows coalesced.
+template <bool k16>
 __device__ __forceinline__ void cand_search_threads(const DevState& S, int32_t cnt,
                                                     int32_t ngated) {
-  const int32_t cap = S.max_cand;
   for (int32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ngated;
        g += gridDim.x * blockDim.x) {
     int32_t t;
     const int32_t i = gated_particle(S, cnt, g, &t);
     const TissueDev& T = S.tissues[t];
     const SearchWindow W(S, T, i);
-    const int32_t any = T.any, anz = T.anz, binbase = T.binbase;
-    const uint32_t pbase = (uint32_t)T.pbase;
-    RowWriter row(S, i);
-    int32_t count = 0;
-    for (int xr = 0; xr < W.nxr; ++xr) {
-      const float ex = W.pxe[xr];
-      for (int32_t bx = W.xlo[xr]; bx <= W.xhi[xr]; ++bx) {
-        for (int yr = 0; yr < W.nyr; ++yr) {
-          const float ey = W.pye[yr];
-          for (int32_t by = W.ylo[yr]; by <= W.yhi[yr]; ++by) {
-            const int32_t col = binbase + (bx * any + by) * anz;
-            const int32_t s_hi = S.starts[col + W.z1 + 1];
-            for (int32_t s = S.starts[col + W.z0]; s < s_hi; s += 4) {
-              uint32_t key[4];
-              float4 q[4];
-#pragma unroll
-              for (int u = 0; u < 4; ++u) {
-                key[u] = s + u < s_hi ? S.skey[s + u] : 0u;
-                q[u] = s + u < s_hi ? S.spos[s + u] : make_float4(0.f, 0.f, 0.f, 0.f);
-              }
-#pragma unroll
-              for (int u = 0; u < 4; ++u) {
-                if (s + u < s_hi && W.hit(i, key[u], q[u], ex, ey)) {
-                  if (count < cap) row.put((key[u] & 0x7fffffffu) - pbase);
-                  ++count;
-                }
-              }
-            }
-          }
-        }
-      }
-    }
-    row.close();
-    finish_search(S, i, count);
+    if (W.wrap_x || W.wrap_y) search_particle<k16, true>(S, T, W, i);
+    else search_particle<k16, false>(S, T, W, i);
   }
 }
 
 // Below `thread_from` gated particles the warp-per-particle search (which
 // keeps the GPU busy with few particles) runs, from there on one thread per
 // particle. Both emit every row in the same order.
+template <bool k16>
 __global__ void __launch_bounds__(256, 4) k_cand_search(DevState S, int32_t thread_from) {
   pdl_entry();
   count_launch(S.launches);
@@ -705,7 +756,7 @@ __global__ void __launch_bounds__(256, 4) k_cand_search(DevState S, int32_t thre
   if (cnt == 0) return;
   const int32_t ngated = S.rl_ppre[cnt];
   if (ngated < thread_from) cand_search_groups<32>(S, cnt, ngated);
-  else cand_search_threads(S, cnt, ngated);
+  else cand_search_threads<k16>(S, cnt, ngated);
 }
 
 // Condition of the rebuild node in the captured step graph: builds the work
@@ -1605,7 +1656,8 @@ void launch_rebuild(const DevState& S, const Range& r, const ScanScratch&,
   launch_pdl(k_binsort, grid, B, s, S);
   timer_end(tm, KC_REBUILD_SORT, s);
   timer_begin(tm, KC_REBUILD_SEARCH, s);
-  launch_pdl(k_cand_search, grid, B, s, S, (int32_t)lc.search_switch);
+  if (S.cand16) launch_pdl(k_cand_search<true>, grid, B, s, S, (int32_t)lc.search_switch);
+  else launch_pdl(k_cand_search<false>, grid, B, s, S, (int32_t)lc.search_switch);
   timer_end(tm, KC_REBUILD_SEARCH, s);
 }
 
