@@ -585,8 +585,8 @@ void range_thresholds(TissueDev& T) {
 void set_fp32_bounds(TissueDev& T) {
   T.lxf = (float)T.lx;
   T.lyf = (float)T.ly;
-  T.hlxf = (float)T.hlx;
-  T.hlyf = (float)T.hly;
+  T.ilxf = (float)(1.0 / T.lx);
+  T.ilyf = (float)(1.0 / T.ly);
   T.lt2f = (float)(T.P.lj_thresh * T.P.lj_thresh);
   const double u = std::ldexp(1.0, -24);
   const double M = std::max(std::max(T.lx, T.ly), T.lz) + 8.0;

@@ -378,12 +378,13 @@ struct TissueDev {
   // to bin 0), gy_hi likewise, z >= gz_hi; connect_proc (non-membrane cells)
   // fails for x >= cx_hi, y >= cy_hi, z >= cz_hi or z <= cz_lo.
   double gx_hi, gy_hi, gz_hi, cx_hi, cy_hi, cz_hi, cz_lo;
-  // Mixed path: the box in FP32, LJ_THRESH^2 in FP32, and ftol, a bound on
-  // |d2_f32 - d2_exact| + |thr_f32 - thr_exact| for any pair that can be
-  // connected (positions rounded to FP32 once, separations and the
-  // threshold evaluated in FP32). A candidate whose FP32 d2 lies within ftol
-  // of the FP32 threshold is decided by the exact FP64 predicate.
-  float lxf, lyf, hlxf, hlyf, lt2f, ftol;
+  // Mixed path: the box and its inverse in FP32, LJ_THRESH^2 in FP32, and
+  // ftol, a bound on |d2_f32 - d2_exact| + |thr_f32 - thr_exact| for any
+  // pair that can be connected (positions rounded to FP32 once, separations
+  // and the threshold evaluated in FP32). A candidate whose FP32 d2 lies
+  // within ftol of the FP32 threshold is decided by the exact FP64 predicate.
+  float lxf, lyf, lt2f, ftol;
+  float ilxf, ilyf;  // 1 / L in FP32 (minimum image as f - L rint(f / L))
   Params P;
   Laws<float> lawf;
   Laws<double> lawd;

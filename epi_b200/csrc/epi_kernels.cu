@@ -843,11 +843,11 @@ struct SiteOffsets<float> {
       : S(S_), pf(S_.posf_cur[i]), T(T_) {}
   __device__ __forceinline__ Vec3<float> operator()(int32_t q) const {
     const float4 o = S.posf_cur[q];
-    float dx = o.x - pf.x, dy = o.y - pf.y;
-    if (dx > T.hlxf) dx -= T.lxf;
-    else if (dx <= -T.hlxf) dx += T.lxf;
-    if (dy > T.hlyf) dy -= T.lyf;
-    else if (dy <= -T.hlyf) dy += T.lyf;
+    // minimum image as d - L rint(d / L): lattice neighbours lie far
+    // closer than L/2, where it equals the compare-and-shift form
+    const float dx0 = o.x - pf.x, dy0 = o.y - pf.y;
+    const float dx = fmaf(-T.lxf, rintf(dx0 * T.ilxf), dx0);
+    const float dy = fmaf(-T.lyf, rintf(dy0 * T.ilyf), dy0);
     return Vec3<float>{dx, dy, o.z - pf.z};
   }
 };
@@ -1166,11 +1166,15 @@ struct Particle {
   }
   __device__ __forceinline__ bool connected(int32_t q, const float4& qf, R& dx, R& dy, R& dz,
                                             R& d2, R& rs) const {
+    // Minimum image as f - L rint(f / L) (positions lie in [0, L], so
+    // |f| <= L): the compare-and-shift of p_diff_x for every |f| away from
+    // L/2 by more than the rounding of f / L, i.e. for every pair within
+    // reach of a connection (LJ_THRESH (r_i + r_j) + skin is far below
+    // L/2); a pair near L/2 apart is rejected under either image. The
+    // multiply-round-fma takes three instructions and no branch.
     float fx = pf.x - qf.x, fy = pf.y - qf.y;
-    if (fx > T.hlxf) fx -= T.lxf;
-    else if (fx <= -T.hlxf) fx += T.lxf;
-    if (fy > T.hlyf) fy -= T.lyf;
-    else if (fy <= -T.hlyf) fy += T.lyf;
+    fx = fmaf(-T.lxf, rintf(fx * T.ilxf), fx);
+    fy = fmaf(-T.lyf, rintf(fy * T.ilyf), fy);
     const float fz = pf.z - qf.z;
     const float f2 = fx * fx + fy * fy + fz * fz;
     const float frs = pf.w + qf.w;
@@ -1192,7 +1196,43 @@ struct Particle {
     return true;
   }
 
+  // Mixed path, simple states: the same test and law as connected() and
+  // candidate(), with the law evaluated for every candidate and masked by
+  // the test, so the lanes of a warp do not diverge on it; only the rare
+  // FP64 decision near the threshold branches. A candidate that is not
+  // connected adds +0 or -0 to the sums, which leaves them unchanged: they
+  // start at +0 and, rounding to nearest, never become -0.
+  __device__ __forceinline__ void candidate_simple(int32_t q, const float4& qf) {
+    float fx = pf.x - qf.x, fy = pf.y - qf.y;
+    fx = fmaf(-T.lxf, rintf(fx * T.ilxf), fx);
+    fy = fmaf(-T.lyf, rintf(fy * T.ilyf), fy);
+    const float fz = pf.z - qf.z;
+    const float f2 = fx * fx + fy * fy + fz * fz;
+    const float frs = pf.w + qf.w;
+    const float thr = T.lt2f * frs * frs;
+    bool conn = !(f2 > thr + T.ftol);
+    if (conn && f2 >= thr - T.ftol) {
+      const double4 pq = S.pos_cur[q];
+      const double d2e = dist_sq_exact(pdiff_h(p.x, pq.x, T.lx, T.hlx),
+                                       pdiff_h(p.y, pq.y, T.ly, T.hly), p.z - pq.z);
+      const double rse = __dadd_rn(p.w, pq.w);
+      conn = d2e <= __dmul_rn(__dmul_rn(lt2, rse), rse);
+    }
+    const bool both_old = kOld && attr_old(a) && attr_old(__ldg(&S.attr[q]));
+    float coef = L.aad_fused(f2, frs, both_old);
+    coef = conn ? coef : 0.f;
+    note_bad(coef, i, q);
+    const float sdt = dt * coef;
+    ax += double(sdt * fx);
+    ay += double(sdt * fy);
+    az += double(sdt * fz);
+  }
+
   __device__ __forceinline__ void candidate(int32_t q, const Pos& pq) {
+    if constexpr (kFloatPos && kSimple) {
+      candidate_simple(q, pq);
+      return;
+    }
     R dx, dy, dz, d2, rs;
     if (!connected(q, pq, dx, dy, dz, d2, rs)) return;
     R coef;
