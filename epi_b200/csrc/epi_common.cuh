@@ -93,11 +93,11 @@ struct DevState {
   int32_t* nn;
   double4* fmemb;   // membrane bending + lattice spring + wall displacement
   int32_t* bin;
-  int32_t* rank;
+  int32_t* rank;    // place in its bin while binning; its slot once sorted
   int32_t* counts;
   int32_t* starts;
   uint32_t* skey;   // sorted particles: global index | (is_memb << 31)
-  float4* spos;     // sorted copy of the positions (and radii) at rebuild
+  float4* spos;     // sorted copy of the positions at rebuild; w: +-LJ_THRESH * radius
   int32_t* gate;    // [0]: some tissue needs a rebuild, [1 + t]: tissue t does
   int32_t* rl_count;  // rebuild work list: number of gated tissues
   int32_t* rl_list;   // their ids

@@ -386,11 +386,15 @@ __device__ __forceinline__ void sort_bin(const DevState& S, const TissueDev& T, 
       continue;
     const bool memb = attr_state(S.attr[gi]) == ST_MEMB;
     S.skey[s] = gi | (memb ? 0x80000000u : 0u);
-    // x and y as grid_init bins them (ref_bin): in [0, L)
+    S.rank[gi] = s;  // the particle's slot from here on (the search skips it)
+    // x and y as grid_init bins them (ref_bin): in [0, L); w: LJ_THRESH *
+    // radius, negative for a membrane particle (the search's reach and its
+    // membrane test)
     const double4 pg = S.pos_cur[gi];
     const double xc = 0.5 * T.lx - pdiff(0.5 * T.lx, pg.x, T.lx);
     const double yc = 0.5 * T.ly - pdiff(0.5 * T.ly, pg.y, T.ly);
-    S.spos[s] = make_float4((float)xc, (float)yc, (float)pg.z, (float)pg.w);
+    const float lw = (float)(T.P.lj_thresh * pg.w);
+    S.spos[s] = make_float4((float)xc, (float)yc, (float)pg.z, memb ? -lw : lw);
   }
 }
 
@@ -468,7 +472,10 @@ struct SearchWindow {
   int32_t xlo[2], xhi[2], ylo[2], yhi[2];
   int nxr, nyr;
   int32_t z0, z1;
-  float pxe[2], pye[2], pz, pw, flx, fly, fhx, fhy, flt, fskin;
+  float pxe[2], pye[2], pz, flx, fly, fhx, fhy;
+  float rw;        // LJ_THRESH * r_i + skin + margin: the reach less the partner's share
+  float memb_lim;  // slots whose w lies below it are excluded (membrane pairs)
+  int32_t s_self;  // the particle's own slot (-1: none)
   bool memb_i, wrap_x, wrap_y;
 
   __device__ __forceinline__ SearchWindow(const DevState& S, const TissueDev& T, int32_t i) {
@@ -498,31 +505,32 @@ struct SearchWindow {
     z0 = z0 < 0 ? 0 : (z0 > T.anz - 1 ? T.anz - 1 : z0);
     z1 = z1 < 0 ? 0 : (z1 > T.anz - 1 ? T.anz - 1 : z1);
     pz = (float)p.z;
-    pw = (float)p.w;
     flx = (float)T.lx;
     fly = (float)T.ly;
     fhx = 0.5f * flx;
     fhy = 0.5f * fly;
-    flt = (float)lt;
-    fskin = (float)(skin + margin);
+    rw = (float)(lt * p.w + skin + margin);
+    memb_lim = memb_i ? 0.f : -INFINITY;
+    s_self = S.bin[i] < 0 ? -1 : S.rank[i];
   }
-  // Is the particle in slot s (key, FP32 copy q) of a column of x range xr
-  // and y range yr a candidate of i? (ex, ey: pxe[xr], pye[yr])
-  // kWrap = false: only for windows with neither wrap_x nor wrap_y.
+  // Is the particle in slot s (FP32 copy q) of a column of x range xr and y
+  // range yr a candidate of i? (ex, ey: pxe[xr], pye[yr]) The reach
+  // rw + |q.w| rounds differently from LJ_THRESH (r_i + r_j) + skin by a few
+  // ulps, far inside the margin, so the candidates still hold every pair
+  // that can be connected. kWrap = false: only for windows with neither
+  // wrap_x nor wrap_y.
   template <bool kWrap>
-  __device__ __forceinline__ bool hit_t(int32_t i, uint32_t key, const float4& q, float ex,
-                                        float ey) const {
-    const int32_t j = (int32_t)(key & 0x7fffffffu);
-    if (j == i || (memb_i && (key >> 31))) return false;
+  __device__ __forceinline__ bool hit_t(int32_t s, const float4& q, float ex, float ey) const {
+    if (s == s_self || q.w < memb_lim) return false;
     float dx = ex - q.x, dy = ey - q.y;
     if (kWrap && wrap_x) dx = dx > fhx ? dx - flx : (dx <= -fhx ? dx + flx : dx);
     if (kWrap && wrap_y) dy = dy > fhy ? dy - fly : (dy <= -fhy ? dy + fly : dy);
     const float dz = pz - q.z;
-    const float reach = flt * (pw + q.w) + fskin;
+    const float reach = rw + fabsf(q.w);
     return dx * dx + dy * dy + dz * dz <= reach * reach;
-  }  __device__ __forceinline__ bool hit(int32_t i, uint32_t key, const float4& q, float ex,
-                                      float ey) const {
-    return hit_t<true>(i, key, q, ex, ey);
+  }
+  __device__ __forceinline__ bool hit(int32_t s, const float4& q, float ex, float ey) const {
+    return hit_t<true>(s, q, ex, ey);
   }
 };
 
@@ -599,7 +607,7 @@ __device__ __forceinline__ void cand_search_groups(const DevState& S, int32_t cn
         uint32_t key = 0;
         if (f < total) {
           key = S.skey[s];
-          hit = W.hit(i, key, S.spos[s], ex, ey);
+          hit = W.hit(s, S.spos[s], ex, ey);
         }
         const unsigned m = (__ballot_sync(gmask, hit) & gmask) >> gbase;
         if (hit) {
@@ -711,8 +719,8 @@ __device__ __forceinline__ void search_particle(const DevState& S, const TissueD
     const float4 q0 = S.spos[s];
     const uint32_t k1 = two ? S.skey[s + 1] : 0u;
     const float4 q1 = two ? S.spos[s + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const bool h0 = W.template hit_t<kWrap>(i, k0, q0, ex, ey);
-    const bool h1 = two && W.template hit_t<kWrap>(i, k1, q1, ex, ey);
+    const bool h0 = W.template hit_t<kWrap>(s, q0, ex, ey);
+    const bool h1 = two && W.template hit_t<kWrap>(s + 1, q1, ex, ey);
     if (h0) {
       if (count < cap) row.put(S, i, (k0 & 0x7fffffffu) - pbase);
       ++count;
