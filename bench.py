@@ -485,6 +485,9 @@ def main():
         if dist is not None:
             dist.barrier()
 
+    # the positions the warm-up starts from: the per-kernel split below
+    # replays the warm-up and the timed steps from them
+    start_pos = None if args.no_extras else tuple(a.copy() for a in ctx.positions())
     # warm-up (also captures the graph)
     if args.warmup:
         ctx.step(args.warmup, args.mode)
@@ -518,8 +521,27 @@ def main():
     if gathered is not None:
         extras["gathered"] = gathered
     if not args.no_extras:
-        # per-kernel device time (events around each kernel class, not captured)
-        tk = ctx.time_kernels(5)
+        # Per-kernel device time over a replay of the timed steps: the
+        # positions the warm-up started from, every tissue's candidates
+        # rebuilt from them (as after the autotuner's last restore, or the
+        # upload), the warm-up, then the timed number of steps with events
+        # around each kernel class (launched one by one, not from the graph).
+        # The replay should reproduce the timed steps' positions bit for bit
+        # (checked below).
+        end_pos = tuple(a.copy() for a in ctx.positions())
+        ctx.set_positions(*start_pos)
+        cfg_now = ctx.config()
+        ctx.set_tuning(cfg_now["skin"], cfg_now["variant"], cfg_now["search_switch"],
+                       cfg_now["rebuild_gate"])
+        if args.warmup:
+            ctx.step(args.warmup, args.mode)
+        tk = ctx.time_kernels(args.steps)
+        replay_pos = ctx.positions()
+        extras["kernel_split"] = {
+            "window": f"replay of the {args.warmup} warm-up and {args.steps} timed steps",
+            "replay_bit_identical": bool(all(np.array_equal(a, b)
+                                             for a, b in zip(end_pos, replay_pos))),
+        }
         # The roofline is the step kernel's: it does the whole per-step work
         # of the reference (exact predicate = connect, forces, commit). In
         # eager timing the rebuild classes also carry their launches on steps
