@@ -825,6 +825,12 @@ __global__ void k_dermis(DevState S, int32_t f0, int32_t f1) {
 // (double: FP64 path; float: mixed path). Sums and positions stay double.
 // ---------------------------------------------------------------------------
 
+// rintf(v) for |v| <= 2^22 on the FMA pipe: adding and subtracting
+// 1.5 * 2^23 rounds v to the nearest integer (ties to even) exactly.
+__device__ __forceinline__ float rint_fma(float v) {
+  return __fsub_rn(__fadd_rn(v, 12582912.f), 12582912.f);
+}
+
 // Offsets of lattice neighbours from membrane particle i (minimum image): from
 // the FP64 positions in the FP64 path, from the FP32 copies in the mixed path.
 template <typename R>
@@ -854,8 +860,8 @@ struct SiteOffsets<float> {
     // minimum image as d - L rint(d / L): lattice neighbours lie far
     // closer than L/2, where it equals the compare-and-shift form
     const float dx0 = o.x - pf.x, dy0 = o.y - pf.y;
-    const float dx = fmaf(-T.lxf, rintf(dx0 * T.ilxf), dx0);
-    const float dy = fmaf(-T.lyf, rintf(dy0 * T.ilyf), dy0);
+    const float dx = fmaf(-T.lxf, rint_fma(dx0 * T.ilxf), dx0);
+    const float dy = fmaf(-T.lyf, rint_fma(dy0 * T.ilyf), dy0);
     return Vec3<float>{dx, dy, o.z - pf.z};
   }
 };
@@ -1179,10 +1185,10 @@ struct Particle {
     // L/2 by more than the rounding of f / L, i.e. for every pair within
     // reach of a connection (LJ_THRESH (r_i + r_j) + skin is far below
     // L/2); a pair near L/2 apart is rejected under either image. The
-    // multiply-round-fma takes three instructions and no branch.
+    // multiply, round and fma take four FMA-pipe instructions, no branch.
     float fx = pf.x - qf.x, fy = pf.y - qf.y;
-    fx = fmaf(-T.lxf, rintf(fx * T.ilxf), fx);
-    fy = fmaf(-T.lyf, rintf(fy * T.ilyf), fy);
+    fx = fmaf(-T.lxf, rint_fma(fx * T.ilxf), fx);
+    fy = fmaf(-T.lyf, rint_fma(fy * T.ilyf), fy);
     const float fz = pf.z - qf.z;
     const float f2 = fx * fx + fy * fy + fz * fz;
     const float frs = pf.w + qf.w;
@@ -1212,8 +1218,8 @@ struct Particle {
   // start at +0 and, rounding to nearest, never become -0.
   __device__ __forceinline__ void candidate_simple(int32_t q, const float4& qf) {
     float fx = pf.x - qf.x, fy = pf.y - qf.y;
-    fx = fmaf(-T.lxf, rintf(fx * T.ilxf), fx);
-    fy = fmaf(-T.lyf, rintf(fy * T.ilyf), fy);
+    fx = fmaf(-T.lxf, rint_fma(fx * T.ilxf), fx);
+    fy = fmaf(-T.lyf, rint_fma(fy * T.ilyf), fy);
     const float fz = pf.z - qf.z;
     const float f2 = fx * fx + fy * fy + fz * fz;
     const float frs = pf.w + qf.w;
