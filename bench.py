@@ -474,6 +474,7 @@ def main():
         from epi_b200.autotune import tuned as autotuned
         tuned = autotuned(ctx, mine, args.tune_steps, device=local, retune=args.retune)
         tuned["grid"] = ("skin {0.05,0.08,0.1,0.15,0.2,0.3} x step-kernel variant 1..4, "
+                         "then rebuild node {conditional, always launched}, "
                          "then search switch {8192,16384,49152,131072}")
     off, _ = ctx.connections()
     kbar = float(off[-1]) / max(n_mine, 1)  # mean connected_cell length incl. lattice links
