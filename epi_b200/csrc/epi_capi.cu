@@ -410,13 +410,13 @@ cudaError_t capture_conditional_rebuild(epi_ctx* c, int cur) {
                                              cudaStreamSetCaptureDependencies);
 }
 
-// The step graph of parity c->cur: one launch runs a whole sequence of steps.
+// The step graph of parity cur0: one launch runs a whole sequence of steps.
 // A WHILE node repeats its body -- two steps (per step: the membrane sums
 // forked beside the conditional rebuild, the dermis, the fused step), then a
 // one-thread kernel that
 // counts down the passes left (set before each launch) and sets the loop
 // condition -- so the device drives the loop and the host launches once.
-cudaError_t capture_step_graph(epi_ctx* c, cudaGraphExec_t* out) {
+cudaError_t capture_step_graph(epi_ctx* c, int cur0, cudaGraphExec_t* out) {
   cudaGraph_t g = nullptr;
   cudaError_t e = cudaGraphCreate(&g, 0);
   if (e != cudaSuccess) return e;
@@ -436,7 +436,7 @@ cudaError_t capture_step_graph(epi_ctx* c, cudaGraphExec_t* out) {
     e = cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0,
                                       cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-      int cur = c->cur;
+      int cur = cur0;
       for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
         e = fork_memb(c, cur, nullptr);
         if (e == cudaSuccess) {
@@ -486,13 +486,18 @@ int check_status(epi_ctx* c) {
 }
 
 // nsteps steps replayed from the two-step graph of the current parity
-// (captured on first use), plus one eager step for an odd count.
+// (both parities' graphs captured on first use), plus one eager step for
+// an odd count.
 int enqueue_graph_steps(epi_ctx* c, int32_t nsteps) {
   ensure_posf(c);  // never inside the captured graph
   const int32_t pairs = nsteps / 2;
   if (pairs > 0) {
+    // both parities' graphs at first use: an odd step count (its last step
+    // runs eagerly) leaves the next run on the other parity, whose capture
+    // would otherwise hold up that run's first launch
+    for (int par = 0; par < 2; ++par)
+      if (!c->graph[par]) EPI_CUDA(capture_step_graph(c, par, &c->graph[par]));
     cudaGraphExec_t& ge = c->graph[c->cur];
-    if (!ge) EPI_CUDA(capture_step_graph(c, &ge));
     launch_set_counter(c->loop_left, pairs, c->stream);
     EPI_CUDA(cudaGraphLaunch(ge, c->stream));
   }
