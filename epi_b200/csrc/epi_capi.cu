@@ -133,6 +133,9 @@ struct epi_ctx {
   bool after_host_step = false;
   DevStatus* status = nullptr;
   DevStatus* status_h = nullptr;  // pinned
+  // pinned host staging of epi_upload's per-particle arrays (grown on demand)
+  unsigned char* upin = nullptr;
+  size_t upin_bytes = 0;
   unsigned long long* rebuilds = nullptr;
   int32_t* loop_left = nullptr;  // passes left in the step graph's device loop
   unsigned long long* launches = nullptr;  // step-sequence kernels executed
@@ -787,6 +790,7 @@ void epi_destroy(epi_ctx* ctx) {
   if (ctx->loop_left) cudaFree(ctx->loop_left);
   if (ctx->launches) cudaFree(ctx->launches);
   if (ctx->status_h) cudaFreeHost(ctx->status_h);
+  if (ctx->upin) cudaFreeHost(ctx->upin);
   if (ctx->copy_in) cudaStreamSynchronize(ctx->copy_in);
   if (ctx->copy_out) cudaStreamSynchronize(ctx->copy_out);
   for (cudaEvent_t e : ctx->ev_in) cudaEventDestroy(e);
@@ -872,11 +876,25 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
   const std::vector<TissueDev> old_tissues = reuse ? c->tissues_h : std::vector<TissueDev>();
   c->tissues_h.assign(ntissues, TissueDev{});
   c->thost.assign(ntissues, TissueHost{});
-  std::vector<double4> pos(n);
-  std::vector<uint32_t> attr(n);
-  std::vector<int32_t> pair(n, -1);
-  std::vector<double> spr(n, 0.0);
-  std::vector<double> agek(n, 0.0);
+  // The per-particle arrays are assembled in pinned host memory, so their
+  // copies to the device run at full bus speed; every entry is written below.
+  const size_t need = (sizeof(double4) + 2 * sizeof(double) + sizeof(uint32_t) +
+                       sizeof(int32_t)) * (size_t)std::max<int64_t>(n, 1);
+  if (c->upin_bytes < need) {
+    if (c->upin) cudaFreeHost(c->upin);
+    c->upin = nullptr;
+    c->upin_bytes = 0;
+    if ((rc = cuda_status(cudaMallocHost((void**)&c->upin, need)))) {
+      free_buffers(c);
+      return rc;
+    }
+    c->upin_bytes = need;
+  }
+  double4* pos = reinterpret_cast<double4*>(c->upin);
+  double* spr = reinterpret_cast<double*>(pos + n);
+  double* agek = spr + n;
+  uint32_t* attr = reinterpret_cast<uint32_t*>(agek + n);
+  int32_t* pair = reinterpret_cast<int32_t*>(attr + n);
   std::vector<int32_t> prep_m, prep_f;
   int32_t pbase = 0, binbase = 0;
   bool simple = true, any_old = false;
@@ -990,13 +1008,13 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
   cudaStream_t s = c->stream;
   EPI_CUDA(cudaMemcpyAsync(c->tissues, c->tissues_h.data(), sizeof(TissueDev) * ntissues,
                            cudaMemcpyHostToDevice, s));
-  EPI_CUDA(cudaMemcpyAsync(c->pos[0], pos.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, s));
-  EPI_CUDA(cudaMemcpyAsync(c->pos[1], pos.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, s));
+  EPI_CUDA(cudaMemcpyAsync(c->pos[0], pos, sizeof(double4) * n, cudaMemcpyHostToDevice, s));
+  EPI_CUDA(cudaMemcpyAsync(c->pos[1], c->pos[0], sizeof(double4) * n, cudaMemcpyDeviceToDevice, s));
   c->posf_stale = true;
-  EPI_CUDA(cudaMemcpyAsync(c->attr, attr.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s));
-  EPI_CUDA(cudaMemcpyAsync(c->pair, pair.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
-  EPI_CUDA(cudaMemcpyAsync(c->spr, spr.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
-  EPI_CUDA(cudaMemcpyAsync(c->agek, agek.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  EPI_CUDA(cudaMemcpyAsync(c->attr, attr, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s));
+  EPI_CUDA(cudaMemcpyAsync(c->pair, pair, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+  EPI_CUDA(cudaMemcpyAsync(c->spr, spr, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  EPI_CUDA(cudaMemcpyAsync(c->agek, agek, sizeof(double) * n, cudaMemcpyHostToDevice, s));
   if (c->field_on) {
     // boxes may have changed: refresh the grids' spacing
     for (int32_t t = 0; t < ntissues; ++t)
@@ -1028,7 +1046,7 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
     }
   }
   c->h_radius.resize(n);
-  c->h_attr.assign(attr.begin(), attr.end());
+  c->h_attr.assign(attr, attr + n);
   for (int64_t i = 0; i < n; ++i) c->h_radius[i] = pos[i].w;
   if (gates.empty()) {
     EPI_CUDA(cudaMemsetAsync(c->nn, 0, sizeof(int32_t) * n, s));
@@ -1045,7 +1063,8 @@ int epi_upload(epi_ctx* c, int32_t ntissues, const epi_tissue_view* tv, const ep
                              cudaMemcpyHostToDevice, s));
     launch_gate_check(make_state(c, c->cur), c->lc, s);
   }
-  // all pending host copies read std::vector storage: finish before return
+  // the copies read the pinned staging, which the next upload rewrites:
+  // finish before return
   return materialize(c);
   EPI_GUARD_END
 }

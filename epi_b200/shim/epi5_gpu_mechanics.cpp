@@ -28,7 +28,9 @@
 // connected_cell, the gap-junction maps and dermis back, storing the new
 // positions -- touches each cell's own members only, so built with OpenMP
 // (-fopenmp) its per-cell loops run on all host threads; without it they
-// run serially and give the same result.
+// run serially and give the same result. Rows and gap-junction maps of
+// cells whose partners did not change since the last connect are left as
+// they are (they already hold what a rewrite would give).
 #include "cell.h"
 #include "cell_connection.h"
 #include "cell_interaction.h"
@@ -66,37 +68,60 @@ class GpuMechanics {
     }
     dermis_.assign(n, -1);
     check(epi_get_dermis(ctx_, dermis_.data()), "connect_cell");
-#pragma omp parallel for schedule(static)
+    const size_t nprev = prev_cells_.size();
+#pragma omp parallel for schedule(dynamic, 256)
     for (int32_t i = 0; i < n; ++i) {
       Cell* c = cells_[i];
-      if (c->state == MEMB) {
-        // the lattice links _memb_init pushed stay first (cellmanager.cpp:70-166)
-        c->connected_cell.force_set_count(cont::MEMB_ADJ_CONN_NUM);
+      // connected_cell: the lattice links _memb_init pushed stay first
+      // (cellmanager.cpp:70-166), then the listed partners; rewritten only
+      // where it differs from that
+      const size_t first = c->state == MEMB ? cont::MEMB_ADJ_CONN_NUM : 0;
+      auto lattice = [&](Cell* o) {
+        bool l = false;
+        for (size_t m = 0; m < first; ++m) l |= c->connected_cell[m] == o;
+        return l;
+      };
+      size_t pos = first;
+      bool same = c->connected_cell.size() >= first;
+      for (int32_t k = off_[i]; same && k < off_[i + 1]; ++k) {
+        Cell* o = cells_[idx_[k]];
+        if (lattice(o)) continue;
+        same = pos < c->connected_cell.size() && c->connected_cell[pos] == o;
+        ++pos;
+      }
+      if (!same || pos != c->connected_cell.size()) {
+        c->connected_cell.force_set_count(first);
         for (int32_t k = off_[i]; k < off_[i + 1]; ++k) {
           Cell* o = cells_[idx_[k]];
-          bool lattice = false;
-          for (unsigned m = 0; m < cont::MEMB_ADJ_CONN_NUM; ++m)
-            lattice |= c->connected_cell[m] == o;
-          if (!lattice) c->connected_cell.push_back(o);
+          if (!lattice(o)) c->connected_cell.push_back(o);
         }
-      } else {
-        c->connected_cell.force_set_count(0);
-        for (int32_t k = off_[i]; k < off_[i + 1]; ++k)
-          c->connected_cell.push_back(cells_[idx_[k]]);
       }
-    }
-    // gj_refresh (cell_connection.cpp:133-152): mark the connected, reset the
-    // rest; and set_dermis (:178-185), FIX and MUSUME only
-#pragma omp parallel for schedule(static)
-    for (int32_t i = 0; i < n; ++i) {
-      Cell* c = cells_[i];
-      for (auto& kv : c->gj) kv.second.uncheck();
-      c->connected_cell.foreach([&](Cell* o) { c->gj[o].check(); });
-      for (auto& kv : c->gj)
-        if (!kv.second.is_checked()) kv.second.reset();
+      // gj_refresh (cell_connection.cpp:133-152): mark the connected, reset
+      // the rest. After a refresh the connected entries are marked and all
+      // others reset, and only this refresh changes marks or touches entries
+      // of cells not connected (the chemistry updates connected ones,
+      // ca2p.cpp:204-207), so a cell that is the same object at the same
+      // index with the same partners as at the last connect keeps its map.
+      bool kept = (size_t)i < nprev && prev_cells_[i] == c &&
+                  prev_off_[i + 1] - prev_off_[i] == off_[i + 1] - off_[i];
+      for (int32_t k = 0; kept && k < off_[i + 1] - off_[i]; ++k)
+        kept = prev_row_[prev_off_[i] + k] == cells_[idx_[off_[i] + k]];
+      if (!kept) {
+        for (auto& kv : c->gj) kv.second.uncheck();
+        c->connected_cell.foreach([&](Cell* o) { c->gj[o].check(); });
+        for (auto& kv : c->gj)
+          if (!kv.second.is_checked()) kv.second.reset();
+      }
+      // set_dermis (:178-185), FIX and MUSUME only
       if (c->state == FIX || c->state == MUSUME)
         c->set_dermis(dermis_[i] >= 0 ? cells_[dermis_[i]] : nullptr);
     }
+    // this connect's rows, for the next one's comparison
+    prev_cells_ = cells_;
+    prev_off_.assign(off_.begin(), off_.begin() + n + 1);
+    prev_row_.resize((size_t)off_[n]);
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < (int64_t)off_[n]; ++k) prev_row_[k] = cells_[idx_[k]];
   }
 
   void interact(CellManager& cman) {
@@ -227,6 +252,9 @@ class GpuMechanics {
   std::vector<double> x_, y_, z_, r_, agek_, spr_, nx_, ny_, nz_;
   std::vector<uint8_t> state_;
   std::vector<int32_t> pair_, rest_, off_, idx_, dermis_;
+  // the previous connect's cells and rows (partner pointers, CSR)
+  std::vector<Cell*> prev_cells_, prev_row_;
+  std::vector<int32_t> prev_off_;
 };
 
 // One GPU context per process, created on first use. It is not destroyed at
