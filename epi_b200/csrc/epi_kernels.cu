@@ -1421,6 +1421,33 @@ __device__ __forceinline__ void gather_candidates(const DevState& S, Part& P, co
 // finish with one load per entry. kMinBlocks bounds the registers so that
 // that many 256-thread blocks stay resident per SM.
 // One particle of the step.
+// Streaming loads that do not allocate in L1 (the particle's own inputs,
+// read once), leaving L1 to the neighbours' gathered positions.
+__device__ __forceinline__ uint4 ld_na(const uint4* p) {
+  uint4 v;
+  asm("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
+      : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float4 ld_na(const float4* p) {
+  float4 v;
+  asm("ld.global.nc.L1::no_allocate.v4.f32 {%0,%1,%2,%3}, [%4];"
+      : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double4 ld_na(const double4* p) {
+  double a, b, c, d;
+  asm("ld.global.nc.L1::no_allocate.v2.f64 {%0,%1}, [%2];" : "=d"(a), "=d"(b) : "l"(p));
+  asm("ld.global.nc.L1::no_allocate.v2.f64 {%0,%1}, [%2];"
+      : "=d"(c), "=d"(d) : "l"(reinterpret_cast<const double2*>(p) + 1));
+  return make_double4(a, b, c, d);
+}
+__device__ __forceinline__ uint32_t ld_na(const uint32_t* p) {
+  uint32_t v;
+  asm("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+
 template <typename R, bool kSimple, bool kOld, bool k16>
 __device__ __forceinline__ void step_particle(const DevState& S, int64_t i) {
   const int64_t N = S.n_total;
@@ -1429,11 +1456,11 @@ __device__ __forceinline__ void step_particle(const DevState& S, int64_t i) {
   constexpr int kG = sizeof(R) == 4 ? 4 : 2;         // gathers in flight
   uint4 c[kChunks];
 #pragma unroll
-  for (int k = 0; k < kChunks; ++k) c[k] = __ldg(S.cand + k * N + i);
-  const uint32_t a = __ldg(&S.attr[i]);
+  for (int k = 0; k < kChunks; ++k) c[k] = ld_na(S.cand + k * N + i);
+  const uint32_t a = ld_na(S.attr + i);
   using Part = Particle<R, kSimple, kOld>;
-  Part P(S, (int32_t)i, a, S.pos_cur[i]);
-  const float4 bp = S.bpos[i];
+  Part P(S, (int32_t)i, a, ld_na(S.pos_cur + i));
+  const float4 bp = ld_na(S.bpos + i);
   const double4 fm = P.st == ST_MEMB ? S.fmemb[i] : make_double4(0.0, 0.0, 0.0, 0.0);
   gather_candidates<k16, kPre, kG>(S, P, c, i);
   P.finish(bp, fm);
@@ -1514,9 +1541,9 @@ __global__ void __launch_bounds__(kStepThreads, kMinBlocks) k_step_async(DevStat
   constexpr int kPre = kChunks * (k16 ? 8 : 4) - 1;
   uint4 c[kChunks];
 #pragma unroll
-  for (int k = 0; k < kChunks; ++k) c[k] = __ldg(S.cand + k * N + i);
-  Part P(S, (int32_t)i, __ldg(&S.attr[i]), S.pos_cur[i]);
-  const float4 bp = S.bpos[i];
+  for (int k = 0; k < kChunks; ++k) c[k] = ld_na(S.cand + k * N + i);
+  Part P(S, (int32_t)i, ld_na(S.attr + i), ld_na(S.pos_cur + i));
+  const float4 bp = ld_na(S.bpos + i);
   const double4 fm = P.st == ST_MEMB ? S.fmemb[i] : make_double4(0.0, 0.0, 0.0, 0.0);
   gather_candidates_async<k16, kPre, kS>(S, P, c, i, slots);
   P.finish(bp, fm);
